@@ -1,0 +1,576 @@
+#!/usr/bin/env python
+"""Benchmark: particle-filter cycle throughput at N = 1M particles on the
+at-scale workload (64 landmarks in a 50 x 50 x 10 m box, 256 observations per
+cycle of which 10 % are outliers, random_inject_ratio 0.01, helix trajectory),
+plus uniform CBGL global-localization solves on 10 x 10 m rooms with 30 box
+obstacles (360 rays, 1M hypotheses = 62 500 positions x 16 yaws, k = 64).
+
+One step = one full ParticleFilter::update cycle (predict, gated weighting,
+softmax, estimate, resample when ESS < N/2 with injection, estimate) over all
+N particles.  Metric: particle-updates/s = N * steps / time.
+
+  value  device-resident inputs (all cycles' observations in HBM), the fused
+         cycle entry point, CUDA events on the library's stream around each
+         step, L2 flushed (256 MiB write) between steps outside the events.
+  e2e    the drop-in path: the C++ mirror of pf_core's ParticleFilter::update
+         calling the pfc_* C-ABI with host observation arrays (host->device
+         copy and device->host estimate read inside every timed step), wall
+         clock per step with L2 flushed between steps.
+
+--impl reference times the reference's CPU implementation of the same cycle
+(the CPU oracle port of crates/pf_core/src/cpu.rs, all host threads) on the
+same workload, a bounded number of cycles per run.
+
+Multi-GPU (torchrun): every rank runs an independent filter of N particles
+(replicas, weak scaling); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "PF particle-updates/s @1M"
+UNIT = "particle-updates/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--particles", type=int, default=1_000_000)
+    ap.add_argument("--seed", type=int, default=11)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip GL, CPU baseline and reference-GPU legs")
+    ap.add_argument("--gl-hyps", type=int, default=1_000_000)
+    ap.add_argument("--gl-trials", type=int, default=20)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- helpers
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during a timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu_id}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in getattr(self, "lines", []):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def gpu_id_for(local_rank: int) -> str:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        if local_rank < len(ids):
+            return ids[local_rank]
+    return str(local_rank)
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def scenario(args, cycles):
+    from cuda_pf_localization_b200 import sim
+    return sim.helix_scenario(cycles, 64, (50.0, 50.0, 10.0), 256, 0.10, args.seed)
+
+
+def obs_array(rows):
+    import cuda_pf_localization_b200 as pkg
+    a = np.zeros(len(rows), dtype=[("id", "<i4"), ("mode", "<i4"), ("dx", "<f4"),
+                                   ("dy", "<f4"), ("dz", "<f4"), ("range", "<f4")])
+    a["id"] = rows[:, 0].astype(np.int32)
+    a["mode"] = rows[:, 1].astype(np.int32)
+    a["dx"], a["dy"], a["dz"], a["range"] = rows[:, 2], rows[:, 3], rows[:, 4], rows[:, 5]
+    assert a.itemsize == C.sizeof(pkg.CObservation)
+    return a
+
+
+FILTER = dict(range_noise=0.05, bearing_noise=0.02, gate_sigma=3.0, resample_ess_ratio=0.5,
+              random_inject_ratio=0.01)
+
+
+# ------------------------------------------------------- reference (CPU) arm
+
+def run_cpu_cycles(sc, n, seconds, max_cycles, warm=1):
+    """The CPU oracle's ParticleFilter::update (cpu.rs restated, OpenMP over the
+    par_iter regions) for a bounded number of cycles; returns (cycles, s)."""
+    import oracle
+    pf = oracle.OraclePF(n, seed=42, range_noise=FILTER["range_noise"],
+                         bearing_noise=FILTER["bearing_noise"], gate=FILTER["gate_sigma"],
+                         ess_ratio=FILTER["resample_ess_ratio"],
+                         inject=FILTER["random_inject_ratio"])
+    pf.reinit(np.r_[sc.prior_p, sc.prior_q], [0.5] * 3, [0.2] * 3)
+    tn, rn = sc.trans_noise, sc.rot_noise
+    steps = sc.steps
+    for k in range(warm):
+        st = steps[k]
+        pf.update(st.odom_t, st.odom_q, tn, rn, sc.landmarks, st.obs)
+    done, t0 = 0, time.perf_counter()
+    while done < max_cycles:
+        st = steps[(warm + done) % len(steps)]
+        pf.update(st.odom_t, st.odom_q, tn, rn, sc.landmarks, st.obs)
+        done += 1
+        if time.perf_counter() - t0 > seconds:
+            break
+    return done, time.perf_counter() - t0
+
+
+def reference_arm(args):
+    import oracle
+    n = args.particles
+    # each step is one cycle; the run is capped at a bounded number of cycles
+    sc = scenario(args, max(4, min(args.steps, 64) + args.warmup + 1))
+    threads = oracle.lib().orc_threads()
+    done, secs = run_cpu_cycles(sc, n, seconds=max(20.0, args.cpu_seconds), max_cycles=args.steps,
+                                warm=max(1, min(args.warmup, 3)))
+    v = n * done / secs
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": done, "warmup": max(1, min(args.warmup, 3)), "ms_per_step": 1e3 * secs / done,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "at-scale PF cycle: N=1M, 64 landmarks (50x50x10 m), 256 obs/cycle "
+                               "(10% outliers), gate 3 sigma, inject 0.01, helix",
+                   "particles": n, "sample": f"{done} of {args.steps} cycles (time-bounded)"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{done} cycles at N={n}"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------ our GPU arm
+
+def run_value(args, sc, torch, dev):
+    """Fused cycles with observations resident in HBM; per-step CUDA events."""
+    import cuda_pf_localization_b200 as pkg
+    lib = pkg.kernels()
+    n = args.particles
+    h = lib.pfc_create(256)
+    assert h
+    try:
+        assert lib.pfc_init(h, n, 42) == 0
+        lm = np.ascontiguousarray(sc.landmarks, np.float32).reshape(-1)
+        assert lib.pfc_upload_landmarks(h, pkg.fptr(lm), len(sc.landmarks)) == 0
+        pri = np.r_[sc.prior_p, sc.prior_q].astype(np.float32)
+        ps = np.full(3, 0.5, np.float32)
+        rs = np.full(3, 0.2, np.float32)
+        assert lib.pfc_reinit(h, *map(float, pri), pkg.fptr(ps), pkg.fptr(rs)) == 0
+        nobs = 256
+        allobs = np.concatenate([obs_array(st.obs) for st in sc.steps])
+        d_obs = torch.from_numpy(allobs.view(np.uint8).copy()).to(dev)
+        base = d_obs.data_ptr()
+        rec = 24 * nobs
+        odoms = []
+        for st in sc.steps:
+            o = pkg.PfcOdom()
+            o.t[:] = list(map(float, st.odom_t))
+            o.q[:] = list(map(float, st.odom_q))
+            o.tstd[:] = list(sc.trans_noise)
+            o.rstd[:] = list(sc.rot_noise)
+            odoms.append(o)
+        prm = pkg.PfcCycleParams(FILTER["range_noise"], FILTER["bearing_noise"],
+                                 FILTER["gate_sigma"], FILTER["resample_ess_ratio"],
+                                 FILTER["random_inject_ratio"], 0)
+        est = np.zeros(pkg.PFC_EST_LEN)
+        stream = torch.cuda.ExternalStream(lib.pfc_stream(h), device=dev)
+        flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+        W, K = args.warmup, args.steps
+        resampled, errs = 0, []
+        for k in range(W):
+            assert lib.pfc_cycle_device(h, C.byref(odoms[k]), C.c_void_p(base + k * rec), nobs,
+                                        C.byref(prm), pkg.dptr(est)) == 0
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(K)]
+        lib.pfc_reset_stats(h)
+        lib.pfc_profile(h, 1)
+        torch.cuda.synchronize(dev)
+        with ClockSampler(gpu_id_for(dev.index)) as clk:
+            t_wall = time.perf_counter()
+            with torch.cuda.stream(stream):
+                for k in range(K):
+                    flush.fill_(k & 0xFF)
+                    evs[k][0].record(stream)
+                    rc = lib.pfc_cycle_device(h, C.byref(odoms[W + k]),
+                                              C.c_void_p(base + (W + k) * rec), nobs,
+                                              C.byref(prm), None)
+                    evs[k][1].record(stream)
+                    if rc != 0:
+                        raise RuntimeError(pkg.last_error())
+            stream.synchronize()
+            t_wall = time.perf_counter() - t_wall
+        ms = np.zeros(10)
+        cnt = np.zeros(10, dtype=np.int64)
+        lib.pfc_profile_read(h, pkg.dptr(ms), cnt.ctypes.data_as(C.POINTER(C.c_longlong)))
+        lib.pfc_profile(h, 0)
+        stats = pkg.PfcStats()
+        lib.pfc_get_stats(h, C.byref(stats))
+        step_ms = np.array([a.elapsed_time(b) for a, b in evs])
+        assert lib.pfc_cycle_result(h, pkg.dptr(est)) == 0
+        final_err = float(np.linalg.norm(est[0:3] - sc.steps[W + K - 1].truth_p))
+        return dict(step_ms=step_ms, wall=t_wall, kernel_ms=ms, kernel_count=cnt,
+                    launches=int(stats.launches), clocks=clk.summary(), final_err=final_err)
+    finally:
+        lib.pfc_destroy(h)
+
+
+def run_e2e(args, sc, torch, dev):
+    """ParticleFilter::update through the drop-in C-ABI with host buffers."""
+    import cuda_pf_localization_b200 as pkg
+    lib = pkg.kernels()
+    n = args.particles
+    pf = pkg.ParticleFilter(n, seed=42, trans_noise=sc.trans_noise, rot_noise=sc.rot_noise,
+                            **FILTER)
+    try:
+        pf.set_map(sc.landmark_dict())
+        pf.reinitialize(np.r_[sc.prior_p, sc.prior_q], [0.5] * 3, [0.2] * 3)
+        odoms = [pkg.make_core_odom(st.odom_t, st.odom_q, sc.trans_noise, sc.rot_noise)
+                 for st in sc.steps]
+        obs = [pkg.make_core_obs(st.obs) for st in sc.steps]
+        nob = [len(st.obs) for st in sc.steps]
+        core = pkg.core()
+        est = pkg.PfcoreEstimate()
+        W, K = args.warmup, args.steps
+        for k in range(W):
+            assert core.pfcore_filter_update(pf._h, C.byref(odoms[k]), obs[k], nob[k],
+                                             C.byref(est)) == 0
+        flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+        h = pf.handle
+        lib.pfc_reset_stats(h)
+        times, errs, resampled = [], [], 0
+        for k in range(K):
+            flush.fill_(k & 0xFF)
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            rc = core.pfcore_filter_update(pf._h, C.byref(odoms[W + k]), obs[W + k], nob[W + k],
+                                           C.byref(est))
+            t1 = time.perf_counter()
+            if rc != 0:
+                raise RuntimeError(core.pfcore_last_error().decode())
+            times.append(t1 - t0)
+            errs.append(float(np.linalg.norm(np.array(est.position[:]) - sc.steps[W + k].truth_p)))
+            resampled += int(est.resampled)
+        stats = pkg.PfcStats()
+        lib.pfc_get_stats(h, C.byref(stats))
+        return dict(times=np.array(times), errs=np.array(errs), resampled=resampled,
+                    h2d=stats.h2d_bytes / K, d2h=stats.d2h_bytes / K,
+                    launches=int(stats.launches), syncs=stats.host_syncs / K)
+    finally:
+        pf.close()
+
+
+def run_ref_gpu_pf(args, sc, cycles):
+    """The reference library (built from its source for sm_100a) driven in the
+    Rust CudaBackend's call order; host Markley mean via numpy."""
+    import oracle
+    import cuda_pf_localization_b200 as pkg
+    ref = oracle.ref_lib()
+    if ref is None:
+        return None
+    n = args.particles
+    h = ref.pfc_create(256)
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)
+    try:
+        assert ref.pfc_init(h, n, 42) == 0
+        lm = f32(sc.landmarks).reshape(-1)
+        ref.pfc_upload_landmarks(h, pkg.fptr(lm), len(sc.landmarks))
+        pri = np.r_[sc.prior_p, sc.prior_q]
+        ps, rs = f32([0.5] * 3), f32([0.2] * 3)
+        ref.pfc_reinit(h, *map(float, pri), pkg.fptr(ps), pkg.fptr(rs))
+        tn, rn = f32(sc.trans_noise), f32(sc.rot_noise)
+        obs = [pkg.make_cobs(st.obs) for st in sc.steps]
+        sums = np.zeros(14)
+        cv = np.zeros(12)
+
+        def cycle(k):
+            st = sc.steps[k]
+            ref.pfc_predict(h, *map(float, st.odom_t), *map(float, st.odom_q), pkg.fptr(tn),
+                            pkg.fptr(rn))
+            ref.pfc_weight(h, C.cast(obs[k], C.c_void_p), len(st.obs), 0.05, 0.02, 3.0)
+
+            def estimate():
+                ref.pfc_est_sums(h, pkg.dptr(sums))
+                m = np.zeros((4, 4))
+                e = 3
+                for r in range(4):
+                    for c in range(r, 4):
+                        m[r, c] = m[c, r] = sums[e]
+                        e += 1
+                vals, vecs = np.linalg.eigh(m)
+                q = vecs[:, int(np.argmax(vals))]
+                q = q if q[0] >= 0 else -q
+                ref.pfc_covs(h, float(sums[0]), float(sums[1]), float(sums[2]), *map(float, q),
+                             pkg.dptr(cv))
+                return 1.0 / sums[13] if sums[13] > 0 else 0.0
+            ess = estimate()
+            if ess < 0.5 * n:
+                ref.pfc_resample(h, 0.01)
+                estimate()
+
+        for k in range(2):
+            cycle(k)
+        t0 = time.perf_counter()
+        for k in range(2, 2 + cycles):
+            cycle(k)
+        return n * cycles / (time.perf_counter() - t0)
+    finally:
+        ref.pfc_destroy(h)
+
+
+def run_gl(args):
+    """Uniform CBGL: 20 trials on a 30-box room, 1M hypotheses, k = 64."""
+    import oracle
+    import cuda_pf_localization_b200 as pkg
+    from cuda_pf_localization_b200 import sim
+    lib = pkg.kernels()
+    g = sim.rooms_grid(args.seed)
+    nh = args.gl_hyps
+    k = 64
+    rng = np.random.default_rng(args.seed + 1)
+    trials = []
+    for t in range(args.gl_trials):
+        x, y, th = sim.free_pose(g, rng)
+        scan = oracle.map_scan(g, 0.05, (0, 0), x, y, th, 360, 2 * math.pi, 10.0)
+        scan = (scan + rng.normal(0, 0.01, 360)).astype(np.float32)
+        trials.append(((x, y, th), scan))
+    cells = np.ascontiguousarray(g)
+    h = lib.pfgl_create(200, 200, 0.05, 0.0, 0.0, pkg.u8ptr(cells), nh)
+    out = np.zeros(3 * k, np.float32)
+    cs = np.zeros(k, np.float32)
+    ids = np.zeros(k, np.int32)
+
+    def err(top, truth):
+        dp = math.hypot(top[0] - truth[0], top[1] - truth[1])
+        dth = abs((top[2] - truth[2] + math.pi) % (2 * math.pi) - math.pi)
+        return dp, dth
+
+    res = {}
+    try:
+        for mode in ("pruned", "abi"):
+            ok_p = ok_pt = 0
+            lib.pfgl_generate_yaws(h, nh // 16, 16, 1)
+            lib.pfgl_localize(h, pkg.fptr(trials[0][1]), 360, 10.0, 2 * math.pi, k,
+                              pkg.fptr(out), pkg.fptr(cs), pkg.iptr(ids))  # warm-up
+            t0 = time.perf_counter()
+            for t, (truth, scan) in enumerate(trials):
+                assert lib.pfgl_generate_yaws(h, nh // 16, 16, 1000 + t) == 0
+                if mode == "pruned":
+                    r = lib.pfgl_localize(h, pkg.fptr(scan), 360, 10.0, 2 * math.pi, k,
+                                          pkg.fptr(out), pkg.fptr(cs), pkg.iptr(ids))
+                else:
+                    assert lib.pfgl_score(h, pkg.fptr(scan), 360, 10.0, 2 * math.pi) == 0
+                    r = lib.pfgl_topk(h, k, pkg.fptr(out))
+                assert r == k
+                dp, dth = err(out[:3], truth)
+                ok_p += dp <= 0.5
+                ok_pt += (dp <= 0.5 and dth <= 0.1)
+            dt = time.perf_counter() - t0
+            res[mode] = dict(solves_per_s=len(trials) / dt, success_pos=ok_p / len(trials),
+                             success_pos_yaw=ok_pt / len(trials))
+    finally:
+        lib.pfgl_destroy(h)
+    # the reference library on the same trials (exhaustive score + CUB sort)
+    ref = oracle.ref_lib()
+    if ref is not None:
+        rh = ref.pfgl_create(200, 200, 0.05, 0.0, 0.0, pkg.u8ptr(cells), nh)
+        try:
+            ok = 0
+            ref.pfgl_generate(rh, nh, 1)
+            ref.pfgl_score(rh, pkg.fptr(trials[0][1]), 360, 10.0, 2 * math.pi)
+            ref.pfgl_topk(rh, k, pkg.fptr(out))
+            t0 = time.perf_counter()
+            n_ref = min(len(trials), 5)
+            for t in range(n_ref):
+                truth, scan = trials[t]
+                ref.pfgl_generate(rh, nh, 1000 + t)
+                ref.pfgl_score(rh, pkg.fptr(scan), 360, 10.0, 2 * math.pi)
+                ref.pfgl_topk(rh, k, pkg.fptr(out))
+                ok += err(out[:3], truth)[0] <= 0.5
+            res["reference_gpu"] = dict(solves_per_s=n_ref / (time.perf_counter() - t0),
+                                        success_pos=ok / n_ref)
+        finally:
+            ref.pfgl_destroy(rh)
+    return res
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        reference_arm(args)
+        return
+
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    sc = scenario(args, args.warmup + args.steps + 1)
+    n = args.particles
+    val = run_value(args, sc, torch, dev)
+    e2e = run_e2e(args, sc, torch, dev)
+    t_value = float(val["step_ms"].sum()) / 1e3
+    t_e2e = float(e2e["times"].sum())
+    if dist is not None:
+        tt = torch.tensor([t_value, t_e2e], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_value, t_e2e = float(tt[0]), float(tt[1])
+        dist.barrier()
+
+    K = args.steps
+    value = world * n * K / t_value
+    e2e_value = world * n * K / t_e2e
+
+    # dominant kernel: gated weighting (fused with the motion update)
+    hbm, peak_kind = peaks()
+    kk = dict(zip(("reinit", "predict", "weight", "est", "covs", "scan", "gather", "inject",
+                   "commit", "misc"), range(10)))
+    w_ms = val["kernel_ms"][kk["weight"]] / max(1, val["kernel_count"][kk["weight"]])
+    # algorithmic bytes per particle of the fused predict+weight pass:
+    # read pose 28 B, write pose 28 B, write log-likelihood 4 B
+    alg_bytes = 60.0 * n
+    achieved = alg_bytes / (w_ms * 1e-3) / 1e9
+    nobs = 256
+    sm_mhz = val["clocks"]["sm_mhz"] or 1965.0
+    issue_peak = 148 * 128 * sm_mhz * 1e6  # FP32 lane-ops/s
+    pair_rate = n * nobs / (w_ms * 1e-3)
+    kernel_share = {name: float(val["kernel_ms"][i]) for name, i in kk.items()}
+    tot_k = sum(kernel_share.values())
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_value / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": "at-scale PF cycle: N=1M f32 particles, 64 landmarks in 50x50x10 m, "
+                        "256 obs/cycle (10% uniform outliers), gate 3 sigma, ESS<N/2 resample, "
+                        "random_inject_ratio 0.01, helix trajectory",
+            "particles": n, "obs_per_cycle": nobs, "parallelism": f"replicas x{world}",
+            "l2": "flushed (256 MiB write) between timed steps, outside the events",
+            "mean_track_err_m": float(e2e["errs"].mean()),
+            "resamples_in_e2e": int(e2e["resampled"]),
+        },
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": float(e2e["h2d"]),
+                "d2h_bytes_per_step": float(e2e["d2h"]),
+                "ms_per_step": 1e3 * t_e2e / K, "host_syncs_per_step": float(e2e["syncs"]),
+                "path": "pf_core ParticleFilter::update mirror -> pfc_* C-ABI"},
+        "gpu_launches": val["launches"],
+        "roofline": {"bound": "hbm", "kernel": "k_weight (fused predict + gated weighting)",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None, "peak_source": peak_kind,
+                     "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": w_ms},
+        "issue_roofline": {"kernel": "k_weight", "unit": "particle-observation pairs/s",
+                           "achieved_pairs_per_s": pair_rate,
+                           "fp32_issue_peak_lane_ops_per_s": issue_peak,
+                           "lane_ops_per_pair_at_peak": issue_peak / pair_rate,
+                           "sm_mhz": sm_mhz},
+        "kernel_ms_share": {k2: v / tot_k for k2, v in kernel_share.items() if tot_k > 0},
+        "clocks": val["clocks"],
+    }
+
+    if rank == 0 and world == 1 and not args.no_extras:
+        import oracle
+        sc_cpu = scenario(args, 8)
+        done, secs = run_cpu_cycles(sc_cpu, n, args.cpu_seconds, 50)
+        line["cpu_baseline"] = {"value": n * done / secs, "unit": UNIT,
+                                "cores": int(oracle.lib().orc_threads()), "kind": "port",
+                                "sample": f"{done} cycles at N={n} (time-bounded)"}
+        try:
+            ref_v = run_ref_gpu_pf(args, sc, 20)
+        except Exception as exc:  # the comparator is informative only
+            ref_v = None
+            line["reference_gpu_error"] = str(exc)[:200]
+        if ref_v:
+            line["reference_gpu"] = {"value": ref_v, "unit": UNIT,
+                                     "what": "reference pf_kernels.cu built for sm_100a, "
+                                             "driven in the Rust CudaBackend call order"}
+        line["gl"] = run_gl(args)
+        line["gl"]["config"] = ("10x10 m room at 0.05 m (200x200), 30 boxes 0.2-1.0 m, 360 rays, "
+                                f"rmax 10, {args.gl_hyps} hyps = positions x 16 yaws, k=64, "
+                                f"{args.gl_trials} trials, scan noise N(0, 0.01 m)")
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

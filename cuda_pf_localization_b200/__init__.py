@@ -1,0 +1,400 @@
+"""B200-native particle-filter localization and CBGL global localization.
+
+The product is the shared library ``libpf_kernels.so`` (hand-written sm_100a
+CUDA behind the reference's ``pfc_*`` / ``pfgl_*`` C-ABI, declared in
+``include/pfc_abi.h``) and ``libpf_core.so`` (the C++ host layer that drives
+it the way the reference's Rust ``pf_core`` does, ``include/pf_core.h``).
+This package loads both with ctypes and exposes thin Python views of them.
+
+Nothing here computes on the CPU: every call goes through the CUDA library,
+and importing the bindings fails loudly when the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from ctypes import POINTER, byref, c_double, c_float, c_int, c_uint, c_ulonglong, c_void_p
+from pathlib import Path
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent
+KERNELS_SO = PKG_DIR / "libpf_kernels.so"
+CORE_SO = PKG_DIR / "libpf_core.so"
+
+__all__ = [
+    "CObservation", "PfcOdom", "PfcCycleParams", "PfcoreConfig", "PfcoreObservation",
+    "PfcoreOdom", "PfcoreEstimate", "PfcoreGlParams", "PfcorePoseHypothesis",
+    "kernels", "core", "ParticleFilter", "GlobalLoc", "PFC_EST_LEN", "PF_ABI_SYMBOLS",
+]
+
+PFC_EST_LEN = 24
+PFC_EST = dict(POS=0, QUAT=3, POSCOV=7, ATTCOV=13, ESS=19, RESAMPLED=20, ESS_PRE=21)
+
+# The 18 drop-in symbols the reference's Rust crate binds
+# (crates/pf_core/src/cuda.rs:33-88, crates/pf_core/src/global_loc.rs:261-271).
+PF_ABI_SYMBOLS = (
+    "pfc_create", "pfc_destroy", "pfc_init", "pfc_upload_landmarks", "pfc_reinit",
+    "pfc_predict", "pfc_weight", "pfc_resample", "pfc_est_sums", "pfc_covs",
+    "pfc_snapshot", "pfc_device_available", "pfgl_create", "pfgl_destroy",
+    "pfgl_free_cells", "pfgl_generate", "pfgl_score", "pfgl_topk",
+)
+
+
+class CObservation(C.Structure):
+    _fields_ = [("id", c_int), ("mode", c_int), ("dx", c_float), ("dy", c_float),
+                ("dz", c_float), ("range", c_float)]
+
+
+class PfcOdom(C.Structure):
+    _fields_ = [("t", c_float * 3), ("q", c_float * 4), ("tstd", c_float * 3),
+                ("rstd", c_float * 3)]
+
+
+class PfcCycleParams(C.Structure):
+    _fields_ = [("sigma_r", c_float), ("sigma_b", c_float), ("gate", c_float),
+                ("resample_ess_ratio", c_double), ("random_inject_ratio", c_float),
+                ("reserved", c_int)]
+
+
+class PfcStats(C.Structure):
+    _fields_ = [("launches", c_ulonglong), ("h2d_bytes", c_ulonglong),
+                ("d2h_bytes", c_ulonglong), ("host_syncs", c_ulonglong)]
+
+
+PFC_KERNEL_KINDS = ("reinit", "predict", "weight", "est", "covs", "scan", "gather",
+                    "inject", "commit", "misc")
+
+
+class PfcoreConfig(C.Structure):
+    _fields_ = [("particle_count", c_int), ("trans_noise", c_double * 3),
+                ("rot_noise", c_double * 3), ("range_noise", c_double),
+                ("bearing_noise", c_double), ("resample_ess_ratio", c_double),
+                ("random_inject_ratio", c_double), ("gate_sigma", c_double),
+                ("seed", c_ulonglong)]
+
+
+class PfcoreObservation(C.Structure):
+    _fields_ = [("landmark_id", c_int), ("mode", c_int), ("vector", c_double * 3),
+                ("range", c_double)]
+
+
+class PfcoreOdom(C.Structure):
+    _fields_ = [("translation", c_double * 3), ("rotation", c_double * 4),
+                ("trans_noise", c_double * 3), ("rot_noise", c_double * 3)]
+
+
+class PfcoreEstimate(C.Structure):
+    _fields_ = [("position", c_double * 3), ("attitude", c_double * 4),
+                ("pos_cov", c_double * 9), ("att_cov", c_double * 9), ("ess", c_double),
+                ("valid", c_int), ("resampled", c_int)]
+
+
+class PfcoreGlParams(C.Structure):
+    _fields_ = [("hypotheses", c_int), ("rays", c_int), ("rmax", c_double),
+                ("ang_span", c_double), ("topk", c_int), ("seed", c_ulonglong)]
+
+
+class PfcorePoseHypothesis(C.Structure):
+    _fields_ = [("x", c_double), ("y", c_double), ("theta", c_double), ("caer", c_double)]
+
+
+assert C.sizeof(CObservation) == 24  # repr(C) layout of cuda.rs:18-27
+
+_fp = POINTER(c_float)
+_dp = POINTER(c_double)
+_ip = POINTER(c_int)
+_u8p = POINTER(C.c_ubyte)
+
+_KERNEL_SIGS = {
+    "pfc_create": (c_void_p, [c_int]),
+    "pfc_destroy": (c_int, [c_void_p]),
+    "pfc_init": (c_int, [c_void_p, c_int, c_uint]),
+    "pfc_upload_landmarks": (c_int, [c_void_p, _fp, c_int]),
+    "pfc_reinit": (c_int, [c_void_p] + [c_float] * 7 + [_fp, _fp]),
+    "pfc_predict": (c_int, [c_void_p] + [c_float] * 7 + [_fp, _fp]),
+    "pfc_weight": (c_int, [c_void_p, POINTER(CObservation), c_int, c_float, c_float, c_float]),
+    "pfc_resample": (c_int, [c_void_p, c_float]),
+    "pfc_est_sums": (c_int, [c_void_p, _dp]),
+    "pfc_covs": (c_int, [c_void_p] + [c_float] * 7 + [_dp]),
+    "pfc_snapshot": (c_int, [c_void_p, _fp, _fp]),
+    "pfc_device_available": (c_int, []),
+    "pfgl_create": (c_void_p, [c_int, c_int, c_float, c_float, c_float, _u8p, c_int]),
+    "pfgl_destroy": (c_int, [c_void_p]),
+    "pfgl_free_cells": (c_int, [c_void_p]),
+    "pfgl_generate": (c_int, [c_void_p, c_int, c_ulonglong]),
+    "pfgl_score": (c_int, [c_void_p, _fp, c_int, c_float, c_float]),
+    "pfgl_topk": (c_int, [c_void_p, c_int, _fp]),
+    "pfc_last_error_message": (C.c_char_p, []),
+    "pfc_version": (c_int, []),
+    "pfc_cycle": (c_int, [c_void_p, POINTER(PfcOdom), POINTER(CObservation), c_int,
+                          POINTER(PfcCycleParams), _dp]),
+    "pfc_cycle_device": (c_int, [c_void_p, POINTER(PfcOdom), c_void_p, c_int,
+                                 POINTER(PfcCycleParams), _dp]),
+    "pfc_cycle_result": (c_int, [c_void_p, _dp]),
+    "pfc_stream": (c_void_p, [c_void_p]),
+    "pfc_size": (c_int, [c_void_p]),
+    "pfc_get_weights": (c_int, [c_void_p, _fp]),
+    "pfc_get_ll": (c_int, [c_void_p, _fp]),
+    "pfc_set_state": (c_int, [c_void_p, _fp, _fp, _fp]),
+    "pfc_resample_u01": (c_int, [c_void_p, c_double, c_float]),
+    "pfc_record_ancestors": (c_int, [c_void_p, c_int]),
+    "pfc_get_ancestors": (c_int, [c_void_p, _ip]),
+    "pfc_pick_from_cum": (c_int, [c_void_p, _dp, c_int, c_double, c_double, _ip]),
+    "pfc_get_lcg": (c_int, [c_void_p, POINTER(c_ulonglong)]),
+    "pfc_set_lcg": (c_int, [c_void_p, c_ulonglong]),
+    "pfc_set_weight_kernel": (c_int, [c_void_p, c_int]),
+    "pfc_get_stats": (c_int, [c_void_p, POINTER(PfcStats)]),
+    "pfc_reset_stats": (c_int, [c_void_p]),
+    "pfc_profile": (c_int, [c_void_p, c_int]),
+    "pfc_profile_read": (c_int, [c_void_p, _dp, POINTER(C.c_longlong)]),
+    "pfgl_generate_yaws": (c_int, [c_void_p, c_int, c_int, c_ulonglong]),
+    "pfgl_set_hyps": (c_int, [c_void_p, _fp, c_int]),
+    "pfgl_get_hyps": (c_int, [c_void_p, _fp]),
+    "pfgl_get_caer": (c_int, [c_void_p, _fp]),
+    "pfgl_topk_ex": (c_int, [c_void_p, c_int, _fp, _fp, _ip]),
+    "pfgl_topk_from_scores": (c_int, [c_void_p, _fp, c_int, c_int, _ip]),
+    "pfgl_localize": (c_int, [c_void_p, _fp, c_int, c_float, c_float, c_int, _fp, _fp, _ip]),
+    "pfgl_cell": (c_int, [c_void_p, c_int, c_int]),
+}
+
+_CORE_SIGS = {
+    "pfcore_config_default": (None, [POINTER(PfcoreConfig)]),
+    "pfcore_filter_new": (c_void_p, [POINTER(PfcoreConfig)]),
+    "pfcore_filter_free": (None, [c_void_p]),
+    "pfcore_map_add": (c_int, [c_void_p, c_int, c_double, c_double, c_double]),
+    "pfcore_map_clear": (c_int, [c_void_p]),
+    "pfcore_map_load_text": (c_int, [c_void_p, C.c_char_p]),
+    "pfcore_map_capacity": (c_int, [c_void_p]),
+    "pfcore_filter_reinitialize": (c_int, [c_void_p, _dp, _dp, _dp]),
+    "pfcore_filter_update": (c_int, [c_void_p, POINTER(PfcoreOdom),
+                                     POINTER(PfcoreObservation), c_int,
+                                     POINTER(PfcoreEstimate)]),
+    "pfcore_filter_update_fused": (c_int, [c_void_p, POINTER(PfcoreOdom),
+                                           POINTER(PfcoreObservation), c_int,
+                                           POINTER(PfcoreEstimate)]),
+    "pfcore_filter_snapshot": (c_int, [c_void_p, _dp, _dp, _dp]),
+    "pfcore_filter_handle": (c_void_p, [c_void_p]),
+    "pfcore_quat_mean": (None, [_dp, _dp]),
+    "pfcore_gl_params_default": (None, [POINTER(PfcoreGlParams)]),
+    "pfcore_gl_new": (c_void_p, [c_int, c_int, c_double, c_double, c_double, _u8p,
+                                 POINTER(PfcoreGlParams)]),
+    "pfcore_gl_free": (None, [c_void_p]),
+    "pfcore_gl_free_cells": (c_int, [c_void_p]),
+    "pfcore_gl_set_seed": (c_int, [c_void_p, c_ulonglong]),
+    "pfcore_gl_localize": (c_int, [c_void_p, _fp, c_int, POINTER(PfcorePoseHypothesis)]),
+    "pfcore_gl_handle": (c_void_p, [c_void_p]),
+    "pfcore_grid_from_pgm_yaml": (c_int, [C.c_char_p, C.c_size_t, C.c_char_p, _ip, _ip,
+                                          _dp, _dp, _dp, _u8p]),
+    "pfcore_last_error": (C.c_char_p, []),
+}
+
+_kernels = None
+_core = None
+
+
+def _bind(lib, sigs):
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+def kernels():
+    """The drop-in CUDA library (raises when it has not been built)."""
+    global _kernels
+    if _kernels is None:
+        if not KERNELS_SO.exists():
+            raise RuntimeError(f"{KERNELS_SO} is missing: run "
+                               "`python -m cuda_pf_localization_b200.build`")
+        _kernels = _bind(C.CDLL(str(KERNELS_SO)), _KERNEL_SIGS)
+    return _kernels
+
+
+def core():
+    """The C++ host layer (pf_core mirror) over the CUDA library."""
+    global _core
+    if _core is None:
+        kernels()
+        if not CORE_SO.exists():
+            raise RuntimeError(f"{CORE_SO} is missing: run "
+                               "`python -m cuda_pf_localization_b200.build`")
+        _core = _bind(C.CDLL(str(CORE_SO)), _CORE_SIGS)
+    return _core
+
+
+def last_error() -> str:
+    return kernels().pfc_last_error_message().decode(errors="replace")
+
+
+def fptr(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_fp)
+
+
+def dptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_dp)
+
+
+def iptr(a: np.ndarray):
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_ip)
+
+
+def u8ptr(a: np.ndarray):
+    assert a.dtype == np.uint8 and a.flags.c_contiguous
+    return a.ctypes.data_as(_u8p)
+
+
+def make_cobs(rows) -> "C.Array":
+    """Array of CObservation from (id, mode, dx, dy, dz, range) rows."""
+    arr = (CObservation * max(1, len(rows)))()
+    for k, r in enumerate(rows):
+        arr[k] = CObservation(int(r[0]), int(r[1]), float(r[2]), float(r[3]),
+                              float(r[4]), float(r[5]))
+    return arr
+
+
+def make_core_obs(rows):
+    arr = (PfcoreObservation * max(1, len(rows)))()
+    for k, r in enumerate(rows):
+        arr[k].landmark_id = int(r[0])
+        arr[k].mode = int(r[1])
+        arr[k].vector[:] = [float(r[2]), float(r[3]), float(r[4])]
+        arr[k].range = float(r[5])
+    return arr
+
+
+def make_core_odom(t, q, tn, rn) -> PfcoreOdom:
+    o = PfcoreOdom()
+    o.translation[:] = list(map(float, t))
+    o.rotation[:] = list(map(float, q))
+    o.trans_noise[:] = list(map(float, tn))
+    o.rot_noise[:] = list(map(float, rn))
+    return o
+
+
+def estimate_dict(e: PfcoreEstimate) -> dict:
+    return dict(position=np.array(e.position[:]), attitude=np.array(e.attitude[:]),
+                pos_cov=np.array(e.pos_cov[:]).reshape(3, 3),
+                att_cov=np.array(e.att_cov[:]).reshape(3, 3), ess=float(e.ess),
+                valid=bool(e.valid), resampled=bool(e.resampled))
+
+
+class ParticleFilter:
+    """``pf_core::ParticleFilter`` with the CUDA backend (through libpf_core)."""
+
+    def __init__(self, particle_count=4096, seed=42, range_noise=0.05,
+                 bearing_noise=0.02, resample_ess_ratio=0.5, random_inject_ratio=0.0,
+                 gate_sigma=0.0, trans_noise=(0.05, 0.05, 0.02), rot_noise=(0.02, 0.02, 0.03)):
+        lib = core()
+        cfg = PfcoreConfig()
+        lib.pfcore_config_default(byref(cfg))
+        cfg.particle_count = int(particle_count)
+        cfg.seed = int(seed)
+        cfg.range_noise = range_noise
+        cfg.bearing_noise = bearing_noise
+        cfg.resample_ess_ratio = resample_ess_ratio
+        cfg.random_inject_ratio = random_inject_ratio
+        cfg.gate_sigma = gate_sigma
+        cfg.trans_noise[:] = list(trans_noise)
+        cfg.rot_noise[:] = list(rot_noise)
+        self.cfg = cfg
+        self.n = int(particle_count)
+        self._h = lib.pfcore_filter_new(byref(cfg))
+        if not self._h:
+            raise RuntimeError("pfcore_filter_new failed: "
+                               + lib.pfcore_last_error().decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            core().pfcore_filter_free(self._h)
+            self._h = None
+
+    __del__ = close
+
+    @property
+    def handle(self):
+        return core().pfcore_filter_handle(self._h)
+
+    def set_map(self, landmarks: dict):
+        lib = core()
+        lib.pfcore_map_clear(self._h)
+        for i, p in landmarks.items():
+            lib.pfcore_map_add(self._h, int(i), float(p[0]), float(p[1]), float(p[2]))
+
+    def load_map_text(self, text: str) -> int:
+        lib = core()
+        lib.pfcore_map_clear(self._h)
+        n = lib.pfcore_map_load_text(self._h, text.encode())
+        if n < 0:
+            raise ValueError(lib.pfcore_last_error().decode())
+        return n
+
+    def reinitialize(self, pose, pos_std, rot_std):
+        pose = np.ascontiguousarray(pose, dtype=np.float64)
+        ps = np.ascontiguousarray(pos_std, dtype=np.float64)
+        rs = np.ascontiguousarray(rot_std, dtype=np.float64)
+        rc = core().pfcore_filter_reinitialize(self._h, dptr(pose), dptr(ps), dptr(rs))
+        if rc != 0:
+            raise RuntimeError("reinitialize failed")
+
+    def update(self, odom: PfcoreOdom, obs_rows, fused=False) -> dict:
+        arr = make_core_obs(obs_rows)
+        est = PfcoreEstimate()
+        fn = core().pfcore_filter_update_fused if fused else core().pfcore_filter_update
+        rc = fn(self._h, byref(odom), arr, len(obs_rows), byref(est))
+        if rc != 0:
+            raise RuntimeError("update failed: " + core().pfcore_last_error().decode())
+        return estimate_dict(est)
+
+    def snapshot(self):
+        pos = np.zeros(3 * self.n)
+        quat = np.zeros(4 * self.n)
+        w = np.zeros(self.n)
+        if core().pfcore_filter_snapshot(self._h, dptr(pos), dptr(quat), dptr(w)) != 0:
+            raise RuntimeError("snapshot failed")
+        return pos.reshape(-1, 3), quat.reshape(-1, 4), w
+
+
+class GlobalLoc:
+    """``pf_core::global_loc::CudaGlobalLoc`` (through libpf_core)."""
+
+    def __init__(self, cells: np.ndarray, res=0.05, origin=(0.0, 0.0), hypotheses=50000,
+                 rays=360, rmax=10.0, ang_span=2 * np.pi, topk=10, seed=42):
+        lib = core()
+        cells = np.ascontiguousarray(cells, dtype=np.uint8)
+        self.h_cells, self.w_cells = cells.shape
+        p = PfcoreGlParams(int(hypotheses), int(rays), float(rmax), float(ang_span),
+                           int(topk), int(seed))
+        self.params = p
+        self._h = lib.pfcore_gl_new(self.w_cells, self.h_cells, res, origin[0], origin[1],
+                                    u8ptr(cells), byref(p))
+        if not self._h:
+            raise RuntimeError("pfcore_gl_new failed")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            core().pfcore_gl_free(self._h)
+            self._h = None
+
+    __del__ = close
+
+    @property
+    def handle(self):
+        return core().pfcore_gl_handle(self._h)
+
+    def free_cells(self) -> int:
+        return core().pfcore_gl_free_cells(self._h)
+
+    def set_seed(self, seed: int):
+        core().pfcore_gl_set_seed(self._h, int(seed))
+
+    def localize(self, scan_f32: np.ndarray):
+        scan = np.ascontiguousarray(scan_f32, dtype=np.float32)
+        out = (PfcorePoseHypothesis * self.params.topk)()
+        k = core().pfcore_gl_localize(self._h, fptr(scan), len(scan), out)
+        if k <= 0:
+            raise RuntimeError("localize failed: " + core().pfcore_last_error().decode())
+        return [(out[j].x, out[j].y, out[j].theta, out[j].caer) for j in range(k)]

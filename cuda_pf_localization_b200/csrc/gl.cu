@@ -1,0 +1,836 @@
+// gl.cu — CBGL-style global localization (Filotheou, arXiv:2307.14247) on
+// the B200: uniform hypothesis dispersion, DDA raycast + CAER scoring, and
+// bottom-k selection, behind the pfgl_* C-ABI.
+//
+// Device layout
+//   grid  (W+2) x (H+2) bytes, row-major, row 0 = lowest y: 0 free,
+//         1 occupied (any nonzero input byte), 2 = the one-cell border that
+//         stands for "outside the map".  A ray that steps onto the border
+//         returns rmax, exactly like the reference's bounds test after each
+//         step (src/cuda/pf_kernels.cu:797-806), so the inner loop needs one
+//         byte load and no bounds compares.
+//   free  int2 list of free cells in row-major order (deterministic, the
+//         order crates/pf_core/src/global_loc.rs:365-368 uses).
+//   hyp   n x (x, y, theta) f32;  caer  n f32;  keys  n u64 composite keys.
+//
+// Scoring: persistent CTAs copy the padded grid and the real scan into shared
+// memory once; each warp owns one hypothesis at a time and lanes cast
+// consecutive rays (neighbouring rays have similar lengths, which keeps the
+// DDA loops of a warp in step).  The DDA arithmetic is the reference's f32
+// sequence (src/cuda/pf_kernels.cu:774-808) so per-ray distances agree bit
+// for bit; only the order of the CAER sum differs (lane-sequential, then an
+// xor butterfly).
+//
+// Early termination (pfgl_localize): the partial CAER of a hypothesis only
+// grows (non-negative terms, monotone rounding), so a hypothesis whose
+// partial sum already exceeds an upper bound of the final k-th best key can
+// never enter the bottom-k.  The bound is the k-th best composite key of a
+// fully scored seed batch, tightened after every chunk.  Selected results
+// are identical to exhaustive scoring.
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <new>
+#include <vector>
+
+#include "pf_common.cuh"
+
+namespace pfb {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kMaxSmem = 200 * 1024;
+
+struct GlCtl {
+    unsigned long long tau;   // pruning bound on the composite key
+    unsigned n_cand;          // survivors appended by the pruned scorer
+    unsigned err;
+};
+
+struct GlHandle {
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    int W = 0, H = 0, Wp = 0, Hp = 0;
+    float res = 0.05f, ox = 0.f, oy = 0.f;
+    int cap_hyp = 0;
+    int nfree = 0;
+    int nh = 0;
+    unsigned char* d_grid = nullptr;  // padded
+    int2* d_free = nullptr;
+    float* d_hyp = nullptr;
+    float* d_caer = nullptr;
+    uint64_t* d_keys = nullptr;
+    uint64_t* d_keys_alt = nullptr;
+    unsigned* d_hist = nullptr;
+    int hist_cap = 0;
+    float* d_scan = nullptr;
+    int scan_cap = 0;
+    float* d_out = nullptr;   // k x 3 (cap_hyp)
+    float* d_outc = nullptr;  // k CAER
+    int* d_outi = nullptr;    // k indices
+    uint64_t* d_cand = nullptr;  // pruned-scorer survivors (cap_hyp)
+    GlCtl* d_ctl = nullptr;
+    GlCtl* h_ctl = nullptr;
+    std::vector<unsigned char> host_grid;  // unpadded 0/1 copy
+    bool caer_valid = false;
+};
+
+GlHandle* as_gl(void* h) { return static_cast<GlHandle*>(h); }
+
+// ---------------------------------------------------------------- dispersion
+
+// Uniform dispersion with the reference's mapping (src/cuda/pf_kernels.cu:
+// 811-823): cell = free[floor(u3 * nfree)], in-cell offset (u0, u1), yaw
+// -pi + 2 pi u2; the uniforms come from Philox4x32-10 keyed by the seed with
+// counter (i, 0, 0, RNG_GL).
+__global__ void k_gl_gen(int n, int n_yaw, int nfree, const int2* __restrict__ free_cells,
+                         float ox, float oy, float res, uint64_t seed,
+                         float* __restrict__ hyp) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= n) return;
+    const int p = i / n_yaw, j = i - p * n_yaw;
+    const U4 r = philox4x32_10({(uint32_t)p, 0u, 0u, RNG_GL}, (uint32_t)seed,
+                               (uint32_t)(seed >> 32));
+    const float ux = u01_open(r.x), uy = u01_open(r.y), uz = u01_open(r.z),
+                uw = u01_open(r.w);
+    const int c = min((int)(uw * (float)nfree), nfree - 1);
+    const int2 cell = free_cells[c];
+    float th = -3.14159265f + 6.28318530f * uz;
+    if (n_yaw > 1) th = th + (6.28318530f / (float)n_yaw) * (float)j;
+    hyp[3 * i] = ox + ((float)cell.x + ux) * res;
+    hyp[3 * i + 1] = oy + ((float)cell.y + uy) * res;
+    hyp[3 * i + 2] = th;
+}
+
+// ------------------------------------------------------------------ raycast
+
+struct GridView {
+    const unsigned char* cells;  // padded grid
+    int W, H, Wp;
+    float res, ox, oy;
+};
+
+// 2-D DDA from the start cell (cx, cy) with in-cell fractions (frx, fry):
+// distance to the first occupied cell, rmax when the ray passes rmax or
+// leaves the map.  Arithmetic follows src/cuda/pf_kernels.cu:784-808.
+__device__ __forceinline__ float cast_ray(const unsigned char* __restrict__ g,
+                                          int Wp, int start, float frx,
+                                          float fry, float dirx, float diry,
+                                          float res, float rmax) {
+    const int sx = dirx > 0 ? 1 : -1;
+    const int sy = diry > 0 ? Wp : -Wp;
+    const float adx = fabsf(dirx), ady = fabsf(diry);
+    const float tdx = adx > 1e-9f ? res / adx : INFINITY;
+    const float tdy = ady > 1e-9f ? res / ady : INFINITY;
+    float tmx = adx > 1e-9f ? ((dirx > 0 ? 1.f - frx : frx) * tdx) : INFINITY;
+    float tmy = ady > 1e-9f ? ((diry > 0 ? 1.f - fry : fry) * tdy) : INFINITY;
+    int idx = start;
+    for (int step = 0; step < 8192; ++step) {
+        float dist;
+        if (tmx <= tmy) {
+            dist = tmx;
+            tmx += tdx;
+            idx += sx;
+        } else {
+            dist = tmy;
+            tmy += tdy;
+            idx += sy;
+        }
+        if (dist > rmax) return rmax;
+        const unsigned char v = g[idx];
+        if (v) return v == 1 ? dist : rmax;
+    }
+    return rmax;
+}
+
+// Start cell of a hypothesis (floor of the f32 cell coordinate, as
+// src/cuda/pf_kernels.cu:774-781); false when outside the map.
+__device__ __forceinline__ bool start_cell(const GridView& gv, float x, float y,
+                                           int& start, float& frx,
+                                           float& fry) {
+    const float fx = (x - gv.ox) / gv.res;
+    const float fy = (y - gv.oy) / gv.res;
+    const int cx = (int)floorf(fx), cy = (int)floorf(fy);
+    if (!(cx >= 0 && cy >= 0 && cx < gv.W && cy < gv.H)) return false;
+    frx = (x - gv.ox) / gv.res - (float)cx;
+    fry = (y - gv.oy) / gv.res - (float)cy;
+    start = (cy + 1) * gv.Wp + (cx + 1);
+    return true;
+}
+
+__device__ __forceinline__ float ray_angle(float th, int r, int nrays,
+                                           float span) {
+    return th + (nrays > 1 ? span * (float)r / (float)(nrays - 1) : 0.f);
+}
+
+__device__ __forceinline__ float warp_sum_f(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(~0u, v, o);
+    return v;
+}
+
+// Copy the padded grid and the scan into shared memory.
+__device__ __forceinline__ void load_smem(unsigned char* s_grid, int grid_bytes,
+                                          const unsigned char* __restrict__ g,
+                                          float* s_scan, const float* scan,
+                                          int nrays) {
+    const int nv = grid_bytes / 16;
+    const uint4* src = reinterpret_cast<const uint4*>(g);
+    uint4* dst = reinterpret_cast<uint4*>(s_grid);
+    for (int k = threadIdx.x; k < nv; k += blockDim.x) dst[k] = __ldg(&src[k]);
+    for (int k = threadIdx.x; k < nrays; k += blockDim.x) s_scan[k] = scan[k];
+    __syncthreads();
+}
+
+// CAER of hypotheses [0, nh): one warp per hypothesis, static striding.
+template <bool kSmem>
+__global__ void __launch_bounds__(kThreads)
+    k_gl_score(GridView gv, int grid_bytes, const float* __restrict__ hyp,
+               int nh, const float* __restrict__ scan, int nrays, float rmax,
+               float span, float* __restrict__ caer) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const unsigned char* g = gv.cells;
+    const float* sc = scan;
+    if (kSmem) {
+        float* s_scan = reinterpret_cast<float*>(smem + grid_bytes);
+        load_smem(smem, grid_bytes, gv.cells, s_scan, scan, nrays);
+        g = smem;
+        sc = s_scan;
+    }
+    const int lane = threadIdx.x & 31;
+    const int gw = blockIdx.x * kWarps + (threadIdx.x >> 5);
+    const int nw = gridDim.x * kWarps;
+    for (int h = gw; h < nh; h += nw) {
+        const float x = hyp[3 * h], y = hyp[3 * h + 1], th = hyp[3 * h + 2];
+        int start = 0;
+        float frx = 0.f, fry = 0.f;
+        const bool inside = start_cell(gv, x, y, start, frx, fry);
+        float acc = 0.f;
+        for (int r = lane; r < nrays; r += 32) {
+            float vm = rmax;
+            if (inside) {
+                float dx, dy;
+                sincosf(ray_angle(th, r, nrays, span), &dy, &dx);
+                vm = cast_ray(g, gv.Wp, start, frx, fry, dx, dy, gv.res, rmax);
+            }
+            acc += fabsf(sc[r] - vm);
+        }
+        acc = warp_sum_f(acc);
+        if (lane == 0) caer[h] = acc;
+    }
+}
+
+// CAER value of a composite key (inverse of composite_key's high word).
+__device__ __forceinline__ float key_to_float(uint64_t key) {
+    const int o = (int)((uint32_t)(key >> 32) ^ 0x80000000u);
+    return __int_as_float(o >= 0 ? o : (o ^ 0x7FFFFFFF));
+}
+
+// Pruned scorer for hypotheses [h0, h1): rays are cast in rounds of 32; after
+// each round the warp's partial CAER (same lane-sequential order as the final
+// sum, so partial <= final) is compared with the bound.  Survivors (final key
+// <= tau) are appended to cand.
+template <bool kSmem>
+__global__ void __launch_bounds__(kThreads)
+    k_gl_score_pruned(GridView gv, int grid_bytes, const float* __restrict__ hyp,
+                      int h0, int h1, const float* __restrict__ scan, int nrays,
+                      float rmax, float span, float* __restrict__ caer,
+                      uint64_t* __restrict__ cand, GlCtl* ctl, int cand_cap) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const unsigned char* g = gv.cells;
+    const float* sc = scan;
+    if (kSmem) {
+        float* s_scan = reinterpret_cast<float*>(smem + grid_bytes);
+        load_smem(smem, grid_bytes, gv.cells, s_scan, scan, nrays);
+        g = smem;
+        sc = s_scan;
+    }
+    const unsigned long long tau = ctl->tau;
+    const float tau_f = key_to_float(tau);
+    const int lane = threadIdx.x & 31;
+    const int gw = blockIdx.x * kWarps + (threadIdx.x >> 5);
+    const int nw = gridDim.x * kWarps;
+    for (int h = h0 + gw; h < h1; h += nw) {
+        const float x = hyp[3 * h], y = hyp[3 * h + 1], th = hyp[3 * h + 2];
+        int start = 0;
+        float frx = 0.f, fry = 0.f;
+        const bool inside = start_cell(gv, x, y, start, frx, fry);
+        float acc = 0.f;
+        bool pruned = false;
+        for (int r0 = 0; r0 < nrays; r0 += 32) {
+            const int r = r0 + lane;
+            if (r < nrays) {
+                float vm = rmax;
+                if (inside) {
+                    float dx, dy;
+                    sincosf(ray_angle(th, r, nrays, span), &dy, &dx);
+                    vm = cast_ray(g, gv.Wp, start, frx, fry, dx, dy, gv.res,
+                                  rmax);
+                }
+                acc += fabsf(sc[r] - vm);
+            }
+            if (r0 + 32 < nrays) {
+                const float part = warp_sum_f(acc);
+                if (part > tau_f) {
+                    pruned = true;
+                    break;
+                }
+            }
+        }
+        if (pruned) {
+            if (lane == 0) caer[h] = -1.0f;  // not scored
+            continue;
+        }
+        const float total = warp_sum_f(acc);
+        if (lane == 0) {
+            caer[h] = total;
+            const uint64_t key = composite_key(total, (uint32_t)h);
+            if (key <= tau) {
+                const unsigned slot = atomicAdd(&ctl->n_cand, 1u);
+                if ((int)slot < cand_cap) cand[slot] = key;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------- radix sort
+// Stable LSD radix sort of 64-bit composite keys on their high 32 bits
+// (8-bit digits, 4 passes).  The low word is the hypothesis index and the
+// input is in index order, so stability yields (CAER, index) order.
+
+constexpr int kRsItems = 8;
+constexpr int kRsTile = kThreads * kRsItems;  // 2048
+
+__global__ void k_make_keys(const float* __restrict__ caer, int n,
+                            uint64_t* __restrict__ keys) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i < n) keys[i] = composite_key(caer[i], (uint32_t)i);
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_rs_hist(const uint64_t* __restrict__ keys, int n, int shift,
+              unsigned* __restrict__ hist, int nb) {
+    __shared__ unsigned s_cnt[256];
+    s_cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const int base = blockIdx.x * kRsTile;
+    for (int k = 0; k < kRsItems; ++k) {
+        const int i = base + k * kThreads + threadIdx.x;
+        if (i < n) atomicAdd(&s_cnt[(keys[i] >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    hist[threadIdx.x * nb + blockIdx.x] = s_cnt[threadIdx.x];
+}
+
+// Exclusive scan of `total` counters in place, one block of 1024 threads.
+__global__ void __launch_bounds__(1024) k_rs_scan(unsigned* hist, int total) {
+    __shared__ unsigned s_w[32];
+    __shared__ unsigned s_carry;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int base = 0; base < total; base += 1024) {
+        const int i = base + threadIdx.x;
+        const unsigned v = i < total ? hist[i] : 0u;
+        unsigned x = v;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const unsigned y = __shfl_up_sync(~0u, x, d);
+            if (lane >= d) x += y;
+        }
+        if (lane == 31) s_w[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            unsigned wv = s_w[lane];
+            unsigned z = wv;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const unsigned y = __shfl_up_sync(~0u, z, d);
+                if (lane >= d) z += y;
+            }
+            s_w[lane] = z - wv;
+        }
+        __syncthreads();
+        const unsigned carry = s_carry;
+        if (i < total) hist[i] = carry + s_w[warp] + x - v;
+        __syncthreads();
+        if (threadIdx.x == 1023) s_carry = carry + s_w[warp] + x;
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_rs_scatter(const uint64_t* __restrict__ in, uint64_t* __restrict__ out,
+                 int n, int shift, const unsigned* __restrict__ hist, int nb) {
+    __shared__ unsigned s_wc[kWarps][256];
+    __shared__ unsigned s_base[256];
+    __shared__ unsigned s_goff[256];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    s_base[tid] = 0;
+    s_goff[tid] = hist[tid * nb + blockIdx.x];
+    const unsigned lt = (1u << lane) - 1u;
+    const int base = blockIdx.x * kRsTile;
+    for (int k = 0; k < kRsItems; ++k) {
+        for (int w = 0; w < kWarps; ++w) s_wc[w][tid] = 0;
+        __syncthreads();
+        const int i = base + k * kThreads + tid;
+        const bool ok = i < n;
+        const uint64_t key = ok ? in[i] : 0ull;
+        const unsigned d = ok ? (unsigned)((key >> shift) & 255u) : 256u + lane;
+        const unsigned peers = __match_any_sync(~0u, d);
+        const unsigned rank = __popc(peers & lt);
+        if (ok && rank == 0) s_wc[warp][d] = __popc(peers);
+        __syncthreads();
+        {
+            unsigned run = s_base[tid];
+            for (int w = 0; w < kWarps; ++w) {
+                const unsigned c = s_wc[w][tid];
+                s_wc[w][tid] = run;
+                run += c;
+            }
+            s_base[tid] = run;
+        }
+        __syncthreads();
+        if (ok) out[s_goff[d] + s_wc[warp][d] + rank] = key;
+        __syncthreads();
+    }
+}
+
+// Sort n composite keys held in d_keys.  index_bits > 0 also sorts the low
+// (index) word over that many bits, for inputs that are not in index order.
+// Returns the buffer that holds the sorted keys.
+uint64_t* radix_sort_keys(GlHandle* h, int n, int index_bits) {
+    const int nb = ceil_div(n, kRsTile);
+    const int need = 256 * nb;
+    if (need > h->hist_cap) {
+        cudaFree(h->d_hist);
+        h->d_hist = nullptr;
+        if (cudaMalloc((void**)&h->d_hist, sizeof(unsigned) * (size_t)need) !=
+            cudaSuccess) {
+            set_error("pf_b200: radix sort histogram allocation failed");
+            return nullptr;
+        }
+        h->hist_cap = need;
+    }
+    std::vector<int> shifts;
+    for (int s = 0; s < 32 && s < index_bits; s += 8) shifts.push_back(s);
+    for (int s = 32; s < 64; s += 8) shifts.push_back(s);
+    uint64_t* a = h->d_keys;
+    uint64_t* b = h->d_keys_alt;
+    for (int shift : shifts) {
+        k_rs_hist<<<nb, kThreads, 0, h->stream>>>(a, n, shift, h->d_hist, nb);
+        k_rs_scan<<<1, 1024, 0, h->stream>>>(h->d_hist, need);
+        k_rs_scatter<<<nb, kThreads, 0, h->stream>>>(a, b, n, shift, h->d_hist,
+                                                     nb);
+        std::swap(a, b);
+    }
+    if (cudaGetLastError() != cudaSuccess) {
+        set_error("pf_b200: radix sort launch failed");
+        return nullptr;
+    }
+    return a;
+}
+
+int index_bit_width(int n) {
+    int b = 0;
+    while (b < 32 && (1ull << b) < (unsigned long long)n) ++b;
+    return b;
+}
+
+__global__ void k_gather_topk(const uint64_t* __restrict__ keys, int k,
+                              const float* __restrict__ hyp,
+                              const float* __restrict__ caer, float* out3,
+                              float* outc, int* outi) {
+    const int j = blockIdx.x * kThreads + threadIdx.x;
+    if (j >= k) return;
+    const int src = (int)(uint32_t)keys[j];
+    out3[3 * j] = hyp[3 * src];
+    out3[3 * j + 1] = hyp[3 * src + 1];
+    out3[3 * j + 2] = hyp[3 * src + 2];
+    outc[j] = caer[src];
+    outi[j] = src;
+}
+
+// k-th smallest key of a sorted array -> pruning bound.
+__global__ void k_set_tau(const uint64_t* sorted, int k, GlCtl* ctl) {
+    ctl->tau = sorted[k - 1];
+    ctl->n_cand = 0;
+}
+
+// ------------------------------------------------------------ host helpers
+
+int ensure_scan(GlHandle* h, const float* scan, int nrays) {
+    if (nrays > h->scan_cap) {
+        cudaFree(h->d_scan);
+        h->d_scan = nullptr;
+        PFB_CK(cudaMalloc((void**)&h->d_scan, sizeof(float) * (size_t)nrays));
+        h->scan_cap = nrays;
+    }
+    PFB_CK(cudaMemcpyAsync(h->d_scan, scan, sizeof(float) * (size_t)nrays,
+                           cudaMemcpyHostToDevice, h->stream));
+    return 0;
+}
+
+GridView grid_view(const GlHandle* h) {
+    return {h->d_grid, h->W, h->H, h->Wp, h->res, h->ox, h->oy};
+}
+
+int grid_bytes_padded(const GlHandle* h) {
+    return (int)(((size_t)h->Wp * h->Hp + 15) / 16 * 16);
+}
+
+template <bool kSmem>
+int score_grid_size(size_t smem) {
+    int per_sm = 0, sms = 0, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gl_score<kSmem>,
+                                                  kThreads, smem);
+    if (per_sm < 1) per_sm = 1;
+    return sms * per_sm;
+}
+
+int launch_score(GlHandle* h, int nrays, float rmax, float span) {
+    const int gb = grid_bytes_padded(h);
+    const size_t smem = (size_t)gb + sizeof(float) * (size_t)nrays;
+    const GridView gv = grid_view(h);
+    const int warps_needed = h->nh;
+    if (smem <= (size_t)kMaxSmem) {
+        PFB_CK(cudaFuncSetAttribute(k_gl_score<true>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+        int grid = score_grid_size<true>(smem);
+        grid = std::min(grid, ceil_div(warps_needed, kWarps));
+        k_gl_score<true><<<grid, kThreads, smem, h->stream>>>(
+            gv, gb, h->d_hyp, h->nh, h->d_scan, nrays, rmax, span, h->d_caer);
+    } else {
+        int grid = score_grid_size<false>(0);
+        grid = std::min(grid, ceil_div(warps_needed, kWarps));
+        k_gl_score<false><<<grid, kThreads, 0, h->stream>>>(
+            gv, gb, h->d_hyp, h->nh, h->d_scan, nrays, rmax, span, h->d_caer);
+    }
+    PFB_KL();
+    return 0;
+}
+
+int launch_score_pruned(GlHandle* h, int h0, int h1, int nrays, float rmax,
+                        float span) {
+    const int gb = grid_bytes_padded(h);
+    const size_t smem = (size_t)gb + sizeof(float) * (size_t)nrays;
+    const GridView gv = grid_view(h);
+    const int warps_needed = h1 - h0;
+    if (smem <= (size_t)kMaxSmem) {
+        PFB_CK(cudaFuncSetAttribute(k_gl_score_pruned<true>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+        int grid = score_grid_size<true>(smem);
+        grid = std::min(grid, ceil_div(warps_needed, kWarps));
+        k_gl_score_pruned<true><<<grid, kThreads, smem, h->stream>>>(
+            gv, gb, h->d_hyp, h0, h1, h->d_scan, nrays, rmax, span, h->d_caer,
+            h->d_cand, h->d_ctl, h->cap_hyp);
+    } else {
+        int grid = score_grid_size<false>(0);
+        grid = std::min(grid, ceil_div(warps_needed, kWarps));
+        k_gl_score_pruned<false><<<grid, kThreads, 0, h->stream>>>(
+            gv, gb, h->d_hyp, h0, h1, h->d_scan, nrays, rmax, span, h->d_caer,
+            h->d_cand, h->d_ctl, h->cap_hyp);
+    }
+    PFB_KL();
+    return 0;
+}
+
+// Sort all current CAERs (index-ordered composite keys); returns the sorted
+// buffer or nullptr.
+uint64_t* sort_current(GlHandle* h) {
+    k_make_keys<<<ceil_div(h->nh, kThreads), kThreads, 0, h->stream>>>(
+        h->d_caer, h->nh, h->d_keys);
+    return radix_sort_keys(h, h->nh, 0);
+}
+
+int copy_topk(GlHandle* h, const uint64_t* sorted, int k, float* out3k,
+              float* caer_k, int* idx_k) {
+    k_gather_topk<<<ceil_div(k, kThreads), kThreads, 0, h->stream>>>(
+        sorted, k, h->d_hyp, h->d_caer, h->d_out, h->d_outc, h->d_outi);
+    PFB_KL();
+    if (out3k)
+        PFB_CK(cudaMemcpyAsync(out3k, h->d_out, sizeof(float) * 3 * (size_t)k,
+                               cudaMemcpyDeviceToHost, h->stream));
+    if (caer_k)
+        PFB_CK(cudaMemcpyAsync(caer_k, h->d_outc, sizeof(float) * (size_t)k,
+                               cudaMemcpyDeviceToHost, h->stream));
+    if (idx_k)
+        PFB_CK(cudaMemcpyAsync(idx_k, h->d_outi, sizeof(int) * (size_t)k,
+                               cudaMemcpyDeviceToHost, h->stream));
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    return k;
+}
+
+}  // namespace
+}  // namespace pfb
+
+using namespace pfb;
+
+extern "C" {
+
+void* pfgl_create(int W, int H, float res, float ox, float oy,
+                  const unsigned char* occ, int cap_hyp) {
+    clear_error();
+    if (W <= 0 || H <= 0 || cap_hyp <= 0 || !occ) {
+        set_error("pf_b200: pfgl_create: bad arguments");
+        return nullptr;
+    }
+    GlHandle* h = new (std::nothrow) GlHandle();
+    if (!h) return nullptr;
+    h->W = W;
+    h->H = H;
+    h->Wp = W + 2;
+    h->Hp = H + 2;
+    h->res = res;
+    h->ox = ox;
+    h->oy = oy;
+    h->cap_hyp = cap_hyp;
+    // Host-side preparation: padded 0/1/2 grid and the row-major free list.
+    std::vector<unsigned char> pad((size_t)h->Wp * h->Hp, 2);
+    std::vector<int2> freel;
+    h->host_grid.resize((size_t)W * H);
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            const unsigned char v = occ[(size_t)y * W + x] ? 1 : 0;
+            h->host_grid[(size_t)y * W + x] = v;
+            pad[(size_t)(y + 1) * h->Wp + (x + 1)] = v;
+            if (!v) freel.push_back(make_int2(x, y));
+        }
+    h->nfree = (int)freel.size();
+    const size_t gb = ((size_t)h->Wp * h->Hp + 15) / 16 * 16;
+    bool ok = false;
+    do {
+        if (cudaGetDevice(&h->dev) != cudaSuccess) break;
+        if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) !=
+            cudaSuccess)
+            break;
+        if (cudaMalloc((void**)&h->d_grid, gb) != cudaSuccess) break;
+        if (cudaMemset(h->d_grid, 2, gb) != cudaSuccess) break;
+        if (cudaMemcpy(h->d_grid, pad.data(), pad.size(),
+                       cudaMemcpyHostToDevice) != cudaSuccess)
+            break;
+        if (cudaMalloc((void**)&h->d_free,
+                       sizeof(int2) * std::max<size_t>(1, freel.size())) !=
+            cudaSuccess)
+            break;
+        if (!freel.empty() &&
+            cudaMemcpy(h->d_free, freel.data(), sizeof(int2) * freel.size(),
+                       cudaMemcpyHostToDevice) != cudaSuccess)
+            break;
+        const size_t c = (size_t)cap_hyp;
+        if (cudaMalloc((void**)&h->d_hyp, 3 * c * sizeof(float)) != cudaSuccess)
+            break;
+        if (cudaMalloc((void**)&h->d_caer, c * sizeof(float)) != cudaSuccess)
+            break;
+        if (cudaMalloc((void**)&h->d_keys, c * sizeof(uint64_t)) != cudaSuccess)
+            break;
+        if (cudaMalloc((void**)&h->d_keys_alt, c * sizeof(uint64_t)) !=
+            cudaSuccess)
+            break;
+        if (cudaMalloc((void**)&h->d_cand, c * sizeof(uint64_t)) != cudaSuccess)
+            break;
+        if (cudaMalloc((void**)&h->d_out, 3 * c * sizeof(float)) != cudaSuccess)
+            break;
+        if (cudaMalloc((void**)&h->d_outc, c * sizeof(float)) != cudaSuccess)
+            break;
+        if (cudaMalloc((void**)&h->d_outi, c * sizeof(int)) != cudaSuccess)
+            break;
+        if (cudaMalloc((void**)&h->d_ctl, sizeof(GlCtl)) != cudaSuccess) break;
+        if (cudaMemset(h->d_ctl, 0, sizeof(GlCtl)) != cudaSuccess) break;
+        if (cudaMallocHost((void**)&h->h_ctl, sizeof(GlCtl)) != cudaSuccess)
+            break;
+        ok = true;
+    } while (0);
+    if (!ok) {
+        set_error("pf_b200: pfgl_create failed: %s",
+                  cudaGetErrorString(cudaGetLastError()));
+        pfgl_destroy(h);
+        return nullptr;
+    }
+    return h;
+}
+
+int pfgl_destroy(void* hv) {
+    GlHandle* h = as_gl(hv);
+    if (!h) return 0;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    cudaFree(h->d_grid);
+    cudaFree(h->d_free);
+    cudaFree(h->d_hyp);
+    cudaFree(h->d_caer);
+    cudaFree(h->d_keys);
+    cudaFree(h->d_keys_alt);
+    cudaFree(h->d_hist);
+    cudaFree(h->d_scan);
+    cudaFree(h->d_out);
+    cudaFree(h->d_outc);
+    cudaFree(h->d_outi);
+    cudaFree(h->d_cand);
+    cudaFree(h->d_ctl);
+    cudaFreeHost(h->h_ctl);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return 0;
+}
+
+int pfgl_free_cells(void* hv) {
+    GlHandle* h = as_gl(hv);
+    return h ? h->nfree : -1;
+}
+
+int pfgl_generate(void* hv, int n, unsigned long long seed) {
+    return pfgl_generate_yaws(hv, n, 1, seed);
+}
+
+int pfgl_generate_yaws(void* hv, int n_pos, int n_yaw, unsigned long long seed) {
+    GlHandle* h = as_gl(hv);
+    if (!h || h->nfree <= 0 || n_pos <= 0 || n_yaw <= 0) return -1;
+    const long long n = (long long)n_pos * n_yaw;
+    if (n > h->cap_hyp) return -1;
+    h->nh = (int)n;
+    k_gl_gen<<<ceil_div(h->nh, kThreads), kThreads, 0, h->stream>>>(
+        h->nh, n_yaw, h->nfree, h->d_free, h->ox, h->oy, h->res, seed,
+        h->d_hyp);
+    PFB_KL();
+    h->caer_valid = false;
+    return 0;
+}
+
+int pfgl_set_hyps(void* hv, const float* hyp3n, int n) {
+    GlHandle* h = as_gl(hv);
+    if (!h || !hyp3n || n <= 0 || n > h->cap_hyp) return -1;
+    h->nh = n;
+    PFB_CK(cudaMemcpyAsync(h->d_hyp, hyp3n, 3 * sizeof(float) * (size_t)n,
+                           cudaMemcpyHostToDevice, h->stream));
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    h->caer_valid = false;
+    return 0;
+}
+
+int pfgl_get_hyps(void* hv, float* hyp3n) {
+    GlHandle* h = as_gl(hv);
+    if (!h || !hyp3n || h->nh <= 0) return -1;
+    PFB_CK(cudaMemcpyAsync(hyp3n, h->d_hyp, 3 * sizeof(float) * (size_t)h->nh,
+                           cudaMemcpyDeviceToHost, h->stream));
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int pfgl_score(void* hv, const float* scan, int nrays, float rmax,
+               float ang_span) {
+    GlHandle* h = as_gl(hv);
+    if (!h || h->nh <= 0 || !scan || nrays <= 0) return -1;
+    if (ensure_scan(h, scan, nrays)) return -1;
+    if (launch_score(h, nrays, rmax, ang_span)) return -1;
+    h->caer_valid = true;
+    return 0;
+}
+
+int pfgl_get_caer(void* hv, float* caer) {
+    GlHandle* h = as_gl(hv);
+    if (!h || !caer || h->nh <= 0 || !h->caer_valid) return -1;
+    PFB_CK(cudaMemcpyAsync(caer, h->d_caer, sizeof(float) * (size_t)h->nh,
+                           cudaMemcpyDeviceToHost, h->stream));
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int pfgl_topk_ex(void* hv, int k, float* out3k, float* caer_k, int* idx_k) {
+    GlHandle* h = as_gl(hv);
+    if (!h || k <= 0 || h->nh <= 0 || !h->caer_valid) return -1;
+    if (k > h->nh) k = h->nh;
+    const uint64_t* sorted = sort_current(h);
+    if (!sorted) return -1;
+    return copy_topk(h, sorted, k, out3k, caer_k, idx_k);
+}
+
+int pfgl_topk(void* hv, int k, float* out) {
+    if (!out) return -1;
+    return pfgl_topk_ex(hv, k, out, nullptr, nullptr);
+}
+
+int pfgl_topk_from_scores(void* hv, const float* caer, int n, int k,
+                          int* idx_out) {
+    GlHandle* h = as_gl(hv);
+    if (!h || !caer || !idx_out || n <= 0 || k <= 0 || n > h->cap_hyp)
+        return -1;
+    if (k > n) k = n;
+    PFB_CK(cudaMemcpyAsync(h->d_caer, caer, sizeof(float) * (size_t)n,
+                           cudaMemcpyHostToDevice, h->stream));
+    k_make_keys<<<ceil_div(n, kThreads), kThreads, 0, h->stream>>>(
+        h->d_caer, n, h->d_keys);
+    PFB_KL();
+    const uint64_t* sorted = radix_sort_keys(h, n, 0);
+    if (!sorted) return -1;
+    std::vector<uint64_t> keys((size_t)k);
+    PFB_CK(cudaMemcpyAsync(keys.data(), sorted, sizeof(uint64_t) * (size_t)k,
+                           cudaMemcpyDeviceToHost, h->stream));
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    for (int j = 0; j < k; ++j) idx_out[j] = (int)(uint32_t)keys[(size_t)j];
+    h->caer_valid = false;  // d_caer now holds caller scores
+    return k;
+}
+
+int pfgl_localize(void* hv, const float* scan, int nrays, float rmax,
+                  float ang_span, int k, float* out3k, float* caer_k,
+                  int* idx_k) {
+    GlHandle* h = as_gl(hv);
+    if (!h || h->nh <= 0 || !scan || nrays <= 0 || k <= 0) return -1;
+    if (k > h->nh) k = h->nh;
+    if (ensure_scan(h, scan, nrays)) return -1;
+    const int nh = h->nh;
+    // Seed batch scored exhaustively, then pruned chunks.
+    const int seed_n = std::min(nh, std::max(4 * k, 8192));
+    const int saved = h->nh;
+    h->nh = seed_n;
+    if (launch_score(h, nrays, rmax, ang_span)) return -1;
+    const uint64_t* seed_sorted = sort_current(h);
+    h->nh = saved;
+    if (!seed_sorted) return -1;
+    if (seed_n == nh) {
+        h->caer_valid = true;
+        return copy_topk(h, seed_sorted, k, out3k, caer_k, idx_k);
+    }
+    // Pruning bound = k-th best key of the seed batch; candidates start with
+    // the seed batch's best k.
+    k_set_tau<<<1, 1, 0, h->stream>>>(seed_sorted, k, h->d_ctl);
+    PFB_KL();
+    PFB_CK(cudaMemcpyAsync(h->d_cand, seed_sorted, sizeof(uint64_t) * (size_t)k,
+                           cudaMemcpyDeviceToDevice, h->stream));
+    unsigned kk = (unsigned)k;
+    PFB_CK(cudaMemcpyAsync(&h->d_ctl->n_cand, &kk, sizeof(unsigned),
+                           cudaMemcpyHostToDevice, h->stream));
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    if (launch_score_pruned(h, seed_n, nh, nrays, rmax, ang_span)) return -1;
+    PFB_CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(GlCtl),
+                           cudaMemcpyDeviceToHost, h->stream));
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    int nc = (int)h->h_ctl->n_cand;
+    if (nc > h->cap_hyp) {
+        set_error("pf_b200: pfgl_localize candidate overflow");
+        return -1;
+    }
+    // Sort the survivors (their keys already carry the index).
+    PFB_CK(cudaMemcpyAsync(h->d_keys, h->d_cand, sizeof(uint64_t) * (size_t)nc,
+                           cudaMemcpyDeviceToDevice, h->stream));
+    const uint64_t* sorted = radix_sort_keys(h, nc, index_bit_width(nh));
+    if (!sorted) return -1;
+    h->caer_valid = false;  // pruned CAERs are not computed
+    return copy_topk(h, sorted, std::min(k, nc), out3k, caer_k, idx_k);
+}
+
+int pfgl_cell(void* hv, int cx, int cy) {
+    GlHandle* h = as_gl(hv);
+    if (!h || cx < 0 || cy < 0 || cx >= h->W || cy >= h->H) return -1;
+    return h->host_grid[(size_t)cy * h->W + cx];
+}
+
+}  // extern "C"

@@ -1,0 +1,99 @@
+// markley.h — Markley quaternion mean: the dominant eigenvector of the
+// symmetrised 4x4 moment matrix M = sum_i w_i q_i q_i^T (Markley, Cheng,
+// Crassidis, Oshman, "Averaging quaternions", JGCD 2007), in FP64, for host
+// and device.
+//
+// Semantics follow crates/pf_core/src/types.rs:128-143: symmetrise
+// (M^T + M)/2, take the eigenvector of the largest eigenvalue (first index on
+// ties), normalise, flip to w >= 0.  The eigen-solve is the cyclic Jacobi
+// method (Golub & Van Loan, "Matrix Computations", section 8.5) rather than
+// nalgebra's tridiagonal QR: both return the same unit eigenvector up to
+// sign for a simple top eigenvalue, and the sign is canonicalised.
+#pragma once
+
+#ifdef __CUDACC__
+#define PFB_HD __host__ __device__
+#else
+#define PFB_HD
+#endif
+
+#include <math.h>
+
+namespace pfb {
+
+// Eigen-decomposition of a symmetric 4x4 matrix a (row-major, destroyed).
+// On return a holds the eigenvalues on its diagonal and v the eigenvectors
+// as columns.  Returns the number of sweeps used.
+PFB_HD inline int jacobi_eig4(double a[16], double v[16]) {
+    for (int i = 0; i < 16; ++i) v[i] = (i % 5 == 0) ? 1.0 : 0.0;
+    int sweep = 0;
+    for (; sweep < 64; ++sweep) {
+        double off = 0.0, diag = 0.0;
+        for (int p = 0; p < 4; ++p) {
+            diag += a[p * 4 + p] * a[p * 4 + p];
+            for (int q = p + 1; q < 4; ++q) off += a[p * 4 + q] * a[p * 4 + q];
+        }
+        if (!(off > 1e-32 * diag) || off == 0.0) break;
+        for (int p = 0; p < 3; ++p) {
+            for (int q = p + 1; q < 4; ++q) {
+                const double apq = a[p * 4 + q];
+                if (apq == 0.0) continue;
+                const double app = a[p * 4 + p], aqq = a[q * 4 + q];
+                // Rutishauser's stable rotation: t = tan(phi) of the smaller
+                // root of t^2 + 2 theta t - 1 = 0.
+                const double theta = (aqq - app) / (2.0 * apq);
+                const double t =
+                    (theta >= 0.0 ? 1.0 : -1.0) /
+                    (fabs(theta) + sqrt(theta * theta + 1.0));
+                const double c = 1.0 / sqrt(t * t + 1.0);
+                const double s = t * c;
+                for (int k = 0; k < 4; ++k) {
+                    const double akp = a[k * 4 + p], akq = a[k * 4 + q];
+                    a[k * 4 + p] = c * akp - s * akq;
+                    a[k * 4 + q] = s * akp + c * akq;
+                }
+                for (int k = 0; k < 4; ++k) {
+                    const double apk = a[p * 4 + k], aqk = a[q * 4 + k];
+                    a[p * 4 + k] = c * apk - s * aqk;
+                    a[q * 4 + k] = s * apk + c * aqk;
+                }
+                for (int k = 0; k < 4; ++k) {
+                    const double vkp = v[k * 4 + p], vkq = v[k * 4 + q];
+                    v[k * 4 + p] = c * vkp - s * vkq;
+                    v[k * 4 + q] = s * vkp + c * vkq;
+                }
+            }
+        }
+    }
+    return sweep;
+}
+
+// Mean quaternion (w,x,y,z) from the 10 packed upper-triangle moments
+// M00,M01,M02,M03,M11,M12,M13,M22,M23,M33 (the layout of pfc_est_sums
+// out[3..12], unpacked by crates/pf_core/src/cuda.rs:277-285).
+PFB_HD inline void markley_mean(const double m10[10], double q_out[4]) {
+    double a[16], v[16];
+    int e = 0;
+    for (int r = 0; r < 4; ++r)
+        for (int c = r; c < 4; ++c) {
+            a[r * 4 + c] = m10[e];
+            a[c * 4 + r] = m10[e];
+            ++e;
+        }
+    jacobi_eig4(a, v);
+    int idx = 0;
+    for (int i = 1; i < 4; ++i)
+        if (a[i * 4 + i] > a[idx * 4 + idx]) idx = i;
+    double q[4] = {v[0 * 4 + idx], v[1 * 4 + idx], v[2 * 4 + idx],
+                   v[3 * 4 + idx]};
+    double nrm = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    if (!(nrm > 0.0)) {
+        q_out[0] = 1.0;
+        q_out[1] = q_out[2] = q_out[3] = 0.0;
+        return;
+    }
+    double sgn = (q[0] < 0.0) ? -1.0 : 1.0;
+    for (int i = 0; i < 4; ++i) q_out[i] = sgn * q[i] / nrm;
+}
+
+}  // namespace pfb

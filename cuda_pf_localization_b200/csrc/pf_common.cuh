@@ -1,0 +1,215 @@
+// pf_common.cuh — device helpers shared by the particle-filter and
+// global-localization kernels: counter-based Philox noise, Hamilton quaternion
+// algebra in f32, order-preserving float keys, launch/error plumbing.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "../../include/pfc_abi.h"
+
+namespace pfb {
+
+// ---------------------------------------------------------------- errors
+// Thread-local last-error text, mirrored to stderr like the reference's
+// CK/KL macros (src/cuda/pf_kernels.cu:37-67).
+void set_error(const char* fmt, ...);
+void clear_error();
+
+#define PFB_CK(x)                                                           \
+    do {                                                                    \
+        cudaError_t e_ = (x);                                               \
+        if (e_ != cudaSuccess) {                                            \
+            ::pfb::set_error("pf_b200 %s:%d %s: %s", __FILE__, __LINE__, #x, \
+                             cudaGetErrorString(e_));                       \
+            return -1;                                                      \
+        }                                                                   \
+    } while (0)
+
+#define PFB_CK_NULL(x)                                                      \
+    do {                                                                    \
+        cudaError_t e_ = (x);                                               \
+        if (e_ != cudaSuccess) {                                            \
+            ::pfb::set_error("pf_b200 %s:%d %s: %s", __FILE__, __LINE__, #x, \
+                             cudaGetErrorString(e_));                       \
+            return nullptr;                                                 \
+        }                                                                   \
+    } while (0)
+
+#define PFB_KL()                                                            \
+    do {                                                                    \
+        cudaError_t e_ = cudaGetLastError();                                \
+        if (e_ != cudaSuccess) {                                            \
+            ::pfb::set_error("pf_b200 %s:%d launch failed: %s", __FILE__,   \
+                             __LINE__, cudaGetErrorString(e_));             \
+            return -1;                                                      \
+        }                                                                   \
+    } while (0)
+
+// Device-side error word bits (written by kernels, read by the host after a
+// sync).  A bounded spin that runs out sets SPIN_TIMEOUT instead of hanging.
+enum : unsigned {
+    ERR_SPIN_TIMEOUT = 1u,
+    ERR_SCAN_OVERFLOW = 2u,
+};
+
+constexpr int kSpinLimit = 1 << 22;  // polls before a look-back gives up
+
+// ---------------------------------------------------------------- Philox
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy
+// as 1, 2, 3", SC'11): 10 rounds of two 32x32->64 multiplies with the published
+// multipliers and Weyl key increments.  Stateless: noise for particle i in
+// generation g is a pure function of (seed, i, g, block).
+struct U4 {
+    uint32_t x, y, z, w;
+};
+
+__host__ __device__ __forceinline__ void philox_mulhilo(uint32_t a, uint32_t b,
+                                                        uint32_t& hi,
+                                                        uint32_t& lo) {
+#ifdef __CUDA_ARCH__
+    hi = __umulhi(a, b);
+    lo = a * b;
+#else
+    uint64_t p = (uint64_t)a * (uint64_t)b;
+    hi = (uint32_t)(p >> 32);
+    lo = (uint32_t)p;
+#endif
+}
+
+__host__ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0,
+                                                     uint32_t k1) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+    const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        if (r > 0) {
+            k0 += W0;
+            k1 += W1;
+        }
+        uint32_t hi0, lo0, hi1, lo1;
+        philox_mulhilo(M0, c.x, hi0, lo0);
+        philox_mulhilo(M1, c.z, hi1, lo1);
+        U4 n;
+        n.x = hi1 ^ c.y ^ k0;
+        n.y = lo1;
+        n.z = hi0 ^ c.w ^ k1;
+        n.w = lo0;
+        c = n;
+    }
+    return c;
+}
+
+// Uniform in the open interval (0,1): 23 random bits + 1/2, exact in f32.
+__host__ __device__ __forceinline__ float u01_open(uint32_t x) {
+    return ((float)(x >> 9) + 0.5f) * (1.0f / 8388608.0f);
+}
+
+// Box–Muller pair (Box & Muller 1958) from two open uniforms.
+__device__ __forceinline__ float2 box_muller(float u1, float u2) {
+    float r = sqrtf(-2.0f * logf(u1));
+    float s, c;
+    sincospif(2.0f * u2, &s, &c);
+    return make_float2(r * c, r * s);
+}
+
+// Counter block ids: one Philox call per block, four uniforms each.
+enum : uint32_t {
+    RNG_PF_A = 0u,   // normals 0..3 of a particle update
+    RNG_PF_B = 1u,   // normals 4..5
+    RNG_GL = 2u,     // hypothesis dispersion
+};
+
+// Six standard normals for particle i in generation gen: translation noise
+// (n0,n1,n2) and rotation noise (n3,n4,n5).
+__device__ __forceinline__ void pf_normals6(uint64_t seed, uint64_t gen,
+                                            uint32_t i, float n[6]) {
+    const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    U4 a = philox4x32_10({i, (uint32_t)gen, (uint32_t)(gen >> 32), RNG_PF_A},
+                         k0, k1);
+    U4 b = philox4x32_10({i, (uint32_t)gen, (uint32_t)(gen >> 32), RNG_PF_B},
+                         k0, k1);
+    float2 g0 = box_muller(u01_open(a.x), u01_open(a.y));
+    float2 g1 = box_muller(u01_open(a.z), u01_open(a.w));
+    float2 g2 = box_muller(u01_open(b.x), u01_open(b.y));
+    n[0] = g0.x;
+    n[1] = g0.y;
+    n[2] = g1.x;
+    n[3] = g1.y;
+    n[4] = g2.x;
+    n[5] = g2.y;
+}
+
+// ------------------------------------------------------- quaternion algebra
+// Hamilton product and the rotation v' = v + 2w(u x v) + 2u x (u x v),
+// written with the same operation order as the reference device helpers
+// (src/cuda/pf_kernels.cu:119-149) so the f32 results match bit for bit
+// under the same compiler contraction rules.
+struct Quat {
+    float w, x, y, z;
+};
+
+__device__ __forceinline__ float3 q_rotate(const Quat& q, float3 v) {
+    float3 t = make_float3(2.f * (q.y * v.z - q.z * v.y),
+                           2.f * (q.z * v.x - q.x * v.z),
+                           2.f * (q.x * v.y - q.y * v.x));
+    float3 c = make_float3(q.y * t.z - q.z * t.y, q.z * t.x - q.x * t.z,
+                           q.x * t.y - q.y * t.x);
+    return make_float3(v.x + q.w * t.x + c.x, v.y + q.w * t.y + c.y,
+                       v.z + q.w * t.z + c.z);
+}
+
+__device__ __forceinline__ Quat q_conjugate(const Quat& q) {
+    return {q.w, -q.x, -q.y, -q.z};
+}
+
+__device__ __forceinline__ Quat q_product(const Quat& a, const Quat& b) {
+    return {a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z,
+            a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y,
+            a.w * b.y - a.x * b.z + a.y * b.w + a.z * b.x,
+            a.w * b.z + a.x * b.y - a.y * b.x + a.z * b.w};
+}
+
+// exp map of a rotation vector with the reference's guards (angle and axis
+// norm must exceed 1e-12, else identity).
+__device__ __forceinline__ Quat q_from_axis_angle(float3 axis, float angle) {
+    float nrm = sqrtf(axis.x * axis.x + axis.y * axis.y + axis.z * axis.z);
+    if (!(angle > 1e-12f) || !(nrm > 1e-12f)) return {1.f, 0.f, 0.f, 0.f};
+    float s = sinf(0.5f * angle) / nrm;
+    return {cosf(0.5f * angle), axis.x * s, axis.y * s, axis.z * s};
+}
+
+// ------------------------------------------------------------ float keys
+// Signed-int image of a float whose integer order equals the float order
+// (the reference's float_as_ordered, pf_kernels.cu:151-155).
+__host__ __device__ __forceinline__ int ordered_key(float f) {
+#ifdef __CUDA_ARCH__
+    int i = __float_as_int(f);
+#else
+    int i;
+    memcpy(&i, &f, 4);
+#endif
+    return (i >= 0) ? i : (i ^ 0x7FFFFFFF);
+}
+
+// 64-bit composite key: unsigned image of ordered_key in the high word,
+// hypothesis index in the low word.  Sorting these ascending equals a stable
+// sort by CAER (ties broken by lower index).
+__host__ __device__ __forceinline__ uint64_t composite_key(float caer,
+                                                           uint32_t idx) {
+    uint32_t u = (uint32_t)ordered_key(caer) ^ 0x80000000u;
+    return ((uint64_t)u << 32) | (uint64_t)idx;
+}
+
+// ------------------------------------------------------------------ sizes
+__host__ __device__ __forceinline__ int ceil_div(int a, int b) {
+    return (a + b - 1) / b;
+}
+__host__ __device__ __forceinline__ long long ceil_div_ll(long long a,
+                                                          long long b) {
+    return (a + b - 1) / b;
+}
+
+}  // namespace pfb

@@ -1,0 +1,224 @@
+// pf_internal.h — particle-filter handle, device layouts and the launchers
+// shared between the kernel translation units and the C-ABI layer.
+//
+// HBM layout (SoA, one plane per component, each plane padded to a multiple
+// of 1024 particles so float4 loads stay aligned):
+//   state[2]  ping-pong particle sets: px py pz qw qx qy qz   (7 planes)
+//   ll        f32 log-likelihood of the last weighting          (1 plane)
+//   w         f32 normalised weight (materialised on demand)    (1 plane)
+//   cum       u64 fixed-point inclusive weight scan (resample)  (n words)
+//   anc       i32 ancestor of each particle in the last resample
+//   inj_head  u64 epoch-tagged injection list heads (one per particle)
+// plus small per-block partial buffers and one CycleCtl control block.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "pf_common.cuh"
+
+namespace pfb {
+
+constexpr int kEstN = 14;  // pfc_est_sums layout
+constexpr int kCovN = 12;  // pfc_covs layout
+
+// Weight plane semantics.
+enum WeightMode : int {
+    WMODE_UNIFORM = 0,  // w_i = 1.0f / n (not stored)
+    WMODE_LL = 1,       // w_i = (float)(exp(ll_i - M) / S), not yet stored
+    WMODE_STORED = 2,   // w plane holds the weights
+};
+
+struct Planes {
+    float* px;
+    float* py;
+    float* pz;
+    float* qw;
+    float* qx;
+    float* qy;
+    float* qz;
+};
+
+// Device control block: reduction results and cross-kernel flags.  One copy
+// lives in device memory, one mirror in pinned host memory.
+struct CycleCtl {
+    // softmax
+    double ll_max;        // M = max ll
+    double ll_sumexp;     // S = sum exp(ll - M)
+    int weights_valid;    // 1 when S is finite and > 0
+    int wmode;            // WeightMode of the current cloud
+    // estimate pass 1
+    double est[kEstN];
+    double qmean[4];      // device Markley mean (FP64)
+    float cov_mean_p[3];  // f32 arguments the covariance pass used
+    float cov_mean_q[4];
+    double covs[kCovN];
+    double ess;           // 1 / sum w^2 of the estimate above
+    // fused-cycle decision and outputs
+    int resample_now;     // 1 when this cycle resamples
+    int resampled;        // set when a resample ran in the current cycle
+    double ess_pre;       // ESS before the resample
+    double out[PFC_EST_LEN];
+    // resample
+    unsigned long long lcg;  // resample offset stream (host LCG in reference)
+    double u01_override;     // >= 0: use this offset fraction instead of LCG
+    uint64_t total_fx;       // fixed-point weight total T
+    double total;            // T * 2^-62
+    double u0, step;         // systematic offsets
+    int resample_valid;      // total finite and > 0
+    // diagnostics
+    unsigned err;            // ERR_* bits
+    unsigned tile_counter;   // dynamic tile ids for the look-back scan
+    int live;                // which ping-pong particle set is current
+};
+
+// Kernel kinds for launch accounting and CUDA-event timing.
+enum KernelKind : int {
+    KK_REINIT = 0,
+    KK_PREDICT,
+    KK_WEIGHT,
+    KK_EST,
+    KK_COVS,
+    KK_SCAN,
+    KK_GATHER,
+    KK_INJECT,
+    KK_COMMIT,
+    KK_MISC,
+    KK_COUNT
+};
+
+struct PfProfiler {
+    bool on = false;
+    static constexpr int kPool = 2048;
+    cudaEvent_t ev[kPool][2] = {};
+    int kind[kPool] = {};
+    int used = 0;
+    double ms[KK_COUNT] = {};
+    long long count[KK_COUNT] = {};
+};
+
+struct PfHandle {
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    int n = 0;
+    int n_pad = 0;
+    int cap_obs = 64;
+    uint64_t seed = 42;
+    uint64_t gen = 0;
+    int cur = 0;  // which ping-pong state is live
+
+    float* d_state[2] = {nullptr, nullptr};  // 7 planes each
+    float* d_ll = nullptr;
+    float* d_w = nullptr;
+    uint64_t* d_cum = nullptr;
+    int* d_anc = nullptr;
+    uint64_t* d_inj_head = nullptr;
+    int* d_inj_next = nullptr;
+    unsigned* d_scan_flags = nullptr;   // look-back tile status words
+    uint64_t* d_scan_vals = nullptr;    // look-back tile values (agg, incl)
+    double* d_part = nullptr;           // per-block partials (max over uses)
+    int part_cap = 0;                   // doubles in d_part
+    unsigned* d_done = nullptr;         // last-block counters
+    CycleCtl* d_ctl = nullptr;
+    CycleCtl* h_ctl = nullptr;          // pinned mirror
+
+    // landmarks: device table + host shadow
+    float* d_lm = nullptr;
+    int lm_count = 0;
+    int lm_cap = 0;
+
+    // observations: device buffer + pinned staging ring
+    CObservation* d_obs = nullptr;
+    int d_obs_cap = 0;
+    static constexpr int kRing = 4;
+    CObservation* h_obs_ring = nullptr;  // kRing * cap_obs records
+    cudaEvent_t ring_ev[kRing] = {};
+    int ring_pos = 0;
+
+    // pending (deferred) predict, fused into the next weighting
+    bool pending_predict = false;
+    uint64_t pending_gen = 0;
+    PfcOdom pending_odom{};
+
+    // speculative estimate bookkeeping
+    bool est_valid = false;    // h_ctl est/covs describe the current cloud
+    bool est_inflight = false; // est + covs launched, not yet synced
+    cudaEvent_t est_ev = nullptr;
+
+    int weight_variant = 0;
+    bool record_anc = false;
+    bool anc_valid = false;
+    unsigned scan_epoch = 0;   // look-back flag epoch (never 0 when used)
+    unsigned inj_epoch = 0;    // injection list epoch (never 0 when used)
+    float* d_stage = nullptr;  // AoS staging for snapshot / set_state (7n)
+
+    // accounting: kernels launched, bytes copied host<->device, host syncs
+    PfcStats stats{};
+    PfProfiler prof;
+
+    Planes planes(int which) const {
+        float* b = d_state[which];
+        size_t p = (size_t)n_pad;
+        return {b, b + p, b + 2 * p, b + 3 * p, b + 4 * p, b + 5 * p,
+                b + 6 * p};
+    }
+    Planes live() const { return planes(cur); }
+};
+
+// ------------------------------------------------------- accounting helpers
+// Bracket one kernel launch: counts it and, when profiling is on, records a
+// pair of CUDA events around it on the handle's stream.
+void prof_begin(PfHandle* h, int kind);
+void prof_drain_public(PfHandle* h);
+void prof_end(PfHandle* h, int kind);
+
+struct KernelScope {
+    PfHandle* h;
+    int kind;
+    KernelScope(PfHandle* hh, int k) : h(hh), kind(k) { prof_begin(h, kind); }
+    ~KernelScope() { prof_end(h, kind); }
+};
+
+// ---------------------------------------------------------------- launchers
+// Each returns 0 or -1 (with the error recorded).  All are asynchronous on
+// h->stream.
+
+struct PredictArgs {
+    int enabled;
+    uint64_t gen;
+    float t[3], q[4], tstd[3], rstd[3];
+};
+
+struct WeightArgs {
+    float sigma_r, sigma_b, gate;
+    int nobs;
+};
+
+int launch_reinit(PfHandle* h, const float p0[3], const float q0[4],
+                  const float pstd[3], const float rstd[3]);
+int launch_predict(PfHandle* h, const PredictArgs& pa);
+// Weighting (optionally fused with a deferred predict): writes ll, block
+// (max, sumexp) partials and the finalised M, S into the control block.
+int launch_weight(PfHandle* h, const PredictArgs& pa, const CObservation* d_obs,
+                  int nobs, float sigma_r, float sigma_b, float gate);
+// Estimate pass 1 (+ device Markley mean) and the speculative covariance pass
+// around (float)mean, (float)qmean.  When use_args is set the covariance pass
+// uses the given f32 means instead.
+int launch_est_sums(PfHandle* h, bool cycle_second);
+int launch_covs(PfHandle* h, bool use_args, const float mp[3],
+                const float mq[4], bool cycle_second);
+// Systematic resampling: fixed-point look-back scan, merge-path gather,
+// deterministic injection.  cond_on_ctl: skip unless ctl->resample_now.
+int launch_resample(PfHandle* h, float inject_ratio, bool cond_on_ctl,
+                    bool use_u01, double u01);
+// Decide whether to resample (device ESS vs ratio * n) for the fused cycle.
+int launch_cycle_decide(PfHandle* h, double ess_ratio);
+// Assemble the fused-cycle output record.
+int launch_cycle_output(PfHandle* h);
+int launch_materialize_weights(PfHandle* h);
+int launch_pick_from_cum(PfHandle* h, const double* d_cum, int n, double u0,
+                         double total, int* d_anc);
+
+}  // namespace pfb

@@ -1,0 +1,339 @@
+// pf_update.cu — prior (reinit), motion update (predict) and landmark
+// weighting kernels on the SoA particle planes.
+//
+// The weighting kernel optionally runs a deferred predict first, so one pass
+// over HBM reads the old pose, writes the new pose and the log-likelihood,
+// and leaves per-block softmax partials (block max, sum exp(ll - block max)
+// in FP64).  The last block to finish combines the partials in block order,
+// so M = max ll and S = sum exp(ll - M) are deterministic.
+#include <math.h>
+
+#include "pf_internal.h"
+
+namespace pfb {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kObsChunk = 256;  // observations staged in shared memory at once
+
+struct PlaneSet {
+    Planes s[2];
+};
+
+PlaneSet plane_set(const PfHandle* h) { return {h->planes(0), h->planes(1)}; }
+
+__device__ __forceinline__ void load_pose(const Planes& s, int i, float3& p,
+                                          Quat& q) {
+    p = make_float3(s.px[i], s.py[i], s.pz[i]);
+    q = {s.qw[i], s.qx[i], s.qy[i], s.qz[i]};
+}
+
+__device__ __forceinline__ void store_pose(const Planes& s, int i, float3 p,
+                                           Quat q) {
+    s.px[i] = p.x;
+    s.py[i] = p.y;
+    s.pz[i] = p.z;
+    s.qw[i] = q.w;
+    s.qx[i] = q.x;
+    s.qy[i] = q.y;
+    s.qz[i] = q.z;
+}
+
+// Motion model of the reference predict (src/cuda/pf_kernels.cu:198-222,
+// semantics crates/pf_core/src/cpu.rs:197-218): body displacement t + sigma_t*n
+// rotated into the world by q, then q <- (q * q_odo) * exp(sigma_r*w).  The
+// quaternion is not renormalised, as in the reference.
+__device__ __forceinline__ void apply_predict(const PredictArgs& pa,
+                                              uint64_t seed, int i, float3& p,
+                                              Quat& q) {
+    float nz[6];
+    pf_normals6(seed, pa.gen, (uint32_t)i, nz);
+    float3 body = make_float3(pa.t[0] + pa.tstd[0] * nz[0],
+                              pa.t[1] + pa.tstd[1] * nz[1],
+                              pa.t[2] + pa.tstd[2] * nz[2]);
+    float3 world = q_rotate(q, body);
+    p.x += world.x;
+    p.y += world.y;
+    p.z += world.z;
+    float3 axis = make_float3(pa.rstd[0] * nz[3], pa.rstd[1] * nz[4],
+                              pa.rstd[2] * nz[5]);
+    float ang = sqrtf(axis.x * axis.x + axis.y * axis.y + axis.z * axis.z);
+    Quat dq = q_from_axis_angle(axis, ang);
+    Quat qo = {pa.q[0], pa.q[1], pa.q[2], pa.q[3]};
+    q = q_product(q_product(q, qo), dq);
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_reinit(PlaneSet ps, int n, uint64_t seed, uint64_t gen, float3 p0,
+             Quat q0, float3 pstd, float3 rstd, CycleCtl* ctl) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= n) return;
+    const Planes s = ps.s[ctl->live];
+    float nz[6];
+    pf_normals6(seed, gen, (uint32_t)i, nz);
+    float3 p = make_float3(p0.x + pstd.x * nz[0], p0.y + pstd.y * nz[1],
+                           p0.z + pstd.z * nz[2]);
+    float3 axis = make_float3(rstd.x * nz[3], rstd.y * nz[4], rstd.z * nz[5]);
+    float ang = sqrtf(axis.x * axis.x + axis.y * axis.y + axis.z * axis.z);
+    Quat dq = q_from_axis_angle(axis, ang);
+    store_pose(s, i, p, q_product(q0, dq));
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_predict(PlaneSet ps, int n, uint64_t seed, PredictArgs pa,
+              CycleCtl* ctl) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= n) return;
+    const Planes s = ps.s[ctl->live];
+    float3 p;
+    Quat q;
+    load_pose(s, i, p, q);
+    apply_predict(pa, seed, i, p, q);
+    store_pose(s, i, p, q);
+}
+
+// Observation staged in shared memory: landmark resolved through the dense
+// table, kind 0 = skipped (id outside the table), 1 = Cartesian, 2 = range +
+// bearing.  a = (lx, ly, lz, kind bits), b = (dx, dy, dz, range).
+__device__ __forceinline__ void stage_obs(const CObservation* __restrict__ obs,
+                                          const float* __restrict__ lm,
+                                          int lm_count, int k, float4* sa,
+                                          float4* sb) {
+    CObservation o = obs[k];
+    float4 a, b;
+    if (o.id < 0 || o.id >= lm_count) {
+        a = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
+    } else {
+        a = make_float4(lm[3 * o.id], lm[3 * o.id + 1], lm[3 * o.id + 2],
+                        __int_as_float(o.mode == 0 ? 1 : 2));
+    }
+    b = make_float4(o.dx, o.dy, o.dz, o.range);
+    *sa = a;
+    *sb = b;
+}
+
+struct GateConsts {
+    float inv2rr, inv2bb, g2, cart_gate2, rng_gate2, brg_gate2, cart_out,
+        half_out, gate;
+};
+
+// Same f32 expressions as the reference kernel prologue
+// (src/cuda/pf_kernels.cu:229-234) so the gate thresholds are identical.
+__device__ __forceinline__ GateConsts gate_consts(float sigma_r, float sigma_b,
+                                                  float gate) {
+    GateConsts g;
+    g.inv2rr = 1.0f / (2.0f * sigma_r * sigma_r);
+    g.inv2bb = 1.0f / (2.0f * sigma_b * sigma_b);
+    g.g2 = gate * gate;
+    g.cart_gate2 = g.g2 * 3.0f * sigma_r * sigma_r;
+    g.rng_gate2 = g.g2 * sigma_r * sigma_r;
+    g.brg_gate2 = g.g2 * sigma_b * sigma_b;
+    g.cart_out = -0.5f * g.g2 * 3.0f;
+    g.half_out = -0.5f * g.g2;
+    g.gate = gate;
+    return g;
+}
+
+// One particle against one observation, accumulated into acc in the
+// reference's expression order (src/cuda/pf_kernels.cu:240-269; model
+// crates/pf_core/src/cpu.rs:44-97): a range-bearing observation adds its range
+// and bearing terms to acc one after the other.
+__device__ __forceinline__ void obs_loglik(const GateConsts& g, float3 p,
+                                           const Quat& qc, float4 a, float4 b,
+                                           int kind, float& acc) {
+    float3 d = make_float3(a.x - p.x, a.y - p.y, a.z - p.z);
+    float3 pred = q_rotate(qc, d);  // landmark in the body frame
+    if (kind == 1) {
+        float ex = pred.x - b.x, ey = pred.y - b.y, ez = pred.z - b.z;
+        float r2 = ex * ex + ey * ey + ez * ez;
+        acc += (g.gate > 0.0f && r2 > g.cart_gate2) ? g.cart_out
+                                                    : -r2 * g.inv2rr;
+        return;
+    }
+    float rn = fmaxf(
+        sqrtf(pred.x * pred.x + pred.y * pred.y + pred.z * pred.z), 1e-9f);
+    float er = rn - b.w;
+    float dot = -((pred.x * b.x + pred.y * b.y + pred.z * b.z) / rn);
+    dot = fminf(fmaxf(dot, -1.0f), 1.0f);
+    float eb = acosf(dot);
+    acc += (g.gate > 0.0f && er * er > g.rng_gate2) ? g.half_out
+                                                    : -er * er * g.inv2rr;
+    acc += (g.gate > 0.0f && eb * eb > g.brg_gate2) ? g.half_out
+                                                    : -eb * eb * g.inv2bb;
+}
+
+// Fixed-order block reductions (xor-butterfly inside warps, warps in index
+// order) — results do not depend on scheduling.
+__device__ __forceinline__ float warp_max_f(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(~0u, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(~0u, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(~0u, v, o));
+    return v;
+}
+
+// Softmax partial of one block + the last-block combine.
+__device__ __forceinline__ void softmax_partials(float acc, bool valid,
+                                                 double2* part,
+                                                 unsigned* done,
+                                                 CycleCtl* ctl) {
+    __shared__ float s_m[kThreads / 32];
+    __shared__ double s_s[kThreads / 32];
+    __shared__ double s_bm;
+    __shared__ bool s_last;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    float m = warp_max_f(valid ? acc : -INFINITY);
+    if (lane == 0) s_m[warp] = m;
+    __syncthreads();
+    if (tid == 0) {
+        float bm = s_m[0];
+        for (int k = 1; k < kThreads / 32; ++k) bm = fmaxf(bm, s_m[k]);
+        s_bm = (double)bm;
+    }
+    __syncthreads();
+    const double bm = s_bm;
+    double e = valid ? exp((double)acc - bm) : 0.0;
+    e = warp_sum_d(e);
+    if (lane == 0) s_s[warp] = e;
+    __syncthreads();
+    if (tid == 0) {
+        double sb = 0.0;
+        for (int k = 0; k < kThreads / 32; ++k) sb += s_s[k];
+        part[blockIdx.x] = make_double2(bm, sb);
+        __threadfence();
+        s_last = (atomicAdd(done, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    // Combine: M = max block max, S = sum_b exp(m_b - M) * s_b.
+    const int G = gridDim.x;
+    double mx = -INFINITY;
+    for (int b = tid; b < G; b += kThreads) mx = fmax(mx, __ldcg(&part[b].x));
+    mx = warp_max_d(mx);
+    __shared__ double s_d[kThreads / 32];
+    if (lane == 0) s_d[warp] = mx;
+    __syncthreads();
+    if (tid == 0) {
+        double v = s_d[0];
+        for (int k = 1; k < kThreads / 32; ++k) v = fmax(v, s_d[k]);
+        s_bm = v;
+    }
+    __syncthreads();
+    const double M = s_bm;
+    double sum = 0.0;
+    for (int b = tid; b < G; b += kThreads) {
+        double2 pb = __ldcg(&part[b]);
+        sum += exp(pb.x - M) * pb.y;
+    }
+    sum = warp_sum_d(sum);
+    __syncthreads();
+    if (lane == 0) s_d[warp] = sum;
+    __syncthreads();
+    if (tid == 0) {
+        double S = 0.0;
+        for (int k = 0; k < kThreads / 32; ++k) S += s_d[k];
+        ctl->ll_max = M;
+        ctl->ll_sumexp = S;
+        const int ok = (S > 0.0 && isfinite(S)) ? 1 : 0;
+        ctl->weights_valid = ok;
+        ctl->wmode = ok ? WMODE_LL : WMODE_UNIFORM;
+        *done = 0u;
+    }
+}
+
+template <bool kPredict>
+__global__ void __launch_bounds__(kThreads)
+    k_weight(PlaneSet ps, int n, uint64_t seed, PredictArgs pa,
+             const CObservation* __restrict__ obs, int nobs,
+             const float* __restrict__ lm, int lm_count, float sigma_r,
+             float sigma_b, float gate, float* __restrict__ ll,
+             double2* part, unsigned* done, CycleCtl* ctl) {
+    __shared__ float4 s_a[kObsChunk];
+    __shared__ float4 s_b[kObsChunk];
+    const Planes s = ps.s[ctl->live];
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    const bool valid = i < n;
+    float3 p = make_float3(0.f, 0.f, 0.f);
+    Quat q = {1.f, 0.f, 0.f, 0.f};
+    if (valid) {
+        load_pose(s, i, p, q);
+        if (kPredict) {
+            apply_predict(pa, seed, i, p, q);
+            store_pose(s, i, p, q);
+        }
+    }
+    const GateConsts g = gate_consts(sigma_r, sigma_b, gate);
+    const Quat qc = q_conjugate(q);
+    float acc = 0.0f;
+    for (int c0 = 0; c0 < nobs; c0 += kObsChunk) {
+        const int cn = min(kObsChunk, nobs - c0);
+        __syncthreads();
+        for (int k = threadIdx.x; k < cn; k += kThreads)
+            stage_obs(obs, lm, lm_count, c0 + k, &s_a[k], &s_b[k]);
+        __syncthreads();
+        if (valid) {
+            for (int k = 0; k < cn; ++k) {
+                const float4 a = s_a[k];
+                const int kind = __float_as_int(a.w);
+                if (kind == 0) continue;
+                obs_loglik(g, p, qc, a, s_b[k], kind, acc);
+            }
+        }
+    }
+    if (valid) ll[i] = acc;
+    softmax_partials(acc, valid, part, done, ctl);
+}
+
+}  // namespace
+
+int launch_reinit(PfHandle* h, const float p0[3], const float q0[4],
+                  const float pstd[3], const float rstd[3]) {
+    const int grid = ceil_div(h->n, kThreads);
+    KernelScope ks(h, KK_REINIT);
+    k_reinit<<<grid, kThreads, 0, h->stream>>>(
+        plane_set(h), h->n, h->seed, h->gen, make_float3(p0[0], p0[1], p0[2]),
+        Quat{q0[0], q0[1], q0[2], q0[3]},
+        make_float3(pstd[0], pstd[1], pstd[2]),
+        make_float3(rstd[0], rstd[1], rstd[2]), h->d_ctl);
+    PFB_KL();
+    return 0;
+}
+
+int launch_predict(PfHandle* h, const PredictArgs& pa) {
+    const int grid = ceil_div(h->n, kThreads);
+    KernelScope ks(h, KK_PREDICT);
+    k_predict<<<grid, kThreads, 0, h->stream>>>(plane_set(h), h->n, h->seed,
+                                                pa, h->d_ctl);
+    PFB_KL();
+    return 0;
+}
+
+int launch_weight(PfHandle* h, const PredictArgs& pa, const CObservation* d_obs,
+                  int nobs, float sigma_r, float sigma_b, float gate) {
+    const int grid = ceil_div(h->n, kThreads);
+    double2* part = reinterpret_cast<double2*>(h->d_part);
+    KernelScope ks(h, KK_WEIGHT);
+    if (pa.enabled) {
+        k_weight<true><<<grid, kThreads, 0, h->stream>>>(
+            plane_set(h), h->n, h->seed, pa, d_obs, nobs, h->d_lm, h->lm_count,
+            sigma_r, sigma_b, gate, h->d_ll, part, h->d_done + 0, h->d_ctl);
+    } else {
+        k_weight<false><<<grid, kThreads, 0, h->stream>>>(
+            plane_set(h), h->n, h->seed, pa, d_obs, nobs, h->d_lm, h->lm_count,
+            sigma_r, sigma_b, gate, h->d_ll, part, h->d_done + 0, h->d_ctl);
+    }
+    PFB_KL();
+    return 0;
+}
+
+}  // namespace pfb

@@ -1,0 +1,314 @@
+/*
+ * pfc_abi.h — C-ABI of libpf_kernels.so, the B200 (sm_100a) particle-filter and
+ * CBGL global-localization library.
+ *
+ * The first block (18 functions) is the drop-in surface: same names, argument
+ * meaning, return codes and ownership rules as the reference library that the
+ * Rust crate `pf_core` links (`-l dylib=pf_kernels`, crates/pf_core/build.rs:15).
+ * Every declaration cites the Rust binding it satisfies and the reference
+ * definition it replaces.  The second block holds additive entry points with no
+ * reference counterpart (fused cycle, parity hooks, fed-input scoring, batched
+ * filters); existing signatures are never changed by them.
+ *
+ * Conventions shared by all entry points
+ *   - 0 = success, -1 = error (a message goes to stderr and to
+ *     pfc_last_error_message()); *_create returns NULL on failure.
+ *   - Handles are opaque; the library owns all device memory behind them.
+ *   - Host arrays are caller-owned and are fully consumed before the call
+ *     returns; host outputs are written before the call returns.
+ *   - One handle must not be used by two host threads at once (as in the
+ *     reference: no internal locking).  Each handle runs its device work on its
+ *     own CUDA stream on the device that was current at *_create time.
+ */
+#ifndef PFC_ABI_H
+#define PFC_ABI_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Only the entry points below are exported from the shared library. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* One observation as the Rust side marshals it: `CObservation`,
+ * crates/pf_core/src/cuda.rs:18-27 (#[repr(C)], 24 bytes), identical to the
+ * reference's device record `ObsF`, src/cuda/pf_kernels.cu:79-84. */
+typedef struct CObservation {
+    int id;      /* landmark id (index into the dense landmark table)        */
+    int mode;    /* 0 = Cartesian body-frame offset, 1 = range + unit bearing  */
+    float dx, dy, dz; /* Cartesian offset, or unit bearing direction (body)   */
+    float range; /* range in metres (mode 1 only)                              */
+} CObservation;
+
+/* ======================================================================
+ * Drop-in block: particle filter (pfc_*).
+ * Rust declarations: crates/pf_core/src/cuda.rs:33-88.
+ * ==================================================================== */
+
+/* Allocate a filter handle.  cap_obs outside [1,4096] becomes 64.
+ * Replaces pf_kernels.cu:485-503; Rust: cuda.rs:34. */
+void* pfc_create(int cap_obs);
+
+/* Free a handle (NULL is accepted).  Returns 0.  Rust declares it without a
+ * return value (cuda.rs:35), the reference C definition returns int
+ * (pf_kernels.cu:505-517); both bind to this symbol. */
+int pfc_destroy(void* h);
+
+/* (Re)allocate for n particles; seed 0 becomes 42; resets the generation
+ * counter.  Replaces pf_kernels.cu:519-551; Rust: cuda.rs:36. */
+int pfc_init(void* h, int n, unsigned int seed);
+
+/* Upload the dense landmark table: 3 floats per id, zeros for holes.
+ * count == 0 clears the table.  Replaces pf_kernels.cu:553-565;
+ * Rust: cuda.rs:37-41. */
+int pfc_upload_landmarks(void* h, const float* xyz, int count);
+
+/* Gaussian prior around (x,y,z | qw,qx,qy,qz); weights become 1/n.
+ * Replaces pf_kernels.cu:567-582; Rust: cuda.rs:42-53. */
+int pfc_reinit(void* h, float x, float y, float z, float qw, float qx, float qy,
+               float qz, const float* pos_std3, const float* rot_std3);
+
+/* Odometry delta (body frame) + process noise.  Replaces
+ * pf_kernels.cu:584-598; Rust: cuda.rs:54-60. */
+int pfc_predict(void* h, float tx, float ty, float tz, float qw, float qx,
+                float qy, float qz, const float* tstd3, const float* rstd3);
+
+/* Gated log-likelihoods + softmax.  nobs is clamped to cap_obs; nobs <= 0 or
+ * an invalid normaliser resets the weights to uniform.  Observations whose id
+ * is outside [0, landmark count) are skipped.  Replaces pf_kernels.cu:600-636;
+ * Rust: cuda.rs:61-68. */
+int pfc_weight(void* h, const CObservation* obs, int nobs, float sigma_r,
+               float sigma_b, float gate);
+
+/* Systematic resampling + optional uniform re-injection of
+ * floor(ratio*n) particles; weights become 1/n.  An invalid weight total
+ * resets the weights to uniform and leaves the particles in place.
+ * Replaces pf_kernels.cu:638-676; Rust: cuda.rs:69. */
+int pfc_resample(void* h, float random_inject_ratio);
+
+/* 14 FP64 sums: [0..2] sum w*p, [3..12] upper triangle of sum w q q^T in the
+ * order M00,M01,M02,M03,M11,M12,M13,M22,M23,M33, [13] sum w^2.
+ * Replaces pf_kernels.cu:695-705; Rust: cuda.rs:70, unpacked at :277-285. */
+int pfc_est_sums(void* h, double* out14);
+
+/* 12 FP64 sums around the given means: [0..5] position covariance upper
+ * triangle Pxx,Pxy,Pxz,Pyy,Pyz,Pzz; [6..11] attitude tangent covariance
+ * Axx..Azz of the canonical axis-angle of qm^-1 * q.
+ * Replaces pf_kernels.cu:709-722; Rust: cuda.rs:71-81. */
+int pfc_covs(void* h, float mx, float my, float mz, float qw, float qx,
+             float qy, float qz, double* out12);
+
+/* Copy out positions (3n floats, xyz interleaved) and quaternions (4n floats,
+ * w,x,y,z interleaved).  Replaces pf_kernels.cu:724-733; Rust: cuda.rs:82-86. */
+int pfc_snapshot(void* h, float* pos3n, float* quat4n);
+
+/* 1 when a CUDA device of compute capability >= 3 is present, else 0.
+ * Replaces pf_kernels.cu:477-483; Rust: cuda.rs:87. */
+int pfc_device_available(void);
+
+/* ======================================================================
+ * Drop-in block: global localization (pfgl_*).
+ * Rust declarations: crates/pf_core/src/global_loc.rs:261-271.
+ * ==================================================================== */
+
+/* Occupancy grid: W*H bytes row-major, row 0 = lowest y, any nonzero byte is
+ * occupied.  cap_hyp = largest hypothesis batch.  NULL on failure.
+ * Replaces pf_kernels.cu:898-952; Rust: global_loc.rs:263-264. */
+void* pfgl_create(int W, int H, float res, float ox, float oy,
+                  const unsigned char* occ, int cap_hyp);
+
+/* Free a handle (NULL accepted).  Replaces pf_kernels.cu:954-963;
+ * Rust: global_loc.rs:265. */
+int pfgl_destroy(void* h);
+
+/* Number of free (zero) cells, or -1.  Replaces pf_kernels.cu:965-968;
+ * Rust: global_loc.rs:266. */
+int pfgl_free_cells(void* h);
+
+/* Disperse n hypotheses uniformly over free cells, yaw uniform in [-pi,pi).
+ * Replaces pf_kernels.cu:971-979; Rust: global_loc.rs:267. */
+int pfgl_generate(void* h, int n, unsigned long long seed);
+
+/* CAER = sum_r |scan[r] - raycast_r| for every current hypothesis.
+ * Ray r points at theta + span*r/(nrays-1).  Replaces pf_kernels.cu:982-993;
+ * Rust: global_loc.rs:268-269. */
+int pfgl_score(void* h, const float* scan, int nrays, float rmax,
+               float ang_span);
+
+/* Bottom-k hypotheses by CAER ascending (ties: lower index first), written
+ * as k*(x,y,theta).  Returns the count written (k clamped to the batch) or -1.
+ * Replaces pf_kernels.cu:996-1023; Rust: global_loc.rs:270. */
+int pfgl_topk(void* h, int k, float* out3k);
+
+/* ======================================================================
+ * Additive block (no reference counterpart).
+ * ==================================================================== */
+
+/* Last error message of the calling thread ("" when none). */
+const char* pfc_last_error_message(void);
+
+/* Library version, major*10000 + minor*100 + patch. */
+int pfc_version(void);
+
+/* Odometry record for the fused cycle (same meaning as pfc_predict's
+ * arguments). */
+typedef struct PfcOdom {
+    float t[3];     /* body-frame translation                */
+    float q[4];     /* rotation (w,x,y,z)                     */
+    float tstd[3];  /* translation noise std dev per axis     */
+    float rstd[3];  /* rotation noise std dev per axis        */
+} PfcOdom;
+
+/* Parameters of one fused cycle (the fields of PfConfig that
+ * ParticleFilter::update reads, crates/pf_core/src/particle_filter.rs:111-124). */
+typedef struct PfcCycleParams {
+    float sigma_r, sigma_b, gate;
+    double resample_ess_ratio;   /* resample when ess < ratio * n (0 = never) */
+    float random_inject_ratio;
+    int   reserved;
+} PfcCycleParams;
+
+/* Layout of the fused-cycle estimate (doubles). */
+enum {
+    PFC_EST_POS = 0,      /* 3: mean position                              */
+    PFC_EST_QUAT = 3,     /* 4: mean attitude (w,x,y,z), w >= 0            */
+    PFC_EST_POSCOV = 7,   /* 6: Pxx,Pxy,Pxz,Pyy,Pyz,Pzz                    */
+    PFC_EST_ATTCOV = 13,  /* 6: Axx,Axy,Axz,Ayy,Ayz,Azz                    */
+    PFC_EST_ESS = 19,     /* 1: effective sample size of the returned cloud */
+    PFC_EST_RESAMPLED = 20, /* 1: 1.0 when the cycle resampled             */
+    PFC_EST_ESS_PRE = 21, /* 1: ESS before resampling                       */
+    PFC_EST_LEN = 24
+};
+
+/* One full ParticleFilter::update on the device with a single host sync:
+ * predict -> weight -> estimate -> (ess < ratio*n ? resample + estimate).
+ * The Markley mean and the resample decision run on the device. */
+int pfc_cycle(void* h, const PfcOdom* odom, const CObservation* obs, int nobs,
+              const PfcCycleParams* prm, double* est_out);
+
+/* Same, with the observations already resident in device memory
+ * (d_obs = device pointer to nobs CObservation records).  est_out may be a
+ * host pointer (synchronous) or NULL (asynchronous; read it with
+ * pfc_cycle_result). */
+int pfc_cycle_device(void* h, const PfcOdom* odom, const void* d_obs, int nobs,
+                     const PfcCycleParams* prm, double* est_out);
+
+/* Wait for the last asynchronous cycle and copy its estimate. */
+int pfc_cycle_result(void* h, double* est_out);
+
+/* The CUDA stream (cudaStream_t) the handle runs on. */
+void* pfc_stream(void* h);
+
+/* Particle count of the handle (0 before pfc_init). */
+int pfc_size(void* h);
+
+/* Normalised f32 weights (n floats) as the resampler and the estimator
+ * see them. */
+int pfc_get_weights(void* h, float* w);
+
+/* f32 log-likelihoods from the last pfc_weight (n floats). */
+int pfc_get_ll(void* h, float* ll);
+
+/* Overwrite the particle set: AoS positions (3n) and quaternions (4n, w first)
+ * as pfc_snapshot returns them; w = n weights or NULL for uniform 1/n. */
+int pfc_set_state(void* h, const float* pos3n, const float* quat4n,
+                  const float* w);
+
+/* Resample with an explicit offset fraction u01 in [0,1) instead of the
+ * handle's LCG draw (the LCG is left untouched); injection as pfc_resample. */
+int pfc_resample_u01(void* h, double u01, float random_inject_ratio);
+
+/* Record ancestor indices in later resamples (off by default: 4 B/particle
+ * of extra HBM writes). */
+int pfc_record_ancestors(void* h, int on);
+
+/* Ancestor index of every particle in the last recorded resample (n ints). */
+int pfc_get_ancestors(void* h, int* anc);
+
+/* The reference's pick rule (pf_kernels.cu:304-321) applied to a caller
+ * cumulative-weight array: anc[i] = first j with cum[j] >= u0 + i*(total/n),
+ * clamped to n-1, evaluated on the device.  Host arrays of n entries. */
+int pfc_pick_from_cum(void* h, const double* cum, int n, double u0,
+                      double total, int* anc);
+
+/* Device-side LCG word that drives the resampling offset (see
+ * pf_kernels.cu:653-657); set it to replay a resample. */
+int pfc_get_lcg(void* h, unsigned long long* lcg);
+int pfc_set_lcg(void* h, unsigned long long lcg);
+
+/* Accounting of one handle since creation / the last reset: kernels launched,
+ * bytes copied host->device and device->host, host waits on the device. */
+typedef struct PfcStats {
+    unsigned long long launches;
+    unsigned long long h2d_bytes;
+    unsigned long long d2h_bytes;
+    unsigned long long host_syncs;
+} PfcStats;
+int pfc_get_stats(void* h, PfcStats* out);
+int pfc_reset_stats(void* h);
+
+/* Kernel kinds of the per-kind timing below. */
+enum {
+    PFC_K_REINIT = 0, PFC_K_PREDICT, PFC_K_WEIGHT, PFC_K_EST, PFC_K_COVS,
+    PFC_K_SCAN, PFC_K_GATHER, PFC_K_INJECT, PFC_K_COMMIT, PFC_K_MISC,
+    PFC_K_COUNT
+};
+
+/* Per-kernel-kind device time: when on, every launch is bracketed by CUDA
+ * events on the handle's stream; pfc_profile_read waits for them and returns
+ * the accumulated milliseconds and launch counts (PFC_K_COUNT entries each)
+ * since the last read. */
+int pfc_profile(void* h, int on);
+int pfc_profile_read(void* h, double* ms, long long* counts);
+
+/* Weighting kernel variant: 0 = quaternion form in the reference's
+ * expression order (default), 1 = two particles per thread with packed f32x2
+ * arithmetic in the same per-element operation order. */
+int pfc_set_weight_kernel(void* h, int variant);
+
+/* ---------------------------------------------------------------------
+ * Global localization, additive.
+ * ------------------------------------------------------------------- */
+
+/* n_pos uniform free-space positions x n_yaw yaws theta0 + j*2*pi/n_yaw
+ * (theta0 uniform per position); hypothesis index = pos*n_yaw + j. */
+int pfgl_generate_yaws(void* h, int n_pos, int n_yaw, unsigned long long seed);
+
+/* Set / read hypotheses directly (3n floats x,y,theta). */
+int pfgl_set_hyps(void* h, const float* hyp3n, int n);
+int pfgl_get_hyps(void* h, float* hyp3n);
+
+/* CAER of every current hypothesis (n floats) from the last pfgl_score. */
+int pfgl_get_caer(void* h, float* caer);
+
+/* Bottom-k with scores and indices: out3k may be NULL; caer_k / idx_k may be
+ * NULL.  Returns the count written or -1. */
+int pfgl_topk_ex(void* h, int k, float* out3k, float* caer_k, int* idx_k);
+
+/* Bottom-k of caller scores (host array of n floats), ordered by
+ * (CAER ascending, index ascending); writes min(k,n) indices. */
+int pfgl_topk_from_scores(void* h, const float* caer, int n, int k,
+                          int* idx_out);
+
+/* Fused global localization over the current hypotheses: raycast + CAER with
+ * exact early termination against the running k-th best, and bottom-k
+ * selection.  Same results as pfgl_score + pfgl_topk_ex for those k.  CAERs
+ * of pruned hypotheses are not computed. */
+int pfgl_localize(void* h, const float* scan, int nrays, float rmax,
+                  float ang_span, int k, float* out3k, float* caer_k,
+                  int* idx_k);
+
+/* Occupancy value the device sees for cell (cx,cy): 0 free, 1 occupied. */
+int pfgl_cell(void* h, int cx, int cy);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PFC_ABI_H */
