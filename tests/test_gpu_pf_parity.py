@@ -28,6 +28,7 @@ from tests.pf_helpers import (RawPF, cloud, f32p, f64p, i32p, ours_ll, ours_set_
 pytestmark = pytest.mark.gpu
 
 N = 50_000  # not a multiple of the 256-thread block nor of the 4096 scan tile
+SR = 1.0    # range sigma of the comparison fixture
 
 
 @pytest.fixture(scope="module")
@@ -43,8 +44,10 @@ def weighted_pair(kernels, ref):
     ref_set_state(ref, theirs, pos, quat)
     ours.landmarks(lm)
     theirs.landmarks(lm)
-    assert ours.weight(obs) == 0
-    assert theirs.weight(obs) == 0
+    # sigma_r = 1 m keeps many weights non-negligible (at 0.05 m the posterior
+    # of 256 observations sits on one particle and the comparison is empty)
+    assert ours.weight(obs, SR, 0.02, 3.0) == 0
+    assert theirs.weight(obs, SR, 0.02, 3.0) == 0
     yield dict(ours=ours, theirs=theirs, pos=pos, quat=quat, lm=lm, obs=obs)
     ours.close()
     theirs.close()
@@ -64,7 +67,7 @@ def test_loglik_matches_fp64_oracle(weighted_pair):
     o = oracle.loglik(d["pos"].astype(np.float64), d["quat"].astype(np.float64),
                       d["lm"].astype(np.float32).astype(np.float64),
                       [tuple(r[:2]) + tuple(np.float32(r[2:]).astype(np.float64)) for r in d["obs"]],
-                      0.05, 0.02, 3.0)
+                      SR, 0.02, 3.0)
     # f32 evaluation of 256 gated terms against FP64
     assert np.all(np.abs(a - o) <= 1e-5 * np.abs(o) + 5e-3), np.max(np.abs(a - o))
 
@@ -78,6 +81,7 @@ def test_weights_match_reference(weighted_pair, ref):
     big = b > 1e-12 * b.max()
     rel = np.abs(a[big] - b[big]) / b[big]
     print(f"max weight rel diff {rel.max():.3e} over {big.sum()} weights")
+    assert big.sum() > 100
     assert rel.max() <= 1e-5
 
 
@@ -112,7 +116,9 @@ def test_covs_fp64_vs_oracle_and_reference(weighted_pair, ref):
     ref_set_state(ref, theirs, pos, quat, w)
     theirs.est_sums()
     r = theirs.covs(mp, mq)
+    # relative to the largest variance of each block (off-diagonals can be ~0)
     scale = np.r_[np.full(6, np.abs(r[[0, 3, 5]]).max()), np.full(6, np.abs(r[[6, 9, 11]]).max())]
+    assert np.all(scale > 0)
     assert np.all(np.abs(c - r) <= 1e-5 * scale), np.max(np.abs(c - r) / scale)
 
 
@@ -129,20 +135,23 @@ def test_covs_speculation_hits_and_misses(weighted_pair):
     assert np.array_equal(again, hit)
 
 
-def _weighted_state(kernels, n, seed):
+def _weighted_state(kernels, n, seed, sr=1.0):
     lm, obs, tp, tq = scale_obs(seed=seed)
     yaw = 2.0 * np.arctan2(tq[3], tq[0])
     pos, quat = cloud(n, seed, centre=tp, pos_std=0.2, rot_std=0.03, yaw=yaw)
     pf = RawPF(kernels, n, seed=3)
     ours_set_state(pf, pos, quat)
     pf.landmarks(lm)
-    assert pf.weight(obs) == 0
+    assert pf.weight(obs, sr, 0.02, 3.0) == 0
     return pf
 
 
-@pytest.mark.parametrize("n", [1, 7, 4096, 4097, 50_000, 1_000_000])
-def test_resample_ancestors_bit_exact_vs_spec(kernels, n):
-    pf = _weighted_state(kernels, n, 21)
+# sr = 0.05 m puts (nearly) all weight on one particle: one scan tile then owns
+# every output, the load-imbalance case of the merge-path gather.
+@pytest.mark.parametrize("n,sr", [(1, 1.0), (7, 1.0), (4096, 1.0), (4097, 1.0), (50_000, 1.0),
+                                  (1_000_000, 1.0), (1_000_000, 0.05)])
+def test_resample_ancestors_bit_exact_vs_spec(kernels, n, sr):
+    pf = _weighted_state(kernels, n, 21, sr)
     try:
         w = ours_weights(pf)
         pos0, quat0 = pf.snapshot()
@@ -271,8 +280,9 @@ def test_weight_edge_cases(kernels):
         pf.reinit([5, 5, 1, 1, 0, 0, 0], [3.0] * 3, [0.1] * 3)
         pf.landmarks(lm)
         uni = np.float32(1.0) / np.float32(n)
-        # informative observation collapses the weights
-        assert pf.weight([(0, 0, 0.0, 0.0, 0.0, 0.0)]) == 0
+        # informative observation collapses the weights (ungated, as in
+        # crates/pf_core/tests/cuda_agreement.rs:82-131)
+        assert pf.weight([(0, 0, 0.0, 0.0, 0.0, 0.0)], gate=0.0) == 0
         w = ours_weights(pf)
         assert 1.0 / np.sum(w.astype(np.float64) ** 2) < n / 2
         # no observations -> uniform
