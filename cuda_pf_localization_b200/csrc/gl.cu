@@ -32,6 +32,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -834,3 +835,101 @@ int pfgl_cell(void* hv, int cx, int cy) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------ allocation-free bottom-k
+//
+// Some callers cannot allocate device memory at the time they need a
+// bottom-k: a localization step inside a fixed-rate control loop (cudaMalloc
+// and cudaFree can block for milliseconds and synchronise the device, which a
+// real-time thread must not do), or an application that hands all device
+// memory to its own pool allocator and forbids other allocations after
+// start-up.  pfgl_topk_noalloc serves them: the caller passes the scores and
+// the output buffer, and the working memory of the radix sort lives in the
+// fixed array below, which is part of the library's device image.
+//
+// Limits and sharing:
+//   * at most kNoAllocMaxN scores per call (larger inputs are rejected);
+//   * every GPU that loads the library holds the array (1 MiB + 32 KiB)
+//     until the process exits;
+//   * all calls on a device share the array: calls whose work overlaps on the
+//     GPU (different streams, or different host threads) race and corrupt
+//     each other's results; serialise them on one stream;
+//   * the array keeps the last call's contents; every word a call reads is
+//     written earlier by the same call (keys, then each pass's histogram), so
+//     nothing needs clearing between calls.
+namespace pfb {
+namespace noalloc {
+
+constexpr int kNoAllocMaxN = 65536;
+constexpr int kNoAllocBlocks = kNoAllocMaxN / kRsTile;  // 32 radix tiles
+constexpr size_t kNoAllocKeyBytes = (size_t)kNoAllocMaxN * sizeof(uint64_t);
+constexpr size_t kNoAllocBytes =
+    2 * kNoAllocKeyBytes + 256 * (size_t)kNoAllocBlocks * sizeof(unsigned);
+
+static __device__ __align__(256) unsigned char g_topk_scratch[kNoAllocBytes];
+
+// Device address of g_topk_scratch per device, looked up once per device
+// (host code must not use the symbol itself as a device pointer).
+std::mutex g_scratch_mu;
+std::vector<void*> g_scratch_addr;
+
+void* scratch_address(int dev) {
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if ((int)g_scratch_addr.size() <= dev) g_scratch_addr.resize(dev + 1, nullptr);
+    if (!g_scratch_addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_topk_scratch);
+        if (e != cudaSuccess) {
+            set_error("pf_b200: pfgl_topk_noalloc: cudaGetSymbolAddress failed: %s",
+                      cudaGetErrorString(e));
+            return nullptr;
+        }
+        g_scratch_addr[dev] = p;
+    }
+    return g_scratch_addr[dev];
+}
+
+__global__ void k_keys_to_index(const uint64_t* __restrict__ sorted, int k,
+                                int* __restrict__ idx) {
+    const int j = blockIdx.x * kThreads + threadIdx.x;
+    if (j < k) idx[j] = (int)(uint32_t)sorted[j];
+}
+
+}  // namespace noalloc
+}  // namespace pfb
+
+using namespace pfb::noalloc;
+
+extern "C" int pfgl_topk_noalloc(const float* d_scores, int n, int k,
+                                 int* d_idx, void* stream) {
+    if (!d_scores || !d_idx || n <= 0 || k <= 0) {
+        set_error("pf_b200: pfgl_topk_noalloc: bad arguments");
+        return -1;
+    }
+    if (n > kNoAllocMaxN) {
+        set_error("pf_b200: pfgl_topk_noalloc: n = %d exceeds the fixed scratch "
+                  "capacity of %d scores", n, kNoAllocMaxN);
+        return -1;
+    }
+    int dev = 0;
+    PFB_CK(cudaGetDevice(&dev));
+    unsigned char* base = static_cast<unsigned char*>(scratch_address(dev));
+    if (!base) return -1;
+    uint64_t* a = reinterpret_cast<uint64_t*>(base);
+    uint64_t* b = reinterpret_cast<uint64_t*>(base + kNoAllocKeyBytes);
+    unsigned* hist = reinterpret_cast<unsigned*>(base + 2 * kNoAllocKeyBytes);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (k > n) k = n;
+    const int nb = ceil_div(n, kRsTile);
+    const int need = 256 * nb;
+    k_make_keys<<<ceil_div(n, kThreads), kThreads, 0, s>>>(d_scores, n, a);
+    for (int shift = 32; shift < 64; shift += 8) {
+        k_rs_hist<<<nb, kThreads, 0, s>>>(a, n, shift, hist, nb);
+        k_rs_scan<<<1, 1024, 0, s>>>(hist, need);
+        k_rs_scatter<<<nb, kThreads, 0, s>>>(a, b, n, shift, hist, nb);
+        std::swap(a, b);
+    }
+    k_keys_to_index<<<ceil_div(k, kThreads), kThreads, 0, s>>>(a, k, d_idx);
+    PFB_KL();
+    return k;
+}

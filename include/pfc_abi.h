@@ -303,6 +303,24 @@ int pfgl_localize(void* h, const float* scan, int nrays, float rmax,
 /* Occupancy value the device sees for cell (cx,cy): 0 free, 1 occupied. */
 int pfgl_cell(void* h, int cx, int cy);
 
+/* Allocation-free bottom-k (no counterpart in the reference).  For callers
+ * that must not allocate device memory when they select winners — a
+ * localization step inside a fixed-rate control loop, where cudaMalloc /
+ * cudaFree can block and synchronise the device, or an application whose
+ * device memory all belongs to its own pool allocator.  The caller passes the
+ * scores (device array of n floats) and the output (device array of k ints);
+ * the sort's working memory is a fixed 1 MiB + 32 KiB array inside the
+ * library, held by every GPU that loads the library until the process exits.
+ * Writes the indices of the min(k,n) smallest scores ordered by (score,
+ * index), as pfgl_topk_from_scores, asynchronously on `stream` (a
+ * cudaStream_t; NULL = the legacy default stream).  Returns min(k,n), or -1
+ * for n > 65536 or bad arguments.  All calls on a device share the working
+ * array, so calls that overlap on the GPU race: issue them on one stream.
+ * The first call on each device looks up the array's device address (once);
+ * make that first call before any stream capture or real-time section. */
+int pfgl_topk_noalloc(const float* d_scores, int n, int k, int* d_idx,
+                      void* stream);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif
