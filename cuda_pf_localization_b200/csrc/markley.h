@@ -5,9 +5,12 @@
 //
 // Semantics follow crates/pf_core/src/types.rs:128-143: symmetrise
 // (M^T + M)/2, take the eigenvector of the largest eigenvalue (first index on
-// ties), normalise, flip to w >= 0.  The eigen-solve is the cyclic Jacobi
-// method (Golub & Van Loan, "Matrix Computations", section 8.5) rather than
-// nalgebra's tridiagonal QR: both return the same unit eigenvector up to
+// ties), normalise, flip to w >= 0.  The dominant eigenvector comes from
+// repeated squaring of M (a few hundred FP64 operations with no divisions in
+// the loop, so a single GPU thread finishes it in about a microsecond),
+// checked by its Rayleigh residual; near-degenerate spectra fall back to the
+// cyclic Jacobi method (Golub & Van Loan, "Matrix Computations", section
+// 8.5).  nalgebra's tridiagonal QR returns the same unit eigenvector up to
 // sign for a simple top eigenvalue, and the sign is canonicalised.
 #pragma once
 
@@ -68,6 +71,55 @@ PFB_HD inline int jacobi_eig4(double a[16], double v[16]) {
     return sweep;
 }
 
+// Dominant eigenvector of a symmetric positive semi-definite 4x4 matrix by
+// repeated squaring (the power method on M^(2^k)): after 12 squarings the
+// other eigen-directions are damped by (lambda2/lambda1)^4096.  Accepted only
+// when the Rayleigh residual |M v - (v'Mv) v| is below 1e-13 |M|; returns
+// false otherwise (near-degenerate top eigenvalue), and the caller falls back
+// to the Jacobi solve.
+PFB_HD inline bool dominant_eigvec_psd4(const double a[16], double v[4]) {
+    double p[16], t[16];
+    double tr = a[0] + a[5] + a[10] + a[15];
+    if (!(tr > 0.0)) return false;
+    const double itr = 1.0 / tr;
+    for (int i = 0; i < 16; ++i) p[i] = a[i] * itr;
+    for (int s = 0; s < 12; ++s) {
+        for (int r = 0; r < 4; ++r)
+            for (int c = 0; c < 4; ++c)
+                t[r * 4 + c] = p[r * 4 + 0] * p[0 * 4 + c] + p[r * 4 + 1] * p[1 * 4 + c] +
+                               p[r * 4 + 2] * p[2 * 4 + c] + p[r * 4 + 3] * p[3 * 4 + c];
+        const double tt = t[0] + t[5] + t[10] + t[15];
+        if (!(tt > 0.0)) return false;
+        const double itt = 1.0 / tt;
+        for (int i = 0; i < 16; ++i) p[i] = t[i] * itt;
+    }
+    // p ~ v v^T: take the column with the largest diagonal entry.
+    int c = 0;
+    for (int i = 1; i < 4; ++i)
+        if (p[i * 4 + i] > p[c * 4 + c]) c = i;
+    double x[4] = {p[0 * 4 + c], p[1 * 4 + c], p[2 * 4 + c], p[3 * 4 + c]};
+    // two power steps with the original matrix polish the direction
+    for (int it = 0; it < 2; ++it) {
+        double y[4];
+        for (int r = 0; r < 4; ++r)
+            y[r] = a[r * 4 + 0] * x[0] + a[r * 4 + 1] * x[1] + a[r * 4 + 2] * x[2] +
+                   a[r * 4 + 3] * x[3];
+        const double ny = sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2] + y[3] * y[3]);
+        if (!(ny > 0.0)) return false;
+        for (int r = 0; r < 4; ++r) x[r] = y[r] / ny;
+    }
+    double y[4];
+    for (int r = 0; r < 4; ++r)
+        y[r] = a[r * 4 + 0] * x[0] + a[r * 4 + 1] * x[1] + a[r * 4 + 2] * x[2] +
+               a[r * 4 + 3] * x[3];
+    const double lam = x[0] * y[0] + x[1] * y[1] + x[2] * y[2] + x[3] * y[3];
+    double res = 0.0;
+    for (int r = 0; r < 4; ++r) res += (y[r] - lam * x[r]) * (y[r] - lam * x[r]);
+    if (!(sqrt(res) <= 1e-13 * tr)) return false;
+    for (int r = 0; r < 4; ++r) v[r] = x[r];
+    return true;
+}
+
 // Mean quaternion (w,x,y,z) from the 10 packed upper-triangle moments
 // M00,M01,M02,M03,M11,M12,M13,M22,M23,M33 (the layout of pfc_est_sums
 // out[3..12], unpacked by crates/pf_core/src/cuda.rs:277-285).
@@ -80,12 +132,14 @@ PFB_HD inline void markley_mean(const double m10[10], double q_out[4]) {
             a[c * 4 + r] = m10[e];
             ++e;
         }
-    jacobi_eig4(a, v);
-    int idx = 0;
-    for (int i = 1; i < 4; ++i)
-        if (a[i * 4 + i] > a[idx * 4 + idx]) idx = i;
-    double q[4] = {v[0 * 4 + idx], v[1 * 4 + idx], v[2 * 4 + idx],
-                   v[3 * 4 + idx]};
+    double q[4];
+    if (!dominant_eigvec_psd4(a, q)) {
+        jacobi_eig4(a, v);
+        int idx = 0;
+        for (int i = 1; i < 4; ++i)
+            if (a[i * 4 + i] > a[idx * 4 + idx]) idx = i;
+        for (int r = 0; r < 4; ++r) q[r] = v[r * 4 + idx];
+    }
     double nrm = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
     if (!(nrm > 0.0)) {
         q_out[0] = 1.0;

@@ -141,6 +141,8 @@ void free_particles(PfHandle* h) {
     cudaFree(h->d_scan_flags);
     cudaFree(h->d_scan_vals);
     cudaFree(h->d_part);
+    cudaFree(h->d_part_u64);
+    cudaFree(h->d_heavy);
     cudaFree(h->d_stage);
     h->d_state[0] = h->d_state[1] = nullptr;
     h->d_ll = h->d_w = nullptr;
@@ -151,6 +153,9 @@ void free_particles(PfHandle* h) {
     h->d_scan_flags = nullptr;
     h->d_scan_vals = nullptr;
     h->d_part = nullptr;
+    h->d_part_u64 = nullptr;
+    h->d_heavy = nullptr;
+    h->heavy_cap = 0;
     h->d_stage = nullptr;
     h->n = 0;
 }
@@ -386,6 +391,7 @@ int pfc_init(void* hv, int n, unsigned int seed) {
     h->pending_predict = false;
     h->est_valid = h->est_inflight = false;
     h->anc_valid = false;
+    h->total_valid = false;
     const size_t np = (size_t)h->n_pad;
     const int ntiles = ceil_div(n, 4096);
     const int part = std::max(2 * ceil_div(n, kThreads), 1184 * 16);
@@ -393,7 +399,9 @@ int pfc_init(void* hv, int n, unsigned int seed) {
     PFB_CK(cudaMalloc((void**)&h->d_state[1], 7 * np * sizeof(float)));
     PFB_CK(cudaMalloc((void**)&h->d_ll, np * sizeof(float)));
     PFB_CK(cudaMalloc((void**)&h->d_w, np * sizeof(float)));
-    PFB_CK(cudaMalloc((void**)&h->d_cum, (size_t)n * sizeof(uint64_t)));
+    h->heavy_cap = n / 32 + 2;
+    PFB_CK(cudaMalloc((void**)&h->d_heavy, (size_t)h->heavy_cap * sizeof(HeavyRun)));
+    PFB_CK(cudaMalloc((void**)&h->d_part_u64, 2 * 1184 * sizeof(unsigned long long)));
     PFB_CK(cudaMalloc((void**)&h->d_anc, (size_t)n * sizeof(int)));
     PFB_CK(cudaMalloc((void**)&h->d_inj_head, (size_t)n * sizeof(uint64_t)));
     PFB_CK(cudaMalloc((void**)&h->d_inj_next, (size_t)n * sizeof(int)));
@@ -450,6 +458,7 @@ int pfc_reinit(void* hv, float x, float y, float z, float qw, float qx,
     if (launch_reinit(h, p0, q0, pos_std, rot_std)) return -1;
     if (set_wmode(h, WMODE_UNIFORM)) return -1;
     h->est_valid = h->est_inflight = false;
+    h->total_valid = false;
     return 0;
 }
 
@@ -672,6 +681,7 @@ int pfc_set_state(void* hv, const float* pos3n, const float* quat4n,
     }
     PFB_CK(cudaStreamSynchronize(h->stream));
     h->est_valid = h->est_inflight = false;
+    h->total_valid = false;
     return 0;
 }
 

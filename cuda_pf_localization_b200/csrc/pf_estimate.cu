@@ -4,12 +4,19 @@
 // Pass 1 (k_est_sums) reads pose + weight (28 + 4 B per particle) and writes
 // the 14 sums of the reference's pfc_est_sums layout
 // (src/cuda/pf_kernels.cu:354-404).  Every per-particle product and every
-// partial is FP64 (the reference accumulates per thread in f32).  The last
-// block combines the per-block partials in block order, runs the Markley
-// eigen-solve and stores the f32 means that the covariance pass uses.
+// partial is FP64 (the reference accumulates per thread in f32).  As a
+// by-product it forms the exact fixed-point weight total sum_j rn(w_j 2^62)
+// that the resampler needs before it starts, and flags weights outside
+// [0, 1].  The last block combines the per-block partials in block order,
+// runs the Markley eigen-solve and stores the f32 means that the covariance
+// pass uses.
 // Pass 2 (k_covs) reads pose + weight again and writes the 12 covariance sums
 // of the reference's pfc_covs layout (src/cuda/pf_kernels.cu:406-471), with
 // the attitude residual of (qm^-1 * q) in FP64.
+//
+// Both passes read four particles per iteration with 16-byte loads from each
+// SoA plane (eight loads in flight per thread), which is what keeps HBM busy
+// at two resident blocks per SM.
 #include <math.h>
 
 #include "markley.h"
@@ -20,7 +27,9 @@ namespace pfb {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kMaxBlocks = 1184;  // 148 SMs x 8 resident blocks
+// Two resident blocks per SM keep enough 16-byte loads in flight; a fixed,
+// small grid also keeps the last block's combine short.
+constexpr int kMaxBlocks = 2 * 148;
 
 struct PlaneSet {
     Planes s[2];
@@ -33,23 +42,29 @@ __device__ __forceinline__ double warp_sum_d(double v) {
     return v;
 }
 
-// Normalised f32 weight of particle i under the cloud's weight mode.
-__device__ __forceinline__ float weight_of(int wmode, int i, int n,
-                                           const float* __restrict__ w,
-                                           const float* __restrict__ ll,
-                                           double M, double S) {
-    if (wmode == WMODE_UNIFORM) return 1.0f / (float)n;
-    if (wmode == WMODE_STORED) return w[i];
-    return (float)(exp((double)ll[i] - M) / S);
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(~0u, v, o);
+    return v;
+}
+
+__device__ __forceinline__ float comp(const float4& v, int c) {
+    return c == 0 ? v.x : (c == 1 ? v.y : (c == 2 ? v.z : v.w));
 }
 
 // Reduce NV per-thread FP64 accumulators over the block into part[blk*NV+k];
 // the last block to finish sums the partials of all blocks in block order
-// into out[k] and returns true (in every thread of that block).
+// into out[k] and returns true (in every thread of that block).  With
+// partu != nullptr an integer partial (and a flag in its top bit) is
+// reduced alongside.
 template <int NV>
 __device__ bool block_reduce_last(double (&acc)[NV], double* part,
-                                  unsigned* done, double* out) {
+                                  unsigned long long tfx, int bad,
+                                  unsigned long long* partu, unsigned* done,
+                                  double* out, unsigned long long* out_u,
+                                  int* out_bad) {
     __shared__ double s_w[NV][kThreads / 32];
+    __shared__ unsigned long long s_u[kThreads / 32];
     __shared__ bool s_last;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 #pragma unroll
@@ -57,11 +72,21 @@ __device__ bool block_reduce_last(double (&acc)[NV], double* part,
         double v = warp_sum_d(acc[k]);
         if (lane == 0) s_w[k][warp] = v;
     }
-    __syncthreads();
+    if (partu) {
+        const unsigned long long u = warp_sum_u64(tfx);
+        if (lane == 0) s_u[warp] = u;
+    }
+    const int any_bad = __syncthreads_or(bad);
     if (tid < NV) {
         double v = 0.0;
         for (int k = 0; k < kThreads / 32; ++k) v += s_w[tid][k];
         part[(size_t)blockIdx.x * NV + tid] = v;
+    }
+    if (partu && tid == 32) {
+        unsigned long long u = 0;
+        for (int k = 0; k < kThreads / 32; ++k) u += s_u[k];
+        partu[2 * (size_t)blockIdx.x] = u;
+        partu[2 * (size_t)blockIdx.x + 1] = any_bad ? 1ull : 0ull;
     }
     __threadfence();
     __syncthreads();
@@ -70,48 +95,96 @@ __device__ bool block_reduce_last(double (&acc)[NV], double* part,
     if (!s_last) return false;
     __threadfence();
     const int G = gridDim.x;
-    // warp w combines components w, w+8, ...; lanes stride over blocks.
     for (int k = warp; k < NV; k += kThreads / 32) {
         double v = 0.0;
+#pragma unroll 4
         for (int b = lane; b < G; b += 32) v += __ldcg(&part[(size_t)b * NV + k]);
         v = warp_sum_d(v);
         if (lane == 0) out[k] = v;
+    }
+    if (partu && warp == kThreads / 32 - 1) {
+        unsigned long long u = 0, f = 0;
+        for (int b = lane; b < G; b += 32) {
+            u += __ldcg(&partu[2 * (size_t)b]);
+            f |= __ldcg(&partu[2 * (size_t)b + 1]);
+        }
+        u = warp_sum_u64(u);
+        const unsigned anyf = __ballot_sync(~0u, f != 0);
+        if (lane == 0) {
+            *out_u = u;
+            *out_bad = anyf ? 1 : 0;
+        }
     }
     __syncthreads();
     if (tid == 0) *done = 0u;
     return true;
 }
 
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
     k_est_sums(PlaneSet ps, int n, const float* __restrict__ ll,
-               float* __restrict__ w, double* part, unsigned* done,
-               CycleCtl* ctl, int cond_second) {
+               float* __restrict__ w, double* part, unsigned long long* partu,
+               unsigned* done, CycleCtl* ctl, int cond_second) {
     if (cond_second && !ctl->resample_now) return;
     const Planes s = ps.s[ctl->live];
     const int wmode = ctl->wmode;
     const double M = ctl->ll_max, S = ctl->ll_sumexp;
+    const float wuni = 1.0f / (float)n;
     double acc[kEstN];
 #pragma unroll
     for (int k = 0; k < kEstN; ++k) acc[k] = 0.0;
-    for (int i = blockIdx.x * kThreads + threadIdx.x; i < n;
-         i += gridDim.x * kThreads) {
-        const float wf = weight_of(wmode, i, n, w, ll, M, S);
-        if (wmode == WMODE_LL) w[i] = wf;
-        const double wd = (double)wf;
-        acc[0] += wd * (double)s.px[i];
-        acc[1] += wd * (double)s.py[i];
-        acc[2] += wd * (double)s.pz[i];
-        const double q[4] = {(double)s.qw[i], (double)s.qx[i], (double)s.qy[i],
-                             (double)s.qz[i]};
-        int e = 3;
+    unsigned long long tfx = 0;
+    int bad = 0;
+    const int n4 = (n + 3) >> 2;
+    const float4* px = reinterpret_cast<const float4*>(s.px);
+    const float4* py = reinterpret_cast<const float4*>(s.py);
+    const float4* pz = reinterpret_cast<const float4*>(s.pz);
+    const float4* qw = reinterpret_cast<const float4*>(s.qw);
+    const float4* qx = reinterpret_cast<const float4*>(s.qx);
+    const float4* qy = reinterpret_cast<const float4*>(s.qy);
+    const float4* qz = reinterpret_cast<const float4*>(s.qz);
+    for (int i4 = blockIdx.x * kThreads + threadIdx.x; i4 < n4;
+         i4 += gridDim.x * kThreads) {
+        const float4 X = px[i4], Y = py[i4], Z = pz[i4];
+        const float4 QW = qw[i4], QX = qx[i4], QY = qy[i4], QZ = qz[i4];
+        float4 W;
+        if (wmode == WMODE_STORED) {
+            W = reinterpret_cast<const float4*>(w)[i4];
+        } else if (wmode == WMODE_UNIFORM) {
+            W = make_float4(wuni, wuni, wuni, wuni);
+        } else {
+            const float4 L = reinterpret_cast<const float4*>(ll)[i4];
+            W = make_float4((float)(exp((double)L.x - M) / S),
+                            (float)(exp((double)L.y - M) / S),
+                            (float)(exp((double)L.z - M) / S),
+                            (float)(exp((double)L.w - M) / S));
+            reinterpret_cast<float4*>(w)[i4] = W;
+        }
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) {
+            if (4 * i4 + c >= n) break;
+            const float wf = comp(W, c);
+            bad |= weight_bad(wf) ? 1 : 0;
+            tfx += weight_bad(wf) ? 0ull : weight_fx(wf);
+            const double wd = (double)wf;
+            acc[0] += wd * (double)comp(X, c);
+            acc[1] += wd * (double)comp(Y, c);
+            acc[2] += wd * (double)comp(Z, c);
+            const double q[4] = {(double)comp(QW, c), (double)comp(QX, c),
+                                 (double)comp(QY, c), (double)comp(QZ, c)};
+            int e = 3;
 #pragma unroll
-            for (int c = r; c < 4; ++c) acc[e++] += wd * q[r] * q[c];
-        acc[13] += wd * wd;
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int cc = r; cc < 4; ++cc) acc[e++] += wd * q[r] * q[cc];
+            acc[13] += wd * wd;
+        }
     }
     __shared__ double s_out[kEstN];
-    if (!block_reduce_last<kEstN>(acc, part, done, s_out)) return;
+    __shared__ unsigned long long s_tfx;
+    __shared__ int s_bad;
+    if (!block_reduce_last<kEstN>(acc, part, tfx, bad, partu, done, s_out, &s_tfx,
+                                  &s_bad))
+        return;
     if (threadIdx.x == 0) {
         for (int k = 0; k < kEstN; ++k) ctl->est[k] = s_out[k];
         ctl->ess = s_out[13] > 0.0 ? 1.0 / s_out[13] : 0.0;
@@ -120,6 +193,8 @@ __global__ void __launch_bounds__(kThreads)
         for (int k = 0; k < 4; ++k) ctl->qmean[k] = qm[k];
         for (int k = 0; k < 3; ++k) ctl->cov_mean_p[k] = (float)s_out[k];
         for (int k = 0; k < 4; ++k) ctl->cov_mean_q[k] = (float)qm[k];
+        ctl->w_total_fx = s_tfx;
+        ctl->w_bad = s_bad;
         if (wmode == WMODE_LL) ctl->wmode = WMODE_STORED;
     }
 }
@@ -142,11 +217,11 @@ __device__ __forceinline__ void att_residual(const double qm[4],
         dz = -dz;
     }
     const double hv = sqrt(dx * dx + dy * dy + dz * dz);
-    const double ang = 2.0 * atan2(hv, dw);
     if (hv > 1e-12) {
-        aav[0] = dx / hv * ang;
-        aav[1] = dy / hv * ang;
-        aav[2] = dz / hv * ang;
+        const double f = 2.0 * atan2(hv, dw) / hv;
+        aav[0] = dx * f;
+        aav[1] = dy * f;
+        aav[2] = dz * f;
     } else {
         aav[0] = aav[1] = aav[2] = 0.0;
     }
@@ -154,7 +229,7 @@ __device__ __forceinline__ void att_residual(const double qm[4],
 
 // mode: 0 plain, 1 first pass of a fused cycle (decide resample), 2 second
 // pass of a fused cycle (skip unless resampling; emit the output record).
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
     k_covs(PlaneSet ps, int n, const float* __restrict__ ll,
            const float* __restrict__ w, double* part, unsigned* done,
            CycleCtl* ctl, int use_args, float3 mp_arg, float4 mq_arg,
@@ -163,6 +238,7 @@ __global__ void __launch_bounds__(kThreads)
     const Planes s = ps.s[ctl->live];
     const int wmode = ctl->wmode;
     const double M = ctl->ll_max, S = ctl->ll_sumexp;
+    const float wuni = 1.0f / (float)n;
     float3 mpf;
     float4 mqf;
     if (use_args) {
@@ -180,27 +256,56 @@ __global__ void __launch_bounds__(kThreads)
     double acc[kCovN];
 #pragma unroll
     for (int k = 0; k < kCovN; ++k) acc[k] = 0.0;
-    for (int i = blockIdx.x * kThreads + threadIdx.x; i < n;
-         i += gridDim.x * kThreads) {
-        const double wd = (double)weight_of(wmode, i, n, w, ll, M, S);
-        const double dp[3] = {(double)s.px[i] - mp[0], (double)s.py[i] - mp[1],
-                              (double)s.pz[i] - mp[2]};
-        int e = 0;
+    const int n4 = (n + 3) >> 2;
+    const float4* px = reinterpret_cast<const float4*>(s.px);
+    const float4* py = reinterpret_cast<const float4*>(s.py);
+    const float4* pz = reinterpret_cast<const float4*>(s.pz);
+    const float4* qw = reinterpret_cast<const float4*>(s.qw);
+    const float4* qx = reinterpret_cast<const float4*>(s.qx);
+    const float4* qy = reinterpret_cast<const float4*>(s.qy);
+    const float4* qz = reinterpret_cast<const float4*>(s.qz);
+    for (int i4 = blockIdx.x * kThreads + threadIdx.x; i4 < n4;
+         i4 += gridDim.x * kThreads) {
+        const float4 X = px[i4], Y = py[i4], Z = pz[i4];
+        const float4 QW = qw[i4], QX = qx[i4], QY = qy[i4], QZ = qz[i4];
+        float4 W;
+        if (wmode == WMODE_STORED) {
+            W = reinterpret_cast<const float4*>(w)[i4];
+        } else if (wmode == WMODE_UNIFORM) {
+            W = make_float4(wuni, wuni, wuni, wuni);
+        } else {
+            const float4 L = reinterpret_cast<const float4*>(ll)[i4];
+            W = make_float4((float)(exp((double)L.x - M) / S),
+                            (float)(exp((double)L.y - M) / S),
+                            (float)(exp((double)L.z - M) / S),
+                            (float)(exp((double)L.w - M) / S));
+        }
 #pragma unroll
-        for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 4; ++c) {
+            if (4 * i4 + c >= n) break;
+            const double wd = (double)comp(W, c);
+            const double dp[3] = {(double)comp(X, c) - mp[0],
+                                  (double)comp(Y, c) - mp[1],
+                                  (double)comp(Z, c) - mp[2]};
+            int e = 0;
 #pragma unroll
-            for (int c = r; c < 3; ++c) acc[e++] += wd * dp[r] * dp[c];
-        const double q[4] = {(double)s.qw[i], (double)s.qx[i], (double)s.qy[i],
-                             (double)s.qz[i]};
-        double aav[3];
-        att_residual(qm, q, aav);
+            for (int r = 0; r < 3; ++r)
 #pragma unroll
-        for (int r = 0; r < 3; ++r)
+                for (int cc = r; cc < 3; ++cc) acc[e++] += wd * dp[r] * dp[cc];
+            const double q[4] = {(double)comp(QW, c), (double)comp(QX, c),
+                                 (double)comp(QY, c), (double)comp(QZ, c)};
+            double aav[3];
+            att_residual(qm, q, aav);
 #pragma unroll
-            for (int c = r; c < 3; ++c) acc[e++] += wd * aav[r] * aav[c];
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int cc = r; cc < 3; ++cc) acc[e++] += wd * aav[r] * aav[cc];
+        }
     }
     __shared__ double s_out[kCovN];
-    if (!block_reduce_last<kCovN>(acc, part, done, s_out)) return;
+    if (!block_reduce_last<kCovN>(acc, part, 0ull, 0, nullptr, done, s_out,
+                                  nullptr, nullptr))
+        return;
     if (threadIdx.x == 0) {
         for (int k = 0; k < kCovN; ++k) ctl->covs[k] = s_out[k];
         ctl->cov_mean_p[0] = mpf.x;
@@ -247,7 +352,7 @@ __global__ void k_materialize_w(int n, const float* __restrict__ ll,
 __global__ void k_set_stored(CycleCtl* ctl) { ctl->wmode = WMODE_STORED; }
 
 int est_grid(int n) {
-    int g = ceil_div(n, kThreads);
+    int g = ceil_div(ceil_div(n, 4), kThreads);
     return g < kMaxBlocks ? g : kMaxBlocks;
 }
 
@@ -256,9 +361,10 @@ int est_grid(int n) {
 int launch_est_sums(PfHandle* h, bool cycle_second) {
     KernelScope ks(h, KK_EST);
     k_est_sums<<<est_grid(h->n), kThreads, 0, h->stream>>>(
-        plane_set(h), h->n, h->d_ll, h->d_w, h->d_part, h->d_done + 1,
-        h->d_ctl, cycle_second ? 1 : 0);
+        plane_set(h), h->n, h->d_ll, h->d_w, h->d_part, h->d_part_u64,
+        h->d_done + 1, h->d_ctl, cycle_second ? 1 : 0);
     PFB_KL();
+    h->total_valid = true;
     return 0;
 }
 

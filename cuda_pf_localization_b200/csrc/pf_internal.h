@@ -72,6 +72,40 @@ struct CycleCtl {
     unsigned err;            // ERR_* bits
     unsigned tile_counter;   // dynamic tile ids for the look-back scan
     int live;                // which ping-pong particle set is current
+    // exact fixed-point weight total of the current weights (by-product of
+    // the estimate pass) and whether any weight is outside [0,1] / NaN
+    uint64_t w_total_fx;
+    int w_bad;
+    int heavy_count;                 // deferred long copy runs of a resample
+    unsigned long long lcg_next;     // LCG word after the running resample
+};
+
+// Fixed-point image of a normalised f32 weight: round-to-nearest-even of
+// w * 2^62 (exact in FP64 for w in [0,1]).
+__device__ __forceinline__ uint64_t weight_fx(float w) {
+    return __double2ull_rn((double)w * 0x1p62);
+}
+__device__ __forceinline__ bool weight_bad(float w) {
+    return !(w >= 0.0f) || !(w <= 1.0f);
+}
+
+// Normalised f32 weight of particle i under the cloud's weight mode.
+__device__ __forceinline__ float weight_of(int wmode, long long i, int n,
+                                           const float* __restrict__ w,
+                                           const float* __restrict__ ll,
+                                           double M, double S) {
+    if (wmode == 0) return 1.0f / (float)n;
+    if (wmode == 2) return w[i];
+    return (float)(exp((double)ll[i] - M) / S);
+}
+
+// A copy run of the resampler too long for one thread: particle j fills
+// outputs [start, end).
+struct HeavyRun {
+    int j;
+    int start;
+    int end;
+    int pad;
 };
 
 // Kernel kinds for launch accounting and CUDA-event timing.
@@ -120,6 +154,10 @@ struct PfHandle {
     uint64_t* d_scan_vals = nullptr;    // look-back tile values (agg, incl)
     double* d_part = nullptr;           // per-block partials (max over uses)
     int part_cap = 0;                   // doubles in d_part
+    unsigned long long* d_part_u64 = nullptr;  // per-block integer partials
+    HeavyRun* d_heavy = nullptr;        // deferred copy runs (n/32 + 1)
+    int heavy_cap = 0;
+    bool total_valid = false;  // ctl w_total_fx describes the current weights
     unsigned* d_done = nullptr;         // last-block counters
     CycleCtl* d_ctl = nullptr;
     CycleCtl* h_ctl = nullptr;          // pinned mirror

@@ -1,28 +1,37 @@
-// pf_resample.cu — systematic resampling with an exact fixed-point scan.
+// pf_resample.cu — systematic resampling with an exact fixed-point scan,
+// fused with the ancestor gather.
 //
 // Specification (semantics of src/cuda/pf_kernels.cu:638-676 and
 // crates/pf_core/src/cpu.rs:262-306, made exact and deterministic):
 //   W_j   = round_nearest_even(w_j * 2^62)             (u64, w_j in [0,1])
 //   C_j   = W_0 + ... + W_j                            (exact integer scan)
-//   total = (double)C_{n-1} * 2^-62;  invalid (no resample, weights reset to
-//           uniform) when C_{n-1} == 0 or any w_j is outside [0,1] / NaN
+//   T     = C_{n-1};  invalid (no resample, weights reset to uniform) when
+//           T == 0 or any w_j is outside [0,1] / NaN
 //   u01   = (lcg >> 11) * 2^-53 after lcg <- lcg*6364136223846793005
 //           + 1442695040888963407 (the reference's host LCG, advanced only
-//           for a valid total), step = total / n, u0 = u01 * step
+//           for a valid total); total = T * 2^-62, step = total / n,
+//           u0 = u01 * step
 //   t_i   = u0 + (double)i * step   (two roundings, as cpu.rs)
 //   anc_i = min(first j with C_j >= ceil(t_i * 2^62), n - 1)
 // Because C_j is an integer, C_j >= ceil(t * 2^62) is exactly C_j * 2^-62 >= t.
 //
-// Kernels: (1) single-pass scan with decoupled look-back (Merrill & Garland,
-// "Single-pass parallel prefix scan with decoupled look-back", 2016) over
-// 4096-particle tiles with dynamic tile ids and bounded spins; (2) merge-path
-// gather (Green, McColl, Bader, "GPU merge path", 2012) over the merged
-// sequence of thresholds and cumulative weights, so every thread handles the
-// same number of merge steps whatever the weight distribution; (3) uniform
-// re-injection with the reference's splitmix64 streams
+// Single pass.  The estimate pass that precedes every resample already holds
+// T (it forms sum_j W_j), so thresholds are known before the scan starts.
+// A decoupled look-back scan (Merrill & Garland, "Single-pass parallel prefix
+// scan with decoupled look-back", 2016; dynamic tile ids, warp-parallel
+// look-back, bounded spins) gives each particle j its C_{j-1} and C_j; the
+// outputs whose ancestor is j are exactly the run [cnt(C_{j-1}), cnt(C_j)),
+// cnt(X) = #{i : T_i <= X} computed in closed form from the arithmetic
+// threshold sequence and corrected against the exact T_i.  So each source
+// particle is read once, in order, and copied to its run; no cumulative
+// array is stored.  Runs longer than kHeavy (one particle holding most of
+// the weight) are appended to a list and expanded by a second, output-
+// parallel kernel, so no thread copies more than kHeavy outputs.
+//
+// Injection uses the reference's splitmix64 streams
 // (src/cuda/pf_kernels.cu:323-352), applied per particle in ascending draw
-// order so the f32 result is deterministic; (4) a one-thread commit that flips
-// the live ping-pong buffer.
+// order so the f32 result is deterministic; a one-thread commit flips the
+// live ping-pong buffer and advances the LCG.
 #include <math.h>
 
 #include "pf_internal.h"
@@ -34,29 +43,13 @@ namespace {
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 16;
 constexpr int kScanTile = kScanThreads * kScanItems;  // 4096
-constexpr int kMergeItems = 16;                       // merge steps per thread
+constexpr int kHeavy = 32;  // longest copy run a scan thread performs
 constexpr int kThreads = 256;
 
 struct PlaneSet {
     Planes s[2];
 };
 PlaneSet plane_set(const PfHandle* h) { return {h->planes(0), h->planes(1)}; }
-
-__device__ __forceinline__ float weight_of(int wmode, int i, int n,
-                                           const float* __restrict__ w,
-                                           const float* __restrict__ ll,
-                                           double M, double S) {
-    if (wmode == WMODE_UNIFORM) return 1.0f / (float)n;
-    if (wmode == WMODE_STORED) return w[i];
-    return (float)(exp((double)ll[i] - M) / S);
-}
-
-__device__ __forceinline__ uint64_t shfl_up_u64(uint64_t v, int d) {
-    unsigned lo = (unsigned)v, hi = (unsigned)(v >> 32);
-    lo = __shfl_up_sync(~0u, lo, d);
-    hi = __shfl_up_sync(~0u, hi, d);
-    return ((uint64_t)hi << 32) | lo;
-}
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
     unsigned v;
@@ -69,135 +62,23 @@ __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
                  : "memory");
 }
 
-enum : unsigned { TILE_AGG = 1u, TILE_INCL = 2u };
-
-__global__ void __launch_bounds__(kScanThreads)
-    k_scan(int n, const float* __restrict__ w, const float* __restrict__ ll,
-           uint64_t* __restrict__ cum, unsigned* flags, uint64_t* vals,
-           CycleCtl* ctl, int cond, unsigned epoch, int use_u01,
-           double u01_arg) {
-    if (cond && !ctl->resample_now) return;
-    __shared__ unsigned s_tile;
-    __shared__ uint64_t s_warp[kScanThreads / 32];
-    __shared__ uint64_t s_prefix;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) s_tile = atomicAdd(&ctl->tile_counter, 1u);
-    __syncthreads();
-    const int tile = (int)s_tile;
-    const int ntiles = ceil_div(n, kScanTile);
-    const int wmode = ctl->wmode;
-    const double M = ctl->ll_max, S = ctl->ll_sumexp;
-
-    // Load and convert this thread's 16 consecutive weights.
-    const long long base = (long long)tile * kScanTile + tid * kScanItems;
-    uint64_t v[kScanItems];
-    bool bad = false;
-    uint64_t run = 0;
-#pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        const long long j = base + k;
-        uint64_t W = 0;
-        if (j < n) {
-            const float wf = weight_of(wmode, (int)j, n, w, ll, M, S);
-            if (!(wf >= 0.0f) || !(wf <= 1.0f)) {
-                bad = true;
-            } else {
-                W = __double2ull_rn((double)wf * 0x1p62);
-            }
-        }
-        run += W;
-        v[k] = run;
-    }
-    // Block exclusive scan of the thread totals.
-    uint64_t x = run;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        uint64_t y = shfl_up_u64(x, d);
-        if (lane >= d) x += y;
-    }
-    if (lane == 31) s_warp[warp] = x;
-    const int any_bad = __syncthreads_or(bad ? 1 : 0);
-    if (tid == 0) {
-        uint64_t acc = 0;
-        for (int k = 0; k < kScanThreads / 32; ++k) {
-            uint64_t t = s_warp[k];
-            s_warp[k] = acc;
-            acc += t;
-        }
-        // acc = tile aggregate; publish and look back.
-        if (any_bad) atomicOr(&ctl->err, ERR_SCAN_OVERFLOW);
-        uint64_t prefix = 0;
-        if (tile == 0) {
-            vals[1] = acc;
-            __threadfence();
-            st_release(&flags[0], (epoch << 2) | TILE_INCL);
-        } else {
-            vals[2 * (size_t)tile] = acc;
-            __threadfence();
-            st_release(&flags[tile], (epoch << 2) | TILE_AGG);
-            int j = tile - 1;
-            int spins = 0;
-            while (j >= 0) {
-                const unsigned f = ld_acquire(&flags[j]);
-                if ((f >> 2) != epoch || (f & 3u) == 0u) {
-                    if (++spins > kSpinLimit) {
-                        atomicOr(&ctl->err, ERR_SPIN_TIMEOUT);
-                        break;
-                    }
-                    continue;
-                }
-                if ((f & 3u) == TILE_INCL) {
-                    prefix += __ldcg(&vals[2 * (size_t)j + 1]);
-                    break;
-                }
-                prefix += __ldcg(&vals[2 * (size_t)j]);
-                --j;
-            }
-            vals[2 * (size_t)tile + 1] = prefix + acc;
-            __threadfence();
-            st_release(&flags[tile], (epoch << 2) | TILE_INCL);
-        }
-        s_prefix = prefix;
-        if (tile == ntiles - 1) {
-            // Last tile: every predecessor has published, so the error bits
-            // of all tiles are visible here.
-            const uint64_t T = prefix + acc;
-            const bool ok = (T != 0) && !(atomicOr(&ctl->err, 0u) &
-                                          (ERR_SCAN_OVERFLOW | ERR_SPIN_TIMEOUT));
-            ctl->total_fx = T;
-            ctl->resample_valid = ok ? 1 : 0;
-            if (ok) {
-                double u01;
-                if (use_u01) {
-                    u01 = u01_arg;
-                } else {
-                    unsigned long long l = ctl->lcg;
-                    l = l * 6364136223846793005ull + 1442695040888963407ull;
-                    ctl->lcg = l;
-                    u01 = (double)(l >> 11) * (1.0 / 9007199254740992.0);
-                }
-                const double total = (double)T * 0x1p-62;
-                const double step = total / (double)n;
-                ctl->total = total;
-                ctl->step = step;
-                ctl->u0 = u01 * step;
-            } else {
-                ctl->total = (double)T * 0x1p-62;
-                ctl->wmode = WMODE_UNIFORM;
-            }
-        }
-    }
-    __syncthreads();
-    const uint64_t off = s_prefix + s_warp[warp] + (x - run);
-#pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        const long long j = base + k;
-        if (j < n) cum[j] = off + v[k];
-    }
+__device__ __forceinline__ uint64_t shfl_up_u64(uint64_t v, int d) {
+    unsigned lo = (unsigned)v, hi = (unsigned)(v >> 32);
+    lo = __shfl_up_sync(~0u, lo, d);
+    hi = __shfl_up_sync(~0u, hi, d);
+    return ((uint64_t)hi << 32) | lo;
 }
 
+__device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(~0u, v, o);
+    return v;
+}
+
+enum : unsigned { TILE_AGG = 1u, TILE_INCL = 2u };
+
 // Fixed-point threshold of output i (see the specification above).
-__device__ __forceinline__ uint64_t threshold_fx(int i, double u0,
+__device__ __forceinline__ uint64_t threshold_fx(long long i, double u0,
                                                  double step) {
     const double t = __dadd_rn(u0, __dmul_rn((double)i, step));
     const double s = t * 0x1p62;
@@ -206,49 +87,248 @@ __device__ __forceinline__ uint64_t threshold_fx(int i, double u0,
     return __double2ull_ru(s);
 }
 
-__global__ void __launch_bounds__(kThreads)
-    k_gather(PlaneSet ps, int n, const uint64_t* __restrict__ cum,
-             int* __restrict__ anc_out, int record_anc, CycleCtl* ctl,
-             int cond) {
+// cnt(X) = number of outputs i in [0, n) with threshold_fx(i) <= X.  The
+// thresholds are non-decreasing in i, so this is one more than the last such
+// index; it is estimated from the arithmetic sequence and then corrected
+// against the exact thresholds.
+__device__ __forceinline__ long long count_le(uint64_t X, int n, double u0,
+                                              double step) {
+    const double e = floor(((double)X * 0x1p-62 - u0) / step);
+    long long i;
+    if (!(e >= -1.0))
+        i = -1;
+    else if (e > (double)(n - 1))
+        i = n - 1;
+    else
+        i = (long long)e;
+    while (i + 1 <= n - 1 && threshold_fx(i + 1, u0, step) <= X) ++i;
+    while (i >= 0 && threshold_fx(i, u0, step) > X) --i;
+    return i + 1;
+}
+
+__device__ __forceinline__ void copy_particle(const Planes& src, const Planes& dst,
+                                              int j, long long s, long long e,
+                                              int* anc, int record) {
+    const float x = src.px[j], y = src.py[j], z = src.pz[j];
+    const float a = src.qw[j], b = src.qx[j], c = src.qy[j], d = src.qz[j];
+    for (long long i = s; i < e; ++i) {
+        dst.px[i] = x;
+        dst.py[i] = y;
+        dst.pz[i] = z;
+        dst.qw[i] = a;
+        dst.qx[i] = b;
+        dst.qy[i] = c;
+        dst.qz[i] = d;
+        if (record) anc[i] = j;
+    }
+}
+
+// Warp-parallel look-back (run by warp 0 of a tile > 0): returns the sum of
+// all predecessors' weights.  Lane l inspects tile base - l; the nearest
+// predecessor that already knows its inclusive prefix ends the walk.
+__device__ uint64_t look_back(const unsigned* flags, const uint64_t* vals,
+                              int tile, unsigned epoch, CycleCtl* ctl) {
+    const int lane = threadIdx.x & 31;
+    uint64_t prefix = 0;
+    int base = tile - 1;
+    int spins = 0;
+    for (;;) {
+        const int j = base - lane;
+        unsigned f = 0;
+        bool ready = true;
+        if (j >= 0) {
+            f = ld_acquire(&flags[j]);
+            ready = (f >> 2) == epoch && (f & 3u) != 0u;
+        }
+        if (!__all_sync(~0u, ready)) {
+            if (++spins > kSpinLimit) {
+                if (lane == 0) atomicOr(&ctl->err, ERR_SPIN_TIMEOUT);
+                return prefix;
+            }
+            continue;
+        }
+        const unsigned incl = __ballot_sync(~0u, j < 0 || (f & 3u) == TILE_INCL);
+        const int first = incl ? __ffs(incl) - 1 : 31;
+        uint64_t v = 0;
+        if (lane <= first && j >= 0)
+            v = (lane == first && incl) ? __ldcg(&vals[2 * (size_t)j + 1])
+                                        : __ldcg(&vals[2 * (size_t)j]);
+        prefix += warp_sum_u64(v);
+        if (incl) return prefix;
+        base -= 32;
+    }
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    k_resample(PlaneSet ps, int n, const float* __restrict__ w,
+               const float* __restrict__ ll, unsigned* flags, uint64_t* vals,
+               int* __restrict__ anc, int record, HeavyRun* heavy,
+               int heavy_cap, CycleCtl* ctl, int cond, unsigned epoch,
+               int use_u01, double u01_arg) {
     if (cond && !ctl->resample_now) return;
-    if (!ctl->resample_valid) return;
-    const double u0 = ctl->u0, step = ctl->step;
+    const uint64_t T = ctl->w_total_fx;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (T == 0 || ctl->w_bad) {
+        if (blockIdx.x == 0 && tid == 0) ctl->resample_valid = 0;
+        return;
+    }
+    // Offsets: every block derives the same values from T and the LCG.
+    const unsigned long long lcg0 = ctl->lcg;
+    const unsigned long long lcg1 =
+        use_u01 ? lcg0 : lcg0 * 6364136223846793005ull + 1442695040888963407ull;
+    const double u01 =
+        use_u01 ? u01_arg : (double)(lcg1 >> 11) * (1.0 / 9007199254740992.0);
+    const double total = (double)T * 0x1p-62;
+    const double step = total / (double)n;
+    const double u0 = u01 * step;
+    __shared__ unsigned s_tile;
+    __shared__ uint64_t s_warp[kScanThreads / 32];
+    __shared__ uint64_t s_prefix, s_agg;
+    if (tid == 0) {
+        s_tile = atomicAdd(&ctl->tile_counter, 1u);
+        if (blockIdx.x == 0) {
+            ctl->lcg_next = lcg1;
+            ctl->resample_valid = 1;
+            ctl->total_fx = T;
+            ctl->total = total;
+            ctl->step = step;
+            ctl->u0 = u0;
+        }
+    }
+    __syncthreads();
+    const int tile = (int)s_tile;
+    const int wmode = ctl->wmode;
+    const double M = ctl->ll_max, S = ctl->ll_sumexp;
     const int live = ctl->live;
     const Planes src = ps.s[live], dst = ps.s[1 - live];
-    const long long g = (long long)blockIdx.x * kThreads + threadIdx.x;
-    const long long diag = g * kMergeItems;
-    const long long total_len = 2LL * n;
-    if (diag >= total_len) return;
-    // Merge-path split of the first `diag` merged items: thresholds A_i
-    // precede cumulative values B_j when A_i <= B_j.
-    long long lo = diag > n ? diag - n : 0;
-    long long hi = diag < n ? diag : n;
-    while (lo < hi) {
-        const long long mid = (lo + hi) >> 1;
-        if (threshold_fx((int)mid, u0, step) <= __ldg(&cum[diag - 1 - mid]))
-            lo = mid + 1;
-        else
-            hi = mid;
-    }
-    long long a = lo, b = diag - lo;
-    uint64_t ta = a < n ? threshold_fx((int)a, u0, step) : 0ull;
-    for (int it = 0; it < kMergeItems && a + b < total_len; ++it) {
-        if (a < n && (b >= n || ta <= __ldg(&cum[b]))) {
-            const int j = (int)(b < n ? b : n - 1);
-            const int i = (int)a;
-            dst.px[i] = src.px[j];
-            dst.py[i] = src.py[j];
-            dst.pz[i] = src.pz[j];
-            dst.qw[i] = src.qw[j];
-            dst.qx[i] = src.qx[j];
-            dst.qy[i] = src.qy[j];
-            dst.qz[i] = src.qz[j];
-            if (record_anc) anc_out[i] = j;
-            ++a;
-            if (a < n) ta = threshold_fx((int)a, u0, step);
-        } else {
-            ++b;
+
+    // This thread's 16 consecutive weights -> inclusive fixed-point sums.
+    const long long j0 = (long long)tile * kScanTile + tid * kScanItems;
+    uint64_t v[kScanItems];
+    uint64_t run = 0;
+    if (wmode == WMODE_STORED && j0 + kScanItems <= n) {
+        const float4* w4 = reinterpret_cast<const float4*>(w + j0);
+#pragma unroll
+        for (int q = 0; q < kScanItems / 4; ++q) {
+            const float4 a = w4[q];
+            run += weight_fx(a.x);
+            v[4 * q] = run;
+            run += weight_fx(a.y);
+            v[4 * q + 1] = run;
+            run += weight_fx(a.z);
+            v[4 * q + 2] = run;
+            run += weight_fx(a.w);
+            v[4 * q + 3] = run;
         }
+    } else {
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) {
+            const long long j = j0 + k;
+            if (j < n) run += weight_fx(weight_of(wmode, j, n, w, ll, M, S));
+            v[k] = run;
+        }
+    }
+    // Block scan of the thread totals.
+    uint64_t x = run;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint64_t y = shfl_up_u64(x, d);
+        if (lane >= d) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (tid == 0) {
+        uint64_t acc = 0;
+        for (int k = 0; k < kScanThreads / 32; ++k) {
+            const uint64_t t = s_warp[k];
+            s_warp[k] = acc;
+            acc += t;
+        }
+        s_agg = acc;
+        if (tile == 0) {
+            vals[1] = acc;
+            __threadfence();
+            st_release(&flags[0], (epoch << 2) | TILE_INCL);
+            s_prefix = 0;
+        } else {
+            vals[2 * (size_t)tile] = acc;
+            __threadfence();
+            st_release(&flags[tile], (epoch << 2) | TILE_AGG);
+        }
+    }
+    __syncthreads();
+    if (tile > 0 && warp == 0) {
+        const uint64_t prefix = look_back(flags, vals, tile, epoch, ctl);
+        if (lane == 0) {
+            vals[2 * (size_t)tile + 1] = prefix + s_agg;
+            __threadfence();
+            st_release(&flags[tile], (epoch << 2) | TILE_INCL);
+            s_prefix = prefix;
+        }
+    }
+    __syncthreads();
+
+    // Copy runs.  C_{j0-1} = prefix + exclusive offset of this thread.
+    const uint64_t c_prev = s_prefix + s_warp[warp] + (x - run);
+    long long s = (j0 == 0) ? 0 : count_le(c_prev, n, u0, step);
+#pragma unroll 1
+    for (int k = 0; k < kScanItems; ++k) {
+        const long long j = j0 + k;
+        if (j >= n) break;
+        const long long e =
+            (j == n - 1) ? (long long)n : count_le(c_prev + v[k], n, u0, step);
+        const long long cnt = e - s;
+        if (cnt > kHeavy) {
+            const int slot = atomicAdd(&ctl->heavy_count, 1);
+            if (slot < heavy_cap)
+                heavy[slot] = HeavyRun{(int)j, (int)s, (int)e, 0};
+            else
+                atomicOr(&ctl->err, ERR_SCAN_OVERFLOW);
+        } else if (cnt > 0) {
+            copy_particle(src, dst, (int)j, s, e, anc, record);
+        }
+        s = e;
+    }
+}
+
+// Output-parallel expansion of the long runs: a run of at least kSplit
+// outputs is spread over the whole grid, shorter ones take one block each.
+constexpr int kSplit = 8192;
+
+__device__ __forceinline__ void fill_range(const Planes& src, const Planes& dst,
+                                           int j, int lo, int hi, int stride,
+                                           int* anc, int record) {
+    const float x = src.px[j], y = src.py[j], z = src.pz[j];
+    const float a = src.qw[j], b = src.qx[j], c = src.qy[j], d = src.qz[j];
+    for (int i = lo; i < hi; i += stride) {
+        dst.px[i] = x;
+        dst.py[i] = y;
+        dst.pz[i] = z;
+        dst.qw[i] = a;
+        dst.qx[i] = b;
+        dst.qy[i] = c;
+        dst.qz[i] = d;
+        if (record) anc[i] = j;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_expand_runs(PlaneSet ps, const HeavyRun* heavy, int heavy_cap,
+                  int* __restrict__ anc, int record, CycleCtl* ctl, int cond) {
+    if (cond && !ctl->resample_now) return;
+    if (!ctl->resample_valid) return;
+    const int count = min(ctl->heavy_count, heavy_cap);
+    const int live = ctl->live;
+    const Planes src = ps.s[live], dst = ps.s[1 - live];
+    const int gthreads = gridDim.x * kThreads;
+    const int gid = blockIdx.x * kThreads + threadIdx.x;
+    for (int r = 0; r < count; ++r) {
+        const HeavyRun h = heavy[r];
+        if (h.end - h.start >= kSplit)
+            fill_range(src, dst, h.j, h.start + gid, h.end, gthreads, anc, record);
+        else if (r % (int)gridDim.x == (int)blockIdx.x)
+            fill_range(src, dst, h.j, h.start + (int)threadIdx.x, h.end, kThreads,
+                       anc, record);
     }
 }
 
@@ -296,7 +376,7 @@ __global__ void k_inject_link(int n, int k, uint64_t gen, uint64_t* head,
     if (!ctl->resample_valid) return;
     const int j = blockIdx.x * kThreads + threadIdx.x;
     if (j >= k) return;
-    const InjDraw d = inj_draw(ctl->lcg, gen, j, n);
+    const InjDraw d = inj_draw(ctl->lcg_next, gen, j, n);
     const uint64_t tag = ((uint64_t)epoch << 32) | (uint32_t)j;
     const uint64_t prev = atomicExch((unsigned long long*)&head[d.idx],
                                      (unsigned long long)tag);
@@ -310,7 +390,7 @@ __global__ void k_inject_apply(PlaneSet ps, int n, int k, uint64_t gen,
     if (!ctl->resample_valid) return;
     const int j = blockIdx.x * kThreads + threadIdx.x;
     if (j >= k) return;
-    const uint64_t lcg = ctl->lcg;
+    const uint64_t lcg = ctl->lcg_next;
     const InjDraw d = inj_draw(lcg, gen, j, n);
     const uint64_t h = head[d.idx];
     if ((uint32_t)(h >> 32) != epoch || (int)(uint32_t)h != j) return;
@@ -340,10 +420,12 @@ __global__ void k_commit(CycleCtl* ctl, int cond) {
         if (ctl->resample_valid) {
             ctl->live = 1 - ctl->live;
             ctl->resampled = 1;
+            ctl->lcg = ctl->lcg_next;
         }
         ctl->wmode = WMODE_UNIFORM;
     }
     ctl->tile_counter = 0u;
+    ctl->heavy_count = 0;
     ctl->err &= ~ERR_SCAN_OVERFLOW;
 }
 
@@ -372,25 +454,27 @@ int launch_resample(PfHandle* h, float inject_ratio, bool cond_on_ctl,
                     bool use_u01, double u01) {
     const int n = h->n;
     const int ntiles = ceil_div(n, kScanTile);
+    // The weight total comes from the estimate pass; run one when the
+    // weights changed since the last.
+    if (!h->total_valid && launch_est_sums(h, false)) return -1;
     // Look-back epochs are per handle and fit in 30 bits; 0 is never used.
     h->scan_epoch = (h->scan_epoch + 1u) & 0x3FFFFFFFu;
     if (h->scan_epoch == 0u) h->scan_epoch = 1u;
     const unsigned epoch = h->scan_epoch;
     const int cond = cond_on_ctl ? 1 : 0;
+    const int rec = h->record_anc ? 1 : 0;
     {
         KernelScope ks(h, KK_SCAN);
-        k_scan<<<ntiles, kScanThreads, 0, h->stream>>>(
-            n, h->d_w, h->d_ll, h->d_cum, h->d_scan_flags, h->d_scan_vals,
-            h->d_ctl, cond, epoch, use_u01 ? 1 : 0, u01);
+        k_resample<<<ntiles, kScanThreads, 0, h->stream>>>(
+            plane_set(h), n, h->d_w, h->d_ll, h->d_scan_flags, h->d_scan_vals,
+            h->d_anc, rec, h->d_heavy, h->heavy_cap, h->d_ctl, cond, epoch,
+            use_u01 ? 1 : 0, u01);
     }
     PFB_KL();
-    const long long merge_threads = ceil_div_ll(2LL * n, kMergeItems);
-    const int mgrid = (int)ceil_div_ll(merge_threads, kThreads);
     {
         KernelScope ks(h, KK_GATHER);
-        k_gather<<<mgrid, kThreads, 0, h->stream>>>(
-            plane_set(h), n, h->d_cum, h->d_anc, h->record_anc ? 1 : 0,
-            h->d_ctl, cond);
+        k_expand_runs<<<2 * 148, kThreads, 0, h->stream>>>(
+            plane_set(h), h->d_heavy, h->heavy_cap, h->d_anc, rec, h->d_ctl, cond);
     }
     PFB_KL();
     // k = floor(ratio * n) with the reference's f32 product
@@ -422,6 +506,9 @@ int launch_resample(PfHandle* h, float inject_ratio, bool cond_on_ctl,
     }
     PFB_KL();
     h->anc_valid = h->record_anc;
+    // The weights are uniform afterwards; the next estimate pass recomputes
+    // their fixed-point total.
+    h->total_valid = false;
     return 0;
 }
 

@@ -93,26 +93,9 @@ __global__ void __launch_bounds__(kThreads)
     store_pose(s, i, p, q);
 }
 
-// Observation staged in shared memory: landmark resolved through the dense
-// table, kind 0 = skipped (id outside the table), 1 = Cartesian, 2 = range +
-// bearing.  a = (lx, ly, lz, kind bits), b = (dx, dy, dz, range).
-__device__ __forceinline__ void stage_obs(const CObservation* __restrict__ obs,
-                                          const float* __restrict__ lm,
-                                          int lm_count, int k, float4* sa,
-                                          float4* sb) {
-    CObservation o = obs[k];
-    float4 a, b;
-    if (o.id < 0 || o.id >= lm_count) {
-        a = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
-    } else {
-        a = make_float4(lm[3 * o.id], lm[3 * o.id + 1], lm[3 * o.id + 2],
-                        __int_as_float(o.mode == 0 ? 1 : 2));
-    }
-    b = make_float4(o.dx, o.dy, o.dz, o.range);
-    *sa = a;
-    *sb = b;
-}
-
+// Observations staged in shared memory: the landmark resolved through the
+// dense table and the observation, a = (lx, ly, lz, kind bits) with kind 1 =
+// Cartesian, 2 = range + bearing; b = (dx, dy, dz, range).
 struct GateConsts {
     float inv2rr, inv2bb, g2, cart_gate2, rng_gate2, brg_gate2, cart_out,
         half_out, gate;
@@ -181,8 +164,10 @@ __device__ __forceinline__ double warp_max_d(double v) {
     return v;
 }
 
-// Softmax partial of one block + the last-block combine.
-__device__ __forceinline__ void softmax_partials(float acc, bool valid,
+// Softmax partial of one block (two log-likelihoods per thread) + the
+// last-block combine.
+__device__ __forceinline__ void softmax_partials(float acc0, bool v0,
+                                                 float acc1, bool v1,
                                                  double2* part,
                                                  unsigned* done,
                                                  CycleCtl* ctl) {
@@ -191,7 +176,7 @@ __device__ __forceinline__ void softmax_partials(float acc, bool valid,
     __shared__ double s_bm;
     __shared__ bool s_last;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    float m = warp_max_f(valid ? acc : -INFINITY);
+    float m = warp_max_f(fmaxf(v0 ? acc0 : -INFINITY, v1 ? acc1 : -INFINITY));
     if (lane == 0) s_m[warp] = m;
     __syncthreads();
     if (tid == 0) {
@@ -201,7 +186,7 @@ __device__ __forceinline__ void softmax_partials(float acc, bool valid,
     }
     __syncthreads();
     const double bm = s_bm;
-    double e = valid ? exp((double)acc - bm) : 0.0;
+    double e = (v0 ? exp((double)acc0 - bm) : 0.0) + (v1 ? exp((double)acc1 - bm) : 0.0);
     e = warp_sum_d(e);
     if (lane == 0) s_s[warp] = e;
     __syncthreads();
@@ -218,6 +203,7 @@ __device__ __forceinline__ void softmax_partials(float acc, bool valid,
     // Combine: M = max block max, S = sum_b exp(m_b - M) * s_b.
     const int G = gridDim.x;
     double mx = -INFINITY;
+#pragma unroll 4
     for (int b = tid; b < G; b += kThreads) mx = fmax(mx, __ldcg(&part[b].x));
     mx = warp_max_d(mx);
     __shared__ double s_d[kThreads / 32];
@@ -231,6 +217,7 @@ __device__ __forceinline__ void softmax_partials(float acc, bool valid,
     __syncthreads();
     const double M = s_bm;
     double sum = 0.0;
+#pragma unroll 4
     for (int b = tid; b < G; b += kThreads) {
         double2 pb = __ldcg(&part[b]);
         sum += exp(pb.x - M) * pb.y;
@@ -251,6 +238,62 @@ __device__ __forceinline__ void softmax_partials(float acc, bool valid,
     }
 }
 
+// Stage observations [c0, c0 + cn) into shared memory, dropping the ones
+// whose id is outside the landmark table (the reference skips them with
+// `continue`, pf_kernels.cu:242) and keeping the order of the rest, so the
+// f32 accumulation order is unchanged.  Returns the number kept; *all_cart
+// is set when every kept observation is Cartesian.
+__device__ __forceinline__ int stage_chunk(const CObservation* __restrict__ obs,
+                                           const float* __restrict__ lm,
+                                           int lm_count, int c0, int cn,
+                                           float4* s_a, float4* s_b,
+                                           bool* all_cart) {
+    __shared__ int s_wcount[kThreads / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    CObservation o;
+    bool keep = false;
+    if (tid < cn) {
+        o = obs[c0 + tid];
+        keep = o.id >= 0 && o.id < lm_count;
+    }
+    const unsigned ballot = __ballot_sync(~0u, keep);
+    if (lane == 0) s_wcount[warp] = __popc(ballot);
+    const int cart = __syncthreads_and(!keep || o.mode == 0);
+    int off = 0, total = 0;
+    for (int k = 0; k < kThreads / 32; ++k) {
+        const int c = s_wcount[k];
+        off += (k < warp) ? c : 0;
+        total += c;
+    }
+    if (keep) {
+        const int slot = off + __popc(ballot & ((1u << lane) - 1u));
+        s_a[slot] = make_float4(lm[3 * o.id], lm[3 * o.id + 1], lm[3 * o.id + 2],
+                                __int_as_float(o.mode == 0 ? 1 : 2));
+        s_b[slot] = make_float4(o.dx, o.dy, o.dz, o.range);
+    }
+    *all_cart = cart != 0;
+    __syncthreads();
+    return total;
+}
+
+// Gated Cartesian term of the reference (pf_kernels.cu:247-252) for the
+// specialised all-Cartesian loop; gate > 0 is hoisted out as kGated.
+template <bool kGated>
+__device__ __forceinline__ void cart_term(const GateConsts& g, float3 p,
+                                          const Quat& qc, float4 a, float4 b,
+                                          float& acc) {
+    float3 d = make_float3(a.x - p.x, a.y - p.y, a.z - p.z);
+    float3 pred = q_rotate(qc, d);
+    float ex = pred.x - b.x, ey = pred.y - b.y, ez = pred.z - b.z;
+    float r2 = ex * ex + ey * ey + ez * ez;
+    if (kGated)
+        acc += (r2 > g.cart_gate2) ? g.cart_out : -r2 * g.inv2rr;
+    else
+        acc += -r2 * g.inv2rr;
+}
+
+// Two particles per thread (i and i + 256): every staged observation read
+// from shared memory serves both.
 template <bool kPredict>
 __global__ void __launch_bounds__(kThreads)
     k_weight(PlaneSet ps, int n, uint64_t seed, PredictArgs pa,
@@ -261,37 +304,59 @@ __global__ void __launch_bounds__(kThreads)
     __shared__ float4 s_a[kObsChunk];
     __shared__ float4 s_b[kObsChunk];
     const Planes s = ps.s[ctl->live];
-    const int i = blockIdx.x * kThreads + threadIdx.x;
-    const bool valid = i < n;
-    float3 p = make_float3(0.f, 0.f, 0.f);
-    Quat q = {1.f, 0.f, 0.f, 0.f};
-    if (valid) {
-        load_pose(s, i, p, q);
+    const int i0 = blockIdx.x * (2 * kThreads) + threadIdx.x;
+    const int i1 = i0 + kThreads;
+    const bool v0 = i0 < n, v1 = i1 < n;
+    float3 p0 = make_float3(0.f, 0.f, 0.f), p1 = p0;
+    Quat q0 = {1.f, 0.f, 0.f, 0.f}, q1 = q0;
+    if (v0) {
+        load_pose(s, i0, p0, q0);
         if (kPredict) {
-            apply_predict(pa, seed, i, p, q);
-            store_pose(s, i, p, q);
+            apply_predict(pa, seed, i0, p0, q0);
+            store_pose(s, i0, p0, q0);
+        }
+    }
+    if (v1) {
+        load_pose(s, i1, p1, q1);
+        if (kPredict) {
+            apply_predict(pa, seed, i1, p1, q1);
+            store_pose(s, i1, p1, q1);
         }
     }
     const GateConsts g = gate_consts(sigma_r, sigma_b, gate);
-    const Quat qc = q_conjugate(q);
-    float acc = 0.0f;
+    const Quat qc0 = q_conjugate(q0), qc1 = q_conjugate(q1);
+    float acc0 = 0.0f, acc1 = 0.0f;
     for (int c0 = 0; c0 < nobs; c0 += kObsChunk) {
-        const int cn = min(kObsChunk, nobs - c0);
+        bool all_cart;
         __syncthreads();
-        for (int k = threadIdx.x; k < cn; k += kThreads)
-            stage_obs(obs, lm, lm_count, c0 + k, &s_a[k], &s_b[k]);
-        __syncthreads();
-        if (valid) {
+        const int cn = stage_chunk(obs, lm, lm_count, c0, min(kObsChunk, nobs - c0),
+                                   s_a, s_b, &all_cart);
+        if (all_cart && gate > 0.0f) {
+#pragma unroll 2
             for (int k = 0; k < cn; ++k) {
-                const float4 a = s_a[k];
+                const float4 a = s_a[k], b = s_b[k];
+                cart_term<true>(g, p0, qc0, a, b, acc0);
+                cart_term<true>(g, p1, qc1, a, b, acc1);
+            }
+        } else if (all_cart) {
+#pragma unroll 2
+            for (int k = 0; k < cn; ++k) {
+                const float4 a = s_a[k], b = s_b[k];
+                cart_term<false>(g, p0, qc0, a, b, acc0);
+                cart_term<false>(g, p1, qc1, a, b, acc1);
+            }
+        } else {
+            for (int k = 0; k < cn; ++k) {
+                const float4 a = s_a[k], b = s_b[k];
                 const int kind = __float_as_int(a.w);
-                if (kind == 0) continue;
-                obs_loglik(g, p, qc, a, s_b[k], kind, acc);
+                obs_loglik(g, p0, qc0, a, b, kind, acc0);
+                obs_loglik(g, p1, qc1, a, b, kind, acc1);
             }
         }
     }
-    if (valid) ll[i] = acc;
-    softmax_partials(acc, valid, part, done, ctl);
+    if (v0) ll[i0] = acc0;
+    if (v1) ll[i1] = acc1;
+    softmax_partials(acc0, v0, acc1, v1, part, done, ctl);
 }
 
 }  // namespace
@@ -320,7 +385,7 @@ int launch_predict(PfHandle* h, const PredictArgs& pa) {
 
 int launch_weight(PfHandle* h, const PredictArgs& pa, const CObservation* d_obs,
                   int nobs, float sigma_r, float sigma_b, float gate) {
-    const int grid = ceil_div(h->n, kThreads);
+    const int grid = ceil_div(h->n, 2 * kThreads);
     double2* part = reinterpret_cast<double2*>(h->d_part);
     KernelScope ks(h, KK_WEIGHT);
     if (pa.enabled) {
