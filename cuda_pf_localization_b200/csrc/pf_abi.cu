@@ -84,9 +84,6 @@ namespace {
 
 constexpr int kThreads = 256;
 
-struct PlaneSet {
-    Planes s[2];
-};
 PlaneSet plane_set(const PfHandle* h) { return {h->planes(0), h->planes(1)}; }
 
 __global__ void k_ctl_reset(CycleCtl* ctl, int first) {
@@ -103,7 +100,7 @@ __global__ void k_pack(PlaneSet ps, int n, float* pos3, float* quat4,
                        const CycleCtl* ctl) {
     const int i = blockIdx.x * kThreads + threadIdx.x;
     if (i >= n) return;
-    const Planes s = ps.s[ctl->live];
+    const Planes s = pick_planes(ps, ctl->live);
     pos3[3 * i] = s.px[i];
     pos3[3 * i + 1] = s.py[i];
     pos3[3 * i + 2] = s.pz[i];
@@ -117,7 +114,7 @@ __global__ void k_unpack(PlaneSet ps, int n, const float* pos3,
                          const float* quat4, const CycleCtl* ctl) {
     const int i = blockIdx.x * kThreads + threadIdx.x;
     if (i >= n) return;
-    const Planes s = ps.s[ctl->live];
+    const Planes s = pick_planes(ps, ctl->live);
     s.px[i] = pos3[3 * i];
     s.py[i] = pos3[3 * i + 1];
     s.pz[i] = pos3[3 * i + 2];

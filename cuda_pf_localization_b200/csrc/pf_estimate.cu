@@ -31,9 +31,6 @@ constexpr int kThreads = 256;
 // small grid also keeps the last block's combine short.
 constexpr int kMaxBlocks = 2 * 148;
 
-struct PlaneSet {
-    Planes s[2];
-};
 PlaneSet plane_set(const PfHandle* h) { return {h->planes(0), h->planes(1)}; }
 
 __device__ __forceinline__ double warp_sum_d(double v) {
@@ -125,7 +122,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                float* __restrict__ w, double* part, unsigned long long* partu,
                unsigned* done, CycleCtl* ctl, int cond_second) {
     if (cond_second && !ctl->resample_now) return;
-    const Planes s = ps.s[ctl->live];
+    const Planes s = pick_planes(ps, ctl->live);
     const int wmode = ctl->wmode;
     const double M = ctl->ll_max, S = ctl->ll_sumexp;
     const float wuni = 1.0f / (float)n;
@@ -235,7 +232,7 @@ __global__ void __launch_bounds__(kThreads, 2)
            CycleCtl* ctl, int use_args, float3 mp_arg, float4 mq_arg,
            int mode, double ess_ratio) {
     if (mode == 2 && !ctl->resample_now) return;
-    const Planes s = ps.s[ctl->live];
+    const Planes s = pick_planes(ps, ctl->live);
     const int wmode = ctl->wmode;
     const double M = ctl->ll_max, S = ctl->ll_sumexp;
     const float wuni = 1.0f / (float)n;

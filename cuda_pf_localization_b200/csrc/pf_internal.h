@@ -6,9 +6,9 @@
 //   state[2]  ping-pong particle sets: px py pz qw qx qy qz   (7 planes)
 //   ll        f32 log-likelihood of the last weighting          (1 plane)
 //   w         f32 normalised weight (materialised on demand)    (1 plane)
-//   cum       u64 fixed-point inclusive weight scan (resample)  (n words)
 //   anc       i32 ancestor of each particle in the last resample
 //   inj_head  u64 epoch-tagged injection list heads (one per particle)
+//   inj_next  i32 injection list links
 // plus small per-block partial buffers and one CycleCtl control block.
 #pragma once
 
@@ -107,6 +107,26 @@ struct HeavyRun {
     int end;
     int pad;
 };
+
+// Both ping-pong particle sets, passed to kernels by value.
+struct PlaneSet {
+    Planes s[2];
+};
+
+// Select a set with a register select rather than an indexed parameter
+// array (indexing the kernel parameter array with a run-time value makes
+// the compiler copy it to local memory).
+__device__ __forceinline__ Planes pick_planes(const PlaneSet& ps, int which) {
+    Planes p;
+    p.px = which ? ps.s[1].px : ps.s[0].px;
+    p.py = which ? ps.s[1].py : ps.s[0].py;
+    p.pz = which ? ps.s[1].pz : ps.s[0].pz;
+    p.qw = which ? ps.s[1].qw : ps.s[0].qw;
+    p.qx = which ? ps.s[1].qx : ps.s[0].qx;
+    p.qy = which ? ps.s[1].qy : ps.s[0].qy;
+    p.qz = which ? ps.s[1].qz : ps.s[0].qz;
+    return p;
+}
 
 // Kernel kinds for launch accounting and CUDA-event timing.
 enum KernelKind : int {

@@ -46,9 +46,6 @@ constexpr int kScanTile = kScanThreads * kScanItems;  // 4096
 constexpr int kHeavy = 32;  // longest copy run a scan thread performs
 constexpr int kThreads = 256;
 
-struct PlaneSet {
-    Planes s[2];
-};
 PlaneSet plane_set(const PfHandle* h) { return {h->planes(0), h->planes(1)}; }
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
@@ -200,7 +197,7 @@ __global__ void __launch_bounds__(kScanThreads)
     const int wmode = ctl->wmode;
     const double M = ctl->ll_max, S = ctl->ll_sumexp;
     const int live = ctl->live;
-    const Planes src = ps.s[live], dst = ps.s[1 - live];
+    const Planes src = pick_planes(ps, live), dst = pick_planes(ps, 1 - live);
 
     // This thread's 16 consecutive weights -> inclusive fixed-point sums.
     const long long j0 = (long long)tile * kScanTile + tid * kScanItems;
@@ -271,7 +268,7 @@ __global__ void __launch_bounds__(kScanThreads)
     // Copy runs.  C_{j0-1} = prefix + exclusive offset of this thread.
     const uint64_t c_prev = s_prefix + s_warp[warp] + (x - run);
     long long s = (j0 == 0) ? 0 : count_le(c_prev, n, u0, step);
-#pragma unroll 1
+#pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
         const long long j = j0 + k;
         if (j >= n) break;
@@ -319,7 +316,7 @@ __global__ void __launch_bounds__(kThreads)
     if (!ctl->resample_valid) return;
     const int count = min(ctl->heavy_count, heavy_cap);
     const int live = ctl->live;
-    const Planes src = ps.s[live], dst = ps.s[1 - live];
+    const Planes src = pick_planes(ps, live), dst = pick_planes(ps, 1 - live);
     const int gthreads = gridDim.x * kThreads;
     const int gid = blockIdx.x * kThreads + threadIdx.x;
     for (int r = 0; r < count; ++r) {
@@ -396,7 +393,7 @@ __global__ void k_inject_apply(PlaneSet ps, int n, int k, uint64_t gen,
     if ((uint32_t)(h >> 32) != epoch || (int)(uint32_t)h != j) return;
     // This thread inserted last for particle d.idx: apply every draw of the
     // list in ascending j (selection over the short list).
-    const Planes dst = ps.s[1 - ctl->live];
+    const Planes dst = pick_planes(ps, 1 - ctl->live);
     float px = dst.px[d.idx], py = dst.py[d.idx], pz = dst.pz[d.idx];
     int last = -1;
     for (;;) {

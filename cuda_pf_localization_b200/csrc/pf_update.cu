@@ -17,9 +17,6 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kObsChunk = 256;  // observations staged in shared memory at once
 
-struct PlaneSet {
-    Planes s[2];
-};
 
 PlaneSet plane_set(const PfHandle* h) { return {h->planes(0), h->planes(1)}; }
 
@@ -69,7 +66,7 @@ __global__ void __launch_bounds__(kThreads)
              Quat q0, float3 pstd, float3 rstd, CycleCtl* ctl) {
     const int i = blockIdx.x * kThreads + threadIdx.x;
     if (i >= n) return;
-    const Planes s = ps.s[ctl->live];
+    const Planes s = pick_planes(ps, ctl->live);
     float nz[6];
     pf_normals6(seed, gen, (uint32_t)i, nz);
     float3 p = make_float3(p0.x + pstd.x * nz[0], p0.y + pstd.y * nz[1],
@@ -85,7 +82,7 @@ __global__ void __launch_bounds__(kThreads)
               CycleCtl* ctl) {
     const int i = blockIdx.x * kThreads + threadIdx.x;
     if (i >= n) return;
-    const Planes s = ps.s[ctl->live];
+    const Planes s = pick_planes(ps, ctl->live);
     float3 p;
     Quat q;
     load_pose(s, i, p, q);
@@ -247,7 +244,7 @@ __device__ __forceinline__ int stage_chunk(const CObservation* __restrict__ obs,
                                            const float* __restrict__ lm,
                                            int lm_count, int c0, int cn,
                                            float4* s_a, float4* s_b,
-                                           bool* all_cart) {
+                                           float4* s_p, bool* all_cart) {
     __shared__ int s_wcount[kThreads / 32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     CObservation o;
@@ -267,9 +264,13 @@ __device__ __forceinline__ int stage_chunk(const CObservation* __restrict__ obs,
     }
     if (keep) {
         const int slot = off + __popc(ballot & ((1u << lane) - 1u));
-        s_a[slot] = make_float4(lm[3 * o.id], lm[3 * o.id + 1], lm[3 * o.id + 2],
-                                __int_as_float(o.mode == 0 ? 1 : 2));
+        const float lx = lm[3 * o.id], ly = lm[3 * o.id + 1], lz = lm[3 * o.id + 2];
+        s_a[slot] = make_float4(lx, ly, lz, __int_as_float(o.mode == 0 ? 1 : 2));
         s_b[slot] = make_float4(o.dx, o.dy, o.dz, o.range);
+        // broadcast pairs for the packed two-particle path
+        s_p[3 * slot] = make_float4(lx, lx, ly, ly);
+        s_p[3 * slot + 1] = make_float4(lz, lz, -o.dx, -o.dx);
+        s_p[3 * slot + 2] = make_float4(-o.dy, -o.dy, -o.dz, -o.dz);
     }
     *all_cart = cart != 0;
     __syncthreads();
@@ -286,10 +287,78 @@ __device__ __forceinline__ void cart_term(const GateConsts& g, float3 p,
     float3 pred = q_rotate(qc, d);
     float ex = pred.x - b.x, ey = pred.y - b.y, ez = pred.z - b.z;
     float r2 = ex * ex + ey * ey + ez * ez;
+    // The reference rounds the product and the sum separately in both the
+    // gated and the ungated case; the ungated form uses the intrinsics that
+    // are never merged into a multiply-add.
     if (kGated)
         acc += (r2 > g.cart_gate2) ? g.cart_out : -r2 * g.inv2rr;
     else
-        acc += -r2 * g.inv2rr;
+        acc = __fadd_rn(acc, __fmul_rn(-r2, g.inv2rr));
+}
+
+// ---------------------------------------------------------- packed path
+// The Cartesian term evaluated for two particles at once with packed f32x2
+// arithmetic.  nvcc compiles the reference expression (q_rotate + squared
+// residual) with these contractions, each operation rounded once:
+//   t'  = fma(-q.z, v.y, q.y*v.z)  (likewise y, z);   t = 2 t' exactly
+//   c.x = fma(-q.z, t.y, q.y*t.z)  (likewise y, z)
+//   r.x = fma(q.w, t.x, v.x) + c.x;  e = r - o
+//   r2  = fma(ez, ez, fma(ex, ex, ey*ey)),  term = -r2 * inv2rr
+// (established by comparing candidate orderings against the compiled
+// expression bit for bit).  Scaling by 2 is exact and commutes with rounding,
+// so the products with t = 2t' are formed from t' and pre-doubled quaternion
+// components, which removes the three multiplications by two; every rounded
+// operation of the reference is still performed, so the log-likelihoods are
+// identical.
+struct PackedPose {
+    float2 npx, npy, npz;      // -p
+    float2 k1, k2, k3, k4, k5, k6;  // t' coefficients
+    float2 m1, m2, m3, m4, m5, m6;  // c coefficients (doubled)
+    float2 w2;                  // 2 q.w
+};
+
+__device__ __forceinline__ PackedPose pack_pose(float3 p0, const Quat& c0,
+                                                float3 p1, const Quat& c1) {
+    PackedPose k;
+    k.npx = make_float2(-p0.x, -p1.x);
+    k.npy = make_float2(-p0.y, -p1.y);
+    k.npz = make_float2(-p0.z, -p1.z);
+    k.k1 = make_float2(-c0.z, -c1.z);
+    k.k2 = make_float2(c0.y, c1.y);
+    k.k3 = make_float2(-c0.x, -c1.x);
+    k.k4 = make_float2(c0.z, c1.z);
+    k.k5 = make_float2(-c0.y, -c1.y);
+    k.k6 = make_float2(c0.x, c1.x);
+    k.m1 = make_float2(2.f * k.k1.x, 2.f * k.k1.y);
+    k.m2 = make_float2(2.f * k.k2.x, 2.f * k.k2.y);
+    k.m3 = make_float2(2.f * k.k3.x, 2.f * k.k3.y);
+    k.m4 = make_float2(2.f * k.k4.x, 2.f * k.k4.y);
+    k.m5 = make_float2(2.f * k.k5.x, 2.f * k.k5.y);
+    k.m6 = make_float2(2.f * k.k6.x, 2.f * k.k6.y);
+    k.w2 = make_float2(2.f * c0.w, 2.f * c1.w);
+    return k;
+}
+
+// One observation (broadcast pairs A = (lx,lx,ly,ly), B = (lz,lz,-ox,-ox),
+// C = (-oy,-oy,-oz,-oz)) against two particles; returns the packed term.
+__device__ __forceinline__ float2 packed_r2(const PackedPose& k, float4 A,
+                                            float4 B, float4 C) {
+    const float2 dx = __fadd2_rn(make_float2(A.x, A.y), k.npx);
+    const float2 dy = __fadd2_rn(make_float2(A.z, A.w), k.npy);
+    const float2 dz = __fadd2_rn(make_float2(B.x, B.y), k.npz);
+    const float2 tx = __ffma2_rn(k.k1, dy, __fmul2_rn(k.k2, dz));
+    const float2 ty = __ffma2_rn(k.k3, dz, __fmul2_rn(k.k4, dx));
+    const float2 tz = __ffma2_rn(k.k5, dx, __fmul2_rn(k.k6, dy));
+    const float2 cx = __ffma2_rn(k.m1, ty, __fmul2_rn(k.m2, tz));
+    const float2 cy = __ffma2_rn(k.m3, tz, __fmul2_rn(k.m4, tx));
+    const float2 cz = __ffma2_rn(k.m5, tx, __fmul2_rn(k.m6, ty));
+    const float2 rx = __fadd2_rn(__ffma2_rn(k.w2, tx, dx), cx);
+    const float2 ry = __fadd2_rn(__ffma2_rn(k.w2, ty, dy), cy);
+    const float2 rz = __fadd2_rn(__ffma2_rn(k.w2, tz, dz), cz);
+    const float2 ex = __fadd2_rn(rx, make_float2(B.z, B.w));
+    const float2 ey = __fadd2_rn(ry, make_float2(C.x, C.y));
+    const float2 ez = __fadd2_rn(rz, make_float2(C.z, C.w));
+    return __ffma2_rn(ez, ez, __ffma2_rn(ex, ex, __fmul2_rn(ey, ey)));
 }
 
 // Two particles per thread (i and i + 256): every staged observation read
@@ -300,10 +369,11 @@ __global__ void __launch_bounds__(kThreads)
              const CObservation* __restrict__ obs, int nobs,
              const float* __restrict__ lm, int lm_count, float sigma_r,
              float sigma_b, float gate, float* __restrict__ ll,
-             double2* part, unsigned* done, CycleCtl* ctl) {
+             double2* part, unsigned* done, CycleCtl* ctl, int use_packed) {
     __shared__ float4 s_a[kObsChunk];
     __shared__ float4 s_b[kObsChunk];
-    const Planes s = ps.s[ctl->live];
+    __shared__ float4 s_p[3 * kObsChunk];
+    const Planes s = pick_planes(ps, ctl->live);
     const int i0 = blockIdx.x * (2 * kThreads) + threadIdx.x;
     const int i1 = i0 + kThreads;
     const bool v0 = i0 < n, v1 = i1 < n;
@@ -325,13 +395,39 @@ __global__ void __launch_bounds__(kThreads)
     }
     const GateConsts g = gate_consts(sigma_r, sigma_b, gate);
     const Quat qc0 = q_conjugate(q0), qc1 = q_conjugate(q1);
+    const PackedPose pk = pack_pose(p0, qc0, p1, qc1);
+    const float2 ninv = make_float2(-g.inv2rr, -g.inv2rr);
     float acc0 = 0.0f, acc1 = 0.0f;
     for (int c0 = 0; c0 < nobs; c0 += kObsChunk) {
         bool all_cart;
         __syncthreads();
         const int cn = stage_chunk(obs, lm, lm_count, c0, min(kObsChunk, nobs - c0),
-                                   s_a, s_b, &all_cart);
-        if (all_cart && gate > 0.0f) {
+                                   s_a, s_b, s_p, &all_cart);
+        if (all_cart && use_packed) {
+            float2 acc = make_float2(acc0, acc1);
+            if (gate > 0.0f) {
+#pragma unroll 2
+                for (int k = 0; k < cn; ++k) {
+                    const float2 r2 = packed_r2(pk, s_p[3 * k], s_p[3 * k + 1],
+                                                s_p[3 * k + 2]);
+                    const float2 t = __fmul2_rn(r2, ninv);
+                    const float a0 = (r2.x > g.cart_gate2) ? g.cart_out : t.x;
+                    const float a1 = (r2.y > g.cart_gate2) ? g.cart_out : t.y;
+                    acc = __fadd2_rn(acc, make_float2(a0, a1));
+                }
+            } else {
+#pragma unroll 2
+                for (int k = 0; k < cn; ++k) {
+                    const float2 r2 = packed_r2(pk, s_p[3 * k], s_p[3 * k + 1],
+                                                s_p[3 * k + 2]);
+                    // two roundings, as the reference (see cart_term)
+                    acc.x = __fadd_rn(acc.x, __fmul_rn(r2.x, ninv.x));
+                    acc.y = __fadd_rn(acc.y, __fmul_rn(r2.y, ninv.y));
+                }
+            }
+            acc0 = acc.x;
+            acc1 = acc.y;
+        } else if (all_cart && gate > 0.0f) {
 #pragma unroll 2
             for (int k = 0; k < cn; ++k) {
                 const float4 a = s_a[k], b = s_b[k];
@@ -391,11 +487,13 @@ int launch_weight(PfHandle* h, const PredictArgs& pa, const CObservation* d_obs,
     if (pa.enabled) {
         k_weight<true><<<grid, kThreads, 0, h->stream>>>(
             plane_set(h), h->n, h->seed, pa, d_obs, nobs, h->d_lm, h->lm_count,
-            sigma_r, sigma_b, gate, h->d_ll, part, h->d_done + 0, h->d_ctl);
+            sigma_r, sigma_b, gate, h->d_ll, part, h->d_done + 0, h->d_ctl,
+            h->weight_variant == 0 ? 1 : 0);
     } else {
         k_weight<false><<<grid, kThreads, 0, h->stream>>>(
             plane_set(h), h->n, h->seed, pa, d_obs, nobs, h->d_lm, h->lm_count,
-            sigma_r, sigma_b, gate, h->d_ll, part, h->d_done + 0, h->d_ctl);
+            sigma_r, sigma_b, gate, h->d_ll, part, h->d_done + 0, h->d_ctl,
+            h->weight_variant == 0 ? 1 : 0);
     }
     PFB_KL();
     return 0;

@@ -263,9 +263,11 @@ enum {
 int pfc_profile(void* h, int on);
 int pfc_profile_read(void* h, double* ms, long long* counts);
 
-/* Weighting kernel variant: 0 = quaternion form in the reference's
- * expression order (default), 1 = two particles per thread with packed f32x2
- * arithmetic in the same per-element operation order. */
+/* Weighting kernel variant.  Both perform every rounded operation of the
+ * reference expression (src/cuda/pf_kernels.cu:240-269) in its order, so the
+ * log-likelihoods are identical: 0 = packed f32x2 arithmetic over two
+ * particles for chunks of Cartesian observations (default), 1 = scalar
+ * arithmetic throughout. */
 int pfc_set_weight_kernel(void* h, int variant);
 
 /* ---------------------------------------------------------------------

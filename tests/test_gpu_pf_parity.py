@@ -340,3 +340,34 @@ def test_range_bearing_loglik_matches_reference(kernels, ref):
     finally:
         ours.close()
         theirs.close()
+
+
+@pytest.mark.parametrize("gate", [0.0, 3.0])
+def test_weight_variants_bit_identical(kernels, ref, gate):
+    """The packed f32x2 path and the scalar path perform the same rounded
+    operations as the reference kernel: all three agree bit for bit."""
+    lm, obs, tp, tq = scale_obs(seed=4)
+    yaw = 2.0 * np.arctan2(tq[3], tq[0])
+    n = 30_001
+    pos, quat = cloud(n, 2, centre=tp, pos_std=0.5, rot_std=0.05, yaw=yaw)
+    outs = []
+    for variant in (0, 1):
+        pf = RawPF(kernels, n, seed=1)
+        try:
+            assert kernels.pfc_set_weight_kernel(pf.h, variant) == 0
+            ours_set_state(pf, pos, quat)
+            pf.landmarks(lm)
+            assert pf.weight(obs, 0.05, 0.02, gate) == 0
+            outs.append(ours_ll(pf))
+        finally:
+            pf.close()
+    theirs = RawPF(ref, n, seed=1)
+    try:
+        ref_set_state(ref, theirs, pos, quat)
+        theirs.landmarks(lm)
+        assert theirs.weight(obs, 0.05, 0.02, gate) == 0
+        r = ref_ll(ref, theirs)
+    finally:
+        theirs.close()
+    assert np.array_equal(outs[0], outs[1])
+    assert np.array_equal(outs[0], r)
