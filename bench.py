@@ -55,10 +55,16 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--particles", type=int, default=1_000_000)
     ap.add_argument("--seed", type=int, default=11)
+    ap.add_argument("--gl-only", action="store_true",
+                    help="run only the global-localization legs and print their JSON")
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip GL, CPU baseline and reference-GPU legs")
+                    help="skip the GL and CPU-baseline legs")
     ap.add_argument("--gl-hyps", type=int, default=1_000_000)
     ap.add_argument("--gl-trials", type=int, default=20)
+    ap.add_argument("--gl-maps", type=int, default=16)
+    ap.add_argument("--gl-queries", type=int, default=1000)
+    ap.add_argument("--gl-pairs", type=int, default=2_000_000)
+    ap.add_argument("--gl-train-steps", type=int, default=3000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     return ap.parse_args()
 
@@ -327,137 +333,135 @@ def run_e2e(args, sc, torch, dev):
         pf.close()
 
 
-def run_ref_gpu_pf(args, sc, cycles):
-    """The reference library (built from its source for sm_100a) driven in the
-    Rust CudaBackend's call order; host Markley mean via numpy."""
-    import oracle
-    import cuda_pf_localization_b200 as pkg
-    ref = oracle.ref_lib()
-    if ref is None:
-        return None
-    n = args.particles
-    h = ref.pfc_create(256)
-    f32 = lambda a: np.ascontiguousarray(a, np.float32)
-    try:
-        assert ref.pfc_init(h, n, 42) == 0
-        lm = f32(sc.landmarks).reshape(-1)
-        ref.pfc_upload_landmarks(h, pkg.fptr(lm), len(sc.landmarks))
-        pri = np.r_[sc.prior_p, sc.prior_q]
-        ps, rs = f32([0.5] * 3), f32([0.2] * 3)
-        ref.pfc_reinit(h, *map(float, pri), pkg.fptr(ps), pkg.fptr(rs))
-        tn, rn = f32(sc.trans_noise), f32(sc.rot_noise)
-        obs = [pkg.make_cobs(st.obs) for st in sc.steps]
-        sums = np.zeros(14)
-        cv = np.zeros(12)
+# Tensor-core work of one training sample: forward (2 * sum in*out) + weight
+# gradients (the same) + input gradients of layers 1..4.
+LP_FLOPS_PER_SAMPLE = 2 * (2 * (384 * 1024 + 3 * 1024 * 1024 + 1024 * 384)
+                           + 3 * 1024 * 1024 + 1024 * 384)
 
-        def cycle(k):
-            st = sc.steps[k]
-            ref.pfc_predict(h, *map(float, st.odom_t), *map(float, st.odom_q), pkg.fptr(tn),
-                            pkg.fptr(rn))
-            ref.pfc_weight(h, C.cast(obs[k], C.c_void_p), len(st.obs), 0.05, 0.02, 3.0)
 
-            def estimate():
-                ref.pfc_est_sums(h, pkg.dptr(sums))
-                m = np.zeros((4, 4))
-                e = 3
-                for r in range(4):
-                    for c in range(r, 4):
-                        m[r, c] = m[c, r] = sums[e]
-                        e += 1
-                vals, vecs = np.linalg.eigh(m)
-                q = vecs[:, int(np.argmax(vals))]
-                q = q if q[0] >= 0 else -q
-                ref.pfc_covs(h, float(sums[0]), float(sums[1]), float(sums[2]), *map(float, q),
-                             pkg.dptr(cv))
-                return 1.0 / sums[13] if sums[13] > 0 else 0.0
-            ess = estimate()
-            if ess < 0.5 * n:
-                ref.pfc_resample(h, 0.01)
-                estimate()
-
-        for k in range(2):
-            cycle(k)
-        t0 = time.perf_counter()
-        for k in range(2, 2 + cycles):
-            cycle(k)
-        return n * cycles / (time.perf_counter() - t0)
-    finally:
-        ref.pfc_destroy(h)
+def _pose_err(top, truth):
+    dp = math.hypot(top[0] - truth[0], top[1] - truth[1])
+    dth = abs((top[2] - truth[2] + math.pi) % (2 * math.pi) - math.pi)
+    return dp, dth
 
 
 def run_gl(args):
-    """Uniform CBGL: 20 trials on a 30-box room, 1M hypotheses, k = 64."""
-    import oracle
+    """CBGL on 10 x 10 m rooms with 30 boxes (200 x 200 at 0.05 m), 360-ray
+    scans (rmax 10 m, N(0, 0.01 m) noise) rendered by the library's raycaster.
+
+    uniform: free positions x 16 yaws at each hypothesis count, k = 64, the
+             fused pruned localizer and the reference's call pattern
+             (pfgl_score + pfgl_topk).
+    learned: per map, 2M (scan, pose) pairs generated on the device, the MLP
+             trained by the library's tcgen05 kernels, the fallback threshold
+             calibrated on held-out poses; then unseen poses localized from
+             20k mixture samples (200k uniform fallback), and the same poses
+             with uniform CBGL at the largest hypothesis count."""
     import cuda_pf_localization_b200 as pkg
     from cuda_pf_localization_b200 import sim
     lib = pkg.kernels()
-    g = sim.rooms_grid(args.seed)
-    nh = args.gl_hyps
-    k = 64
-    rng = np.random.default_rng(args.seed + 1)
-    trials = []
-    for t in range(args.gl_trials):
-        x, y, th = sim.free_pose(g, rng)
-        scan = oracle.map_scan(g, 0.05, (0, 0), x, y, th, 360, 2 * math.pi, 10.0)
-        scan = (scan + rng.normal(0, 0.01, 360)).astype(np.float32)
-        trials.append(((x, y, th), scan))
-    cells = np.ascontiguousarray(g)
-    h = lib.pfgl_create(200, 200, 0.05, 0.0, 0.0, pkg.u8ptr(cells), nh)
+    span, rmax, k = 2 * math.pi, 10.0, 64
+    res = {"uniform": {}, "learned": {}}
     out = np.zeros(3 * k, np.float32)
-    cs = np.zeros(k, np.float32)
-    ids = np.zeros(k, np.int32)
 
-    def err(top, truth):
-        dp = math.hypot(top[0] - truth[0], top[1] - truth[1])
-        dth = abs((top[2] - truth[2] + math.pi) % (2 * math.pi) - math.pi)
-        return dp, dth
+    def trials_for(g, rng, n, h):
+        poses = np.array([sim.free_pose(g, rng) for _ in range(n)], np.float32)
+        return poses, pkg.render_scans(h, poses, noise=0.01, seed=int(rng.integers(1 << 31)))
 
-    res = {}
+    # ---- uniform CBGL, the reference method (config sizes, 20 trials each)
+    g = np.ascontiguousarray(sim.rooms_grid(args.seed))
+    h = lib.pfgl_create(200, 200, 0.05, 0.0, 0.0, pkg.u8ptr(g), max(args.gl_hyps, 200_000))
     try:
-        for mode in ("pruned", "abi"):
-            ok_p = ok_pt = 0
-            lib.pfgl_generate_yaws(h, nh // 16, 16, 1)
-            lib.pfgl_localize(h, pkg.fptr(trials[0][1]), 360, 10.0, 2 * math.pi, k,
-                              pkg.fptr(out), pkg.fptr(cs), pkg.iptr(ids))  # warm-up
-            t0 = time.perf_counter()
-            for t, (truth, scan) in enumerate(trials):
-                assert lib.pfgl_generate_yaws(h, nh // 16, 16, 1000 + t) == 0
-                if mode == "pruned":
-                    r = lib.pfgl_localize(h, pkg.fptr(scan), 360, 10.0, 2 * math.pi, k,
-                                          pkg.fptr(out), pkg.fptr(cs), pkg.iptr(ids))
-                else:
-                    assert lib.pfgl_score(h, pkg.fptr(scan), 360, 10.0, 2 * math.pi) == 0
-                    r = lib.pfgl_topk(h, k, pkg.fptr(out))
-                assert r == k
-                dp, dth = err(out[:3], truth)
-                ok_p += dp <= 0.5
-                ok_pt += (dp <= 0.5 and dth <= 0.1)
-            dt = time.perf_counter() - t0
-            res[mode] = dict(solves_per_s=len(trials) / dt, success_pos=ok_p / len(trials),
-                             success_pos_yaw=ok_pt / len(trials))
+        poses, scans = trials_for(g, np.random.default_rng(args.seed + 1), args.gl_trials, h)
+        for nh in sorted({50_000, 200_000, args.gl_hyps}):
+            for mode in ("pruned", "abi"):
+                lib.pfgl_generate_yaws(h, nh // 16, 16, 1)
+                lib.pfgl_localize(h, pkg.fptr(scans[0]), 360, rmax, span, k, pkg.fptr(out),
+                                  None, None)  # warm-up
+                ok_p = ok_pt = 0
+                t0 = time.perf_counter()
+                for t in range(len(poses)):
+                    assert lib.pfgl_generate_yaws(h, nh // 16, 16, 1000 + t) == 0
+                    if mode == "pruned":
+                        r = lib.pfgl_localize(h, pkg.fptr(scans[t]), 360, rmax, span, k,
+                                              pkg.fptr(out), None, None)
+                    else:
+                        assert lib.pfgl_score(h, pkg.fptr(scans[t]), 360, rmax, span) == 0
+                        r = lib.pfgl_topk(h, k, pkg.fptr(out))
+                    assert r == k
+                    dp, dth = _pose_err(out[:3], poses[t])
+                    ok_p += dp <= 0.5
+                    ok_pt += dp <= 0.5 and dth <= 0.1
+                dt = time.perf_counter() - t0
+                res["uniform"][f"{nh}_{mode}"] = dict(
+                    solves_per_s=len(poses) / dt, success_pos=ok_p / len(poses),
+                    success_pos_yaw=ok_pt / len(poses), trials=len(poses))
     finally:
         lib.pfgl_destroy(h)
-    # the reference library on the same trials (exhaustive score + CUB sort)
-    ref = oracle.ref_lib()
-    if ref is not None:
-        rh = ref.pfgl_create(200, 200, 0.05, 0.0, 0.0, pkg.u8ptr(cells), nh)
+
+    # ---- learned proposal vs uniform at the largest size on the same poses
+    tot_q = ok_q = fb_q = 0
+    t_learn = t_train = t_steps = 0.0
+    uni_q = uni_ok = 0
+    t_uni = 0.0
+    losses, taus = [], []
+    for m in range(args.gl_maps):
+        gseed = 1000 + 17 * m
+        g = np.ascontiguousarray(sim.rooms_grid(gseed))
+        h = lib.pfgl_create(200, 200, 0.05, 0.0, 0.0, pkg.u8ptr(g), max(args.gl_hyps, 200_000))
+        lp = None
         try:
-            ok = 0
-            ref.pfgl_generate(rh, nh, 1)
-            ref.pfgl_score(rh, pkg.fptr(trials[0][1]), 360, 10.0, 2 * math.pi)
-            ref.pfgl_topk(rh, k, pkg.fptr(out))
+            lp = pkg.LearnedProposal(h, batch=2048, seed=gseed)
             t0 = time.perf_counter()
-            n_ref = min(len(trials), 5)
-            for t in range(n_ref):
-                truth, scan = trials[t]
-                ref.pfgl_generate(rh, nh, 1000 + t)
-                ref.pfgl_score(rh, pkg.fptr(scan), 360, 10.0, 2 * math.pi)
-                ref.pfgl_topk(rh, k, pkg.fptr(out))
-                ok += err(out[:3], truth)[0] <= 0.5
-            res["reference_gpu"] = dict(solves_per_s=n_ref / (time.perf_counter() - t0),
-                                        success_pos=ok / n_ref)
+            lp.make_data(args.gl_pairs, seed=gseed + 1)
+            t1 = time.perf_counter()
+            loss = lp.train(args.gl_train_steps, lr=1e-3)
+            t2 = time.perf_counter()
+            t_train += t2 - t0
+            t_steps += t2 - t1
+            losses.append(float(loss[-50:].mean()))
+            tau, _ = lp.calibrate(n_queries=200, n_samples=20000, seed=gseed + 2)
+            taus.append(tau)
+            poses, scans = trials_for(g, np.random.default_rng(gseed + 3), args.gl_queries, h)
+            lp.localize(scans[0], n_samples=20000, n_fallback=200_000, k=k)  # warm-up
+            t0 = time.perf_counter()
+            for q in range(len(poses)):
+                top, _, _, info = lp.localize(scans[q], n_samples=20000, n_fallback=200_000, k=k)
+                dp, dth = _pose_err(top[0], poses[q])
+                ok_q += dp <= 0.5 and dth <= 0.1
+                fb_q += info > 0
+            t_learn += time.perf_counter() - t0
+            tot_q += len(poses)
+            nu = min(args.gl_trials, len(poses))
+            t0 = time.perf_counter()
+            for q in range(nu):
+                lib.pfgl_generate_yaws(h, args.gl_hyps // 16, 16, 7000 + q)
+                lib.pfgl_localize(h, pkg.fptr(scans[q]), 360, rmax, span, k, pkg.fptr(out),
+                                  None, None)
+                dp, dth = _pose_err(out[:3], poses[q])
+                uni_ok += dp <= 0.5 and dth <= 0.1
+            t_uni += time.perf_counter() - t0
+            uni_q += nu
         finally:
-            ref.pfgl_destroy(rh)
+            if lp is not None:
+                lp.close()
+            lib.pfgl_destroy(h)
+    learned_sps = tot_q / t_learn
+    uniform_sps = uni_q / t_uni
+    res["learned"] = dict(
+        maps=args.gl_maps, queries=tot_q, success_pos_yaw=ok_q / tot_q,
+        fallback_rate=fb_q / tot_q, solves_per_s=learned_sps,
+        samples_per_query=20000, fallback_hyps=200_000,
+        train_pairs_per_map=args.gl_pairs, train_steps_per_map=args.gl_train_steps,
+        train_seconds_per_map=t_train / args.gl_maps, final_loss_mean=float(np.mean(losses)),
+        train_step_ms=1e3 * t_steps / (args.gl_maps * args.gl_train_steps),
+        train_tflops=LP_FLOPS_PER_SAMPLE * 2048 * args.gl_train_steps * args.gl_maps
+        / t_steps / 1e12,
+        tau_mean=float(np.mean(taus)))
+    res["uniform_same_maps"] = dict(hyps=args.gl_hyps, queries=uni_q,
+                                    success_pos_yaw=uni_ok / max(1, uni_q),
+                                    solves_per_s=uniform_sps)
+    res["learned_vs_uniform_solves_ratio"] = learned_sps / uniform_sps
     return res
 
 
@@ -475,6 +479,10 @@ def main():
     import torch
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    if args.gl_only:
+        if rank == 0:
+            print(json.dumps({"gl": run_gl(args)}), flush=True)
+        return
     dist = None
     if world > 1:
         import datetime
@@ -552,19 +560,12 @@ def main():
         line["cpu_baseline"] = {"value": n * done / secs, "unit": UNIT,
                                 "cores": int(oracle.lib().orc_threads()), "kind": "port",
                                 "sample": f"{done} cycles at N={n} (time-bounded)"}
-        try:
-            ref_v = run_ref_gpu_pf(args, sc, 20)
-        except Exception as exc:  # the comparator is informative only
-            ref_v = None
-            line["reference_gpu_error"] = str(exc)[:200]
-        if ref_v:
-            line["reference_gpu"] = {"value": ref_v, "unit": UNIT,
-                                     "what": "reference pf_kernels.cu built for sm_100a, "
-                                             "driven in the Rust CudaBackend call order"}
         line["gl"] = run_gl(args)
-        line["gl"]["config"] = ("10x10 m room at 0.05 m (200x200), 30 boxes 0.2-1.0 m, 360 rays, "
-                                f"rmax 10, {args.gl_hyps} hyps = positions x 16 yaws, k=64, "
-                                f"{args.gl_trials} trials, scan noise N(0, 0.01 m)")
+        line["gl"]["config"] = ("10x10 m rooms at 0.05 m (200x200), 30 boxes 0.2-1.0 m, 360 rays, "
+                                "rmax 10, scan noise N(0, 0.01 m); uniform: positions x 16 yaws, "
+                                f"k=64, {args.gl_trials} trials per size; learned: "
+                                f"{args.gl_maps} maps x {args.gl_queries} unseen poses, success "
+                                "within 0.5 m and 0.1 rad")
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -155,6 +155,26 @@ _KERNEL_SIGS = {
     "pfgl_topk_from_scores": (c_int, [c_void_p, _fp, c_int, c_int, _ip]),
     "pfgl_localize": (c_int, [c_void_p, _fp, c_int, c_float, c_float, c_int, _fp, _fp, _ip]),
     "pfgl_cell": (c_int, [c_void_p, c_int, c_int]),
+    "pfgl_learned_create": (c_void_p, [c_void_p, c_int, c_ulonglong]),
+    "pfgl_learned_destroy": (c_int, [c_void_p]),
+    "pfgl_learned_num_params": (C.c_longlong, []),
+    "pfgl_learned_get_params": (c_int, [c_void_p, _fp]),
+    "pfgl_learned_set_params": (c_int, [c_void_p, _fp]),
+    "pfgl_render_scans": (c_int, [c_void_p, _fp, c_int, c_int, c_float, c_float, c_float,
+                                  c_ulonglong, _fp]),
+    "pfgl_learned_make_data": (c_int, [c_void_p, C.c_longlong, c_int, c_float, c_float,
+                                       c_float, c_ulonglong]),
+    "pfgl_learned_train": (c_int, [c_void_p, c_int, c_int, c_float, _fp]),
+    "pfgl_learned_grad": (c_int, [c_void_p, _fp, _fp, _fp, _fp]),
+    "pfgl_learned_forward": (c_int, [c_void_p, _fp, c_int, _fp]),
+    "pfgl_learned_norm": (c_int, [c_void_p, _fp]),
+    "pfgl_learned_localize": (c_int, [c_void_p, _fp, c_int, c_float, c_float, c_int, c_int,
+                                      c_int, _fp, _fp, _ip, _ip]),
+    "pfgl_learned_calibrate": (c_int, [c_void_p, c_int, c_int, c_float, c_float, c_float,
+                                       c_int, c_float, c_ulonglong, _fp, _fp]),
+    "pfgl_learned_set_threshold": (c_int, [c_void_p, c_float]),
+    "pfgl_learned_gemm": (c_int, [c_int, c_int, c_int, POINTER(C.c_ushort),
+                                  POINTER(C.c_ushort), _fp]),
 }
 
 _CORE_SIGS = {
@@ -398,3 +418,133 @@ class GlobalLoc:
         if k <= 0:
             raise RuntimeError("localize failed: " + core().pfcore_last_error().decode())
         return [(out[j].x, out[j].y, out[j].theta, out[j].caer) for j in range(k)]
+
+
+# ----------------------------------------------------------- learned proposal
+
+LP_IN, LP_HIDDEN, LP_OUT, LP_COMP, LP_LAYERS = 384, 1024, 384, 32, 5
+
+
+class LearnedProposal:
+    """Per-map learned proposal for global localization (``pfgl_learned_*``).
+
+    Borrows a raw ``pfgl_*`` handle (map, scorer, stream); close this object
+    before destroying that handle.
+    """
+
+    def __init__(self, gl_handle, batch: int = 1024, seed: int = 1):
+        self.lib = kernels()
+        self.gl = gl_handle
+        self.batch = int(batch)
+        self._h = self.lib.pfgl_learned_create(gl_handle, self.batch, int(seed))
+        if not self._h:
+            raise RuntimeError("pfgl_learned_create failed: " + last_error())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.pfgl_learned_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def _ok(self, rc, what):
+        if rc < 0:
+            raise RuntimeError(f"{what} failed: {last_error()}")
+        return rc
+
+    @staticmethod
+    def num_params() -> int:
+        return int(kernels().pfgl_learned_num_params())
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(self.num_params(), np.float32)
+        self._ok(self.lib.pfgl_learned_get_params(self._h, fptr(out)), "get_params")
+        return out
+
+    def set_params(self, flat: np.ndarray):
+        flat = np.ascontiguousarray(flat, np.float32)
+        self._ok(self.lib.pfgl_learned_set_params(self._h, fptr(flat)), "set_params")
+
+    def norm(self):
+        c = np.zeros(4, np.float32)
+        self._ok(self.lib.pfgl_learned_norm(self._h, fptr(c)), "norm")
+        return c
+
+    def make_data(self, n_pairs: int, nrays=360, rmax=10.0, span=2 * np.pi, noise=0.01,
+                  seed=7):
+        self._ok(self.lib.pfgl_learned_make_data(self._h, int(n_pairs), nrays, rmax, span,
+                                                 noise, int(seed)), "make_data")
+
+    def train(self, steps: int, total_steps: int | None = None, lr: float = 1e-3):
+        loss = np.zeros(steps, np.float32)
+        self._ok(self.lib.pfgl_learned_train(self._h, int(steps), int(total_steps or steps),
+                                             float(lr), fptr(loss)), "train")
+        return loss
+
+    def grad(self, x: np.ndarray, y: np.ndarray):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        assert x.shape == (self.batch, LP_IN) and y.shape == (self.batch, 4)
+        g = np.zeros(self.num_params(), np.float32)
+        loss = np.zeros(1, np.float32)
+        self._ok(self.lib.pfgl_learned_grad(self._h, fptr(x), fptr(y), fptr(loss), fptr(g)),
+                 "grad")
+        return float(loss[0]), g
+
+    def forward(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float32)
+        out = np.zeros((x.shape[0], LP_COMP * 9), np.float32)
+        self._ok(self.lib.pfgl_learned_forward(self._h, fptr(x), x.shape[0], fptr(out)),
+                 "forward")
+        return out
+
+    def calibrate(self, n_queries=200, nrays=360, rmax=10.0, span=2 * np.pi, noise=0.01,
+                  n_samples=20000, quantile=0.98, seed=99):
+        tau = np.zeros(1, np.float32)
+        ok = np.zeros(1, np.float32)
+        self._ok(self.lib.pfgl_learned_calibrate(self._h, n_queries, nrays, rmax, span, noise,
+                                                 n_samples, quantile, int(seed), fptr(tau),
+                                                 fptr(ok)), "calibrate")
+        return float(tau[0]), float(ok[0])
+
+    def set_threshold(self, tau: float):
+        self._ok(self.lib.pfgl_learned_set_threshold(self._h, float(tau)), "set_threshold")
+
+    def localize(self, scan: np.ndarray, n_samples=20000, n_fallback=200000, k=64,
+                 rmax=10.0, span=2 * np.pi):
+        scan = np.ascontiguousarray(scan, np.float32)
+        out = np.zeros(3 * k, np.float32)
+        cs = np.zeros(k, np.float32)
+        ids = np.zeros(k, np.int32)
+        info = np.zeros(1, np.int32)
+        r = self._ok(self.lib.pfgl_learned_localize(self._h, fptr(scan), len(scan), rmax, span,
+                                                    n_samples, n_fallback, k, fptr(out),
+                                                    fptr(cs), iptr(ids), iptr(info)),
+                     "localize")
+        return out[:3 * r].reshape(r, 3), cs[:r], ids[:r], int(info[0])
+
+
+def render_scans(gl_handle, poses: np.ndarray, nrays=360, rmax=10.0, span=2 * np.pi,
+                 noise=0.0, seed=0) -> np.ndarray:
+    """Scans at poses (n x 3) from the library's raycaster (CAER ray geometry)."""
+    poses = np.ascontiguousarray(poses, np.float32).reshape(-1, 3)
+    out = np.zeros((len(poses), nrays), np.float32)
+    rc = kernels().pfgl_render_scans(gl_handle, fptr(poses), len(poses), nrays, rmax, span,
+                                     noise, int(seed), fptr(out))
+    if rc != 0:
+        raise RuntimeError("pfgl_render_scans failed: " + last_error())
+    return out
+
+
+def learned_gemm(a_bf16: np.ndarray, b_bf16: np.ndarray) -> np.ndarray:
+    """D = A B^T on the tcgen05 GEMM (A: M x K, B: N x K as uint16 bf16 bits)."""
+    a = np.ascontiguousarray(a_bf16, np.uint16)
+    b = np.ascontiguousarray(b_bf16, np.uint16)
+    M, K = a.shape
+    N = b.shape[0]
+    d = np.zeros((M, N), np.float32)
+    rc = kernels().pfgl_learned_gemm(M, N, K, a.ctypes.data_as(POINTER(C.c_ushort)),
+                                     b.ctypes.data_as(POINTER(C.c_ushort)), fptr(d))
+    if rc != 0:
+        raise RuntimeError("pfgl_learned_gemm failed: " + last_error())
+    return d

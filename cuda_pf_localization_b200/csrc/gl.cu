@@ -36,7 +36,7 @@
 #include <new>
 #include <vector>
 
-#include "pf_common.cuh"
+#include "gl_internal.h"
 
 namespace pfb {
 
@@ -45,40 +45,6 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxSmem = 200 * 1024;
-
-struct GlCtl {
-    unsigned long long tau;   // pruning bound on the composite key
-    unsigned n_cand;          // survivors appended by the pruned scorer
-    unsigned err;
-};
-
-struct GlHandle {
-    int dev = 0;
-    cudaStream_t stream = nullptr;
-    int W = 0, H = 0, Wp = 0, Hp = 0;
-    float res = 0.05f, ox = 0.f, oy = 0.f;
-    int cap_hyp = 0;
-    int nfree = 0;
-    int nh = 0;
-    unsigned char* d_grid = nullptr;  // padded
-    int2* d_free = nullptr;
-    float* d_hyp = nullptr;
-    float* d_caer = nullptr;
-    uint64_t* d_keys = nullptr;
-    uint64_t* d_keys_alt = nullptr;
-    unsigned* d_hist = nullptr;
-    int hist_cap = 0;
-    float* d_scan = nullptr;
-    int scan_cap = 0;
-    float* d_out = nullptr;   // k x 3 (cap_hyp)
-    float* d_outc = nullptr;  // k CAER
-    int* d_outi = nullptr;    // k indices
-    uint64_t* d_cand = nullptr;  // pruned-scorer survivors (cap_hyp)
-    GlCtl* d_ctl = nullptr;
-    GlCtl* h_ctl = nullptr;
-    std::vector<unsigned char> host_grid;  // unpadded 0/1 copy
-    bool caer_valid = false;
-};
 
 GlHandle* as_gl(void* h) { return static_cast<GlHandle*>(h); }
 
@@ -108,71 +74,6 @@ __global__ void k_gl_gen(int n, int n_yaw, int nfree, const int2* __restrict__ f
 }
 
 // ------------------------------------------------------------------ raycast
-
-struct GridView {
-    const unsigned char* cells;  // padded grid
-    int W, H, Wp;
-    float res, ox, oy;
-};
-
-// 2-D DDA from the start cell (cx, cy) with in-cell fractions (frx, fry):
-// distance to the first occupied cell, rmax when the ray passes rmax or
-// leaves the map.  Arithmetic follows src/cuda/pf_kernels.cu:784-808.
-__device__ __forceinline__ float cast_ray(const unsigned char* __restrict__ g,
-                                          int Wp, int start, float frx,
-                                          float fry, float dirx, float diry,
-                                          float res, float rmax) {
-    const int sx = dirx > 0 ? 1 : -1;
-    const int sy = diry > 0 ? Wp : -Wp;
-    const float adx = fabsf(dirx), ady = fabsf(diry);
-    const float tdx = adx > 1e-9f ? res / adx : INFINITY;
-    const float tdy = ady > 1e-9f ? res / ady : INFINITY;
-    float tmx = adx > 1e-9f ? ((dirx > 0 ? 1.f - frx : frx) * tdx) : INFINITY;
-    float tmy = ady > 1e-9f ? ((diry > 0 ? 1.f - fry : fry) * tdy) : INFINITY;
-    int idx = start;
-    for (int step = 0; step < 8192; ++step) {
-        float dist;
-        if (tmx <= tmy) {
-            dist = tmx;
-            tmx += tdx;
-            idx += sx;
-        } else {
-            dist = tmy;
-            tmy += tdy;
-            idx += sy;
-        }
-        if (dist > rmax) return rmax;
-        const unsigned char v = g[idx];
-        if (v) return v == 1 ? dist : rmax;
-    }
-    return rmax;
-}
-
-// Start cell of a hypothesis (floor of the f32 cell coordinate, as
-// src/cuda/pf_kernels.cu:774-781); false when outside the map.
-__device__ __forceinline__ bool start_cell(const GridView& gv, float x, float y,
-                                           int& start, float& frx,
-                                           float& fry) {
-    const float fx = (x - gv.ox) / gv.res;
-    const float fy = (y - gv.oy) / gv.res;
-    const int cx = (int)floorf(fx), cy = (int)floorf(fy);
-    if (!(cx >= 0 && cy >= 0 && cx < gv.W && cy < gv.H)) return false;
-    frx = (x - gv.ox) / gv.res - (float)cx;
-    fry = (y - gv.oy) / gv.res - (float)cy;
-    start = (cy + 1) * gv.Wp + (cx + 1);
-    return true;
-}
-
-__device__ __forceinline__ float ray_angle(float th, int r, int nrays,
-                                           float span) {
-    return th + (nrays > 1 ? span * (float)r / (float)(nrays - 1) : 0.f);
-}
-
-__device__ __forceinline__ float warp_sum_f(float v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(~0u, v, o);
-    return v;
-}
 
 // Copy the padded grid and the scan into shared memory.
 __device__ __forceinline__ void load_smem(unsigned char* s_grid, int grid_bytes,
@@ -476,14 +377,6 @@ int ensure_scan(GlHandle* h, const float* scan, int nrays) {
     return 0;
 }
 
-GridView grid_view(const GlHandle* h) {
-    return {h->d_grid, h->W, h->H, h->Wp, h->res, h->ox, h->oy};
-}
-
-int grid_bytes_padded(const GlHandle* h) {
-    return (int)(((size_t)h->Wp * h->Hp + 15) / 16 * 16);
-}
-
 template <bool kSmem>
 int score_grid_size(size_t smem) {
     int per_sm = 0, sms = 0, dev = 0;
@@ -571,6 +464,71 @@ int copy_topk(GlHandle* h, const uint64_t* sorted, int k, float* out3k,
 }
 
 }  // namespace
+
+// ------------------------------------------- entry points shared across units
+
+int gl_upload_scan(GlHandle* h, const float* scan, int nrays) {
+    return ensure_scan(h, scan, nrays);
+}
+
+int gl_generate(GlHandle* h, int n_pos, int n_yaw, uint64_t seed) {
+    if (h->nfree <= 0 || n_pos <= 0 || n_yaw <= 0) return -1;
+    const long long n = (long long)n_pos * n_yaw;
+    if (n > h->cap_hyp) return -1;
+    h->nh = (int)n;
+    k_gl_gen<<<ceil_div(h->nh, kThreads), kThreads, 0, h->stream>>>(
+        h->nh, n_yaw, h->nfree, h->d_free, h->ox, h->oy, h->res, seed,
+        h->d_hyp);
+    PFB_KL();
+    h->caer_valid = false;
+    return 0;
+}
+
+int gl_localize_loaded(GlHandle* h, int nrays, float rmax, float ang_span,
+                       int k, float* out3k, float* caer_k, int* idx_k) {
+    if (h->nh <= 0 || k <= 0) return -1;
+    if (k > h->nh) k = h->nh;
+    const int nh = h->nh;
+    // Seed batch scored exhaustively, then pruned chunks.
+    const int seed_n = std::min(nh, std::max(4 * k, 8192));
+    const int saved = h->nh;
+    h->nh = seed_n;
+    if (launch_score(h, nrays, rmax, ang_span)) return -1;
+    const uint64_t* seed_sorted = sort_current(h);
+    h->nh = saved;
+    if (!seed_sorted) return -1;
+    if (seed_n == nh) {
+        h->caer_valid = true;
+        return copy_topk(h, seed_sorted, k, out3k, caer_k, idx_k);
+    }
+    // Pruning bound = k-th best key of the seed batch; candidates start with
+    // the seed batch's best k.
+    k_set_tau<<<1, 1, 0, h->stream>>>(seed_sorted, k, h->d_ctl);
+    PFB_KL();
+    PFB_CK(cudaMemcpyAsync(h->d_cand, seed_sorted, sizeof(uint64_t) * (size_t)k,
+                           cudaMemcpyDeviceToDevice, h->stream));
+    unsigned kk = (unsigned)k;
+    PFB_CK(cudaMemcpyAsync(&h->d_ctl->n_cand, &kk, sizeof(unsigned),
+                           cudaMemcpyHostToDevice, h->stream));
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    if (launch_score_pruned(h, seed_n, nh, nrays, rmax, ang_span)) return -1;
+    PFB_CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(GlCtl),
+                           cudaMemcpyDeviceToHost, h->stream));
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    int nc = (int)h->h_ctl->n_cand;
+    if (nc > h->cap_hyp) {
+        set_error("pf_b200: pfgl_localize candidate overflow");
+        return -1;
+    }
+    // Sort the survivors (their keys already carry the index).
+    PFB_CK(cudaMemcpyAsync(h->d_keys, h->d_cand, sizeof(uint64_t) * (size_t)nc,
+                           cudaMemcpyDeviceToDevice, h->stream));
+    const uint64_t* sorted = radix_sort_keys(h, nc, index_bit_width(nh));
+    if (!sorted) return -1;
+    h->caer_valid = false;  // pruned CAERs are not computed
+    return copy_topk(h, sorted, std::min(k, nc), out3k, caer_k, idx_k);
+}
+
 }  // namespace pfb
 
 using namespace pfb;
@@ -693,16 +651,8 @@ int pfgl_generate(void* hv, int n, unsigned long long seed) {
 
 int pfgl_generate_yaws(void* hv, int n_pos, int n_yaw, unsigned long long seed) {
     GlHandle* h = as_gl(hv);
-    if (!h || h->nfree <= 0 || n_pos <= 0 || n_yaw <= 0) return -1;
-    const long long n = (long long)n_pos * n_yaw;
-    if (n > h->cap_hyp) return -1;
-    h->nh = (int)n;
-    k_gl_gen<<<ceil_div(h->nh, kThreads), kThreads, 0, h->stream>>>(
-        h->nh, n_yaw, h->nfree, h->d_free, h->ox, h->oy, h->res, seed,
-        h->d_hyp);
-    PFB_KL();
-    h->caer_valid = false;
-    return 0;
+    if (!h) return -1;
+    return gl_generate(h, n_pos, n_yaw, seed);
 }
 
 int pfgl_set_hyps(void* hv, const float* hyp3n, int n) {
@@ -785,47 +735,8 @@ int pfgl_localize(void* hv, const float* scan, int nrays, float rmax,
                   int* idx_k) {
     GlHandle* h = as_gl(hv);
     if (!h || h->nh <= 0 || !scan || nrays <= 0 || k <= 0) return -1;
-    if (k > h->nh) k = h->nh;
-    if (ensure_scan(h, scan, nrays)) return -1;
-    const int nh = h->nh;
-    // Seed batch scored exhaustively, then pruned chunks.
-    const int seed_n = std::min(nh, std::max(4 * k, 8192));
-    const int saved = h->nh;
-    h->nh = seed_n;
-    if (launch_score(h, nrays, rmax, ang_span)) return -1;
-    const uint64_t* seed_sorted = sort_current(h);
-    h->nh = saved;
-    if (!seed_sorted) return -1;
-    if (seed_n == nh) {
-        h->caer_valid = true;
-        return copy_topk(h, seed_sorted, k, out3k, caer_k, idx_k);
-    }
-    // Pruning bound = k-th best key of the seed batch; candidates start with
-    // the seed batch's best k.
-    k_set_tau<<<1, 1, 0, h->stream>>>(seed_sorted, k, h->d_ctl);
-    PFB_KL();
-    PFB_CK(cudaMemcpyAsync(h->d_cand, seed_sorted, sizeof(uint64_t) * (size_t)k,
-                           cudaMemcpyDeviceToDevice, h->stream));
-    unsigned kk = (unsigned)k;
-    PFB_CK(cudaMemcpyAsync(&h->d_ctl->n_cand, &kk, sizeof(unsigned),
-                           cudaMemcpyHostToDevice, h->stream));
-    PFB_CK(cudaStreamSynchronize(h->stream));
-    if (launch_score_pruned(h, seed_n, nh, nrays, rmax, ang_span)) return -1;
-    PFB_CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(GlCtl),
-                           cudaMemcpyDeviceToHost, h->stream));
-    PFB_CK(cudaStreamSynchronize(h->stream));
-    int nc = (int)h->h_ctl->n_cand;
-    if (nc > h->cap_hyp) {
-        set_error("pf_b200: pfgl_localize candidate overflow");
-        return -1;
-    }
-    // Sort the survivors (their keys already carry the index).
-    PFB_CK(cudaMemcpyAsync(h->d_keys, h->d_cand, sizeof(uint64_t) * (size_t)nc,
-                           cudaMemcpyDeviceToDevice, h->stream));
-    const uint64_t* sorted = radix_sort_keys(h, nc, index_bit_width(nh));
-    if (!sorted) return -1;
-    h->caer_valid = false;  // pruned CAERs are not computed
-    return copy_topk(h, sorted, std::min(k, nc), out3k, caer_k, idx_k);
+    if (gl_upload_scan(h, scan, nrays)) return -1;
+    return gl_localize_loaded(h, nrays, rmax, ang_span, k, out3k, caer_k, idx_k);
 }
 
 int pfgl_cell(void* hv, int cx, int cy) {

@@ -1,0 +1,144 @@
+// gl_internal.h — global-localization handle, the padded-grid raycaster and
+// the entry points shared between the CBGL translation unit (gl.cu) and the
+// learned proposal (gl_learned.cu).
+//
+// Device layout of a handle
+//   grid  (W+2) x (H+2) bytes, row-major, row 0 = lowest y: 0 free,
+//         1 occupied (any nonzero input byte), 2 = the one-cell border that
+//         stands for "outside the map".
+//   free  int2 list of free cells in row-major order.
+//   hyp   cap_hyp x (x, y, theta) f32;  caer  cap_hyp f32;  keys  u64.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "pf_common.cuh"
+
+namespace pfb {
+
+struct GlCtl {
+    unsigned long long tau;   // pruning bound on the composite key
+    unsigned n_cand;          // survivors appended by the pruned scorer
+    unsigned err;
+};
+
+struct GlHandle {
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    int W = 0, H = 0, Wp = 0, Hp = 0;
+    float res = 0.05f, ox = 0.f, oy = 0.f;
+    int cap_hyp = 0;
+    int nfree = 0;
+    int nh = 0;
+    unsigned char* d_grid = nullptr;  // padded
+    int2* d_free = nullptr;
+    float* d_hyp = nullptr;
+    float* d_caer = nullptr;
+    uint64_t* d_keys = nullptr;
+    uint64_t* d_keys_alt = nullptr;
+    unsigned* d_hist = nullptr;
+    int hist_cap = 0;
+    float* d_scan = nullptr;
+    int scan_cap = 0;
+    float* d_out = nullptr;   // k x 3 (cap_hyp)
+    float* d_outc = nullptr;  // k CAER
+    int* d_outi = nullptr;    // k indices
+    uint64_t* d_cand = nullptr;  // pruned-scorer survivors (cap_hyp)
+    GlCtl* d_ctl = nullptr;
+    GlCtl* h_ctl = nullptr;
+    std::vector<unsigned char> host_grid;  // unpadded 0/1 copy
+    bool caer_valid = false;
+};
+
+struct GridView {
+    const unsigned char* cells;  // padded grid
+    int W, H, Wp;
+    float res, ox, oy;
+};
+
+// 2-D DDA from the padded start index with in-cell fractions (frx, fry):
+// distance to the first occupied cell, rmax when the ray passes rmax or
+// leaves the map.  The f32 arithmetic follows src/cuda/pf_kernels.cu:784-808
+// (tMax/tDelta stepping, x step on ties, 8192-step limit); stepping onto the
+// border byte (2) is the reference's out-of-grid test.
+__device__ __forceinline__ float cast_ray(const unsigned char* __restrict__ g,
+                                          int Wp, int start, float frx,
+                                          float fry, float dirx, float diry,
+                                          float res, float rmax) {
+    const int sx = dirx > 0 ? 1 : -1;
+    const int sy = diry > 0 ? Wp : -Wp;
+    const float adx = fabsf(dirx), ady = fabsf(diry);
+    const float tdx = adx > 1e-9f ? res / adx : INFINITY;
+    const float tdy = ady > 1e-9f ? res / ady : INFINITY;
+    float tmx = adx > 1e-9f ? ((dirx > 0 ? 1.f - frx : frx) * tdx) : INFINITY;
+    float tmy = ady > 1e-9f ? ((diry > 0 ? 1.f - fry : fry) * tdy) : INFINITY;
+    int idx = start;
+    for (int step = 0; step < 8192; ++step) {
+        float dist;
+        if (tmx <= tmy) {
+            dist = tmx;
+            tmx += tdx;
+            idx += sx;
+        } else {
+            dist = tmy;
+            tmy += tdy;
+            idx += sy;
+        }
+        if (dist > rmax) return rmax;
+        const unsigned char v = g[idx];
+        if (v) return v == 1 ? dist : rmax;
+    }
+    return rmax;
+}
+
+// Start cell of a pose (floor of the f32 cell coordinate, as
+// src/cuda/pf_kernels.cu:774-781); false when outside the map.
+__device__ __forceinline__ bool start_cell(const GridView& gv, float x, float y,
+                                           int& start, float& frx,
+                                           float& fry) {
+    const float fx = (x - gv.ox) / gv.res;
+    const float fy = (y - gv.oy) / gv.res;
+    const int cx = (int)floorf(fx), cy = (int)floorf(fy);
+    if (!(cx >= 0 && cy >= 0 && cx < gv.W && cy < gv.H)) return false;
+    frx = (x - gv.ox) / gv.res - (float)cx;
+    fry = (y - gv.oy) / gv.res - (float)cy;
+    start = (cy + 1) * gv.Wp + (cx + 1);
+    return true;
+}
+
+// Angle of ray r: the reference spaces nrays rays over span with
+// (nrays - 1) gaps (src/cuda/pf_kernels.cu:784).
+__device__ __forceinline__ float ray_angle(float th, int r, int nrays,
+                                           float span) {
+    return th + (nrays > 1 ? span * (float)r / (float)(nrays - 1) : 0.f);
+}
+
+__device__ __forceinline__ float warp_sum_f(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(~0u, v, o);
+    return v;
+}
+
+inline GridView grid_view(const GlHandle* h) {
+    return {h->d_grid, h->W, h->H, h->Wp, h->res, h->ox, h->oy};
+}
+
+inline int grid_bytes_padded(const GlHandle* h) {
+    return (int)(((size_t)h->Wp * h->Hp + 15) / 16 * 16);
+}
+
+// ------------------------------------------- entry points shared across units
+// Copy a host scan into the handle's device scan buffer (stream-ordered).
+int gl_upload_scan(GlHandle* h, const float* scan, int nrays);
+// Bottom-k of the h->nh hypotheses in d_hyp against the loaded scan, using the
+// pruned scorer; results as pfgl_localize.  Returns k written or -1.
+int gl_localize_loaded(GlHandle* h, int nrays, float rmax, float span, int k,
+                       float* out3k, float* caer_k, int* idx_k);
+// Uniform dispersion of n_pos positions x n_yaw yaws into d_hyp.
+int gl_generate(GlHandle* h, int n_pos, int n_yaw, uint64_t seed);
+
+}  // namespace pfb

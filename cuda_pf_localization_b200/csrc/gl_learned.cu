@@ -1,0 +1,1461 @@
+// gl_learned.cu — learned proposal for CBGL global localization.
+//
+// A per-map MLP maps a range scan (rays / rmax, zero padded to 384) to a
+// 32-component Gaussian mixture over the pose (x_n, y_n, cos yaw, sin yaw),
+// with x_n, y_n the position normalised to [-1, 1] over the map.  A query
+// draws hypotheses from the mixture and scores them with the plain CAER
+// scorer of gl.cu; when the best CAER is above a threshold calibrated on
+// held-out poses, uniform hypotheses are scored as well (the fallback).
+//
+// Network (all widths padded to multiples of 128):
+//   Z0 = X W0^T + b0     384 -> 1024,  H0 = relu(Z0)
+//   Z1..Z3               1024 -> 1024, H_l = relu(Z_l)
+//   Z4 = H3 W4^T + b4    1024 -> 384 (288 used: 32 logits, 32 x 4 means,
+//                                    32 x 4 log-sigma pre-activations)
+// Weights are kept as f32 masters (Adam state beside them) and as bf16
+// copies in both orientations, W [out][in] and W^T [in][out], so that every
+// GEMM of the forward and backward pass reads two K-major bf16 operands:
+//   forward    Z_l  = H_{l-1} . W_l^T        A = H_{l-1} [B][in],  B = W_l [out][in]
+//   input grad dZ_{l-1} = (dZ_l . W_l) * relu'  A = dZ_l [B][out], B = W_l^T [in][out]
+//   weight grad dW_l = dZ_l^T . H_{l-1}      A = dZ_l^T [out][B], B = H_{l-1}^T [in][B]
+// The forward and input-gradient epilogues write their bf16 result in both
+// orientations, so no separate transposes are needed for the next GEMMs.
+//
+// GEMM kernel (sm_100a): one 128 x 128 output tile per CTA, 4-stage TMA ring
+// of 128 x 64 bf16 tiles (128-byte swizzle), one thread issuing
+// tcgen05.mma (128 x 128 x 16, f32 accumulator in 128 TMEM columns), one
+// thread issuing the TMA loads, and all four warps draining TMEM through
+// tcgen05.ld in the fused epilogue.  Every mbarrier wait is bounded; a wait
+// that runs out sets an error word the host turns into -1.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "gl_internal.h"
+#include "umma.cuh"
+
+namespace pfb {
+namespace lp {
+
+using bf16 = __nv_bfloat16;
+using namespace pfb::umma;
+
+constexpr int kIn = PFGL_LP_IN;
+constexpr int kHid = PFGL_LP_HIDDEN;
+constexpr int kOut = PFGL_LP_OUT;
+constexpr int kComp = PFGL_LP_COMP;
+constexpr int kLayers = PFGL_LP_LAYERS;
+constexpr int kUsedOut = kComp * 9;           // 288
+constexpr int kMeanOff = kComp;               // 32
+constexpr int kSigOff = kComp + 4 * kComp;    // 160
+constexpr float kLsLo = -5.5f, kLsHi = 0.0f;  // log-sigma range
+constexpr float kHalfLog2Pi = 0.91893853320467274f;
+
+constexpr int layer_in(int l) { return l == 0 ? kIn : kHid; }
+constexpr int layer_out(int l) { return l == kLayers - 1 ? kOut : kHid; }
+
+// ------------------------------------------------------------------ GEMM
+constexpr int BM = 128, BN = 128, BK = 64, kStages = 4;
+constexpr int kTileBytes = BM * BK * 2;  // 16 KiB per operand tile
+constexpr int kGemmSmem = kStages * 2 * kTileBytes + 1024 + 256;
+constexpr uint32_t kWaitLimit = 1u << 24;
+
+enum Epi : int {
+    EPI_RELU_BF16 = 0,   // bf16 relu(acc + bias), row-major and transposed
+    EPI_BIAS_F32 = 1,    // f32 acc + bias, row-major
+    EPI_DRELU_BF16 = 2,  // bf16 acc * (mask > 0), row-major and transposed
+    EPI_F32 = 3,         // f32 acc * scale, row-major
+};
+
+struct EpiArgs {
+    void* out;
+    void* outT;         // transposed copy (bf16 epilogues; may be null)
+    const float* bias;  // [N]
+    const bf16* mask;   // [M][ldm] activations whose sign gates the gradient
+    int ldo, ldt, ldm;
+    float scale;
+};
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t*>(&h);
+}
+
+// Epilogue of 32 consecutive columns [col0, col0 + 32) of one output row.
+template <int EPI>
+__device__ __forceinline__ void epilogue_chunk(const uint32_t (&r)[32], int row,
+                                               int col0, const EpiArgs& ep) {
+    float v[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+    if (EPI == EPI_RELU_BF16 || EPI == EPI_BIAS_F32) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] += __ldg(&ep.bias[col0 + j]);
+    }
+    if (EPI == EPI_RELU_BF16) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] = fmaxf(v[j], 0.0f);
+    }
+    if (EPI == EPI_DRELU_BF16) {
+        const uint4* mp = reinterpret_cast<const uint4*>(
+            ep.mask + (size_t)row * ep.ldm + col0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint4 u = mp[q];
+            const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                // relu'(z) = 1 exactly when the stored activation is > 0:
+                // a bf16 bit pattern in [1, 0x7fff].
+                const int lo = (int)(short)(w[t] & 0xFFFFu);
+                const int hi = (int)(short)(w[t] >> 16);
+                if (lo <= 0) v[q * 8 + 2 * t] = 0.0f;
+                if (hi <= 0) v[q * 8 + 2 * t + 1] = 0.0f;
+            }
+        }
+    }
+    if (EPI == EPI_BIAS_F32 || EPI == EPI_F32) {
+        const float s = EPI == EPI_F32 ? ep.scale : 1.0f;
+        float4* o = reinterpret_cast<float4*>(reinterpret_cast<float*>(ep.out) +
+                                              (size_t)row * ep.ldo + col0);
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            o[q] = make_float4(v[4 * q] * s, v[4 * q + 1] * s, v[4 * q + 2] * s,
+                               v[4 * q + 3] * s);
+    } else {
+        uint4* o = reinterpret_cast<uint4*>(reinterpret_cast<bf16*>(ep.out) +
+                                            (size_t)row * ep.ldo + col0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            uint4 u;
+            u.x = pack_bf16x2(v[8 * q], v[8 * q + 1]);
+            u.y = pack_bf16x2(v[8 * q + 2], v[8 * q + 3]);
+            u.z = pack_bf16x2(v[8 * q + 4], v[8 * q + 5]);
+            u.w = pack_bf16x2(v[8 * q + 6], v[8 * q + 7]);
+            o[q] = u;
+        }
+        if (ep.outT) {
+            // Lanes hold consecutive rows: each store writes 64 contiguous
+            // bytes of one transposed row.
+            bf16* t = reinterpret_cast<bf16*>(ep.outT) + (size_t)col0 * ep.ldt + row;
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+                t[(size_t)j * ep.ldt] = __float2bfloat16_rn(v[j]);
+        }
+    }
+}
+
+// D[M][N] = A[M][K] . B[N][K]^T for one 128 x 128 tile per CTA.  Operand
+// tiles are read through tensor maps at (k0 + k, row0 + tile row).
+template <int EPI>
+__global__ void __launch_bounds__(128, 1)
+    k_gemm_bf16(const __grid_constant__ CUtensorMap tmA,
+                const __grid_constant__ CUtensorMap tmB, int K, int a_row0,
+                int a_k0, int b_row0, int b_k0, EpiArgs ep,
+                unsigned* __restrict__ err) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const uint32_t s0 = smem_u32(smem_raw);
+    unsigned char* base = smem_raw + ((1024u - (s0 & 1023u)) & 1023u);
+    unsigned char* sA = base;
+    unsigned char* sB = base + kStages * kTileBytes;
+    uint64_t* full = reinterpret_cast<uint64_t*>(base + 2 * kStages * kTileBytes);
+    uint64_t* empty = full + kStages;
+    uint64_t* accb = empty + kStages;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(accb + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int nkb = K / BK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(accb, 1);
+        fence_mbar_init();
+        tma_prefetch_map(&tmA);
+        tma_prefetch_map(&tmB);
+    }
+    if (warp == 0) {
+        tmem_alloc(tslot, BN);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+
+    bool fail = false;
+    if (warp == 0) {
+        if (lane == 0) {  // TMA producer
+            for (int kb = 0; kb < nkb; ++kb) {
+                const int s = kb % kStages;
+                if (kb >= kStages &&
+                    !mbar_wait(&empty[s], ((kb / kStages) - 1) & 1, kWaitLimit)) {
+                    fail = true;
+                    break;
+                }
+                mbar_expect_tx(&full[s], 2 * kTileBytes);
+                tma_load_2d(sA + s * kTileBytes, &tmA, &full[s], a_k0 + kb * BK,
+                            a_row0 + m0);
+                tma_load_2d(sB + s * kTileBytes, &tmB, &full[s], b_k0 + kb * BK,
+                            b_row0 + n0);
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {  // MMA issuer
+            constexpr uint32_t idesc = idesc_bf16_f32(BM, BN);
+            for (int kb = 0; kb < nkb; ++kb) {
+                const int s = kb % kStages;
+                if (!mbar_wait(&full[s], (kb / kStages) & 1, kWaitLimit)) {
+                    fail = true;
+                    break;
+                }
+                tc_fence_after();
+                const uint64_t ad = desc_kmajor_sw128(smem_u32(sA + s * kTileBytes));
+                const uint64_t bd = desc_kmajor_sw128(smem_u32(sB + s * kTileBytes));
+#pragma unroll
+                for (int k = 0; k < BK / 16; ++k)
+                    mma_bf16(tmem, ad + 2 * k, bd + 2 * k, idesc,
+                             (kb | k) != 0 ? 1u : 0u);
+                mma_commit(&empty[s]);
+            }
+            // Arrives once every MMA issued above has completed (also after a
+            // failed wait, so the epilogue never reads a live accumulator).
+            mma_commit(accb);
+        }
+        __syncwarp();
+    }
+    if (fail) atomicOr(err, ERR_SPIN_TIMEOUT);
+
+    // Epilogue: warp w drains TMEM lanes [32w, 32w + 32) = tile rows.
+    const bool got = __all_sync(~0u, mbar_wait(accb, 0, kWaitLimit));
+    tc_fence_after();
+    if (!got) {
+        if (lane == 0) atomicOr(err, ERR_SPIN_TIMEOUT);
+    } else {
+        const int row = m0 + warp * 32 + lane;
+        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+        for (int c = 0; c < BN / 32; ++c) {
+            uint32_t r[32];
+            tmem_ld32(trow + (uint32_t)(c * 32), r);
+            tmem_wait_ld();
+            epilogue_chunk<EPI>(r, row, n0 + c * 32, ep);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, BN);
+}
+
+// ------------------------------------------------------------ tensor maps
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
+                                  void*, const cuuint64_t*, const cuuint64_t*,
+                                  const cuuint32_t*, const cuuint32_t*,
+                                  CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion,
+                                  CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static std::once_flag once;
+    static EncodeTiledFn fn = nullptr;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p,
+                                    cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+
+// Tensor map of a row-major rows x cols bf16 matrix with 128 x 64 boxes and
+// the 128-byte swizzle.
+int make_map(CUtensorMap* m, const void* ptr, long long rows, long long cols) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) {
+        set_error("pf_b200: cuTensorMapEncodeTiled is unavailable");
+        return -1;
+    }
+    if (((uintptr_t)ptr & 15u) || (cols * 2) % 16 || rows < BM || cols < BK) {
+        set_error("pf_b200: tensor map: bad matrix %lld x %lld", rows, cols);
+        return -1;
+    }
+    const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)BM};
+    const cuuint32_t es[2] = {1, 1};
+    const CUresult r =
+        fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims,
+           strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+           CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("pf_b200: cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return -1;
+    }
+    return 0;
+}
+
+struct MapRef {
+    const CUtensorMap* map;
+    int row0;
+    int k0;
+};
+
+template <int EPI>
+int gemm(cudaStream_t s, MapRef a, MapRef b, int M, int N, int K,
+         const EpiArgs& ep, unsigned* err) {
+    if (M <= 0 || N <= 0 || K <= 0 || M % BM || N % BN || K % BK ||
+        (a.k0 % 8) || (b.k0 % 8)) {
+        set_error("pf_b200: gemm shape %d x %d x %d not tileable", M, N, K);
+        return -1;
+    }
+    PFB_CK(cudaFuncSetAttribute(k_gemm_bf16<EPI>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                kGemmSmem));
+    const dim3 grid(N / BN, M / BM);
+    k_gemm_bf16<EPI><<<grid, 128, kGemmSmem, s>>>(*a.map, *b.map, K, a.row0,
+                                                  a.k0, b.row0, b.k0, ep, err);
+    PFB_KL();
+    return 0;
+}
+
+// ------------------------------------------------------- elementwise kernels
+
+__device__ __forceinline__ float warp_max_f(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(~0u, v, o));
+    return v;
+}
+
+__device__ __forceinline__ float sigmoidf_(float x) { return 1.0f / (1.0f + expf(-x)); }
+
+// Mixture negative log-likelihood and its gradient with respect to the 288
+// used outputs, one warp per sample (lane c = component c):
+//   log pi_c = logit_c - LSE(logit)
+//   ls_cd = LS_LO + (LS_HI - LS_LO) sigmoid(raw_cd),  sigma = exp(ls)
+//   z_cd = (y_d - mu_cd) / sigma_cd
+//   a_c = log pi_c - sum_d (z^2 / 2 + ls_cd + log(2 pi) / 2)
+//   loss = -LSE(a),  r_c = exp(a_c + loss)   (responsibilities)
+//   dloss/dlogit_c = pi_c - r_c;  dloss/dmu = -r z / sigma;
+//   dloss/draw = r (1 - z^2) (LS_HI - LS_LO) s (1 - s)
+// Gradients are scaled by inv_b (mean over the batch) and written as bf16
+// (padding columns 288..383 zero).
+__global__ void k_gmm_loss(const float* __restrict__ Z, const float* __restrict__ Y,
+                           int y_row0, int rows, float inv_b,
+                           bf16* __restrict__ dZ, float* __restrict__ loss_acc) {
+    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (wid >= rows) return;
+    const float* z = Z + (size_t)wid * kOut;
+    const float* y = Y + (size_t)(y_row0 + wid) * 4;
+    const float logit = z[lane];
+    const float yv[4] = {y[0], y[1], y[2], y[3]};
+    const float mx = warp_max_f(logit);
+    const float lse_l = mx + logf(warp_sum_f(expf(logit - mx)));
+    const float logpi = logit - lse_l;
+    const float pi = expf(logpi);
+    float zz[4], sg[4], sig[4], mu[4];
+    float nll = 4.0f * kHalfLog2Pi;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+        mu[d] = z[kMeanOff + 4 * lane + d];
+        const float s = sigmoidf_(z[kSigOff + 4 * lane + d]);
+        const float ls = kLsLo + (kLsHi - kLsLo) * s;
+        sg[d] = s;
+        sig[d] = expf(ls);
+        zz[d] = (yv[d] - mu[d]) / sig[d];
+        nll += 0.5f * zz[d] * zz[d] + ls;
+    }
+    const float a = logpi - nll;
+    const float amx = warp_max_f(a);
+    const float logp = amx + logf(warp_sum_f(expf(a - amx)));
+    const float r = expf(a - logp);
+    if (lane == 0) atomicAdd(loss_acc, -logp * inv_b);
+    bf16* o = dZ + (size_t)wid * kOut;
+    o[lane] = __float2bfloat16_rn((pi - r) * inv_b);
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+        o[kMeanOff + 4 * lane + d] = __float2bfloat16_rn(-r * zz[d] / sig[d] * inv_b);
+        o[kSigOff + 4 * lane + d] = __float2bfloat16_rn(
+            r * (1.0f - zz[d] * zz[d]) * (kLsHi - kLsLo) * sg[d] * (1.0f - sg[d]) *
+            inv_b);
+    }
+    for (int p = kUsedOut + lane; p < kOut; p += 32) o[p] = __float2bfloat16_rn(0.0f);
+}
+
+// out[c][r] = in[r][c] for an R x C bf16 matrix; 32 x 32 tiles, block 32 x 8.
+__global__ void k_transpose_bf16(const bf16* __restrict__ in, long long ld_in,
+                                 bf16* __restrict__ out, long long ld_out,
+                                 long long R, long long C) {
+    __shared__ bf16 t[32][34];
+    const long long c0 = (long long)blockIdx.x * 32, r0 = (long long)blockIdx.y * 32;
+    for (int i = threadIdx.y; i < 32; i += 8) {
+        const long long r = r0 + i, c = c0 + threadIdx.x;
+        if (r < R && c < C) t[i][threadIdx.x] = in[r * ld_in + c];
+    }
+    __syncthreads();
+    for (int i = threadIdx.y; i < 32; i += 8) {
+        const long long c = c0 + i, r = r0 + threadIdx.x;
+        if (r < R && c < C) out[c * ld_out + r] = t[threadIdx.x][i];
+    }
+}
+
+// out[o] = sum over cols of in[o][*] (bf16 rows, f32 sum), one warp per row.
+__global__ void k_rowsum_bf16(const bf16* __restrict__ in, int ld, int cols,
+                              int rows, float* __restrict__ out) {
+    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (wid >= rows) return;
+    const __nv_bfloat162* p =
+        reinterpret_cast<const __nv_bfloat162*>(in + (size_t)wid * ld);
+    float acc = 0.0f;
+    for (int c = lane; c < cols / 2; c += 32) {
+        const float2 f = __bfloat1622float2(p[c]);
+        acc += f.x + f.y;
+    }
+    acc = warp_sum_f(acc);
+    if (lane == 0) out[wid] = acc;
+}
+
+// Adam on one weight matrix [out][in] (f32 master, moments) followed by the
+// bf16 copies W [out][in] and W^T [in][out]; 32 x 32 tiles, block 32 x 8.
+// With update == 0 only the bf16 copies are refreshed from the masters.
+__global__ void k_adam_w(int out, int in, float* __restrict__ w,
+                         float* __restrict__ m, float* __restrict__ v,
+                         const float* __restrict__ g, bf16* __restrict__ wb,
+                         bf16* __restrict__ wtb, int update, float lr, float b1,
+                         float b2, float eps, float bc1, float bc2) {
+    __shared__ bf16 t[32][34];
+    const int i0 = blockIdx.x * 32, o0 = blockIdx.y * 32;
+    for (int rr = threadIdx.y; rr < 32; rr += 8) {
+        const size_t idx = (size_t)(o0 + rr) * in + i0 + threadIdx.x;
+        float ww = w[idx];
+        if (update) {
+            const float gg = g[idx];
+            const float mm = b1 * m[idx] + (1.0f - b1) * gg;
+            const float vv = b2 * v[idx] + (1.0f - b2) * gg * gg;
+            m[idx] = mm;
+            v[idx] = vv;
+            ww -= lr * (mm / bc1) / (sqrtf(vv / bc2) + eps);
+            w[idx] = ww;
+        }
+        const bf16 h = __float2bfloat16_rn(ww);
+        wb[idx] = h;
+        t[rr][threadIdx.x] = h;
+    }
+    __syncthreads();
+    for (int cc = threadIdx.y; cc < 32; cc += 8)
+        wtb[(size_t)(i0 + cc) * out + o0 + threadIdx.x] = t[threadIdx.x][cc];
+}
+
+__global__ void k_adam_b(int n, float* __restrict__ b, float* __restrict__ m,
+                         float* __restrict__ v, const float* __restrict__ g,
+                         float lr, float b1, float b2, float eps, float bc1,
+                         float bc2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gg = g[i];
+    const float mm = b1 * m[i] + (1.0f - b1) * gg;
+    const float vv = b2 * v[i] + (1.0f - b2) * gg * gg;
+    m[i] = mm;
+    v[i] = vv;
+    b[i] -= lr * (mm / bc1) / (sqrtf(vv / bc2) + eps);
+}
+
+// He-uniform initialisation from Philox (counter (i, layer, part, INIT)).
+__global__ void k_init_uniform(float* __restrict__ p, long long n, float lo,
+                               float hi, uint32_t layer, uint32_t part,
+                               uint64_t seed) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const U4 r = philox4x32_10({(uint32_t)i, layer, part, RNG_LP_INIT},
+                               (uint32_t)seed, (uint32_t)(seed >> 32));
+    p[i] = lo + (hi - lo) * u01_open(r.x);
+}
+
+__global__ void k_f32_to_bf16(const float* __restrict__ in, bf16* __restrict__ out,
+                              long long n) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = __float2bfloat16_rn(in[i]);
+}
+
+// --------------------------------------------------------- scan rendering
+
+struct RenderArgs {
+    GridView gv;
+    int grid_bytes;
+    int nrays;
+    float rmax, span, noise;
+    uint64_t seed;
+    float cx, cy, sx, sy;  // pose normalisation
+};
+
+// Scan of one pose by one warp: lanes take groups of 4 consecutive rays; the
+// range noise of group q of sample `id` comes from Philox counter
+// (id, q, 0, LP_NOISE).  Writes f32 ranges (out_f, may be null) and/or the
+// network input row bf16(range / rmax) padded with zeros to kIn (out_x).
+__device__ __forceinline__ void render_pose(const RenderArgs& a,
+                                            const unsigned char* g, float x,
+                                            float y, float th, uint32_t id,
+                                            float* out_f, bf16* out_x) {
+    const int lane = threadIdx.x & 31;
+    int start = 0;
+    float frx = 0.f, fry = 0.f;
+    const bool inside = start_cell(a.gv, x, y, start, frx, fry);
+    const float inv_rmax = 1.0f / a.rmax;
+    const int ngroups = (a.nrays + 3) / 4;
+    for (int q = lane; q < ngroups; q += 32) {
+        const U4 u = philox4x32_10({id, (uint32_t)q, 0u, RNG_LP_NOISE},
+                                   (uint32_t)a.seed, (uint32_t)(a.seed >> 32));
+        const float2 n01 = box_muller(u01_open(u.x), u01_open(u.y));
+        const float2 n23 = box_muller(u01_open(u.z), u01_open(u.w));
+        const float nz[4] = {n01.x, n01.y, n23.x, n23.y};
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const int r = 4 * q + t;
+            if (r >= a.nrays) break;
+            float d = a.rmax;
+            if (inside) {
+                float dx, dy;
+                sincosf(ray_angle(th, r, a.nrays, a.span), &dy, &dx);
+                d = cast_ray(g, a.gv.Wp, start, frx, fry, dx, dy, a.gv.res, a.rmax);
+            }
+            const float val = d + a.noise * nz[t];
+            if (out_f) out_f[r] = val;
+            if (out_x) out_x[r] = __float2bfloat16_rn(val * inv_rmax);
+        }
+    }
+    if (out_x)
+        for (int r = a.nrays + lane; r < kIn; r += 32)
+            out_x[r] = __float2bfloat16_rn(0.0f);
+}
+
+// Uniform pose of sample id: free cell + in-cell offset, yaw in [0, 2 pi).
+__device__ __forceinline__ void random_pose(const RenderArgs& a, int nfree,
+                                            const int2* __restrict__ free_cells,
+                                            uint32_t id, uint32_t stream,
+                                            float& x, float& y, float& th) {
+    const U4 u = philox4x32_10({id, stream, 0u, RNG_LP_POSE}, (uint32_t)a.seed,
+                               (uint32_t)(a.seed >> 32));
+    const int c = min((int)(u01_open(u.w) * (float)nfree), nfree - 1);
+    const int2 cell = free_cells[c];
+    x = a.gv.ox + ((float)cell.x + u01_open(u.x)) * a.gv.res;
+    y = a.gv.oy + ((float)cell.y + u01_open(u.y)) * a.gv.res;
+    th = 6.28318530f * (u01_open(u.z) - 0.5f / 8388608.0f);
+}
+
+__device__ __forceinline__ const unsigned char* stage_grid(const RenderArgs& a,
+                                                           unsigned char* smem) {
+    const int nv = a.grid_bytes / 16;
+    const uint4* src = reinterpret_cast<const uint4*>(a.gv.cells);
+    uint4* dst = reinterpret_cast<uint4*>(smem);
+    for (int k = threadIdx.x; k < nv; k += blockDim.x) dst[k] = __ldg(&src[k]);
+    __syncthreads();
+    return smem;
+}
+
+// Training pairs [i0, i0 + n): random pose, rendered scan -> X row, target
+// (x_n, y_n, cos, sin) -> Y row.  Persistent blocks, grid in shared memory.
+__global__ void __launch_bounds__(256)
+    k_make_pairs(RenderArgs a, int nfree, const int2* __restrict__ free_cells,
+                 long long i0, long long n, bf16* __restrict__ X,
+                 float* __restrict__ Y) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const unsigned char* g = stage_grid(a, smem);
+    const int lane = threadIdx.x & 31;
+    const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+         w < n; w += nw) {
+        const long long i = i0 + w;
+        float x, y, th;
+        random_pose(a, nfree, free_cells, (uint32_t)i, (uint32_t)(i >> 32), x, y, th);
+        render_pose(a, g, x, y, th, (uint32_t)i, nullptr, X + (size_t)i * kIn);
+        if (lane == 0) {
+            float* t = Y + (size_t)i * 4;
+            t[0] = (x - a.cx) / a.sx;
+            t[1] = (y - a.cy) / a.sy;
+            t[2] = cosf(th);
+            t[3] = sinf(th);
+        }
+    }
+}
+
+// Scans at caller poses (one warp per pose).
+__global__ void __launch_bounds__(256)
+    k_render(RenderArgs a, const float* __restrict__ pose, int n,
+             float* __restrict__ out) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const unsigned char* g = stage_grid(a, smem);
+    const int nw = gridDim.x * (blockDim.x >> 5);
+    for (int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < n; w += nw)
+        render_pose(a, g, pose[3 * w], pose[3 * w + 1], pose[3 * w + 2],
+                    (uint32_t)w, out + (size_t)w * a.nrays, nullptr);
+}
+
+// Uniform held-out poses (same generator as the training pairs, own seed).
+__global__ void k_random_poses(RenderArgs a, int nfree,
+                               const int2* __restrict__ free_cells, int n,
+                               float* __restrict__ pose) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float x, y, th;
+    random_pose(a, nfree, free_cells, (uint32_t)i, 0u, x, y, th);
+    pose[3 * i] = x;
+    pose[3 * i + 1] = y;
+    pose[3 * i + 2] = th;
+}
+
+// Network input row 0 from a device scan: bf16(scan / rmax), zero padded.
+__global__ void k_query_row(const float* __restrict__ scan, int nrays,
+                            float inv_rmax, bf16* __restrict__ x) {
+    for (int r = threadIdx.x; r < kIn; r += blockDim.x)
+        x[r] = __float2bfloat16_rn(r < nrays ? scan[r] * inv_rmax : 0.0f);
+}
+
+// n hypotheses from the mixture in Z row 0: component by inverse CDF of
+// softmax(logits), then a diagonal Gaussian draw in (x_n, y_n, c, s); yaw =
+// atan2(s, c).  Sample i uses Philox counters (i, query, 0/1, LP_SAMPLE).
+__global__ void k_lp_sample(const float* __restrict__ Z, int n, uint64_t seed,
+                            uint32_t query, float cx, float cy, float sx,
+                            float sy, float* __restrict__ hyp) {
+    __shared__ float s_cum[kComp];
+    __shared__ float s_mu[4 * kComp], s_sig[4 * kComp];
+    const int t = threadIdx.x;
+    if (t < 32) {
+        const float l = Z[t];
+        const float mx = warp_max_f(l);
+        float e = expf(l - mx);
+        float c = e;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const float o = __shfl_up_sync(~0u, c, d);
+            if (t >= d) c += o;
+        }
+        const float tot = __shfl_sync(~0u, c, 31);
+        s_cum[t] = c / tot;
+    }
+    if (t < 4 * kComp) {
+        s_mu[t] = Z[kMeanOff + t];
+        const float s = sigmoidf_(Z[kSigOff + t]);
+        s_sig[t] = expf(kLsLo + (kLsHi - kLsLo) * s);
+    }
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + t;
+    if (i >= n) return;
+    const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    const U4 a = philox4x32_10({(uint32_t)i, query, 0u, RNG_LP_SAMPLE}, k0, k1);
+    const U4 b = philox4x32_10({(uint32_t)i, query, 1u, RNG_LP_SAMPLE}, k0, k1);
+    const float uc = u01_open(a.x);
+    int c = kComp - 1;
+    for (int j = 0; j < kComp; ++j)
+        if (s_cum[j] >= uc) {
+            c = j;
+            break;
+        }
+    const float2 n01 = box_muller(u01_open(a.y), u01_open(a.z));
+    const float2 n23 = box_muller(u01_open(a.w), u01_open(b.x));
+    const float* mu = s_mu + 4 * c;
+    const float* sg = s_sig + 4 * c;
+    const float xn = mu[0] + sg[0] * n01.x;
+    const float yn = mu[1] + sg[1] * n01.y;
+    const float cc = mu[2] + sg[2] * n23.x;
+    const float ss = mu[3] + sg[3] * n23.y;
+    hyp[3 * i] = cx + sx * xn;
+    hyp[3 * i + 1] = cy + sy * yn;
+    hyp[3 * i + 2] = atan2f(ss, cc);
+}
+
+// ------------------------------------------------------------------ handle
+
+struct Layer {
+    int in = 0, out = 0;
+    float* w = nullptr;   // [out][in] f32 master
+    float* b = nullptr;   // [out]
+    float* mw = nullptr;  // Adam moments
+    float* vw = nullptr;
+    float* mb = nullptr;
+    float* vb = nullptr;
+    float* gw = nullptr;  // gradients
+    float* gb = nullptr;
+    bf16* wb = nullptr;   // [out][in]
+    bf16* wtb = nullptr;  // [in][out]
+    CUtensorMap tm_w, tm_wt;
+};
+
+struct LpHandle {
+    GlHandle* gl = nullptr;
+    cudaStream_t stream = nullptr;
+    int batch = 0;
+    uint64_t seed = 0;
+    Layer L[kLayers];
+    bf16* H[kLayers - 1] = {};
+    bf16* HT[kLayers - 1] = {};
+    bf16* dZ[kLayers] = {};
+    bf16* dZT[kLayers] = {};
+    float* Z4 = nullptr;
+    CUtensorMap tm_H[kLayers - 1], tm_HT[kLayers - 1], tm_dZ[kLayers],
+        tm_dZT[kLayers];
+    // training pairs
+    bf16* X = nullptr;
+    bf16* XT = nullptr;
+    float* Y = nullptr;
+    long long n_pairs = 0;
+    CUtensorMap tm_X, tm_XT;
+    int data_nrays = 360;
+    float data_rmax = 10.0f;
+    // caller inputs (gradient check, forward, queries): batch rows
+    bf16* Xp = nullptr;
+    bf16* XpT = nullptr;
+    float* Xp_f = nullptr;
+    float* Yp = nullptr;
+    CUtensorMap tm_Xp, tm_XpT;
+    // bookkeeping
+    unsigned* d_err = nullptr;
+    float* d_loss = nullptr;
+    int loss_cap = 0;
+    long long adam_t = 0;
+    long long train_step = 0;
+    float cx = 0, cy = 0, sx = 1, sy = 1;
+    float tau = INFINITY;
+    uint32_t query_count = 0;
+    float* d_best = nullptr;
+};
+
+LpHandle* as_lp(void* p) { return static_cast<LpHandle*>(p); }
+
+RenderArgs render_args_gl(const GlHandle* g, int nrays, float rmax, float span,
+                          float noise, uint64_t seed) {
+    RenderArgs a;
+    a.gv = grid_view(g);
+    a.grid_bytes = grid_bytes_padded(g);
+    a.nrays = nrays;
+    a.rmax = rmax;
+    a.span = span;
+    a.noise = noise;
+    a.seed = seed;
+    a.cx = g->ox + 0.5f * g->W * g->res;
+    a.cy = g->oy + 0.5f * g->H * g->res;
+    a.sx = 0.5f * g->W * g->res;
+    a.sy = 0.5f * g->H * g->res;
+    return a;
+}
+
+RenderArgs render_args(const LpHandle* h, int nrays, float rmax, float span,
+                       float noise, uint64_t seed) {
+    return render_args_gl(h->gl, nrays, rmax, span, noise, seed);
+}
+
+int check_err(LpHandle* h) {
+    unsigned e = 0;
+    PFB_CK(cudaMemcpyAsync(&e, h->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                           h->stream));
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    if (e) {
+        set_error("pf_b200: learned proposal kernel wait timed out (err %u)", e);
+        cudaMemsetAsync(h->d_err, 0, sizeof(unsigned), h->stream);
+        return -1;
+    }
+    return 0;
+}
+
+// Refresh the bf16 weight copies of every layer from the f32 masters.
+int round_weights(LpHandle* h) {
+    for (int l = 0; l < kLayers; ++l) {
+        Layer& L = h->L[l];
+        k_adam_w<<<dim3(L.in / 32, L.out / 32), dim3(32, 8), 0, h->stream>>>(
+            L.out, L.in, L.w, L.mw, L.vw, L.gw, L.wb, L.wtb, 0, 0.f, 0.f, 0.f,
+            0.f, 1.f, 1.f);
+    }
+    PFB_KL();
+    return 0;
+}
+
+// Forward pass over `rows` rows of the input map x (rows a multiple of 128).
+int forward(LpHandle* h, MapRef x, int rows, bool write_t) {
+    cudaStream_t s = h->stream;
+    for (int l = 0; l < kLayers - 1; ++l) {
+        EpiArgs ep{};
+        ep.out = h->H[l];
+        ep.outT = write_t ? h->HT[l] : nullptr;
+        ep.bias = h->L[l].b;
+        ep.ldo = h->L[l].out;
+        ep.ldt = h->batch;
+        const MapRef a = l == 0 ? x : MapRef{&h->tm_H[l - 1], 0, 0};
+        if (gemm<EPI_RELU_BF16>(s, a, MapRef{&h->L[l].tm_w, 0, 0}, rows,
+                                h->L[l].out, h->L[l].in, ep, h->d_err))
+            return -1;
+    }
+    EpiArgs ep{};
+    ep.out = h->Z4;
+    ep.bias = h->L[kLayers - 1].b;
+    ep.ldo = kOut;
+    return gemm<EPI_BIAS_F32>(s, MapRef{&h->tm_H[kLayers - 2], 0, 0},
+                              MapRef{&h->L[kLayers - 1].tm_w, 0, 0}, rows, kOut,
+                              kHid, ep, h->d_err);
+}
+
+// Loss + backward over one batch (after forward); the loss is accumulated
+// into *d_loss_slot.  xt: the transposed input rows (columns = samples); Y:
+// the batch's targets.
+int backward(LpHandle* h, MapRef xt, const float* Y, float* d_loss_slot) {
+    cudaStream_t s = h->stream;
+    const int B = h->batch;
+    k_gmm_loss<<<ceil_div(B * 32, 256), 256, 0, s>>>(
+        h->Z4, Y, 0, B, 1.0f / (float)B, h->dZ[kLayers - 1], d_loss_slot);
+    PFB_KL();
+    k_transpose_bf16<<<dim3(kOut / 32, B / 32), dim3(32, 8), 0, s>>>(
+        h->dZ[kLayers - 1], kOut, h->dZT[kLayers - 1], B, B, kOut);
+    PFB_KL();
+    for (int l = kLayers - 1; l >= 0; --l) {
+        Layer& L = h->L[l];
+        EpiArgs eg{};
+        eg.out = L.gw;
+        eg.ldo = L.in;
+        eg.scale = 1.0f;
+        const MapRef bt = l == 0 ? xt : MapRef{&h->tm_HT[l - 1], 0, 0};
+        if (gemm<EPI_F32>(s, MapRef{&h->tm_dZT[l], 0, 0}, bt, L.out, L.in, B, eg,
+                          h->d_err))
+            return -1;
+        k_rowsum_bf16<<<ceil_div(L.out * 32, 256), 256, 0, s>>>(h->dZT[l], B, B,
+                                                                 L.out, L.gb);
+        PFB_KL();
+        if (l > 0) {
+            EpiArgs ed{};
+            ed.out = h->dZ[l - 1];
+            ed.outT = h->dZT[l - 1];
+            ed.mask = h->H[l - 1];
+            ed.ldo = L.in;
+            ed.ldt = B;
+            ed.ldm = L.in;
+            if (gemm<EPI_DRELU_BF16>(s, MapRef{&h->tm_dZ[l], 0, 0},
+                                     MapRef{&L.tm_wt, 0, 0}, B, L.in, L.out, ed,
+                                     h->d_err))
+                return -1;
+        }
+    }
+    return 0;
+}
+
+int adam_update(LpHandle* h, float lr) {
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    h->adam_t += 1;
+    const float bc1 = 1.0f - powf(b1, (float)h->adam_t);
+    const float bc2 = 1.0f - powf(b2, (float)h->adam_t);
+    for (int l = 0; l < kLayers; ++l) {
+        Layer& L = h->L[l];
+        k_adam_w<<<dim3(L.in / 32, L.out / 32), dim3(32, 8), 0, h->stream>>>(
+            L.out, L.in, L.w, L.mw, L.vw, L.gw, L.wb, L.wtb, 1, lr, b1, b2, eps,
+            bc1, bc2);
+        k_adam_b<<<ceil_div(L.out, 256), 256, 0, h->stream>>>(
+            L.out, L.b, L.mb, L.vb, L.gb, lr, b1, b2, eps, bc1, bc2);
+    }
+    PFB_KL();
+    return 0;
+}
+
+// Training pairs: the Y pointer passed to the loss kernel is already offset
+// to the batch's first row.
+int train_one(LpHandle* h, long long row0, float lr, float* d_loss_slot) {
+    const MapRef x{&h->tm_X, (int)row0, 0};
+    const MapRef xt{&h->tm_XT, 0, (int)row0};
+    if (forward(h, x, h->batch, true)) return -1;
+    if (backward(h, xt, h->Y + (size_t)row0 * 4, d_loss_slot)) return -1;
+    return adam_update(h, lr);
+}
+
+void free_lp(LpHandle* h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (int l = 0; l < kLayers; ++l) {
+        Layer& L = h->L[l];
+        cudaFree(L.w);
+        cudaFree(L.b);
+        cudaFree(L.mw);
+        cudaFree(L.vw);
+        cudaFree(L.mb);
+        cudaFree(L.vb);
+        cudaFree(L.gw);
+        cudaFree(L.gb);
+        cudaFree(L.wb);
+        cudaFree(L.wtb);
+        cudaFree(h->dZ[l]);
+        cudaFree(h->dZT[l]);
+    }
+    for (int l = 0; l < kLayers - 1; ++l) {
+        cudaFree(h->H[l]);
+        cudaFree(h->HT[l]);
+    }
+    cudaFree(h->Z4);
+    cudaFree(h->X);
+    cudaFree(h->XT);
+    cudaFree(h->Y);
+    cudaFree(h->Xp);
+    cudaFree(h->XpT);
+    cudaFree(h->Xp_f);
+    cudaFree(h->Yp);
+    cudaFree(h->d_err);
+    cudaFree(h->d_loss);
+    cudaFree(h->d_best);
+    delete h;
+}
+
+template <class T>
+int dalloc(T** p, size_t count) {
+    PFB_CK(cudaMalloc((void**)p, sizeof(T) * std::max<size_t>(count, 1)));
+    return 0;
+}
+
+long long num_params() {
+    long long n = 0;
+    for (int l = 0; l < kLayers; ++l)
+        n += (long long)layer_out(l) * layer_in(l) + layer_out(l);
+    return n;
+}
+
+// Localize against the scan already in gl->d_scan with n learned samples.
+int learned_pass(LpHandle* h, int nrays, float rmax, float span, int n_samples,
+                 int k, float* out3k, float* caer_k, int* idx_k) {
+    GlHandle* g = h->gl;
+    k_query_row<<<1, 128, 0, h->stream>>>(g->d_scan, nrays, 1.0f / rmax, h->Xp);
+    PFB_KL();
+    if (forward(h, MapRef{&h->tm_Xp, 0, 0}, BM, false)) return -1;
+    k_lp_sample<<<ceil_div(n_samples, 256), 256, 0, h->stream>>>(
+        h->Z4, n_samples, h->seed ^ 0x5DEECE66DULL, h->query_count++, h->cx,
+        h->cy, h->sx, h->sy, g->d_hyp);
+    PFB_KL();
+    g->nh = n_samples;
+    g->caer_valid = false;
+    return gl_localize_loaded(g, nrays, rmax, span, k, out3k, caer_k, idx_k);
+}
+
+}  // namespace lp
+}  // namespace pfb
+
+using namespace pfb;
+using namespace pfb::lp;
+
+extern "C" {
+
+long long pfgl_learned_num_params(void) { return num_params(); }
+
+void* pfgl_learned_create(void* glv, int batch, unsigned long long seed) {
+    clear_error();
+    GlHandle* g = static_cast<GlHandle*>(glv);
+    if (!g || batch < BM || batch % BM) {
+        set_error("pf_b200: pfgl_learned_create: batch must be a positive multiple of 128");
+        return nullptr;
+    }
+    LpHandle* h = new (std::nothrow) LpHandle();
+    if (!h) return nullptr;
+    h->gl = g;
+    h->stream = g->stream;
+    h->batch = batch;
+    h->seed = seed;
+    h->cx = g->ox + 0.5f * g->W * g->res;
+    h->cy = g->oy + 0.5f * g->H * g->res;
+    h->sx = 0.5f * g->W * g->res;
+    h->sy = 0.5f * g->H * g->res;
+    bool ok = false;
+    do {
+        bool bad = false;
+        for (int l = 0; l < kLayers && !bad; ++l) {
+            Layer& L = h->L[l];
+            L.in = layer_in(l);
+            L.out = layer_out(l);
+            const size_t nw = (size_t)L.in * L.out;
+            bad = dalloc(&L.w, nw) || dalloc(&L.b, L.out) || dalloc(&L.mw, nw) ||
+                  dalloc(&L.vw, nw) || dalloc(&L.mb, L.out) ||
+                  dalloc(&L.vb, L.out) || dalloc(&L.gw, nw) ||
+                  dalloc(&L.gb, L.out) || dalloc(&L.wb, nw) || dalloc(&L.wtb, nw) ||
+                  dalloc(&h->dZ[l], (size_t)batch * L.out) ||
+                  dalloc(&h->dZT[l], (size_t)batch * L.out);
+            if (bad) break;
+            bad = make_map(&L.tm_w, L.wb, L.out, L.in) ||
+                  make_map(&L.tm_wt, L.wtb, L.in, L.out) ||
+                  make_map(&h->tm_dZ[l], h->dZ[l], batch, L.out) ||
+                  make_map(&h->tm_dZT[l], h->dZT[l], L.out, batch);
+        }
+        if (bad) break;
+        for (int l = 0; l < kLayers - 1 && !bad; ++l) {
+            bad = dalloc(&h->H[l], (size_t)batch * kHid) ||
+                  dalloc(&h->HT[l], (size_t)batch * kHid) ||
+                  make_map(&h->tm_H[l], h->H[l], batch, kHid) ||
+                  make_map(&h->tm_HT[l], h->HT[l], kHid, batch);
+        }
+        if (bad) break;
+        if (dalloc(&h->Z4, (size_t)batch * kOut) ||
+            dalloc(&h->Xp, (size_t)batch * kIn) ||
+            dalloc(&h->XpT, (size_t)batch * kIn) ||
+            dalloc(&h->Xp_f, (size_t)batch * kIn) ||
+            dalloc(&h->Yp, (size_t)batch * 4) || dalloc(&h->d_err, 1) ||
+            dalloc(&h->d_best, 64))
+            break;
+        if (make_map(&h->tm_Xp, h->Xp, batch, kIn) ||
+            make_map(&h->tm_XpT, h->XpT, kIn, batch))
+            break;
+        if (cudaMemsetAsync(h->Xp, 0, sizeof(bf16) * (size_t)batch * kIn,
+                            h->stream) != cudaSuccess ||
+            cudaMemsetAsync(h->d_err, 0, sizeof(unsigned), h->stream) != cudaSuccess)
+            break;
+        // Initialisation: He-uniform hidden layers; small output layer with
+        // spread mixture means.
+        for (int l = 0; l < kLayers; ++l) {
+            Layer& L = h->L[l];
+            const long long nw = (long long)L.in * L.out;
+            float bound = sqrtf(6.0f / (float)(l == 0 ? 360 : L.in));
+            if (l == kLayers - 1) bound *= 0.1f;
+            k_init_uniform<<<(unsigned)((nw + 255) / 256), 256, 0, h->stream>>>(
+                L.w, nw, -bound, bound, (uint32_t)l, 0u, seed);
+            cudaMemsetAsync(L.b, 0, sizeof(float) * L.out, h->stream);
+            cudaMemsetAsync(L.mw, 0, sizeof(float) * nw, h->stream);
+            cudaMemsetAsync(L.vw, 0, sizeof(float) * nw, h->stream);
+            cudaMemsetAsync(L.mb, 0, sizeof(float) * L.out, h->stream);
+            cudaMemsetAsync(L.vb, 0, sizeof(float) * L.out, h->stream);
+        }
+        {
+            // Output layer: rows >= 288 (padding) zero; mean biases spread.
+            Layer& L = h->L[kLayers - 1];
+            cudaMemsetAsync(L.w + (size_t)kUsedOut * L.in, 0,
+                            sizeof(float) * (size_t)(kOut - kUsedOut) * L.in,
+                            h->stream);
+            k_init_uniform<<<1, 128, 0, h->stream>>>(L.b + kMeanOff, 4 * kComp,
+                                                     -0.8f, 0.8f,
+                                                     (uint32_t)kLayers, 1u, seed);
+        }
+        if (cudaGetLastError() != cudaSuccess) break;
+        if (round_weights(h)) break;
+        if (cudaStreamSynchronize(h->stream) != cudaSuccess) break;
+        ok = true;
+    } while (0);
+    if (!ok) {
+        set_error("pf_b200: pfgl_learned_create failed: %s",
+                  cudaGetErrorString(cudaGetLastError()));
+        free_lp(h);
+        return nullptr;
+    }
+    return h;
+}
+
+int pfgl_learned_destroy(void* p) {
+    free_lp(as_lp(p));
+    return 0;
+}
+
+int pfgl_learned_norm(void* p, float* c4) {
+    LpHandle* h = as_lp(p);
+    if (!h || !c4) return -1;
+    c4[0] = h->cx;
+    c4[1] = h->cy;
+    c4[2] = h->sx;
+    c4[3] = h->sy;
+    return 0;
+}
+
+int pfgl_learned_get_params(void* p, float* out) {
+    LpHandle* h = as_lp(p);
+    if (!h || !out) return -1;
+    size_t off = 0;
+    for (int l = 0; l < kLayers; ++l) {
+        Layer& L = h->L[l];
+        const size_t nw = (size_t)L.in * L.out;
+        PFB_CK(cudaMemcpyAsync(out + off, L.w, sizeof(float) * nw,
+                               cudaMemcpyDeviceToHost, h->stream));
+        off += nw;
+        PFB_CK(cudaMemcpyAsync(out + off, L.b, sizeof(float) * L.out,
+                               cudaMemcpyDeviceToHost, h->stream));
+        off += L.out;
+    }
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int pfgl_learned_set_params(void* p, const float* in) {
+    LpHandle* h = as_lp(p);
+    if (!h || !in) return -1;
+    size_t off = 0;
+    for (int l = 0; l < kLayers; ++l) {
+        Layer& L = h->L[l];
+        const size_t nw = (size_t)L.in * L.out;
+        PFB_CK(cudaMemcpyAsync(L.w, in + off, sizeof(float) * nw,
+                               cudaMemcpyHostToDevice, h->stream));
+        off += nw;
+        PFB_CK(cudaMemcpyAsync(L.b, in + off, sizeof(float) * L.out,
+                               cudaMemcpyHostToDevice, h->stream));
+        off += L.out;
+    }
+    if (round_weights(h)) return -1;
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int pfgl_render_scans(void* glv, const float* pose3n, int n, int nrays,
+                      float rmax, float ang_span, float noise_std,
+                      unsigned long long seed, float* out) {
+    GlHandle* g = static_cast<GlHandle*>(glv);
+    if (!g || !pose3n || !out || n <= 0 || nrays <= 0) return -1;
+    const RenderArgs a = render_args_gl(g, nrays, rmax, ang_span, noise_std, seed);
+    float* d_pose = nullptr;
+    float* d_out = nullptr;
+    int rc = -1;
+    do {
+        if (cudaMalloc((void**)&d_pose, sizeof(float) * 3 * (size_t)n) != cudaSuccess ||
+            cudaMalloc((void**)&d_out, sizeof(float) * (size_t)n * nrays) != cudaSuccess)
+            break;
+        if (cudaMemcpyAsync(d_pose, pose3n, sizeof(float) * 3 * (size_t)n,
+                            cudaMemcpyHostToDevice, g->stream) != cudaSuccess)
+            break;
+        const size_t smem = (size_t)a.grid_bytes;
+        if (smem > 200 * 1024) {
+            set_error("pf_b200: pfgl_render_scans: map too large for shared memory");
+            break;
+        }
+        if (cudaFuncSetAttribute(k_render, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess)
+            break;
+        k_render<<<std::min(ceil_div(n, 8), 1184), 256, smem, g->stream>>>(a, d_pose, n,
+                                                                         d_out);
+        if (cudaGetLastError() != cudaSuccess) break;
+        if (cudaMemcpyAsync(out, d_out, sizeof(float) * (size_t)n * nrays,
+                            cudaMemcpyDeviceToHost, g->stream) != cudaSuccess)
+            break;
+        if (cudaStreamSynchronize(g->stream) != cudaSuccess) break;
+        rc = 0;
+    } while (0);
+    if (rc) set_error("pf_b200: pfgl_render_scans failed: %s",
+                      cudaGetErrorString(cudaGetLastError()));
+    cudaFree(d_pose);
+    cudaFree(d_out);
+    return rc;
+}
+
+int pfgl_learned_make_data(void* p, long long n_pairs, int nrays, float rmax,
+                           float ang_span, float noise_std,
+                           unsigned long long seed) {
+    LpHandle* h = as_lp(p);
+    if (!h || n_pairs < h->batch || nrays <= 0 || nrays > kIn) {
+        set_error("pf_b200: pfgl_learned_make_data: bad arguments");
+        return -1;
+    }
+    if (h->gl->nfree <= 0) return -1;
+    // Round to whole batches.
+    n_pairs = n_pairs / h->batch * h->batch;
+    if (n_pairs > (1ll << 31) - h->batch) return -1;
+    cudaFree(h->X);
+    cudaFree(h->XT);
+    cudaFree(h->Y);
+    h->X = h->XT = nullptr;
+    h->Y = nullptr;
+    h->n_pairs = 0;
+    if (dalloc(&h->X, (size_t)n_pairs * kIn) || dalloc(&h->XT, (size_t)n_pairs * kIn) ||
+        dalloc(&h->Y, (size_t)n_pairs * 4))
+        return -1;
+    const RenderArgs a = render_args(h, nrays, rmax, ang_span, noise_std, seed);
+    const size_t smem = (size_t)a.grid_bytes;
+    if (smem > 200 * 1024) {
+        set_error("pf_b200: pfgl_learned_make_data: map too large for shared memory");
+        return -1;
+    }
+    PFB_CK(cudaFuncSetAttribute(k_make_pairs,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    k_make_pairs<<<sms * 4, 256, smem, h->stream>>>(a, h->gl->nfree, h->gl->d_free, 0,
+                                                    n_pairs, h->X, h->Y);
+    PFB_KL();
+    // XT[c][r] = X[r][c], in column chunks of at most 65535 * 32 rows.
+    const long long chunk = 65535ll * 32;
+    for (long long r0 = 0; r0 < n_pairs; r0 += chunk) {
+        const long long rows = std::min(chunk, n_pairs - r0);
+        k_transpose_bf16<<<dim3(kIn / 32, (unsigned)((rows + 31) / 32)), dim3(32, 8), 0,
+                           h->stream>>>(h->X + (size_t)r0 * kIn, kIn, h->XT + r0,
+                                        n_pairs, rows, kIn);
+    }
+    PFB_KL();
+    if (make_map(&h->tm_X, h->X, n_pairs, kIn) ||
+        make_map(&h->tm_XT, h->XT, kIn, n_pairs))
+        return -1;
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    h->n_pairs = n_pairs;
+    h->data_nrays = nrays;
+    h->data_rmax = rmax;
+    return 0;
+}
+
+int pfgl_learned_train(void* p, int steps, int total_steps, float lr,
+                       float* loss_out) {
+    LpHandle* h = as_lp(p);
+    if (!h || steps <= 0 || h->n_pairs < h->batch) {
+        set_error("pf_b200: pfgl_learned_train: no training pairs");
+        return -1;
+    }
+    if (total_steps < steps) total_steps = steps;
+    if (steps > h->loss_cap) {
+        cudaFree(h->d_loss);
+        h->d_loss = nullptr;
+        if (dalloc(&h->d_loss, (size_t)steps)) return -1;
+        h->loss_cap = steps;
+    }
+    PFB_CK(cudaMemsetAsync(h->d_loss, 0, sizeof(float) * steps, h->stream));
+    const long long nb = h->n_pairs / h->batch;
+    const int warm = std::max(1, total_steps / 20);
+    for (int i = 0; i < steps; ++i) {
+        const long long t = h->train_step++;
+        float lr_t;
+        if (t < warm)
+            lr_t = lr * (float)(t + 1) / (float)warm;
+        else {
+            const double f = std::min(1.0, (double)(t - warm) / std::max(1, total_steps - warm));
+            lr_t = (float)(lr * (0.02 + 0.98 * 0.5 * (1.0 + std::cos(M_PI * f))));
+        }
+        const long long row0 = (t % nb) * h->batch;
+        if (train_one(h, row0, lr_t, h->d_loss + i)) return -1;
+    }
+    if (loss_out)
+        PFB_CK(cudaMemcpyAsync(loss_out, h->d_loss, sizeof(float) * steps,
+                               cudaMemcpyDeviceToHost, h->stream));
+    return check_err(h);
+}
+
+int pfgl_learned_grad(void* p, const float* x, const float* y, float* loss,
+                      float* grad) {
+    LpHandle* h = as_lp(p);
+    if (!h || !x || !y || !grad) return -1;
+    const int B = h->batch;
+    const size_t nx = (size_t)B * kIn;
+    PFB_CK(cudaMemcpyAsync(h->Xp_f, x, sizeof(float) * nx, cudaMemcpyHostToDevice,
+                           h->stream));
+    PFB_CK(cudaMemcpyAsync(h->Yp, y, sizeof(float) * 4 * B, cudaMemcpyHostToDevice,
+                           h->stream));
+    k_f32_to_bf16<<<(unsigned)((nx + 255) / 256), 256, 0, h->stream>>>(h->Xp_f, h->Xp,
+                                                                      (long long)nx);
+    k_transpose_bf16<<<dim3(kIn / 32, B / 32), dim3(32, 8), 0, h->stream>>>(
+        h->Xp, kIn, h->XpT, B, B, kIn);
+    PFB_KL();
+    if (h->loss_cap < 1) {
+        if (dalloc(&h->d_loss, 1)) return -1;
+        h->loss_cap = 1;
+    }
+    PFB_CK(cudaMemsetAsync(h->d_loss, 0, sizeof(float), h->stream));
+    if (forward(h, MapRef{&h->tm_Xp, 0, 0}, B, true)) return -1;
+    if (backward(h, MapRef{&h->tm_XpT, 0, 0}, h->Yp, h->d_loss))
+        return -1;
+    size_t off = 0;
+    for (int l = 0; l < kLayers; ++l) {
+        Layer& L = h->L[l];
+        const size_t nw = (size_t)L.in * L.out;
+        PFB_CK(cudaMemcpyAsync(grad + off, L.gw, sizeof(float) * nw,
+                               cudaMemcpyDeviceToHost, h->stream));
+        off += nw;
+        PFB_CK(cudaMemcpyAsync(grad + off, L.gb, sizeof(float) * L.out,
+                               cudaMemcpyDeviceToHost, h->stream));
+        off += L.out;
+    }
+    if (loss)
+        PFB_CK(cudaMemcpyAsync(loss, h->d_loss, sizeof(float), cudaMemcpyDeviceToHost,
+                               h->stream));
+    return check_err(h);
+}
+
+int pfgl_learned_forward(void* p, const float* x, int rows, float* out) {
+    LpHandle* h = as_lp(p);
+    if (!h || !x || !out || rows <= 0 || rows > BM) return -1;
+    const size_t nx = (size_t)BM * kIn;
+    PFB_CK(cudaMemsetAsync(h->Xp_f, 0, sizeof(float) * nx, h->stream));
+    PFB_CK(cudaMemcpyAsync(h->Xp_f, x, sizeof(float) * (size_t)rows * kIn,
+                           cudaMemcpyHostToDevice, h->stream));
+    k_f32_to_bf16<<<(unsigned)((nx + 255) / 256), 256, 0, h->stream>>>(h->Xp_f, h->Xp,
+                                                                      (long long)nx);
+    PFB_KL();
+    if (forward(h, MapRef{&h->tm_Xp, 0, 0}, BM, false)) return -1;
+    PFB_CK(cudaMemcpy2DAsync(out, sizeof(float) * kUsedOut, h->Z4,
+                             sizeof(float) * kOut, sizeof(float) * kUsedOut, rows,
+                             cudaMemcpyDeviceToHost, h->stream));
+    return check_err(h);
+}
+
+int pfgl_learned_set_threshold(void* p, float tau) {
+    LpHandle* h = as_lp(p);
+    if (!h) return -1;
+    h->tau = tau;
+    return 0;
+}
+
+int pfgl_learned_localize(void* p, const float* scan, int nrays, float rmax,
+                          float ang_span, int n_samples, int n_fallback, int k,
+                          float* out3k, float* caer_k, int* idx_k, int* info) {
+    LpHandle* h = as_lp(p);
+    if (!h || !scan || nrays <= 0 || nrays > kIn || n_samples <= 0 || k <= 0 ||
+        n_samples > h->gl->cap_hyp || n_fallback > h->gl->cap_hyp)
+        return -1;
+    GlHandle* g = h->gl;
+    if (k > n_samples) k = n_samples;
+    std::vector<float> c1((size_t)k), o1(3 * (size_t)k);
+    std::vector<int> i1((size_t)k);
+    if (gl_upload_scan(g, scan, nrays)) return -1;
+    const int r1 = learned_pass(h, nrays, rmax, ang_span, n_samples, k, o1.data(),
+                                c1.data(), i1.data());
+    if (r1 <= 0) return -1;
+    if (check_err(h)) return -1;
+    int which = 0;
+    int rk = r1;
+    std::vector<float> c2, o2;
+    std::vector<int> i2;
+    if (n_fallback > 0 && !(c1[0] <= h->tau)) {
+        const int n_pos = std::max(1, n_fallback / 16);
+        if (gl_generate(g, n_pos, 16, h->seed + 0x9E3779B97F4A7C15ULL * (h->query_count + 1)))
+            return -1;
+        const int kk = std::min(k, n_pos * 16);
+        c2.resize(kk);
+        o2.resize(3 * (size_t)kk);
+        i2.resize(kk);
+        const int r2 = gl_localize_loaded(g, nrays, rmax, ang_span, kk, o2.data(),
+                                          c2.data(), i2.data());
+        if (r2 <= 0) return -1;
+        which = 1;
+        if (c2[0] < c1[0]) {
+            which = 2;
+            rk = r2;
+        }
+    }
+    const std::vector<float>& cs = which == 2 ? c2 : c1;
+    const std::vector<float>& os = which == 2 ? o2 : o1;
+    const std::vector<int>& is = which == 2 ? i2 : i1;
+    if (out3k) memcpy(out3k, os.data(), sizeof(float) * 3 * (size_t)rk);
+    if (caer_k) memcpy(caer_k, cs.data(), sizeof(float) * (size_t)rk);
+    if (idx_k) memcpy(idx_k, is.data(), sizeof(int) * (size_t)rk);
+    if (info) *info = which;
+    return rk;
+}
+
+int pfgl_learned_calibrate(void* p, int n_queries, int nrays, float rmax,
+                           float ang_span, float noise_std, int n_samples,
+                           float quantile, unsigned long long seed,
+                           float* tau_out, float* success_out) {
+    LpHandle* h = as_lp(p);
+    if (!h || n_queries <= 0 || nrays <= 0 || nrays > kIn || n_samples <= 0 ||
+        n_samples > h->gl->cap_hyp)
+        return -1;
+    GlHandle* g = h->gl;
+    const RenderArgs a = render_args(h, nrays, rmax, ang_span, noise_std, seed);
+    std::vector<float> poses(3 * (size_t)n_queries), scans((size_t)n_queries * nrays);
+    float* d_pose = nullptr;
+    if (dalloc(&d_pose, 3 * (size_t)n_queries)) return -1;
+    k_random_poses<<<ceil_div(n_queries, 128), 128, 0, h->stream>>>(
+        a, g->nfree, g->d_free, n_queries, d_pose);
+    const bool ok_launch = cudaGetLastError() == cudaSuccess &&
+                           cudaMemcpyAsync(poses.data(), d_pose,
+                                           sizeof(float) * poses.size(),
+                                           cudaMemcpyDeviceToHost,
+                                           h->stream) == cudaSuccess &&
+                           cudaStreamSynchronize(h->stream) == cudaSuccess;
+    cudaFree(d_pose);
+    if (!ok_launch) return -1;
+    if (pfgl_render_scans(g, poses.data(), n_queries, nrays, rmax, ang_span,
+                          noise_std, seed ^ 0xA5A5A5A5ULL, scans.data()))
+        return -1;
+    std::vector<float> good;
+    int n_ok = 0;
+    float out3[3], c0;
+    int i0;
+    for (int q = 0; q < n_queries; ++q) {
+        if (gl_upload_scan(g, scans.data() + (size_t)q * nrays, nrays)) return -1;
+        if (learned_pass(h, nrays, rmax, ang_span, n_samples, 1, out3, &c0, &i0) <= 0)
+            return -1;
+        const float* t = poses.data() + 3 * (size_t)q;
+        const double dp = std::hypot((double)out3[0] - t[0], (double)out3[1] - t[1]);
+        double dth = std::fmod((double)out3[2] - t[2] + M_PI, 2 * M_PI);
+        if (dth < 0) dth += 2 * M_PI;
+        dth = std::fabs(dth - M_PI);
+        if (dp <= 0.5 && dth <= 0.1) {
+            ++n_ok;
+            good.push_back(c0);
+        }
+    }
+    if (check_err(h)) return -1;
+    float tau = INFINITY;
+    if (!good.empty()) {
+        std::sort(good.begin(), good.end());
+        // Nearest-rank quantile.
+        const double qq = std::min(1.0, std::max(0.0, (double)quantile));
+        long long idx = (long long)std::ceil(qq * (double)good.size()) - 1;
+        idx = std::max(0ll, std::min((long long)good.size() - 1, idx));
+        tau = good[(size_t)idx];
+    }
+    h->tau = tau;
+    if (tau_out) *tau_out = tau;
+    if (success_out) *success_out = (float)n_ok / (float)n_queries;
+    return 0;
+}
+
+int pfgl_learned_gemm(int M, int N, int K, const unsigned short* A,
+                      const unsigned short* B, float* D) {
+    clear_error();
+    if (!A || !B || !D || M <= 0 || N <= 0 || K <= 0 || M % BM || N % BN || K % BK)
+        return -1;
+    bf16* dA = nullptr;
+    bf16* dB = nullptr;
+    float* dD = nullptr;
+    unsigned* dErr = nullptr;
+    int rc = -1;
+    cudaStream_t s = nullptr;
+    do {
+        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) break;
+        if (cudaMalloc((void**)&dA, sizeof(bf16) * (size_t)M * K) != cudaSuccess ||
+            cudaMalloc((void**)&dB, sizeof(bf16) * (size_t)N * K) != cudaSuccess ||
+            cudaMalloc((void**)&dD, sizeof(float) * (size_t)M * N) != cudaSuccess ||
+            cudaMalloc((void**)&dErr, sizeof(unsigned)) != cudaSuccess)
+            break;
+        if (cudaMemcpyAsync(dA, A, sizeof(bf16) * (size_t)M * K, cudaMemcpyHostToDevice,
+                            s) != cudaSuccess ||
+            cudaMemcpyAsync(dB, B, sizeof(bf16) * (size_t)N * K, cudaMemcpyHostToDevice,
+                            s) != cudaSuccess ||
+            cudaMemsetAsync(dErr, 0, sizeof(unsigned), s) != cudaSuccess)
+            break;
+        CUtensorMap ta, tb;
+        if (make_map(&ta, dA, M, K) || make_map(&tb, dB, N, K)) break;
+        EpiArgs ep{};
+        ep.out = dD;
+        ep.ldo = N;
+        ep.scale = 1.0f;
+        if (gemm<EPI_F32>(s, MapRef{&ta, 0, 0}, MapRef{&tb, 0, 0}, M, N, K, ep, dErr))
+            break;
+        unsigned e = 0;
+        if (cudaMemcpyAsync(D, dD, sizeof(float) * (size_t)M * N, cudaMemcpyDeviceToHost,
+                            s) != cudaSuccess ||
+            cudaMemcpyAsync(&e, dErr, sizeof(unsigned), cudaMemcpyDeviceToHost, s) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            break;
+        if (e) {
+            set_error("pf_b200: pfgl_learned_gemm: pipeline wait timed out");
+            break;
+        }
+        rc = 0;
+    } while (0);
+    if (rc && cudaGetLastError() != cudaSuccess)
+        set_error("pf_b200: pfgl_learned_gemm failed");
+    cudaFree(dA);
+    cudaFree(dB);
+    cudaFree(dD);
+    cudaFree(dErr);
+    if (s) cudaStreamDestroy(s);
+    return rc;
+}
+
+}  // extern "C"

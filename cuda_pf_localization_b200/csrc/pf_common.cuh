@@ -107,7 +107,7 @@ __host__ __device__ __forceinline__ float u01_open(uint32_t x) {
     return ((float)(x >> 9) + 0.5f) * (1.0f / 8388608.0f);
 }
 
-// Box–Muller pair (Box & Muller 1958) from two open uniforms.
+// Box-Muller pair (Box & Muller 1958) from two open uniforms.
 __device__ __forceinline__ float2 box_muller(float u1, float u2) {
     float r = sqrtf(-2.0f * logf(u1));
     float s, c;
@@ -120,6 +120,10 @@ enum : uint32_t {
     RNG_PF_A = 0u,   // normals 0..3 of a particle update
     RNG_PF_B = 1u,   // normals 4..5
     RNG_GL = 2u,     // hypothesis dispersion
+    RNG_LP_POSE = 3u,    // learned proposal: training / held-out poses
+    RNG_LP_NOISE = 4u,   // learned proposal: range noise of rendered scans
+    RNG_LP_SAMPLE = 5u,  // learned proposal: mixture samples
+    RNG_LP_INIT = 6u,    // learned proposal: weight initialisation
 };
 
 // Six standard normals for particle i in generation gen: translation noise

@@ -323,6 +323,81 @@ int pfgl_cell(void* h, int cx, int cy);
 int pfgl_topk_noalloc(const float* d_scores, int n, int k, int* d_idx,
                       void* stream);
 
+/* ------------------------------------------------------------------------
+ * Learned proposal for global localization (no counterpart in the
+ * reference).  A per-map MLP maps a normalised range scan to a 32-component
+ * Gaussian mixture over (x, y, cos yaw, sin yaw); queries sample hypotheses
+ * from the mixture and score them with plain CAER, falling back to uniform
+ * dispersion when the best CAER exceeds a threshold calibrated on held-out
+ * poses.  Network: 384 (360 rays + zero padding) -> 4 x 1024 ReLU -> 384
+ * (288 used: 32 logits, 32x4 means, 32x4 log-sigma pre-activations), BF16
+ * weights and activations, FP32 accumulation and master weights, trained with
+ * Adam by the library's own tcgen05 kernels.  A handle borrows the pfgl
+ * handle (map, scorer, stream) it is created on and must be destroyed first.
+ * ------------------------------------------------------------------------ */
+enum {
+    PFGL_LP_IN = 384,      /* padded input width (rays / rmax, then zeros) */
+    PFGL_LP_HIDDEN = 1024, /* hidden width (4 hidden layers) */
+    PFGL_LP_OUT = 384,     /* padded output width */
+    PFGL_LP_COMP = 32,     /* mixture components */
+    PFGL_LP_LAYERS = 5
+};
+
+/* batch: training minibatch rows (multiple of 128).  Returns NULL on error. */
+void* pfgl_learned_create(void* gl, int batch, unsigned long long seed);
+int pfgl_learned_destroy(void* lp);
+/* Number of f32 parameters in the flattened order W0,b0,...,W4,b4 with
+ * W_l row-major [out_l][in_l] over the padded widths. */
+long long pfgl_learned_num_params(void);
+int pfgl_learned_get_params(void* lp, float* out);
+int pfgl_learned_set_params(void* lp, const float* in);
+/* Render scans at caller poses with the library's raycaster (the CAER ray
+ * geometry) plus N(0, noise_std^2) range noise; out is n x nrays. */
+int pfgl_render_scans(void* gl, const float* pose3n, int n, int nrays,
+                      float rmax, float ang_span, float noise_std,
+                      unsigned long long seed, float* out);
+/* Generate n_pairs (scan, pose) training pairs on the device: poses uniform
+ * over free cells with yaw uniform in [0, 2 pi), nrays <= 384 rays over
+ * ang_span with range noise noise_std. */
+int pfgl_learned_make_data(void* lp, long long n_pairs, int nrays, float rmax,
+                           float ang_span, float noise_std,
+                           unsigned long long seed);
+/* Run `steps` Adam steps over the generated pairs (peak learning rate lr,
+ * linear warm-up then cosine decay over total_steps).  loss_out (may be
+ * NULL) receives the mean loss of each step. */
+int pfgl_learned_train(void* lp, int steps, int total_steps, float lr,
+                       float* loss_out);
+/* Loss and gradients (no update) for caller inputs: x is batch x 384
+ * normalised scans (padded), y is batch x 4 targets (x_n, y_n, cos, sin).
+ * grad receives pfgl_learned_num_params() floats. */
+int pfgl_learned_grad(void* lp, const float* x, const float* y, float* loss,
+                      float* grad);
+/* Mixture parameters (rows x 288) for rows <= 128 caller inputs (rows x 384). */
+int pfgl_learned_forward(void* lp, const float* x, int rows, float* out);
+/* Map normalisation: x_n = (x - c[0]) / c[2], y_n = (y - c[1]) / c[3]. */
+int pfgl_learned_norm(void* lp, float* c4);
+/* Localize one scan: n_samples mixture samples scored with CAER; when the
+ * best CAER exceeds the calibrated threshold, n_fallback uniform hypotheses
+ * (16 yaws per position) are scored as well and the better list is kept.
+ * info (may be NULL): 0 learned, 1 fallback ran and learned kept, 2 fallback
+ * result returned.  Returns k written or -1. */
+int pfgl_learned_localize(void* lp, const float* scan, int nrays, float rmax,
+                          float ang_span, int n_samples, int n_fallback, int k,
+                          float* out3k, float* caer_k, int* idx_k, int* info);
+/* Calibrate the fallback threshold on n_queries held-out poses: the
+ * `quantile` of the best CAER over held-out successes (within 0.5 m and
+ * 0.1 rad).  Writes the threshold and the held-out success rate. */
+int pfgl_learned_calibrate(void* lp, int n_queries, int nrays, float rmax,
+                           float ang_span, float noise_std, int n_samples,
+                           float quantile, unsigned long long seed,
+                           float* tau_out, float* success_out);
+int pfgl_learned_set_threshold(void* lp, float tau);
+/* Plain tcgen05 GEMM D = A * B^T (A: M x K, B: N x K, bf16 bit patterns,
+ * row-major; D: M x N f32) for numerics tests.  M, N multiples of 128, K a
+ * multiple of 64. */
+int pfgl_learned_gemm(int M, int N, int K, const unsigned short* A,
+                      const unsigned short* B, float* D);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif
