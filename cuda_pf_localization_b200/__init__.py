@@ -155,6 +155,8 @@ _KERNEL_SIGS = {
     "pfgl_topk_from_scores": (c_int, [c_void_p, _fp, c_int, c_int, _ip]),
     "pfgl_localize": (c_int, [c_void_p, _fp, c_int, c_float, c_float, c_int, _fp, _fp, _ip]),
     "pfgl_cell": (c_int, [c_void_p, c_int, c_int]),
+    "pfc_reinit_poses": (c_int, [c_void_p, c_void_p, c_int, c_float, _fp, _fp]),
+    "pfgl_topk_device": (c_void_p, [c_void_p, _ip]),
     "pfgl_learned_create": (c_void_p, [c_void_p, c_int, c_ulonglong]),
     "pfgl_learned_destroy": (c_int, [c_void_p]),
     "pfgl_learned_num_params": (C.c_longlong, []),

@@ -450,6 +450,7 @@ int copy_topk(GlHandle* h, const uint64_t* sorted, int k, float* out3k,
     k_gather_topk<<<ceil_div(k, kThreads), kThreads, 0, h->stream>>>(
         sorted, k, h->d_hyp, h->d_caer, h->d_out, h->d_outc, h->d_outi);
     PFB_KL();
+    h->last_k = k;
     if (out3k)
         PFB_CK(cudaMemcpyAsync(out3k, h->d_out, sizeof(float) * 3 * (size_t)k,
                                cudaMemcpyDeviceToHost, h->stream));
@@ -737,6 +738,13 @@ int pfgl_localize(void* hv, const float* scan, int nrays, float rmax,
     if (!h || h->nh <= 0 || !scan || nrays <= 0 || k <= 0) return -1;
     if (gl_upload_scan(h, scan, nrays)) return -1;
     return gl_localize_loaded(h, nrays, rmax, ang_span, k, out3k, caer_k, idx_k);
+}
+
+const float* pfgl_topk_device(void* hv, int* k) {
+    GlHandle* h = as_gl(hv);
+    if (!h || h->last_k <= 0) return nullptr;
+    if (k) *k = h->last_k;
+    return h->d_out;
 }
 
 int pfgl_cell(void* hv, int cx, int cy) {

@@ -52,6 +52,7 @@ struct GlHandle {
     GlCtl* h_ctl = nullptr;
     std::vector<unsigned char> host_grid;  // unpadded 0/1 copy
     bool caer_valid = false;
+    int last_k = 0;  // entries of d_out written by the last bottom-k
 };
 
 struct GridView {

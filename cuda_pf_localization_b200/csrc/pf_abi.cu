@@ -459,6 +459,20 @@ int pfc_reinit(void* hv, float x, float y, float z, float qw, float qx,
     return 0;
 }
 
+int pfc_reinit_poses(void* hv, const float* d_pose3k, int k, float z,
+                     const float* pos_std, const float* rot_std) {
+    PfHandle* h = as_pf(hv);
+    if (!valid_handle(h) || !d_pose3k || k <= 0 || !pos_std || !rot_std)
+        return -1;
+    h->pending_predict = false;
+    h->gen++;
+    if (launch_reinit_poses(h, d_pose3k, k, z, pos_std, rot_std)) return -1;
+    if (set_wmode(h, WMODE_UNIFORM)) return -1;
+    h->est_valid = h->est_inflight = false;
+    h->total_valid = false;
+    return 0;
+}
+
 int pfc_predict(void* hv, float tx, float ty, float tz, float qw, float qx,
                 float qy, float qz, const float* tstd, const float* rstd) {
     PfHandle* h = as_pf(hv);

@@ -256,6 +256,9 @@ struct WeightArgs {
 
 int launch_reinit(PfHandle* h, const float p0[3], const float q0[4],
                   const float pstd[3], const float rstd[3]);
+// Reinitialisation around k device-resident planar poses (x, y, yaw).
+int launch_reinit_poses(PfHandle* h, const float* d_poses, int k, float z,
+                        const float pstd[3], const float rstd[3]);
 int launch_predict(PfHandle* h, const PredictArgs& pa);
 // Weighting (optionally fused with a deferred predict): writes ll, block
 // (max, sumexp) partials and the finalised M, S into the control block.

@@ -77,6 +77,31 @@ __global__ void __launch_bounds__(kThreads)
     store_pose(s, i, p, q_product(q0, dq));
 }
 
+// Reinitialisation around k planar poses (x, y, yaw) held in device memory:
+// particle i starts from pose i mod k at height z with attitude = yaw about
+// +z, then the same Gaussian perturbation as k_reinit.
+__global__ void __launch_bounds__(kThreads)
+    k_reinit_poses(PlaneSet ps, int n, uint64_t seed, uint64_t gen,
+                   const float* __restrict__ poses, int k, float z, float3 pstd,
+                   float3 rstd, CycleCtl* ctl) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= n) return;
+    const Planes s = pick_planes(ps, ctl->live);
+    const int j = i % k;
+    const float x0 = poses[3 * j], y0 = poses[3 * j + 1], yaw = poses[3 * j + 2];
+    float sh, ch;
+    sincosf(0.5f * yaw, &sh, &ch);
+    const Quat q0{ch, 0.0f, 0.0f, sh};
+    float nz[6];
+    pf_normals6(seed, gen, (uint32_t)i, nz);
+    float3 p = make_float3(x0 + pstd.x * nz[0], y0 + pstd.y * nz[1],
+                           z + pstd.z * nz[2]);
+    float3 axis = make_float3(rstd.x * nz[3], rstd.y * nz[4], rstd.z * nz[5]);
+    float ang = sqrtf(axis.x * axis.x + axis.y * axis.y + axis.z * axis.z);
+    Quat dq = q_from_axis_angle(axis, ang);
+    store_pose(s, i, p, q_product(q0, dq));
+}
+
 __global__ void __launch_bounds__(kThreads)
     k_predict(PlaneSet ps, int n, uint64_t seed, PredictArgs pa,
               CycleCtl* ctl) {
@@ -464,6 +489,18 @@ int launch_reinit(PfHandle* h, const float p0[3], const float q0[4],
     k_reinit<<<grid, kThreads, 0, h->stream>>>(
         plane_set(h), h->n, h->seed, h->gen, make_float3(p0[0], p0[1], p0[2]),
         Quat{q0[0], q0[1], q0[2], q0[3]},
+        make_float3(pstd[0], pstd[1], pstd[2]),
+        make_float3(rstd[0], rstd[1], rstd[2]), h->d_ctl);
+    PFB_KL();
+    return 0;
+}
+
+int launch_reinit_poses(PfHandle* h, const float* d_poses, int k, float z,
+                        const float pstd[3], const float rstd[3]) {
+    const int grid = ceil_div(h->n, kThreads);
+    KernelScope ks(h, KK_REINIT);
+    k_reinit_poses<<<grid, kThreads, 0, h->stream>>>(
+        plane_set(h), h->n, h->seed, h->gen, d_poses, k, z,
         make_float3(pstd[0], pstd[1], pstd[2]),
         make_float3(rstd[0], rstd[1], rstd[2]), h->d_ctl);
     PFB_KL();

@@ -216,6 +216,15 @@ int pfc_get_ll(void* h, float* ll);
 int pfc_set_state(void* h, const float* pos3n, const float* quat4n,
                   const float* w);
 
+/* Global-localization hand-off: reinitialise around k planar poses
+ * (x, y, yaw) held in DEVICE memory, e.g. pfgl_topk_device's result.
+ * Particle i starts from pose i mod k at height z with attitude = yaw about
+ * +z, perturbed like pfc_reinit (position N(0, pos_std3^2), attitude
+ * exp(N(0, rot_std3^2))); weights become 1/n.  The poses must be complete
+ * when the call is made (pfgl_topk_device's are). */
+int pfc_reinit_poses(void* h, const float* d_pose3k, int k, float z,
+                     const float* pos_std3, const float* rot_std3);
+
 /* Resample with an explicit offset fraction u01 in [0,1) instead of the
  * handle's LCG draw (the LCG is left untouched); injection as pfc_resample. */
 int pfc_resample_u01(void* h, double u01, float random_inject_ratio);
@@ -301,6 +310,12 @@ int pfgl_topk_from_scores(void* h, const float* caer, int n, int k,
 int pfgl_localize(void* h, const float* scan, int nrays, float rmax,
                   float ang_span, int k, float* out3k, float* caer_k,
                   int* idx_k);
+
+/* Device pointer to the k x (x, y, theta) poses of the last bottom-k
+ * (pfgl_topk, pfgl_topk_ex, pfgl_localize); *k receives their count.  The
+ * poses are complete when the returning call has returned, and stay valid
+ * until the next bottom-k on this handle.  NULL before any bottom-k. */
+const float* pfgl_topk_device(void* h, int* k);
 
 /* Occupancy value the device sees for cell (cx,cy): 0 free, 1 occupied. */
 int pfgl_cell(void* h, int cx, int cy);
