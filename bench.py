@@ -55,6 +55,11 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--particles", type=int, default=1_000_000)
     ap.add_argument("--seed", type=int, default=11)
+    ap.add_argument("--batch-filters", type=int, default=512)
+    ap.add_argument("--batch-cycles", type=int, default=200)
+    ap.add_argument("--batch-seq-cycles", type=int, default=5)
+    ap.add_argument("--batch-only", action="store_true",
+                    help="run only the batched-filter leg and print its JSON")
     ap.add_argument("--gl-only", action="store_true",
                     help="run only the global-localization legs and print their JSON")
     ap.add_argument("--no-extras", action="store_true",
@@ -465,6 +470,139 @@ def run_gl(args):
     return res
 
 
+def run_batched(args, torch, dev):
+    """Batched filters: sizes log-uniform in [1k, 200k], own landmarks, helix
+    and 4-64 observations per cycle; every cycle of all filters is one graph
+    launch with device-resident inputs (CUDA events per cycle on the batch
+    stream), against the same filters run one after another through the
+    single-filter fused cycle."""
+    import cuda_pf_localization_b200 as pkg
+    from cuda_pf_localization_b200 import sim
+    lib = pkg.kernels()
+    F, cycles = args.batch_filters, args.batch_cycles
+    sizes, scen, counts = sim.batched_config(F, cycles + args.warmup, args.seed + 5)
+    seeds = [1000 + f for f in range(F)]
+    prm = dict(sigma_r=0.05, sigma_b=0.02, gate=3.0, ess_ratio=0.5, inject=0.0)
+
+    def odom(sc, st):
+        o = pkg.PfcOdom()
+        o.t[:] = list(map(float, st.odom_t))
+        o.q[:] = list(map(float, st.odom_q))
+        o.tstd[:] = list(sc.trans_noise)
+        o.rstd[:] = list(sc.rot_noise)
+        return o
+
+    total_cycles = cycles + args.warmup
+    # device-resident inputs of every cycle
+    rec = np.zeros((total_cycles, F), np.dtype((np.void, C.sizeof(pkg.PfcBatchCycle))))
+    obs_blocks, obs_off, n_obs = [], [], []
+    for k in range(total_cycles):
+        recs = (pkg.PfcBatchCycle * F)()
+        off = 0
+        rows = []
+        for f in range(F):
+            st = scen[f].steps[k]
+            recs[f].odom = odom(scen[f], st)
+            recs[f].obs_off = off
+            recs[f].nobs = len(st.obs)
+            off += len(st.obs)
+            rows.append(st.obs)
+        rec[k] = np.frombuffer(bytes(recs), dtype=rec.dtype)
+        obs_blocks.append(pkg.cobs_records(np.concatenate(rows)))
+        n_obs.append(off)
+    max_obs = max(n_obs)
+    obs_all = np.zeros((total_cycles, max_obs), pkg.COBS_DTYPE)
+    for k in range(total_cycles):
+        obs_all[k, :n_obs[k]] = obs_blocks[k]
+    d_rec = torch.from_numpy(rec.view(np.uint8).reshape(total_cycles, -1).copy()).to(dev)
+    d_obs = torch.from_numpy(obs_all.view(np.uint8).reshape(total_cycles, -1).copy()).to(dev)
+    rec_bytes, obs_bytes = d_rec.shape[1], d_obs.shape[1]
+    pose7 = np.array([np.r_[sc.prior_p, sc.prior_q] for sc in scen], np.float32)
+    b = pkg.BatchPF(sizes, seeds=seeds, obs_cap=max_obs)
+    try:
+        b.set_params(**prm)
+        b.set_landmarks([sc.landmarks for sc in scen])
+        b.reinit(pose7, np.full((F, 3), 0.5), np.full((F, 3), 0.2))
+        est = np.zeros((F, pkg.PFC_EST_LEN))
+        for k in range(args.warmup):
+            assert lib.pfc_batch_cycle_device(
+                b.handle, C.c_void_p(d_rec.data_ptr() + k * rec_bytes),
+                C.c_void_p(d_obs.data_ptr() + k * obs_bytes), n_obs[k], pkg.dptr(est)) == 0
+        tiles, packed = b.autotune(reps=3)
+        stream = torch.cuda.ExternalStream(lib.pfc_batch_stream(b.handle), device=dev)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(cycles)]
+        l0 = lib.pfc_batch_launches(b.handle)
+        torch.cuda.synchronize(dev)
+        resampled = 0
+        for i in range(cycles):
+            k = args.warmup + i
+            evs[i][0].record(stream)
+            assert lib.pfc_batch_cycle_device(
+                b.handle, C.c_void_p(d_rec.data_ptr() + k * rec_bytes),
+                C.c_void_p(d_obs.data_ptr() + k * obs_bytes), n_obs[k], None) == 0
+            evs[i][1].record(stream)
+        assert lib.pfc_batch_result(b.handle, pkg.dptr(est)) == 0
+        torch.cuda.synchronize(dev)
+        launches = lib.pfc_batch_launches(b.handle) - l0
+        ms = np.array([a.elapsed_time(c) for a, c in evs])
+        resampled = int(est[:, pkg.PFC_EST_RESAMPLED].sum())
+        errs = [float(np.linalg.norm(est[f, :3] - scen[f].steps[total_cycles - 1].truth_p))
+                for f in range(F)]
+    finally:
+        b.close()
+    # sequential single-filter cycles (the same filters, host inputs, a few cycles)
+    seq_cycles = min(args.batch_seq_cycles, cycles)
+    hs = []
+    seq_ms = float("nan")
+    try:
+        if seq_cycles <= 0:
+            raise StopIteration
+        pc = pkg.PfcCycleParams(prm["sigma_r"], prm["sigma_b"], prm["gate"], prm["ess_ratio"],
+                                prm["inject"], 0)
+        for f in range(F):
+            h = lib.pfc_create(64)
+            hs.append(h)
+            assert lib.pfc_init(h, int(sizes[f]), seeds[f]) == 0
+            lm = np.ascontiguousarray(scen[f].landmarks, np.float32).reshape(-1)
+            assert lib.pfc_upload_landmarks(h, pkg.fptr(lm), len(scen[f].landmarks)) == 0
+            pri = pose7[f]
+            ps, rs = np.full(3, 0.5, np.float32), np.full(3, 0.2, np.float32)
+            assert lib.pfc_reinit(h, *map(float, pri), pkg.fptr(ps), pkg.fptr(rs)) == 0
+        cobs = [[pkg.make_cobs(scen[f].steps[k].obs) for f in range(F)]
+                for k in range(args.warmup + seq_cycles)]
+        odoms = [[odom(scen[f], scen[f].steps[k]) for f in range(F)]
+                 for k in range(args.warmup + seq_cycles)]
+        e1 = np.zeros(pkg.PFC_EST_LEN)
+        for k in range(args.warmup):
+            for f in range(F):
+                assert lib.pfc_cycle(hs[f], C.byref(odoms[k][f]), cobs[k][f],
+                                     len(scen[f].steps[k].obs), C.byref(pc), pkg.dptr(e1)) == 0
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for i in range(seq_cycles):
+            k = args.warmup + i
+            for f in range(F):
+                assert lib.pfc_cycle(hs[f], C.byref(odoms[k][f]), cobs[k][f],
+                                     len(scen[f].steps[k].obs), C.byref(pc), pkg.dptr(e1)) == 0
+        seq_ms = 1e3 * (time.perf_counter() - t0) / seq_cycles
+    except StopIteration:
+        pass
+    finally:
+        for h in hs:
+            lib.pfc_destroy(h)
+    total = int(sizes.sum())
+    return dict(
+        filters=F, particles_total=total, cycles=cycles, ms_per_cycle=float(ms.mean()),
+        particle_updates_per_s=total * cycles / (ms.sum() * 1e-3),
+        sequential_ms_per_cycle=seq_ms, sequential_cycles_timed=seq_cycles,
+        speedup_vs_sequential=seq_ms / float(ms.mean()),
+        kernels_per_cycle=launches / cycles, graph_launches_per_cycle=1,
+        est_tiles_per_bucket=[int(t) for t in tiles],
+        resampled_filters_last_cycle=resampled,
+        mean_track_err_m=float(np.mean(errs)), n_min=int(sizes.min()), n_max=int(sizes.max()))
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -482,6 +620,10 @@ def main():
     if args.gl_only:
         if rank == 0:
             print(json.dumps({"gl": run_gl(args)}), flush=True)
+        return
+    if args.batch_only:
+        if rank == 0:
+            print(json.dumps({"batched": run_batched(args, torch, dev)}), flush=True)
         return
     dist = None
     if world > 1:
@@ -560,6 +702,12 @@ def main():
         line["cpu_baseline"] = {"value": n * done / secs, "unit": UNIT,
                                 "cores": int(oracle.lib().orc_threads()), "kind": "port",
                                 "sample": f"{done} cycles at N={n} (time-bounded)"}
+        line["batched"] = run_batched(args, torch, dev)
+        line["batched"]["config"] = ("512 filters, N log-uniform in [1k, 200k], 8-64 landmarks "
+                                     "in 20x20x5 m each, own helix, 4-64 obs per cycle, "
+                                     "gate 3 sigma, ESS<N/2 resample; one graph launch per "
+                                     "cycle vs the same filters through pfc_cycle one after "
+                                     "another")
         line["gl"] = run_gl(args)
         line["gl"]["config"] = ("10x10 m rooms at 0.05 m (200x200), 30 boxes 0.2-1.0 m, 360 rays, "
                                 "rmax 10, scan noise N(0, 0.01 m); uniform: positions x 16 yaws, "

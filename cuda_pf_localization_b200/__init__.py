@@ -29,6 +29,8 @@ __all__ = [
 
 PFC_EST_LEN = 24
 PFC_EST = dict(POS=0, QUAT=3, POSCOV=7, ATTCOV=13, ESS=19, RESAMPLED=20, ESS_PRE=21)
+PFC_EST_POS, PFC_EST_QUAT, PFC_EST_POSCOV, PFC_EST_ATTCOV = 0, 3, 7, 13
+PFC_EST_ESS, PFC_EST_RESAMPLED, PFC_EST_ESS_PRE = 19, 20, 21
 
 # The 18 drop-in symbols the reference's Rust crate binds
 # (crates/pf_core/src/cuda.rs:33-88, crates/pf_core/src/global_loc.rs:261-271).
@@ -157,6 +159,23 @@ _KERNEL_SIGS = {
     "pfgl_cell": (c_int, [c_void_p, c_int, c_int]),
     "pfc_reinit_poses": (c_int, [c_void_p, c_void_p, c_int, c_float, _fp, _fp]),
     "pfgl_topk_device": (c_void_p, [c_void_p, _ip]),
+    "pfc_batch_create": (c_void_p, [c_int, _ip, POINTER(c_uint), c_int]),
+    "pfc_batch_destroy": (c_int, [c_void_p]),
+    "pfc_batch_set_params": (c_int, [c_void_p, POINTER(PfcCycleParams)]),
+    "pfc_batch_upload_landmarks": (c_int, [c_void_p, _fp, _ip]),
+    "pfc_batch_reinit": (c_int, [c_void_p, _fp, _fp, _fp]),
+    "pfc_batch_cycle": (c_int, [c_void_p, POINTER(PfcOdom), POINTER(CObservation), _ip, _dp]),
+    "pfc_batch_cycle_device": (c_int, [c_void_p, c_void_p, c_void_p, c_int, _dp]),
+    "pfc_batch_result": (c_int, [c_void_p, _dp]),
+    "pfc_batch_use_graph": (c_int, [c_void_p, c_int]),
+    "pfc_batch_set_tiles": (c_int, [c_void_p, _ip, c_int]),
+    "pfc_batch_get_tiles": (c_int, [c_void_p, _ip, _ip]),
+    "pfc_batch_autotune": (c_int, [c_void_p, c_int, _ip, _ip]),
+    "pfc_batch_snapshot": (c_int, [c_void_p, c_int, _fp, _fp]),
+    "pfc_batch_get_weights": (c_int, [c_void_p, c_int, _fp]),
+    "pfc_batch_size": (c_int, [c_void_p, c_int]),
+    "pfc_batch_stream": (c_void_p, [c_void_p]),
+    "pfc_batch_launches": (C.c_longlong, [c_void_p]),
     "pfgl_learned_create": (c_void_p, [c_void_p, c_int, c_ulonglong]),
     "pfgl_learned_destroy": (c_int, [c_void_p]),
     "pfgl_learned_num_params": (C.c_longlong, []),
@@ -269,12 +288,27 @@ def u8ptr(a: np.ndarray):
     return a.ctypes.data_as(_u8p)
 
 
+COBS_DTYPE = np.dtype([("id", "<i4"), ("mode", "<i4"), ("dx", "<f4"), ("dy", "<f4"),
+                       ("dz", "<f4"), ("range", "<f4")])
+
+
+def cobs_records(rows) -> np.ndarray:
+    """CObservation records (numpy, 24 bytes each) from (id, mode, dx, dy, dz,
+    range) rows."""
+    rows = np.asarray(rows, dtype=np.float64).reshape(-1, 6)
+    a = np.zeros(len(rows), COBS_DTYPE)
+    a["id"] = rows[:, 0].astype(np.int32)
+    a["mode"] = rows[:, 1].astype(np.int32)
+    a["dx"], a["dy"], a["dz"], a["range"] = rows[:, 2], rows[:, 3], rows[:, 4], rows[:, 5]
+    return a
+
+
 def make_cobs(rows) -> "C.Array":
     """Array of CObservation from (id, mode, dx, dy, dz, range) rows."""
-    arr = (CObservation * max(1, len(rows)))()
-    for k, r in enumerate(rows):
-        arr[k] = CObservation(int(r[0]), int(r[1]), float(r[2]), float(r[3]),
-                              float(r[4]), float(r[5]))
+    a = cobs_records(rows)
+    arr = (CObservation * max(1, len(a)))()
+    if len(a):
+        C.memmove(arr, a.ctypes.data, a.nbytes)
     return arr
 
 
@@ -550,3 +584,103 @@ def learned_gemm(a_bf16: np.ndarray, b_bf16: np.ndarray) -> np.ndarray:
     if rc != 0:
         raise RuntimeError("pfgl_learned_gemm failed: " + last_error())
     return d
+
+
+# ------------------------------------------------------------ batched filters
+
+class PfcBatchCycle(C.Structure):
+    _fields_ = [("odom", PfcOdom), ("obs_off", c_int), ("nobs", c_int)]
+
+
+class BatchPF:
+    """Many independent filters advanced by one graph launch per cycle
+    (``pfc_batch_*``)."""
+
+    def __init__(self, sizes, seeds=None, obs_cap=1 << 16):
+        self.lib = kernels()
+        self.sizes = np.ascontiguousarray(sizes, np.int32)
+        self.nf = len(self.sizes)
+        sd = None
+        if seeds is not None:
+            self._seeds = (c_uint * self.nf)(*[int(x) for x in seeds])
+            sd = self._seeds
+        self._h = self.lib.pfc_batch_create(self.nf, iptr(self.sizes), sd, int(obs_cap))
+        if not self._h:
+            raise RuntimeError("pfc_batch_create failed: " + last_error())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.pfc_batch_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _ok(self, rc, what):
+        if rc != 0:
+            raise RuntimeError(f"{what} failed: {last_error()}")
+
+    def set_params(self, sigma_r=0.05, sigma_b=0.02, gate=3.0, ess_ratio=0.5, inject=0.0):
+        arr = (PfcCycleParams * self.nf)()
+        for f in range(self.nf):
+            arr[f] = PfcCycleParams(sigma_r, sigma_b, gate, ess_ratio, inject, 0)
+        self._ok(self.lib.pfc_batch_set_params(self._h, arr), "set_params")
+
+    def set_landmarks(self, tables):
+        counts = np.array([len(t) for t in tables], np.int32)
+        xyz = np.ascontiguousarray(np.concatenate([np.asarray(t, np.float32).reshape(-1, 3)
+                                                   for t in tables]).reshape(-1), np.float32)
+        self._ok(self.lib.pfc_batch_upload_landmarks(self._h, fptr(xyz), iptr(counts)),
+                 "upload_landmarks")
+
+    def reinit(self, pose7, pos_std3, rot_std3):
+        p = np.ascontiguousarray(pose7, np.float32).reshape(-1)
+        a = np.ascontiguousarray(pos_std3, np.float32).reshape(-1)
+        b = np.ascontiguousarray(rot_std3, np.float32).reshape(-1)
+        self._ok(self.lib.pfc_batch_reinit(self._h, fptr(p), fptr(a), fptr(b)), "reinit")
+
+    def cycle(self, odoms, obs_rows, want_est=True):
+        """odoms: list of PfcOdom; obs_rows: list of (k, 6) arrays per filter."""
+        od = (PfcOdom * self.nf)(*odoms)
+        nobs = np.array([len(r) for r in obs_rows], np.int32)
+        allrows = [r for r in obs_rows if len(r)]
+        obs = make_cobs(np.concatenate(allrows)) if allrows else None
+        est = np.zeros((self.nf, PFC_EST_LEN)) if want_est else None
+        self._ok(self.lib.pfc_batch_cycle(self._h, od, obs, iptr(nobs),
+                                          dptr(est) if want_est else None), "cycle")
+        return est
+
+    def snapshot(self, f):
+        n = int(self.sizes[f])
+        pos = np.zeros(3 * n, np.float32)
+        quat = np.zeros(4 * n, np.float32)
+        self._ok(self.lib.pfc_batch_snapshot(self._h, f, fptr(pos), fptr(quat)), "snapshot")
+        return pos, quat
+
+    def weights(self, f):
+        w = np.zeros(int(self.sizes[f]), np.float32)
+        self._ok(self.lib.pfc_batch_get_weights(self._h, f, fptr(w)), "get_weights")
+        return w
+
+    def use_graph(self, on: bool):
+        self._ok(self.lib.pfc_batch_use_graph(self._h, 1 if on else 0), "use_graph")
+
+    def tiles(self):
+        t = np.zeros(4, np.int32)
+        pk = np.zeros(1, np.int32)
+        self._ok(self.lib.pfc_batch_get_tiles(self._h, iptr(t), iptr(pk)), "get_tiles")
+        return t, int(pk[0])
+
+    def set_tiles(self, est_tile4, packed=1):
+        t = np.ascontiguousarray(est_tile4, np.int32)
+        self._ok(self.lib.pfc_batch_set_tiles(self._h, iptr(t), int(packed)), "set_tiles")
+
+    def autotune(self, reps=3):
+        t = np.zeros(4, np.int32)
+        pk = np.zeros(1, np.int32)
+        self._ok(self.lib.pfc_batch_autotune(self._h, int(reps), iptr(t), iptr(pk)),
+                 "autotune")
+        return t, int(pk[0])

@@ -21,7 +21,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 KERNEL_SOURCES = ["pf_update.cu", "pf_estimate.cu", "pf_resample.cu",
-                  "pf_abi.cu", "gl.cu", "gl_learned.cu"]
+                  "pf_abi.cu", "pf_batch.cu", "gl.cu", "gl_learned.cu"]
 HOST_SOURCES = ["host/pf_core.cpp"]
 
 

@@ -396,7 +396,7 @@ int pfc_init(void* hv, int n, unsigned int seed) {
     PFB_CK(cudaMalloc((void**)&h->d_state[1], 7 * np * sizeof(float)));
     PFB_CK(cudaMalloc((void**)&h->d_ll, np * sizeof(float)));
     PFB_CK(cudaMalloc((void**)&h->d_w, np * sizeof(float)));
-    h->heavy_cap = n / 32 + 2;
+    h->heavy_cap = n / 32 + n / 4096 + 2;  // runs > 32 outputs, in pieces of <= 4096
     PFB_CK(cudaMalloc((void**)&h->d_heavy, (size_t)h->heavy_cap * sizeof(HeavyRun)));
     PFB_CK(cudaMalloc((void**)&h->d_part_u64, 2 * 1184 * sizeof(unsigned long long)));
     PFB_CK(cudaMalloc((void**)&h->d_anc, (size_t)n * sizeof(int)));

@@ -1,0 +1,1337 @@
+// pf_batch.cu — many independent particle filters of uneven size advanced by
+// one CUDA-graph launch per cycle.
+//
+// Layout.  All filters' particles live in one arena of SoA planes (two
+// ping-pong sets of px py pz qw qx qy qz, plus ll and w); filter f owns the
+// slice [off_f, off_f + n_f), off_f a multiple of 1024.  Every kernel of the
+// cycle covers all filters through a tile table: a tile is a particle range
+// of one filter.  Per-filter reductions are finished by the last tile of that
+// filter to complete (an atomic counter per filter), so a cycle is a fixed
+// chain of kernels whatever the filter sizes:
+//   begin -> weight (+ predict) -> estimate -> covariances + ESS decision ->
+//   resample (look-back scan + run copy) -> long runs -> injection (link,
+//   apply) -> commit -> estimate / covariances of the resampled filters.
+// The chain is captured once into a CUDA graph; a cycle is one graph launch
+// fed by one copy of the per-filter inputs.
+//
+// Equality with the single-filter path.  The weighting tiles are the
+// single-filter kernel's blocks (512 particles, two per thread) and the
+// softmax partials and their combine are the same device routines, so the
+// log-likelihoods, the normaliser, the f32 weights, the fixed-point scan, the
+// ancestors, the injection and hence the particle states of filter f equal
+// those of the same filter run alone through pfc_cycle.  Only the FP64
+// estimate/covariance sums are partitioned differently (the estimate tile
+// size is autotuned per size bucket), which changes them in the last bits.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <new>
+#include <vector>
+
+#include "markley.h"
+#include "pf_device.cuh"
+
+namespace pfb {
+namespace batch {
+
+using namespace pfb::dev;
+
+constexpr int kThreads = kBlk;
+constexpr int kWTile = 2 * kBlk;  // particles per weighting tile
+constexpr int kScanItems = 16;
+constexpr int kRTile = kBlk * kScanItems;  // particles per resampling tile
+constexpr int kHeavy = 32;
+constexpr int kBuckets = 4;
+// Size buckets for the autotuned estimate tile: n < 8k, < 32k, < 128k, more.
+constexpr int kBucketLimit[kBuckets - 1] = {8192, 32768, 131072};
+constexpr int kEstTileChoices[] = {2048, 4096, 8192, 16384, 32768};
+
+struct BFilter {
+    long long off;
+    int n;
+    int lm_off, lm_count;
+    int wtile0, nwtiles;
+    int etile0, netiles;
+    int rtile0, nrtiles;
+    int inj_k, inj_off;
+    uint64_t seed;
+    float sigma_r, sigma_b, gate, inject_ratio;
+    double ess_ratio;
+};
+
+struct BTile {
+    int f;
+    int start;  // filter-local first particle
+    int count;
+    int local;  // tile index within the filter
+};
+
+struct BCtl {
+    double M, S;
+    int wmode, wvalid;
+    double est[kEstN], qmean[4], covs[kCovN];
+    double ess;
+    float cmp[3], cmq[4];
+    int resample_now, resampled, resample_valid, w_bad;
+    unsigned long long w_total_fx;
+    unsigned long long lcg, lcg_next;
+    unsigned long long gen;
+    int live;
+    unsigned done_w, done_e, done_c;
+    unsigned err;
+};
+
+struct BGlobal {
+    unsigned scan_epoch;
+    unsigned inj_epoch;
+    unsigned tile_counter;
+    int heavy_count;
+    unsigned err;
+};
+
+struct Arena {
+    float* p[2][7];
+    float* ll;
+    float* w;
+};
+
+// Planes of one filter in set `which`, selected with register selects (an
+// indexed kernel-parameter array would be copied to local memory).
+__device__ __forceinline__ Planes filter_planes(const Arena& A, int which,
+                                                long long off) {
+    Planes s;
+    s.px = (which ? A.p[1][0] : A.p[0][0]) + off;
+    s.py = (which ? A.p[1][1] : A.p[0][1]) + off;
+    s.pz = (which ? A.p[1][2] : A.p[0][2]) + off;
+    s.qw = (which ? A.p[1][3] : A.p[0][3]) + off;
+    s.qx = (which ? A.p[1][4] : A.p[0][4]) + off;
+    s.qy = (which ? A.p[1][5] : A.p[0][5]) + off;
+    s.qz = (which ? A.p[1][6] : A.p[0][6]) + off;
+    return s;
+}
+
+// ------------------------------------------------------------------ kernels
+
+__global__ void k_b_init(BCtl* C, BGlobal* G, int nf) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f == 0) {
+        G->scan_epoch = 1u;
+        G->inj_epoch = 1u;
+        G->tile_counter = 0u;
+        G->heavy_count = 0;
+        G->err = 0u;
+    }
+    if (f >= nf) return;
+    BCtl c;
+    memset(&c, 0, sizeof(c));
+    c.lcg = 0x243F6A8885A308D3ull;  // the single-filter handle's initial word
+    c.wmode = WMODE_UNIFORM;
+    C[f] = c;
+}
+
+// Generation counter of every filter: the single-filter path increments it
+// at each reinit and predict.
+__global__ void k_b_gen_inc(BCtl* C, int nf) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f < nf) C[f].gen += 1ull;
+}
+
+// Prior: pose7 + pos_std3 + rot_std3 per filter (13 floats).
+__global__ void __launch_bounds__(kThreads)
+    k_b_reinit(Arena A, const BFilter* __restrict__ F, const BTile* __restrict__ T,
+               BCtl* C, const float* __restrict__ prior) {
+    const BTile t = T[blockIdx.x];
+    const BFilter& fl = F[t.f];
+    const float* pr = prior + 13 * t.f;
+    const Planes s = filter_planes(A, C[t.f].live, fl.off);
+    const unsigned long long gen = C[t.f].gen;
+    for (int r = threadIdx.x; r < t.count; r += kThreads) {
+        const int i = t.start + r;
+        float nz[6];
+        pf_normals6(fl.seed, gen, (uint32_t)i, nz);
+        const float3 p = make_float3(pr[0] + pr[7] * nz[0], pr[1] + pr[8] * nz[1],
+                                     pr[2] + pr[9] * nz[2]);
+        const float3 axis =
+            make_float3(pr[10] * nz[3], pr[11] * nz[4], pr[12] * nz[5]);
+        const float ang = norm3(axis);
+        const Quat q0{pr[3], pr[4], pr[5], pr[6]};
+        store_pose(s, i, p, q_product(q0, q_from_axis_angle(axis, ang)));
+    }
+    if (threadIdx.x == 0 && t.local == 0) C[t.f].wmode = WMODE_UNIFORM;
+}
+
+// Predict (generation gen + 1) and gated weighting of one 512-particle tile;
+// the last tile of a filter combines the softmax partials.
+__global__ void __launch_bounds__(kThreads)
+    k_b_weight(Arena A, const BFilter* __restrict__ F, const BTile* __restrict__ T,
+               BCtl* C, const PfcBatchCycle* __restrict__ cyc,
+               const CObservation* __restrict__ obs, const float* __restrict__ lm,
+               double2* __restrict__ wpart, int use_packed) {
+    const BTile t = T[blockIdx.x];
+    const BFilter& fl = F[t.f];
+    BCtl* c = C + t.f;
+    const PfcBatchCycle in = cyc[t.f];
+    const Planes s = filter_planes(A, c->live, fl.off);
+    PredictArgs pa;
+    pa.enabled = 1;
+    pa.gen = c->gen;
+    for (int k = 0; k < 3; ++k) {
+        pa.t[k] = in.odom.t[k];
+        pa.tstd[k] = in.odom.tstd[k];
+        pa.rstd[k] = in.odom.rstd[k];
+    }
+    for (int k = 0; k < 4; ++k) pa.q[k] = in.odom.q[k];
+    const int i0 = t.start + threadIdx.x, i1 = i0 + kThreads;
+    const bool v0 = threadIdx.x < t.count, v1 = threadIdx.x + kThreads < t.count;
+    float3 p0 = make_float3(0.f, 0.f, 0.f), p1 = p0;
+    Quat q0 = {1.f, 0.f, 0.f, 0.f}, q1 = q0;
+    if (v0) {
+        load_pose(s, i0, p0, q0);
+        apply_predict(pa, fl.seed, i0, p0, q0);
+        store_pose(s, i0, p0, q0);
+    }
+    if (v1) {
+        load_pose(s, i1, p1, q1);
+        apply_predict(pa, fl.seed, i1, p1, q1);
+        store_pose(s, i1, p1, q1);
+    }
+    const int nobs = in.nobs;
+    if (nobs <= 0) {
+        // predict only: the single-filter cycle resets the weights to uniform
+        if (threadIdx.x == 0 && t.local == 0) c->wmode = WMODE_UNIFORM;
+        return;
+    }
+    float acc0, acc1;
+    weight_two(obs + in.obs_off, nobs, lm + 3 * (size_t)fl.lm_off, fl.lm_count,
+               fl.sigma_r, fl.sigma_b, fl.gate, p0, q0, p1, q1, use_packed, acc0,
+               acc1);
+    float* ll = A.ll + fl.off;
+    if (v0) ll[i0] = acc0;
+    if (v1) ll[i1] = acc1;
+    const double2 pb = block_softmax_partial(acc0, v0, acc1, v1);
+    __shared__ bool s_last;
+    if (threadIdx.x == 0) {
+        wpart[fl.wtile0 + t.local] = pb;
+        __threadfence();
+        s_last = (atomicAdd(&c->done_w, 1u) == (unsigned)fl.nwtiles - 1u);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    const double2 ms = softmax_combine(wpart + fl.wtile0, fl.nwtiles);
+    if (threadIdx.x == 0) {
+        c->M = ms.x;
+        c->S = ms.y;
+        const int ok = (ms.y > 0.0 && isfinite(ms.y)) ? 1 : 0;
+        c->wvalid = ok;
+        c->wmode = ok ? WMODE_LL : WMODE_UNIFORM;
+        c->done_w = 0u;
+    }
+}
+
+// Block partial of NV FP64 sums (fixed order) into part[NV]; returns true in
+// every thread of the filter's last tile after its partials are visible.
+template <int NV>
+__device__ __forceinline__ bool tile_partial(double (&acc)[NV], double* part,
+                                             unsigned* done, int ntiles) {
+    __shared__ double s_w[NV][kThreads / 32];
+    __shared__ bool s_last;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        const double v = warp_sum_d(acc[k]);
+        if (lane == 0) s_w[k][warp] = v;
+    }
+    __syncthreads();
+    if (tid < NV) {
+        double v = 0.0;
+        for (int k = 0; k < kThreads / 32; ++k) v += s_w[tid][k];
+        part[tid] = v;
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_last = (atomicAdd(done, 1u) == (unsigned)ntiles - 1u);
+    __syncthreads();
+    if (!s_last) return false;
+    __threadfence();
+    return true;
+}
+
+// Sum of the filter's tile partials in tile order (warp k: component k).
+template <int NV>
+__device__ __forceinline__ void tiles_combine(const double* part, int ntiles,
+                                              double* out) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = warp; k < NV; k += kThreads / 32) {
+        double v = 0.0;
+        for (int b = lane; b < ntiles; b += 32) v += __ldcg(&part[(size_t)b * NV + k]);
+        v = warp_sum_d(v);
+        if (lane == 0) out[k] = v;
+    }
+    __syncthreads();
+}
+
+// Estimate pass over one estimate tile: 14 FP64 sums, the exact fixed-point
+// weight total and the weight materialisation; the filter's last tile
+// combines, runs the Markley mean and stores the f32 covariance means.
+// second: only filters that resample this cycle (after the resample).
+__global__ void __launch_bounds__(kThreads, 2)
+    k_b_est(Arena A, const BFilter* __restrict__ F, const BTile* __restrict__ T,
+            BCtl* C, double* __restrict__ epart,
+            unsigned long long* __restrict__ eupart, int second) {
+    const BTile t = T[blockIdx.x];
+    const BFilter& fl = F[t.f];
+    BCtl* c = C + t.f;
+    if (second && !c->resample_now) return;
+    const Planes s = filter_planes(A, c->live, fl.off);
+    const int wmode = c->wmode;
+    const double M = c->M, S = c->S;
+    const float wuni = 1.0f / (float)fl.n;
+    float* w = A.w + fl.off;
+    const float* ll = A.ll + fl.off;
+    double acc[kEstN];
+#pragma unroll
+    for (int k = 0; k < kEstN; ++k) acc[k] = 0.0;
+    unsigned long long tfx = 0;
+    int bad = 0;
+    const int q0 = t.start >> 2, q1 = (t.start + t.count + 3) >> 2;
+    const float4* px = reinterpret_cast<const float4*>(s.px);
+    const float4* py = reinterpret_cast<const float4*>(s.py);
+    const float4* pz = reinterpret_cast<const float4*>(s.pz);
+    const float4* qw = reinterpret_cast<const float4*>(s.qw);
+    const float4* qx = reinterpret_cast<const float4*>(s.qx);
+    const float4* qy = reinterpret_cast<const float4*>(s.qy);
+    const float4* qz = reinterpret_cast<const float4*>(s.qz);
+    for (int i4 = q0 + threadIdx.x; i4 < q1; i4 += kThreads) {
+        const float4 X = px[i4], Y = py[i4], Z = pz[i4];
+        const float4 QW = qw[i4], QX = qx[i4], QY = qy[i4], QZ = qz[i4];
+        float4 W;
+        if (wmode == WMODE_STORED) {
+            W = reinterpret_cast<const float4*>(w)[i4];
+        } else if (wmode == WMODE_UNIFORM) {
+            W = make_float4(wuni, wuni, wuni, wuni);
+        } else {
+            const float4 L = reinterpret_cast<const float4*>(ll)[i4];
+            W = make_float4((float)(exp((double)L.x - M) / S),
+                            (float)(exp((double)L.y - M) / S),
+                            (float)(exp((double)L.z - M) / S),
+                            (float)(exp((double)L.w - M) / S));
+            reinterpret_cast<float4*>(w)[i4] = W;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (4 * i4 + k >= fl.n) break;
+            const float wf = comp(W, k);
+            bad |= weight_bad(wf) ? 1 : 0;
+            tfx += weight_bad(wf) ? 0ull : weight_fx(wf);
+            est_add(acc, wf, comp(X, k), comp(Y, k), comp(Z, k), comp(QW, k),
+                    comp(QX, k), comp(QY, k), comp(QZ, k));
+        }
+    }
+    // integer total and bad flag of the tile
+    __shared__ unsigned long long s_u[kThreads / 32];
+    const unsigned long long u = warp_sum_u64(tfx);
+    if ((threadIdx.x & 31) == 0) s_u[threadIdx.x >> 5] = u;
+    const int any_bad = __syncthreads_or(bad);
+    if (threadIdx.x == 0) {
+        unsigned long long tot = 0;
+        for (int k = 0; k < kThreads / 32; ++k) tot += s_u[k];
+        eupart[2 * (size_t)(fl.etile0 + t.local)] = tot;
+        eupart[2 * (size_t)(fl.etile0 + t.local) + 1] = any_bad ? 1ull : 0ull;
+    }
+    if (!tile_partial<kEstN>(acc, epart + (size_t)(fl.etile0 + t.local) * kEstN,
+                             &c->done_e, fl.netiles))
+        return;
+    __shared__ double s_out[kEstN];
+    tiles_combine<kEstN>(epart + (size_t)fl.etile0 * kEstN, fl.netiles, s_out);
+    if (threadIdx.x == 0) {
+        unsigned long long tot = 0, fb = 0;
+        for (int b = 0; b < fl.netiles; ++b) {
+            tot += __ldcg(&eupart[2 * (size_t)(fl.etile0 + b)]);
+            fb |= __ldcg(&eupart[2 * (size_t)(fl.etile0 + b) + 1]);
+        }
+        for (int k = 0; k < kEstN; ++k) c->est[k] = s_out[k];
+        c->ess = s_out[13] > 0.0 ? 1.0 / s_out[13] : 0.0;
+        double qm[4];
+        markley_mean(&s_out[3], qm);
+        for (int k = 0; k < 4; ++k) c->qmean[k] = qm[k];
+        for (int k = 0; k < 3; ++k) c->cmp[k] = (float)s_out[k];
+        for (int k = 0; k < 4; ++k) c->cmq[k] = (float)qm[k];
+        c->w_total_fx = tot;
+        c->w_bad = fb ? 1 : 0;
+        if (wmode == WMODE_LL) c->wmode = WMODE_STORED;
+        c->done_e = 0u;
+    }
+}
+
+// Covariance pass; mode 1: first pass of the cycle (output record + the
+// ESS decision), mode 2: resampled filters only (output record again).
+__global__ void __launch_bounds__(kThreads, 2)
+    k_b_covs(Arena A, const BFilter* __restrict__ F, const BTile* __restrict__ T,
+             BCtl* C, double* __restrict__ cpart, double* __restrict__ out,
+             int mode) {
+    const BTile t = T[blockIdx.x];
+    const BFilter& fl = F[t.f];
+    BCtl* c = C + t.f;
+    if (mode == 2 && !c->resample_now) return;
+    const Planes s = filter_planes(A, c->live, fl.off);
+    const int wmode = c->wmode;
+    const double M = c->M, S = c->S;
+    const float wuni = 1.0f / (float)fl.n;
+    const float* w = A.w + fl.off;
+    const float* ll = A.ll + fl.off;
+    const double mp[3] = {(double)c->cmp[0], (double)c->cmp[1], (double)c->cmp[2]};
+    const double qm[4] = {(double)c->cmq[0], (double)c->cmq[1], (double)c->cmq[2],
+                          (double)c->cmq[3]};
+    double acc[kCovN];
+#pragma unroll
+    for (int k = 0; k < kCovN; ++k) acc[k] = 0.0;
+    const int q0 = t.start >> 2, q1 = (t.start + t.count + 3) >> 2;
+    const float4* px = reinterpret_cast<const float4*>(s.px);
+    const float4* py = reinterpret_cast<const float4*>(s.py);
+    const float4* pz = reinterpret_cast<const float4*>(s.pz);
+    const float4* qw = reinterpret_cast<const float4*>(s.qw);
+    const float4* qx = reinterpret_cast<const float4*>(s.qx);
+    const float4* qy = reinterpret_cast<const float4*>(s.qy);
+    const float4* qz = reinterpret_cast<const float4*>(s.qz);
+    for (int i4 = q0 + threadIdx.x; i4 < q1; i4 += kThreads) {
+        const float4 X = px[i4], Y = py[i4], Z = pz[i4];
+        const float4 QW = qw[i4], QX = qx[i4], QY = qy[i4], QZ = qz[i4];
+        float4 W;
+        if (wmode == WMODE_STORED) {
+            W = reinterpret_cast<const float4*>(w)[i4];
+        } else if (wmode == WMODE_UNIFORM) {
+            W = make_float4(wuni, wuni, wuni, wuni);
+        } else {
+            const float4 L = reinterpret_cast<const float4*>(ll)[i4];
+            W = make_float4((float)(exp((double)L.x - M) / S),
+                            (float)(exp((double)L.y - M) / S),
+                            (float)(exp((double)L.z - M) / S),
+                            (float)(exp((double)L.w - M) / S));
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (4 * i4 + k >= fl.n) break;
+            cov_add(acc, (double)comp(W, k), comp(X, k), comp(Y, k), comp(Z, k),
+                    comp(QW, k), comp(QX, k), comp(QY, k), comp(QZ, k), mp, qm);
+        }
+    }
+    if (!tile_partial<kCovN>(acc, cpart + (size_t)(fl.etile0 + t.local) * kCovN,
+                             &c->done_c, fl.netiles))
+        return;
+    __shared__ double s_out[kCovN];
+    tiles_combine<kCovN>(cpart + (size_t)fl.etile0 * kCovN, fl.netiles, s_out);
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < kCovN; ++k) c->covs[k] = s_out[k];
+        double* o = out + (size_t)t.f * PFC_EST_LEN;
+        for (int k = 0; k < 3; ++k) o[PFC_EST_POS + k] = c->est[k];
+        for (int k = 0; k < 4; ++k) o[PFC_EST_QUAT + k] = c->qmean[k];
+        for (int k = 0; k < 6; ++k) o[PFC_EST_POSCOV + k] = s_out[k];
+        for (int k = 0; k < 6; ++k) o[PFC_EST_ATTCOV + k] = s_out[6 + k];
+        o[PFC_EST_ESS] = c->ess;
+        if (mode == 1) {
+            // ParticleFilter::update's trigger: ratio > 0 && ess < ratio * N
+            // (crates/pf_core/src/particle_filter.rs:115-117)
+            o[PFC_EST_ESS_PRE] = c->ess;
+            const int go =
+                (fl.ess_ratio > 0.0 && c->ess < fl.ess_ratio * (double)fl.n) ? 1 : 0;
+            c->resample_now = go;
+            c->resampled = 0;
+            o[PFC_EST_RESAMPLED] = 0.0;
+        } else {
+            o[PFC_EST_RESAMPLED] = c->resampled ? 1.0 : 0.0;
+        }
+        c->done_c = 0u;
+    }
+}
+
+// Resampling of one 4096-particle tile of a filter that resamples: the
+// single-filter specification and kernel structure, with tiles taken in a
+// global dynamic order (a filter's tiles are consecutive in that order, so
+// each tile's predecessors are already running when it looks back).
+__global__ void __launch_bounds__(kThreads)
+    k_b_resample(Arena A, const BFilter* __restrict__ F, const BTile* __restrict__ T,
+                 BCtl* C, BGlobal* G, unsigned* flags, uint64_t* vals,
+                 HeavyRun* heavy, int heavy_cap) {
+    __shared__ unsigned s_tile;
+    __shared__ uint64_t s_warp[kThreads / 32];
+    __shared__ uint64_t s_prefix, s_agg;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_tile = atomicAdd(&G->tile_counter, 1u);
+    __syncthreads();
+    const BTile t = T[s_tile];
+    const BFilter& fl = F[t.f];
+    BCtl* c = C + t.f;
+    if (!c->resample_now) return;
+    const int n = fl.n;
+    const uint64_t Tfx = c->w_total_fx;
+    if (Tfx == 0 || c->w_bad) {
+        if (t.local == 0 && tid == 0) c->resample_valid = 0;
+        return;
+    }
+    const unsigned epoch = G->scan_epoch;
+    const unsigned long long lcg1 =
+        c->lcg * 6364136223846793005ull + 1442695040888963407ull;
+    const double u01 = (double)(lcg1 >> 11) * (1.0 / 9007199254740992.0);
+    const double total = (double)Tfx * 0x1p-62;
+    const double step = total / (double)n;
+    const double u0 = u01 * step;
+    if (tid == 0 && t.local == 0) {
+        c->lcg_next = lcg1;
+        c->resample_valid = 1;
+    }
+    const int wmode = c->wmode;
+    const double M = c->M, S = c->S;
+    const int live = c->live;
+    const Planes src = filter_planes(A, live, fl.off);
+    const Planes dst = filter_planes(A, 1 - live, fl.off);
+    const float* w = A.w + fl.off;
+    const float* ll = A.ll + fl.off;
+    unsigned* fflags = flags + fl.rtile0;
+    uint64_t* fvals = vals + 2 * (size_t)fl.rtile0;
+    const int tile = t.local;
+
+    const long long j0 = (long long)tile * kRTile + tid * kScanItems;
+    uint64_t v[kScanItems];
+    uint64_t run = 0;
+    if (wmode == WMODE_STORED && j0 + kScanItems <= n) {
+        const float4* w4 = reinterpret_cast<const float4*>(w + j0);
+#pragma unroll
+        for (int q = 0; q < kScanItems / 4; ++q) {
+            const float4 a = w4[q];
+            run += weight_fx(a.x);
+            v[4 * q] = run;
+            run += weight_fx(a.y);
+            v[4 * q + 1] = run;
+            run += weight_fx(a.z);
+            v[4 * q + 2] = run;
+            run += weight_fx(a.w);
+            v[4 * q + 3] = run;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) {
+            const long long j = j0 + k;
+            if (j < n) run += weight_fx(weight_of(wmode, j, n, w, ll, M, S));
+            v[k] = run;
+        }
+    }
+    uint64_t x = run;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint64_t y = shfl_up_u64(x, d);
+        if (lane >= d) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (tid == 0) {
+        uint64_t acc = 0;
+        for (int k = 0; k < kThreads / 32; ++k) {
+            const uint64_t tt = s_warp[k];
+            s_warp[k] = acc;
+            acc += tt;
+        }
+        s_agg = acc;
+        if (tile == 0) {
+            fvals[1] = acc;
+            __threadfence();
+            st_release(&fflags[0], (epoch << 2) | TILE_INCL);
+            s_prefix = 0;
+        } else {
+            fvals[2 * (size_t)tile] = acc;
+            __threadfence();
+            st_release(&fflags[tile], (epoch << 2) | TILE_AGG);
+        }
+    }
+    __syncthreads();
+    if (tile > 0 && warp == 0) {
+        const uint64_t prefix = look_back(fflags, fvals, tile, epoch, &c->err);
+        if (lane == 0) {
+            fvals[2 * (size_t)tile + 1] = prefix + s_agg;
+            __threadfence();
+            st_release(&fflags[tile], (epoch << 2) | TILE_INCL);
+            s_prefix = prefix;
+        }
+    }
+    __syncthreads();
+    const uint64_t c_prev = s_prefix + s_warp[warp] + (x - run);
+    long long st = (j0 == 0) ? 0 : count_le(c_prev, n, u0, step);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const long long j = j0 + k;
+        if (j >= n) break;
+        const long long e =
+            (j == n - 1) ? (long long)n : count_le(c_prev + v[k], n, u0, step);
+        const long long cnt = e - st;
+        if (cnt > kHeavy) {
+            push_run(heavy, heavy_cap, &G->heavy_count, &G->err, (int)j, st, e, t.f);
+        } else if (cnt > 0) {
+            copy_particle(src, dst, (int)j, st, e, nullptr, 0);
+        }
+        st = e;
+    }
+}
+
+// Long copy runs of all filters (HeavyRun.pad = filter), one block per
+// recorded piece.
+__global__ void __launch_bounds__(kThreads)
+    k_b_expand(Arena A, const BFilter* __restrict__ F, const BCtl* C,
+               const BGlobal* G, const HeavyRun* heavy, int heavy_cap) {
+    const int count = min(G->heavy_count, heavy_cap);
+    for (int r = blockIdx.x; r < count; r += gridDim.x) {
+        const HeavyRun h = heavy[r];
+        const int f = h.pad;
+        const int live = C[f].live;
+        const Planes src = filter_planes(A, live, F[f].off);
+        const Planes dst = filter_planes(A, 1 - live, F[f].off);
+        fill_range(src, dst, h.j, h.start + (int)threadIdx.x, h.end, kThreads, nullptr,
+                   0);
+    }
+}
+
+// Injection: global draw d belongs to filter draw_f[d] (local draw
+// j = d - inj_off).  Lists per arena particle, tags (epoch << 32 | d).
+__global__ void k_b_inject_link(const BFilter* __restrict__ F, const BCtl* C,
+                                const BGlobal* G, const int* __restrict__ draw_f,
+                                int total, uint64_t* head, int* next) {
+    const int d = blockIdx.x * kThreads + threadIdx.x;
+    if (d >= total) return;
+    const int f = draw_f[d];
+    const BCtl& c = C[f];
+    if (!c.resample_now || !c.resample_valid) return;
+    const BFilter& fl = F[f];
+    const InjDraw dr = inj_draw(c.lcg_next, c.gen, d - fl.inj_off, fl.n);
+    const unsigned epoch = G->inj_epoch;
+    const uint64_t tag = ((uint64_t)epoch << 32) | (uint32_t)d;
+    const uint64_t prev = atomicExch((unsigned long long*)&head[fl.off + dr.idx],
+                                     (unsigned long long)tag);
+    next[d] = ((uint32_t)(prev >> 32) == epoch) ? (int)(uint32_t)prev : -1;
+}
+
+__global__ void k_b_inject_apply(Arena A, const BFilter* __restrict__ F,
+                                 const BCtl* C, const BGlobal* G,
+                                 const int* __restrict__ draw_f, int total,
+                                 const uint64_t* head, const int* next) {
+    const int d = blockIdx.x * kThreads + threadIdx.x;
+    if (d >= total) return;
+    const int f = draw_f[d];
+    const BCtl& c = C[f];
+    if (!c.resample_now || !c.resample_valid) return;
+    const BFilter& fl = F[f];
+    const uint64_t lcg = c.lcg_next;
+    const InjDraw dr = inj_draw(lcg, c.gen, d - fl.inj_off, fl.n);
+    const unsigned epoch = G->inj_epoch;
+    const uint64_t h = head[fl.off + dr.idx];
+    if ((uint32_t)(h >> 32) != epoch || (int)(uint32_t)h != d) return;
+    const Planes dst = filter_planes(A, 1 - c.live, fl.off);
+    float px = dst.px[dr.idx], py = dst.py[dr.idx], pz = dst.pz[dr.idx];
+    int last = -1;
+    for (;;) {
+        int best = -1;
+        for (int x = d; x >= 0; x = next[x])
+            if (x > last && (best < 0 || x < best)) best = x;
+        if (best < 0) break;
+        const InjDraw e =
+            (best == d) ? dr : inj_draw(lcg, c.gen, best - fl.inj_off, fl.n);
+        px += e.jx;
+        py += e.jy;
+        pz += e.jz;
+        last = best;
+    }
+    dst.px[dr.idx] = px;
+    dst.py[dr.idx] = py;
+    dst.pz[dr.idx] = pz;
+}
+
+__global__ void k_b_commit(BCtl* C, BGlobal* G, int nf) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f < nf) {
+        BCtl& c = C[f];
+        if (c.resample_now) {
+            if (c.resample_valid) {
+                c.live = 1 - c.live;
+                c.resampled = 1;
+                c.lcg = c.lcg_next;
+            }
+            c.wmode = WMODE_UNIFORM;
+        }
+        if (c.err) atomicOr(&G->err, c.err);
+    }
+    if (f == 0) {
+        G->tile_counter = 0u;
+        G->heavy_count = 0;
+        unsigned e = (G->scan_epoch + 1u) & 0x3FFFFFFFu;
+        G->scan_epoch = e ? e : 1u;
+        e = G->inj_epoch + 1u;
+        G->inj_epoch = e ? e : 1u;
+    }
+}
+
+// Weights of one filter as f32 (materialised from the current mode).
+__global__ void k_b_weights(Arena A, const BFilter* F, const BCtl* C, int f,
+                            float* out) {
+    const BFilter& fl = F[f];
+    const BCtl& c = C[f];
+    for (int i = blockIdx.x * kThreads + threadIdx.x; i < fl.n;
+         i += gridDim.x * kThreads)
+        out[i] = weight_of(c.wmode, i, fl.n, A.w + fl.off, A.ll + fl.off, c.M, c.S);
+}
+
+__global__ void k_b_pack(Arena A, const BFilter* F, const BCtl* C, int f,
+                         float* pos3, float* quat4) {
+    const BFilter& fl = F[f];
+    const Planes s = filter_planes(A, C[f].live, fl.off);
+    for (int i = blockIdx.x * kThreads + threadIdx.x; i < fl.n;
+         i += gridDim.x * kThreads) {
+        pos3[3 * i] = s.px[i];
+        pos3[3 * i + 1] = s.py[i];
+        pos3[3 * i + 2] = s.pz[i];
+        quat4[4 * i] = s.qw[i];
+        quat4[4 * i + 1] = s.qx[i];
+        quat4[4 * i + 2] = s.qy[i];
+        quat4[4 * i + 3] = s.qz[i];
+    }
+}
+
+// ------------------------------------------------------------------ handle
+
+struct BatchHandle {
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    int nf = 0;
+    std::vector<BFilter> filters;
+    std::vector<int> est_tile;  // per bucket
+    int use_packed = 1;
+    long long arena = 0;         // particles incl. padding
+    float* d_planes = nullptr;   // 2 x 7 planes + ll + w
+    Arena A{};
+    BFilter* d_F = nullptr;
+    BTile* d_wt = nullptr;
+    int n_wt = 0;
+    BTile* d_et = nullptr;
+    int n_et = 0;
+    BTile* d_rt = nullptr;
+    int n_rt = 0;
+    BCtl* d_C = nullptr;
+    BGlobal* d_G = nullptr;
+    BGlobal* h_G = nullptr;
+    double2* d_wpart = nullptr;
+    double* d_epart = nullptr;
+    unsigned long long* d_eupart = nullptr;
+    double* d_cpart = nullptr;
+    unsigned* d_flags = nullptr;
+    uint64_t* d_vals = nullptr;
+    HeavyRun* d_heavy = nullptr;
+    int heavy_cap = 0;
+    int* d_draw_f = nullptr;
+    int total_draws = 0;
+    uint64_t* d_inj_head = nullptr;
+    int* d_inj_next = nullptr;
+    float* d_lm = nullptr;
+    int lm_total = 0;
+    PfcBatchCycle* d_cyc = nullptr;
+    PfcBatchCycle* h_cyc = nullptr;  // pinned
+    CObservation* d_obs = nullptr;
+    CObservation* h_obs = nullptr;   // pinned
+    int obs_cap = 0;
+    double* d_out = nullptr;
+    double* h_out = nullptr;         // pinned
+    float* d_prior = nullptr;
+    float* d_tmp = nullptr;
+    long long tmp_cap = 0;
+    bool use_graph = true;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    long long launches = 0;        // kernels launched (a graph counts its kernels)
+    int kernels_per_cycle = 0;
+};
+
+BatchHandle* as_b(void* p) { return static_cast<BatchHandle*>(p); }
+
+int bucket_of(int n) {
+    for (int b = 0; b < kBuckets - 1; ++b)
+        if (n < kBucketLimit[b]) return b;
+    return kBuckets - 1;
+}
+
+std::vector<BTile> make_tiles(const std::vector<BFilter>& F, int which,
+                              const std::vector<int>& est_tile) {
+    std::vector<BTile> t;
+    for (int f = 0; f < (int)F.size(); ++f) {
+        const int sz = which == 0 ? kWTile
+                       : which == 1 ? est_tile[bucket_of(F[f].n)]
+                                    : kRTile;
+        const int nt = ceil_div(F[f].n, sz);
+        for (int k = 0; k < nt; ++k)
+            t.push_back(BTile{f, k * sz, std::min(sz, F[f].n - k * sz), k});
+    }
+    return t;
+}
+
+void drop_graph(BatchHandle* h) {
+    if (h->exec) cudaGraphExecDestroy(h->exec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    h->exec = nullptr;
+    h->graph = nullptr;
+}
+
+// (Re)build the estimate tile table after a tile-size change.
+int rebuild_est_tiles(BatchHandle* h) {
+    std::vector<BTile> et = make_tiles(h->filters, 1, h->est_tile);
+    int e0 = 0;
+    for (int f = 0; f < h->nf; ++f) {
+        h->filters[f].etile0 = e0;
+        h->filters[f].netiles = ceil_div(h->filters[f].n,
+                                         h->est_tile[bucket_of(h->filters[f].n)]);
+        e0 += h->filters[f].netiles;
+    }
+    if ((int)et.size() > h->n_et) {
+        cudaFree(h->d_et);
+        cudaFree(h->d_epart);
+        cudaFree(h->d_eupart);
+        cudaFree(h->d_cpart);
+        h->d_et = nullptr;
+        h->d_epart = nullptr;
+        h->d_eupart = nullptr;
+        h->d_cpart = nullptr;
+        const size_t ne = et.size();
+        PFB_CK(cudaMalloc((void**)&h->d_et, sizeof(BTile) * ne));
+        PFB_CK(cudaMalloc((void**)&h->d_epart, sizeof(double) * kEstN * ne));
+        PFB_CK(cudaMalloc((void**)&h->d_eupart, sizeof(unsigned long long) * 2 * ne));
+        PFB_CK(cudaMalloc((void**)&h->d_cpart, sizeof(double) * kCovN * ne));
+    }
+    h->n_et = (int)et.size();
+    PFB_CK(cudaMemcpyAsync(h->d_et, et.data(), sizeof(BTile) * et.size(),
+                           cudaMemcpyHostToDevice, h->stream));
+    PFB_CK(cudaMemcpyAsync(h->d_F, h->filters.data(), sizeof(BFilter) * h->nf,
+                           cudaMemcpyHostToDevice, h->stream));
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    drop_graph(h);
+    return 0;
+}
+
+int launch_est_covs(BatchHandle* h, int second) {
+    k_b_est<<<h->n_et, kThreads, 0, h->stream>>>(h->A, h->d_F, h->d_et, h->d_C,
+                                                 h->d_epart, h->d_eupart, second);
+    k_b_covs<<<h->n_et, kThreads, 0, h->stream>>>(h->A, h->d_F, h->d_et, h->d_C,
+                                                  h->d_cpart, h->d_out,
+                                                  second ? 2 : 1);
+    h->launches += 2;
+    PFB_KL();
+    return 0;
+}
+
+// The kernel chain of one cycle on h->stream (inputs in d_cyc / d_obs).
+int enqueue_cycle(BatchHandle* h) {
+    cudaStream_t s = h->stream;
+    k_b_gen_inc<<<ceil_div(h->nf, kThreads), kThreads, 0, s>>>(h->d_C, h->nf);
+    k_b_weight<<<h->n_wt, kThreads, 0, s>>>(h->A, h->d_F, h->d_wt, h->d_C, h->d_cyc,
+                                            h->d_obs, h->d_lm, h->d_wpart,
+                                            h->use_packed);
+    h->launches += 2;
+    PFB_KL();
+    if (launch_est_covs(h, 0)) return -1;
+    k_b_resample<<<h->n_rt, kThreads, 0, s>>>(h->A, h->d_F, h->d_rt, h->d_C, h->d_G,
+                                              h->d_flags, h->d_vals, h->d_heavy,
+                                              h->heavy_cap);
+    k_b_expand<<<2 * 148, kThreads, 0, s>>>(h->A, h->d_F, h->d_C, h->d_G, h->d_heavy,
+                                            h->heavy_cap);
+    h->launches += 2;
+    if (h->total_draws > 0) {
+        const int g = ceil_div(h->total_draws, kThreads);
+        k_b_inject_link<<<g, kThreads, 0, s>>>(h->d_F, h->d_C, h->d_G, h->d_draw_f,
+                                               h->total_draws, h->d_inj_head,
+                                               h->d_inj_next);
+        k_b_inject_apply<<<g, kThreads, 0, s>>>(h->A, h->d_F, h->d_C, h->d_G,
+                                                h->d_draw_f, h->total_draws,
+                                                h->d_inj_head, h->d_inj_next);
+        h->launches += 2;
+    }
+    k_b_commit<<<ceil_div(h->nf, kThreads), kThreads, 0, s>>>(h->d_C, h->d_G, h->nf);
+    h->launches += 1;
+    PFB_KL();
+    if (launch_est_covs(h, 1)) return -1;
+    PFB_CK(cudaMemcpyAsync(h->h_G, h->d_G, sizeof(BGlobal), cudaMemcpyDeviceToHost, s));
+    return 0;
+}
+
+int run_cycle(BatchHandle* h) {
+    if (!h->use_graph) return enqueue_cycle(h);
+    if (!h->exec) {
+        PFB_CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        const long long l0 = h->launches;
+        const int rc = enqueue_cycle(h);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+        h->kernels_per_cycle = (int)(h->launches - l0);
+        h->launches = l0;
+        if (rc || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            set_error("pf_b200: batch cycle capture failed: %s", cudaGetErrorString(e));
+            return -1;
+        }
+        h->graph = g;
+        PFB_CK(cudaGraphInstantiate(&h->exec, g, 0));
+    }
+    PFB_CK(cudaGraphLaunch(h->exec, h->stream));
+    h->launches += h->kernels_per_cycle;
+    return 0;
+}
+
+int finish(BatchHandle* h, double* est_out) {
+    if (est_out)
+        PFB_CK(cudaMemcpyAsync(h->h_out, h->d_out,
+                               sizeof(double) * PFC_EST_LEN * (size_t)h->nf,
+                               cudaMemcpyDeviceToHost, h->stream));
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    if (h->h_G->err & ERR_SPIN_TIMEOUT) {
+        set_error("pf_b200: batch look-back wait timed out");
+        return -1;
+    }
+    if (h->h_G->err & ERR_SCAN_OVERFLOW) {
+        set_error("pf_b200: batch long-run list overflow");
+        return -1;
+    }
+    if (est_out)
+        memcpy(est_out, h->h_out, sizeof(double) * PFC_EST_LEN * (size_t)h->nf);
+    return 0;
+}
+
+void free_batch(BatchHandle* h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    drop_graph(h);
+    cudaFree(h->d_planes);
+    cudaFree(h->d_F);
+    cudaFree(h->d_wt);
+    cudaFree(h->d_et);
+    cudaFree(h->d_rt);
+    cudaFree(h->d_C);
+    cudaFree(h->d_G);
+    cudaFreeHost(h->h_G);
+    cudaFree(h->d_wpart);
+    cudaFree(h->d_epart);
+    cudaFree(h->d_eupart);
+    cudaFree(h->d_cpart);
+    cudaFree(h->d_flags);
+    cudaFree(h->d_vals);
+    cudaFree(h->d_heavy);
+    cudaFree(h->d_draw_f);
+    cudaFree(h->d_inj_head);
+    cudaFree(h->d_inj_next);
+    cudaFree(h->d_lm);
+    cudaFree(h->d_cyc);
+    cudaFreeHost(h->h_cyc);
+    cudaFree(h->d_obs);
+    cudaFreeHost(h->h_obs);
+    cudaFree(h->d_out);
+    cudaFreeHost(h->h_out);
+    cudaFree(h->d_prior);
+    cudaFree(h->d_tmp);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+int ensure_tmp(BatchHandle* h, long long floats) {
+    if (floats <= h->tmp_cap) return 0;
+    cudaFree(h->d_tmp);
+    h->d_tmp = nullptr;
+    PFB_CK(cudaMalloc((void**)&h->d_tmp, sizeof(float) * (size_t)floats));
+    h->tmp_cap = floats;
+    return 0;
+}
+
+}  // namespace batch
+}  // namespace pfb
+
+using namespace pfb;
+using namespace pfb::batch;
+
+extern "C" {
+
+void* pfc_batch_create(int n_filters, const int* n, const unsigned* seeds,
+                       int obs_cap) {
+    clear_error();
+    if (n_filters <= 0 || !n || obs_cap < 0) {
+        set_error("pf_b200: pfc_batch_create: bad arguments");
+        return nullptr;
+    }
+    for (int f = 0; f < n_filters; ++f)
+        if (n[f] <= 0) {
+            set_error("pf_b200: pfc_batch_create: filter %d has n = %d", f, n[f]);
+            return nullptr;
+        }
+    BatchHandle* h = new (std::nothrow) BatchHandle();
+    if (!h) return nullptr;
+    h->nf = n_filters;
+    h->est_tile.assign(kBuckets, 8192);
+    h->filters.resize(n_filters);
+    long long off = 0;
+    int w0 = 0, r0 = 0;
+    for (int f = 0; f < n_filters; ++f) {
+        BFilter& b = h->filters[f];
+        memset(&b, 0, sizeof(b));
+        b.off = off;
+        b.n = n[f];
+        off += (n[f] + 1023) / 1024 * 1024;
+        b.wtile0 = w0;
+        b.nwtiles = ceil_div(n[f], kWTile);
+        w0 += b.nwtiles;
+        b.rtile0 = r0;
+        b.nrtiles = ceil_div(n[f], kRTile);
+        r0 += b.nrtiles;
+        const unsigned sd = seeds ? seeds[f] : 42u;
+        b.seed = sd == 0 ? 42ull : (uint64_t)sd;
+        b.sigma_r = 0.05f;
+        b.sigma_b = 0.02f;
+        b.gate = 3.0f;
+        b.ess_ratio = 0.5;
+        b.inject_ratio = 0.0f;
+    }
+    h->arena = off;
+    bool ok = false;
+    do {
+        if (cudaGetDevice(&h->dev) != cudaSuccess) break;
+        if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+            break;
+        const size_t ap = (size_t)h->arena;
+        if (cudaMalloc((void**)&h->d_planes, sizeof(float) * ap * 16) != cudaSuccess)
+            break;
+        if (cudaMemset(h->d_planes, 0, sizeof(float) * ap * 16) != cudaSuccess) break;
+        for (int b = 0; b < 2; ++b)
+            for (int k = 0; k < 7; ++k) h->A.p[b][k] = h->d_planes + ap * (7 * b + k);
+        h->A.ll = h->d_planes + ap * 14;
+        h->A.w = h->d_planes + ap * 15;
+        std::vector<BTile> wt = make_tiles(h->filters, 0, h->est_tile);
+        std::vector<BTile> rt = make_tiles(h->filters, 2, h->est_tile);
+        h->n_wt = (int)wt.size();
+        h->n_rt = (int)rt.size();
+        if (cudaMalloc((void**)&h->d_F, sizeof(BFilter) * n_filters) != cudaSuccess ||
+            cudaMalloc((void**)&h->d_wt, sizeof(BTile) * wt.size()) != cudaSuccess ||
+            cudaMalloc((void**)&h->d_rt, sizeof(BTile) * rt.size()) != cudaSuccess ||
+            cudaMalloc((void**)&h->d_C, sizeof(BCtl) * n_filters) != cudaSuccess ||
+            cudaMalloc((void**)&h->d_G, sizeof(BGlobal)) != cudaSuccess ||
+            cudaMallocHost((void**)&h->h_G, sizeof(BGlobal)) != cudaSuccess ||
+            cudaMalloc((void**)&h->d_wpart, sizeof(double2) * wt.size()) != cudaSuccess ||
+            cudaMalloc((void**)&h->d_flags, sizeof(unsigned) * rt.size()) != cudaSuccess ||
+            cudaMalloc((void**)&h->d_vals, sizeof(uint64_t) * 2 * rt.size()) != cudaSuccess)
+            break;
+        if (cudaMemset(h->d_flags, 0, sizeof(unsigned) * rt.size()) != cudaSuccess) break;
+        h->heavy_cap = (int)std::min<long long>(
+            h->arena / kHeavy + h->arena / kSplit + 2 * n_filters, 1 << 26);
+        if (cudaMalloc((void**)&h->d_heavy, sizeof(HeavyRun) * h->heavy_cap) != cudaSuccess)
+            break;
+        if (cudaMalloc((void**)&h->d_inj_head, sizeof(uint64_t) * ap) != cudaSuccess ||
+            cudaMemset(h->d_inj_head, 0, sizeof(uint64_t) * ap) != cudaSuccess)
+            break;
+        h->obs_cap = std::max(1, obs_cap);
+        if (cudaMalloc((void**)&h->d_cyc, sizeof(PfcBatchCycle) * n_filters) != cudaSuccess ||
+            cudaMallocHost((void**)&h->h_cyc, sizeof(PfcBatchCycle) * n_filters) != cudaSuccess ||
+            cudaMalloc((void**)&h->d_obs, sizeof(CObservation) * h->obs_cap) != cudaSuccess ||
+            cudaMallocHost((void**)&h->h_obs, sizeof(CObservation) * h->obs_cap) != cudaSuccess ||
+            cudaMalloc((void**)&h->d_out, sizeof(double) * PFC_EST_LEN * n_filters) != cudaSuccess ||
+            cudaMallocHost((void**)&h->h_out, sizeof(double) * PFC_EST_LEN * n_filters) != cudaSuccess ||
+            cudaMalloc((void**)&h->d_prior, sizeof(float) * 13 * n_filters) != cudaSuccess)
+            break;
+        if (cudaMemset(h->d_cyc, 0, sizeof(PfcBatchCycle) * n_filters) != cudaSuccess ||
+            cudaMemset(h->d_out, 0, sizeof(double) * PFC_EST_LEN * n_filters) != cudaSuccess)
+            break;
+        // an empty landmark table until landmarks are uploaded
+        if (cudaMalloc((void**)&h->d_lm, sizeof(float) * 3) != cudaSuccess) break;
+        if (cudaMemcpy(h->d_wt, wt.data(), sizeof(BTile) * wt.size(),
+                       cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->d_rt, rt.data(), sizeof(BTile) * rt.size(),
+                       cudaMemcpyHostToDevice) != cudaSuccess)
+            break;
+        k_b_init<<<ceil_div(n_filters, kThreads), kThreads, 0, h->stream>>>(h->d_C, h->d_G,
+                                                                           n_filters);
+        if (cudaGetLastError() != cudaSuccess) break;
+        if (rebuild_est_tiles(h)) break;
+        ok = true;
+    } while (0);
+    if (!ok) {
+        set_error("pf_b200: pfc_batch_create failed: %s",
+                  cudaGetErrorString(cudaGetLastError()));
+        free_batch(h);
+        return nullptr;
+    }
+    return h;
+}
+
+int pfc_batch_destroy(void* p) {
+    free_batch(as_b(p));
+    return 0;
+}
+
+void* pfc_batch_stream(void* p) {
+    BatchHandle* h = as_b(p);
+    return h ? (void*)h->stream : nullptr;
+}
+
+int pfc_batch_size(void* p, int f) {
+    BatchHandle* h = as_b(p);
+    if (!h || f < 0 || f >= h->nf) return -1;
+    return h->filters[f].n;
+}
+
+int pfc_batch_set_params(void* p, const PfcCycleParams* prm) {
+    BatchHandle* h = as_b(p);
+    if (!h || !prm) return -1;
+    // injection counts: k = floor(ratio * n) with the single-filter path's
+    // f32 product; global draw offsets in filter order
+    std::vector<int> draw_f;
+    for (int f = 0; f < h->nf; ++f) {
+        BFilter& b = h->filters[f];
+        b.sigma_r = prm[f].sigma_r;
+        b.sigma_b = prm[f].sigma_b;
+        b.gate = prm[f].gate;
+        b.ess_ratio = prm[f].resample_ess_ratio;
+        b.inject_ratio = prm[f].random_inject_ratio;
+        int k = (b.inject_ratio > 0.f) ? (int)(b.inject_ratio * (float)b.n) : 0;
+        if (k > b.n) k = b.n;
+        b.inj_k = k;
+        b.inj_off = (int)draw_f.size();
+        draw_f.insert(draw_f.end(), (size_t)k, f);
+    }
+    if ((int)draw_f.size() > h->total_draws) {
+        cudaFree(h->d_draw_f);
+        cudaFree(h->d_inj_next);
+        h->d_draw_f = nullptr;
+        h->d_inj_next = nullptr;
+        PFB_CK(cudaMalloc((void**)&h->d_draw_f, sizeof(int) * draw_f.size()));
+        PFB_CK(cudaMalloc((void**)&h->d_inj_next, sizeof(int) * draw_f.size()));
+    }
+    h->total_draws = (int)draw_f.size();
+    if (!draw_f.empty())
+        PFB_CK(cudaMemcpyAsync(h->d_draw_f, draw_f.data(), sizeof(int) * draw_f.size(),
+                               cudaMemcpyHostToDevice, h->stream));
+    PFB_CK(cudaMemcpyAsync(h->d_F, h->filters.data(), sizeof(BFilter) * h->nf,
+                           cudaMemcpyHostToDevice, h->stream));
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    drop_graph(h);
+    return 0;
+}
+
+int pfc_batch_upload_landmarks(void* p, const float* xyz, const int* counts) {
+    BatchHandle* h = as_b(p);
+    if (!h || !counts) return -1;
+    long long tot = 0;
+    for (int f = 0; f < h->nf; ++f) {
+        if (counts[f] < 0) return -1;
+        h->filters[f].lm_off = (int)tot;
+        h->filters[f].lm_count = counts[f];
+        tot += counts[f];
+    }
+    if (tot > 0 && !xyz) return -1;
+    if (tot > h->lm_total) {
+        cudaFree(h->d_lm);
+        h->d_lm = nullptr;
+        PFB_CK(cudaMalloc((void**)&h->d_lm, sizeof(float) * 3 * (size_t)tot));
+        h->lm_total = (int)tot;
+    }
+    if (tot > 0)
+        PFB_CK(cudaMemcpyAsync(h->d_lm, xyz, sizeof(float) * 3 * (size_t)tot,
+                               cudaMemcpyHostToDevice, h->stream));
+    PFB_CK(cudaMemcpyAsync(h->d_F, h->filters.data(), sizeof(BFilter) * h->nf,
+                           cudaMemcpyHostToDevice, h->stream));
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    drop_graph(h);
+    return 0;
+}
+
+int pfc_batch_reinit(void* p, const float* pose7, const float* pos_std3,
+                     const float* rot_std3) {
+    BatchHandle* h = as_b(p);
+    if (!h || !pose7 || !pos_std3 || !rot_std3) return -1;
+    std::vector<float> pr(13 * (size_t)h->nf);
+    for (int f = 0; f < h->nf; ++f) {
+        for (int k = 0; k < 7; ++k) pr[13 * f + k] = pose7[7 * f + k];
+        for (int k = 0; k < 3; ++k) pr[13 * f + 7 + k] = pos_std3[3 * f + k];
+        for (int k = 0; k < 3; ++k) pr[13 * f + 10 + k] = rot_std3[3 * f + k];
+    }
+    PFB_CK(cudaMemcpyAsync(h->d_prior, pr.data(), sizeof(float) * pr.size(),
+                           cudaMemcpyHostToDevice, h->stream));
+    k_b_gen_inc<<<ceil_div(h->nf, kThreads), kThreads, 0, h->stream>>>(h->d_C, h->nf);
+    k_b_reinit<<<h->n_wt, kThreads, 0, h->stream>>>(h->A, h->d_F, h->d_wt, h->d_C,
+                                                    h->d_prior);
+    h->launches += 2;
+    PFB_KL();
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int pfc_batch_cycle(void* p, const PfcOdom* odom, const CObservation* obs,
+                    const int* nobs, double* est_out) {
+    BatchHandle* h = as_b(p);
+    if (!h || !odom || !nobs) return -1;
+    int off = 0;
+    for (int f = 0; f < h->nf; ++f) {
+        h->h_cyc[f].odom = odom[f];
+        h->h_cyc[f].obs_off = off;
+        h->h_cyc[f].nobs = std::max(0, nobs[f]);
+        off += std::max(0, nobs[f]);
+    }
+    if (off > h->obs_cap) {
+        set_error("pf_b200: pfc_batch_cycle: %d observations exceed capacity %d", off,
+                  h->obs_cap);
+        return -1;
+    }
+    if (off > 0 && !obs) return -1;
+    if (off > 0) memcpy(h->h_obs, obs, sizeof(CObservation) * (size_t)off);
+    PFB_CK(cudaMemcpyAsync(h->d_cyc, h->h_cyc, sizeof(PfcBatchCycle) * h->nf,
+                           cudaMemcpyHostToDevice, h->stream));
+    if (off > 0)
+        PFB_CK(cudaMemcpyAsync(h->d_obs, h->h_obs, sizeof(CObservation) * (size_t)off,
+                               cudaMemcpyHostToDevice, h->stream));
+    if (run_cycle(h)) return -1;
+    return finish(h, est_out);
+}
+
+int pfc_batch_cycle_device(void* p, const PfcBatchCycle* d_cycle,
+                           const CObservation* d_obs, int n_obs, double* est_out) {
+    BatchHandle* h = as_b(p);
+    if (!h || !d_cycle || n_obs < 0 || n_obs > h->obs_cap) return -1;
+    PFB_CK(cudaMemcpyAsync(h->d_cyc, d_cycle, sizeof(PfcBatchCycle) * h->nf,
+                           cudaMemcpyDeviceToDevice, h->stream));
+    if (n_obs > 0)
+        PFB_CK(cudaMemcpyAsync(h->d_obs, d_obs, sizeof(CObservation) * (size_t)n_obs,
+                               cudaMemcpyDeviceToDevice, h->stream));
+    if (run_cycle(h)) return -1;
+    if (!est_out) return 0;
+    return finish(h, est_out);
+}
+
+int pfc_batch_result(void* p, double* est_out) {
+    BatchHandle* h = as_b(p);
+    if (!h || !est_out) return -1;
+    return finish(h, est_out);
+}
+
+int pfc_batch_use_graph(void* p, int on) {
+    BatchHandle* h = as_b(p);
+    if (!h) return -1;
+    h->use_graph = on != 0;
+    if (!h->use_graph) drop_graph(h);
+    return 0;
+}
+
+int pfc_batch_set_tiles(void* p, const int* est_tile, int use_packed) {
+    BatchHandle* h = as_b(p);
+    if (!h || !est_tile) return -1;
+    for (int b = 0; b < kBuckets; ++b) {
+        const int t = est_tile[b];
+        if (t < 256 || t % 1024 != 0 || t > (1 << 20)) {
+            set_error("pf_b200: estimate tile %d must be a multiple of 1024", t);
+            return -1;
+        }
+    }
+    h->est_tile.assign(est_tile, est_tile + kBuckets);
+    h->use_packed = use_packed ? 1 : 0;
+    return rebuild_est_tiles(h);
+}
+
+int pfc_batch_get_tiles(void* p, int* est_tile, int* use_packed) {
+    BatchHandle* h = as_b(p);
+    if (!h || !est_tile) return -1;
+    for (int b = 0; b < kBuckets; ++b) est_tile[b] = h->est_tile[b];
+    if (use_packed) *use_packed = h->use_packed;
+    return 0;
+}
+
+// Autotuner: per size bucket, the estimate tile that minimises the time of
+// the estimate + covariance passes (CUDA events, best of `reps`), then the
+// weighting variant.  Timing runs re-evaluate the current state only (the
+// passes are idempotent for a fixed cloud).  Writes the choices.
+int pfc_batch_autotune(void* p, int reps, int* est_tile_out, int* packed_out) {
+    BatchHandle* h = as_b(p);
+    if (!h) return -1;
+    if (reps <= 0) reps = 3;
+    cudaEvent_t e0, e1;
+    PFB_CK(cudaEventCreate(&e0));
+    PFB_CK(cudaEventCreate(&e1));
+    int rc = 0;
+    auto time_est = [&](float* best) -> int {
+        *best = 1e30f;
+        for (int r = 0; r < reps; ++r) {
+            if (cudaEventRecord(e0, h->stream) != cudaSuccess) return -1;
+            if (launch_est_covs(h, 0)) return -1;
+            if (cudaEventRecord(e1, h->stream) != cudaSuccess) return -1;
+            if (cudaEventSynchronize(e1) != cudaSuccess) return -1;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            *best = std::min(*best, ms);
+        }
+        return 0;
+    };
+    for (int b = 0; b < kBuckets && rc == 0; ++b) {
+        bool any = false;
+        for (const BFilter& f : h->filters) any |= bucket_of(f.n) == b;
+        if (!any) continue;
+        int best_t = h->est_tile[b];
+        float best_ms = 1e30f;
+        for (int t : kEstTileChoices) {
+            h->est_tile[b] = t;
+            if (rebuild_est_tiles(h)) {
+                rc = -1;
+                break;
+            }
+            float ms;
+            if (time_est(&ms)) {
+                rc = -1;
+                break;
+            }
+            if (ms < best_ms) {
+                best_ms = ms;
+                best_t = t;
+            }
+        }
+        h->est_tile[b] = best_t;
+    }
+    if (rc == 0) rc = rebuild_est_tiles(h);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return -1;
+    if (est_tile_out)
+        for (int b = 0; b < kBuckets; ++b) est_tile_out[b] = h->est_tile[b];
+    if (packed_out) *packed_out = h->use_packed;
+    return 0;
+}
+
+int pfc_batch_snapshot(void* p, int f, float* pos3n, float* quat4n) {
+    BatchHandle* h = as_b(p);
+    if (!h || f < 0 || f >= h->nf || !pos3n || !quat4n) return -1;
+    const int n = h->filters[f].n;
+    if (ensure_tmp(h, 7ll * n)) return -1;
+    k_b_pack<<<std::min(ceil_div(n, kThreads), 1184), kThreads, 0, h->stream>>>(
+        h->A, h->d_F, h->d_C, f, h->d_tmp, h->d_tmp + 3 * (size_t)n);
+    PFB_KL();
+    PFB_CK(cudaMemcpyAsync(pos3n, h->d_tmp, sizeof(float) * 3 * (size_t)n,
+                           cudaMemcpyDeviceToHost, h->stream));
+    PFB_CK(cudaMemcpyAsync(quat4n, h->d_tmp + 3 * (size_t)n,
+                           sizeof(float) * 4 * (size_t)n, cudaMemcpyDeviceToHost,
+                           h->stream));
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int pfc_batch_get_weights(void* p, int f, float* w) {
+    BatchHandle* h = as_b(p);
+    if (!h || f < 0 || f >= h->nf || !w) return -1;
+    const int n = h->filters[f].n;
+    if (ensure_tmp(h, n)) return -1;
+    k_b_weights<<<std::min(ceil_div(n, kThreads), 1184), kThreads, 0, h->stream>>>(
+        h->A, h->d_F, h->d_C, f, h->d_tmp);
+    PFB_KL();
+    PFB_CK(cudaMemcpyAsync(w, h->d_tmp, sizeof(float) * (size_t)n,
+                           cudaMemcpyDeviceToHost, h->stream));
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+long long pfc_batch_launches(void* p) {
+    BatchHandle* h = as_b(p);
+    return h ? h->launches : -1;
+}
+
+}  // extern "C"

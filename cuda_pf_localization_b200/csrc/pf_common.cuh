@@ -147,42 +147,60 @@ __device__ __forceinline__ void pf_normals6(uint64_t seed, uint64_t gen,
 }
 
 // ------------------------------------------------------- quaternion algebra
-// Hamilton product and the rotation v' = v + 2w(u x v) + 2u x (u x v),
-// written with the same operation order as the reference device helpers
-// (src/cuda/pf_kernels.cu:119-149) so the f32 results match bit for bit
-// under the same compiler contraction rules.
+// Hamilton product and the rotation v' = v + 2w(u x v) + 2u x (u x v).
+// Every rounding is written out with intrinsics, so the results do not
+// depend on how the compiler contracts multiply-adds in the kernel they are
+// inlined into (kernels that share these helpers produce the same bits).
+// q_rotate spells out the contraction nvcc applies to the reference's
+// expression (src/cuda/pf_kernels.cu:119-149), so rotated vectors equal the
+// reference kernel's:
+//   t = 2 fma(-q.z, v.y, q.y v.z) (likewise y, z)
+//   c = fma(-q.z, t.y, q.y t.z)   (likewise y, z)
+//   r = fma(q.w, t.x, v.x) + c.x  (likewise y, z)
 struct Quat {
     float w, x, y, z;
 };
 
 __device__ __forceinline__ float3 q_rotate(const Quat& q, float3 v) {
-    float3 t = make_float3(2.f * (q.y * v.z - q.z * v.y),
-                           2.f * (q.z * v.x - q.x * v.z),
-                           2.f * (q.x * v.y - q.y * v.x));
-    float3 c = make_float3(q.y * t.z - q.z * t.y, q.z * t.x - q.x * t.z,
-                           q.x * t.y - q.y * t.x);
-    return make_float3(v.x + q.w * t.x + c.x, v.y + q.w * t.y + c.y,
-                       v.z + q.w * t.z + c.z);
+    const float tx = __fmul_rn(2.f, __fmaf_rn(-q.z, v.y, __fmul_rn(q.y, v.z)));
+    const float ty = __fmul_rn(2.f, __fmaf_rn(-q.x, v.z, __fmul_rn(q.z, v.x)));
+    const float tz = __fmul_rn(2.f, __fmaf_rn(-q.y, v.x, __fmul_rn(q.x, v.y)));
+    const float cx = __fmaf_rn(-q.z, ty, __fmul_rn(q.y, tz));
+    const float cy = __fmaf_rn(-q.x, tz, __fmul_rn(q.z, tx));
+    const float cz = __fmaf_rn(-q.y, tx, __fmul_rn(q.x, ty));
+    return make_float3(__fadd_rn(__fmaf_rn(q.w, tx, v.x), cx),
+                       __fadd_rn(__fmaf_rn(q.w, ty, v.y), cy),
+                       __fadd_rn(__fmaf_rn(q.w, tz, v.z), cz));
 }
 
 __device__ __forceinline__ Quat q_conjugate(const Quat& q) {
     return {q.w, -q.x, -q.y, -q.z};
 }
 
+// Hamilton product, each component accumulated left to right from the
+// first product.
 __device__ __forceinline__ Quat q_product(const Quat& a, const Quat& b) {
-    return {a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z,
-            a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y,
-            a.w * b.y - a.x * b.z + a.y * b.w + a.z * b.x,
-            a.w * b.z + a.x * b.y - a.y * b.x + a.z * b.w};
+    Quat r;
+    r.w = __fmaf_rn(-a.z, b.z, __fmaf_rn(-a.y, b.y, __fmaf_rn(-a.x, b.x, __fmul_rn(a.w, b.w))));
+    r.x = __fmaf_rn(-a.z, b.y, __fmaf_rn(a.y, b.z, __fmaf_rn(a.x, b.w, __fmul_rn(a.w, b.x))));
+    r.y = __fmaf_rn(a.z, b.x, __fmaf_rn(a.y, b.w, __fmaf_rn(-a.x, b.z, __fmul_rn(a.w, b.y))));
+    r.z = __fmaf_rn(a.z, b.w, __fmaf_rn(-a.y, b.x, __fmaf_rn(a.x, b.y, __fmul_rn(a.w, b.z))));
+    return r;
+}
+
+// |v| with a fixed rounding sequence.
+__device__ __forceinline__ float norm3(float3 v) {
+    return sqrtf(__fmaf_rn(v.z, v.z, __fmaf_rn(v.y, v.y, __fmul_rn(v.x, v.x))));
 }
 
 // exp map of a rotation vector with the reference's guards (angle and axis
 // norm must exceed 1e-12, else identity).
 __device__ __forceinline__ Quat q_from_axis_angle(float3 axis, float angle) {
-    float nrm = sqrtf(axis.x * axis.x + axis.y * axis.y + axis.z * axis.z);
+    const float nrm = norm3(axis);
     if (!(angle > 1e-12f) || !(nrm > 1e-12f)) return {1.f, 0.f, 0.f, 0.f};
-    float s = sinf(0.5f * angle) / nrm;
-    return {cosf(0.5f * angle), axis.x * s, axis.y * s, axis.z * s};
+    const float h = __fmul_rn(0.5f, angle);
+    const float s = __fdiv_rn(sinf(h), nrm);
+    return {cosf(h), __fmul_rn(axis.x, s), __fmul_rn(axis.y, s), __fmul_rn(axis.z, s)};
 }
 
 // ------------------------------------------------------------ float keys

@@ -20,34 +20,19 @@
 #include <math.h>
 
 #include "markley.h"
-#include "pf_internal.h"
+#include "pf_device.cuh"
 
 namespace pfb {
 
 namespace {
 
-constexpr int kThreads = 256;
+using namespace pfb::dev;
+constexpr int kThreads = kBlk;
 // Two resident blocks per SM keep enough 16-byte loads in flight; a fixed,
 // small grid also keeps the last block's combine short.
 constexpr int kMaxBlocks = 2 * 148;
 
 PlaneSet plane_set(const PfHandle* h) { return {h->planes(0), h->planes(1)}; }
-
-__device__ __forceinline__ double warp_sum_d(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(~0u, v, o);
-    return v;
-}
-
-__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(~0u, v, o);
-    return v;
-}
-
-__device__ __forceinline__ float comp(const float4& v, int c) {
-    return c == 0 ? v.x : (c == 1 ? v.y : (c == 2 ? v.z : v.w));
-}
 
 // Reduce NV per-thread FP64 accumulators over the block into part[blk*NV+k];
 // the last block to finish sums the partials of all blocks in block order
@@ -162,18 +147,8 @@ __global__ void __launch_bounds__(kThreads, 2)
             const float wf = comp(W, c);
             bad |= weight_bad(wf) ? 1 : 0;
             tfx += weight_bad(wf) ? 0ull : weight_fx(wf);
-            const double wd = (double)wf;
-            acc[0] += wd * (double)comp(X, c);
-            acc[1] += wd * (double)comp(Y, c);
-            acc[2] += wd * (double)comp(Z, c);
-            const double q[4] = {(double)comp(QW, c), (double)comp(QX, c),
-                                 (double)comp(QY, c), (double)comp(QZ, c)};
-            int e = 3;
-#pragma unroll
-            for (int r = 0; r < 4; ++r)
-#pragma unroll
-                for (int cc = r; cc < 4; ++cc) acc[e++] += wd * q[r] * q[cc];
-            acc[13] += wd * wd;
+            est_add(acc, wf, comp(X, c), comp(Y, c), comp(Z, c), comp(QW, c),
+                    comp(QX, c), comp(QY, c), comp(QZ, c));
         }
     }
     __shared__ double s_out[kEstN];
@@ -193,34 +168,6 @@ __global__ void __launch_bounds__(kThreads, 2)
         ctl->w_total_fx = s_tfx;
         ctl->w_bad = s_bad;
         if (wmode == WMODE_LL) ctl->wmode = WMODE_STORED;
-    }
-}
-
-// Attitude residual of q about qm as a canonical rotation vector
-// (w >= 0, angle = 2 atan2(|v|, w)), in FP64 — the form of
-// src/cuda/pf_kernels.cu:435-447 and crates/pf_core/src/cpu.rs:346-366.
-__device__ __forceinline__ void att_residual(const double qm[4],
-                                             const double q[4], double aav[3]) {
-    // dq = conj(qm) * q
-    const double aw = qm[0], ax = -qm[1], ay = -qm[2], az = -qm[3];
-    double dw = aw * q[0] - ax * q[1] - ay * q[2] - az * q[3];
-    double dx = aw * q[1] + ax * q[0] + ay * q[3] - az * q[2];
-    double dy = aw * q[2] - ax * q[3] + ay * q[0] + az * q[1];
-    double dz = aw * q[3] + ax * q[2] - ay * q[1] + az * q[0];
-    if (dw < 0.0) {
-        dw = -dw;
-        dx = -dx;
-        dy = -dy;
-        dz = -dz;
-    }
-    const double hv = sqrt(dx * dx + dy * dy + dz * dz);
-    if (hv > 1e-12) {
-        const double f = 2.0 * atan2(hv, dw) / hv;
-        aav[0] = dx * f;
-        aav[1] = dy * f;
-        aav[2] = dz * f;
-    } else {
-        aav[0] = aav[1] = aav[2] = 0.0;
     }
 }
 
@@ -280,23 +227,8 @@ __global__ void __launch_bounds__(kThreads, 2)
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             if (4 * i4 + c >= n) break;
-            const double wd = (double)comp(W, c);
-            const double dp[3] = {(double)comp(X, c) - mp[0],
-                                  (double)comp(Y, c) - mp[1],
-                                  (double)comp(Z, c) - mp[2]};
-            int e = 0;
-#pragma unroll
-            for (int r = 0; r < 3; ++r)
-#pragma unroll
-                for (int cc = r; cc < 3; ++cc) acc[e++] += wd * dp[r] * dp[cc];
-            const double q[4] = {(double)comp(QW, c), (double)comp(QX, c),
-                                 (double)comp(QY, c), (double)comp(QZ, c)};
-            double aav[3];
-            att_residual(qm, q, aav);
-#pragma unroll
-            for (int r = 0; r < 3; ++r)
-#pragma unroll
-                for (int cc = r; cc < 3; ++cc) acc[e++] += wd * aav[r] * aav[cc];
+            cov_add(acc, (double)comp(W, c), comp(X, c), comp(Y, c), comp(Z, c),
+                    comp(QW, c), comp(QX, c), comp(QY, c), comp(QZ, c), mp, qm);
         }
     }
     __shared__ double s_out[kCovN];

@@ -34,127 +34,21 @@
 // live ping-pong buffer and advances the LCG.
 #include <math.h>
 
-#include "pf_internal.h"
+#include "pf_device.cuh"
 
 namespace pfb {
 
 namespace {
 
+using namespace pfb::dev;
+
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 16;
 constexpr int kScanTile = kScanThreads * kScanItems;  // 4096
 constexpr int kHeavy = 32;  // longest copy run a scan thread performs
-constexpr int kThreads = 256;
+constexpr int kThreads = kBlk;
 
 PlaneSet plane_set(const PfHandle* h) { return {h->planes(0), h->planes(1)}; }
-
-__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p)
-                 : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v)
-                 : "memory");
-}
-
-__device__ __forceinline__ uint64_t shfl_up_u64(uint64_t v, int d) {
-    unsigned lo = (unsigned)v, hi = (unsigned)(v >> 32);
-    lo = __shfl_up_sync(~0u, lo, d);
-    hi = __shfl_up_sync(~0u, hi, d);
-    return ((uint64_t)hi << 32) | lo;
-}
-
-__device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(~0u, v, o);
-    return v;
-}
-
-enum : unsigned { TILE_AGG = 1u, TILE_INCL = 2u };
-
-// Fixed-point threshold of output i (see the specification above).
-__device__ __forceinline__ uint64_t threshold_fx(long long i, double u0,
-                                                 double step) {
-    const double t = __dadd_rn(u0, __dmul_rn((double)i, step));
-    const double s = t * 0x1p62;
-    if (!(s > 0.0)) return 0ull;
-    if (s >= 0x1p64) return ~0ull;
-    return __double2ull_ru(s);
-}
-
-// cnt(X) = number of outputs i in [0, n) with threshold_fx(i) <= X.  The
-// thresholds are non-decreasing in i, so this is one more than the last such
-// index; it is estimated from the arithmetic sequence and then corrected
-// against the exact thresholds.
-__device__ __forceinline__ long long count_le(uint64_t X, int n, double u0,
-                                              double step) {
-    const double e = floor(((double)X * 0x1p-62 - u0) / step);
-    long long i;
-    if (!(e >= -1.0))
-        i = -1;
-    else if (e > (double)(n - 1))
-        i = n - 1;
-    else
-        i = (long long)e;
-    while (i + 1 <= n - 1 && threshold_fx(i + 1, u0, step) <= X) ++i;
-    while (i >= 0 && threshold_fx(i, u0, step) > X) --i;
-    return i + 1;
-}
-
-__device__ __forceinline__ void copy_particle(const Planes& src, const Planes& dst,
-                                              int j, long long s, long long e,
-                                              int* anc, int record) {
-    const float x = src.px[j], y = src.py[j], z = src.pz[j];
-    const float a = src.qw[j], b = src.qx[j], c = src.qy[j], d = src.qz[j];
-    for (long long i = s; i < e; ++i) {
-        dst.px[i] = x;
-        dst.py[i] = y;
-        dst.pz[i] = z;
-        dst.qw[i] = a;
-        dst.qx[i] = b;
-        dst.qy[i] = c;
-        dst.qz[i] = d;
-        if (record) anc[i] = j;
-    }
-}
-
-// Warp-parallel look-back (run by warp 0 of a tile > 0): returns the sum of
-// all predecessors' weights.  Lane l inspects tile base - l; the nearest
-// predecessor that already knows its inclusive prefix ends the walk.
-__device__ uint64_t look_back(const unsigned* flags, const uint64_t* vals,
-                              int tile, unsigned epoch, CycleCtl* ctl) {
-    const int lane = threadIdx.x & 31;
-    uint64_t prefix = 0;
-    int base = tile - 1;
-    int spins = 0;
-    for (;;) {
-        const int j = base - lane;
-        unsigned f = 0;
-        bool ready = true;
-        if (j >= 0) {
-            f = ld_acquire(&flags[j]);
-            ready = (f >> 2) == epoch && (f & 3u) != 0u;
-        }
-        if (!__all_sync(~0u, ready)) {
-            if (++spins > kSpinLimit) {
-                if (lane == 0) atomicOr(&ctl->err, ERR_SPIN_TIMEOUT);
-                return prefix;
-            }
-            continue;
-        }
-        const unsigned incl = __ballot_sync(~0u, j < 0 || (f & 3u) == TILE_INCL);
-        const int first = incl ? __ffs(incl) - 1 : 31;
-        uint64_t v = 0;
-        if (lane <= first && j >= 0)
-            v = (lane == first && incl) ? __ldcg(&vals[2 * (size_t)j + 1])
-                                        : __ldcg(&vals[2 * (size_t)j]);
-        prefix += warp_sum_u64(v);
-        if (incl) return prefix;
-        base -= 32;
-    }
-}
 
 __global__ void __launch_bounds__(kScanThreads)
     k_resample(PlaneSet ps, int n, const float* __restrict__ w,
@@ -255,7 +149,7 @@ __global__ void __launch_bounds__(kScanThreads)
     }
     __syncthreads();
     if (tile > 0 && warp == 0) {
-        const uint64_t prefix = look_back(flags, vals, tile, epoch, ctl);
+        const uint64_t prefix = look_back(flags, vals, tile, epoch, &ctl->err);
         if (lane == 0) {
             vals[2 * (size_t)tile + 1] = prefix + s_agg;
             __threadfence();
@@ -276,11 +170,7 @@ __global__ void __launch_bounds__(kScanThreads)
             (j == n - 1) ? (long long)n : count_le(c_prev + v[k], n, u0, step);
         const long long cnt = e - s;
         if (cnt > kHeavy) {
-            const int slot = atomicAdd(&ctl->heavy_count, 1);
-            if (slot < heavy_cap)
-                heavy[slot] = HeavyRun{(int)j, (int)s, (int)e, 0};
-            else
-                atomicOr(&ctl->err, ERR_SCAN_OVERFLOW);
+            push_run(heavy, heavy_cap, &ctl->heavy_count, &ctl->err, (int)j, s, e, 0);
         } else if (cnt > 0) {
             copy_particle(src, dst, (int)j, s, e, anc, record);
         }
@@ -288,27 +178,8 @@ __global__ void __launch_bounds__(kScanThreads)
     }
 }
 
-// Output-parallel expansion of the long runs: a run of at least kSplit
-// outputs is spread over the whole grid, shorter ones take one block each.
-constexpr int kSplit = 8192;
-
-__device__ __forceinline__ void fill_range(const Planes& src, const Planes& dst,
-                                           int j, int lo, int hi, int stride,
-                                           int* anc, int record) {
-    const float x = src.px[j], y = src.py[j], z = src.pz[j];
-    const float a = src.qw[j], b = src.qx[j], c = src.qy[j], d = src.qz[j];
-    for (int i = lo; i < hi; i += stride) {
-        dst.px[i] = x;
-        dst.py[i] = y;
-        dst.pz[i] = z;
-        dst.qw[i] = a;
-        dst.qx[i] = b;
-        dst.qy[i] = c;
-        dst.qz[i] = d;
-        if (record) anc[i] = j;
-    }
-}
-
+// Output-parallel expansion of the long runs: each recorded piece (at most
+// kSplit outputs) is copied by one block.
 __global__ void __launch_bounds__(kThreads)
     k_expand_runs(PlaneSet ps, const HeavyRun* heavy, int heavy_cap,
                   int* __restrict__ anc, int record, CycleCtl* ctl, int cond) {
@@ -317,51 +188,11 @@ __global__ void __launch_bounds__(kThreads)
     const int count = min(ctl->heavy_count, heavy_cap);
     const int live = ctl->live;
     const Planes src = pick_planes(ps, live), dst = pick_planes(ps, 1 - live);
-    const int gthreads = gridDim.x * kThreads;
-    const int gid = blockIdx.x * kThreads + threadIdx.x;
-    for (int r = 0; r < count; ++r) {
+    for (int r = blockIdx.x; r < count; r += gridDim.x) {
         const HeavyRun h = heavy[r];
-        if (h.end - h.start >= kSplit)
-            fill_range(src, dst, h.j, h.start + gid, h.end, gthreads, anc, record);
-        else if (r % (int)gridDim.x == (int)blockIdx.x)
-            fill_range(src, dst, h.j, h.start + (int)threadIdx.x, h.end, kThreads,
-                       anc, record);
+        fill_range(src, dst, h.j, h.start + (int)threadIdx.x, h.end, kThreads, anc,
+                   record);
     }
-}
-
-// splitmix64 step (Steele, Lea, Flood, "Fast splittable pseudorandom number
-// generators", OOPSLA 2014), the generator of the reference's k_inject.
-__device__ __forceinline__ uint64_t splitmix_next(uint64_t& z) {
-    z += 0x9E3779B97F4A7C15ull;
-    uint64_t r = z;
-    r = (r ^ (r >> 30)) * 0xBF58476D1CE4E5B9ull;
-    r = (r ^ (r >> 27)) * 0x94D049BB133111EBull;
-    return r ^ (r >> 31);
-}
-
-struct InjDraw {
-    int idx;
-    float jx, jy, jz;
-};
-
-// Draw j of the injection stream: stream seed lcg ^ gen*phi ^ (j+1)*c as in
-// src/cuda/pf_kernels.cu:337-348.
-__device__ __forceinline__ InjDraw inj_draw(uint64_t lcg, uint64_t gen, int j,
-                                            int n) {
-    uint64_t z = lcg ^ (gen * 0x9E3779B97F4A7C15ull) ^
-                 ((uint64_t)j + 1) * 0xBF58476D1CE4E5B9ull;
-    if (z == 0) z = 0x243F6A8885A308D3ull;
-    InjDraw d;
-    double u = (double)(splitmix_next(z) >> 11) * (1.0 / 9007199254740992.0);
-    int idx = (int)(u * n);
-    d.idx = idx >= n ? n - 1 : idx;
-    u = (double)(splitmix_next(z) >> 11) * (1.0 / 9007199254740992.0);
-    d.jx = (float)(u - 0.5);
-    u = (double)(splitmix_next(z) >> 11) * (1.0 / 9007199254740992.0);
-    d.jy = (float)(u - 0.5);
-    u = (double)(splitmix_next(z) >> 11) * (1.0 / 9007199254740992.0);
-    d.jz = (float)(u - 0.5);
-    return d;
 }
 
 // Injection lists: head[idx] holds (epoch << 32 | last inserted j), next[j]

@@ -182,7 +182,8 @@ def room_grid() -> np.ndarray:
 def helix_scenario(cycles: int, n_landmarks: int, box: tuple, n_obs: int | None = None,
                    outlier_frac: float = 0.0, seed: int = 1, obs_sigma: float = 0.05,
                    odo_sigma_t: float = 0.02, odo_sigma_r: float = 0.01,
-                   radius: float = 5.0, arc: float = 0.1, climb: float = 0.005) -> Scenario:
+                   radius: float = 5.0, arc: float = 0.1, climb: float = 0.005,
+                   phase: float = 0.0) -> Scenario:
     """Helix trajectory (radius 5 m, 0.1 m of arc and arc/radius rad of yaw per
     step, 0.005 m climb per step) through a landmark box centred on the helix
     axis.  Each cycle observes either every landmark (n_obs None) or n_obs
@@ -200,7 +201,7 @@ def helix_scenario(cycles: int, n_landmarks: int, box: tuple, n_obs: int | None 
     dyaw = arc / radius
 
     def pose(k):
-        ang = k * dyaw
+        ang = phase + k * dyaw
         p = centre + np.array([radius * math.cos(ang), radius * math.sin(ang),
                                -bz / 4.0 + climb * k])
         return p, q_yaw(ang + math.pi / 2.0)
@@ -296,3 +297,25 @@ def free_pose(cells: np.ndarray, rng: np.random.Generator, res=0.05, origin=(0.0
     x = origin[0] + (xs[k] + rng.uniform()) * res
     y = origin[1] + (ys[k] + rng.uniform()) * res
     return float(x), float(y), float(rng.uniform(0.0, 2 * math.pi))
+
+
+def batched_config(n_filters: int = 512, cycles: int = 200, seed: int = 23,
+                   n_min: int = 1000, n_max: int = 200_000):
+    """Batched PF workload: n_filters independent filters with N drawn
+    log-uniform in [n_min, n_max], each with its own 8-64 landmarks in a
+    20 x 20 x 5 m box and its own helix (random phase), and 4-64 observations
+    per cycle.  Returns (sizes, scenarios, nobs[f][cycle])."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    sizes = np.exp(rng.uniform(math.log(n_min), math.log(n_max), n_filters)).astype(int)
+    scen, counts = [], []
+    for f in range(n_filters):
+        n_lm = int(rng.integers(8, 65))
+        sc = helix_scenario(cycles, n_lm, (20.0, 20.0, 5.0), 64, 0.0,
+                            int(rng.integers(1, 1 << 31)),
+                            phase=float(rng.uniform(0.0, 2 * math.pi)))
+        c = rng.integers(4, 65, size=cycles)
+        for k, st in enumerate(sc.steps):
+            st.obs = st.obs[: int(c[k])]
+        scen.append(sc)
+        counts.append(c)
+    return sizes, scen, np.array(counts)

@@ -339,6 +339,64 @@ int pfgl_topk_noalloc(const float* d_scores, int n, int k, int* d_idx,
                       void* stream);
 
 /* ------------------------------------------------------------------------
+ * Batched particle filters (no counterpart in the reference).  Many
+ * independent filters of uneven size advance together: one cycle of every
+ * filter (predict + gated weighting + softmax + estimate + ESS-triggered
+ * resample with injection + estimate, as pfc_cycle) is one CUDA-graph launch.
+ * Filter f of a batch produces the same particles, weights and resampling as
+ * the same filter run alone through pfc_cycle with the same seed and inputs;
+ * its FP64 estimate sums agree to rounding (different summation tiles).
+ * ------------------------------------------------------------------------ */
+
+/* Per-filter input of one cycle: odometry and the slice
+ * [obs_off, obs_off + nobs) of the cycle's concatenated observations. */
+typedef struct PfcBatchCycle {
+    PfcOdom odom;
+    int obs_off;
+    int nobs;
+} PfcBatchCycle;
+
+/* n_filters filters of n[f] particles; seeds[f] (NULL: 42; 0 becomes 42);
+ * obs_cap = most observations of one cycle over all filters.  NULL on error. */
+void* pfc_batch_create(int n_filters, const int* n, const unsigned* seeds,
+                       int obs_cap);
+int pfc_batch_destroy(void* b);
+/* Per-filter cycle parameters (n_filters entries). */
+int pfc_batch_set_params(void* b, const PfcCycleParams* prm);
+/* Landmark tables: counts[f] landmarks of filter f, concatenated (3 floats
+ * each) in filter order. */
+int pfc_batch_upload_landmarks(void* b, const float* xyz, const int* counts);
+/* Gaussian priors: pose7 (x,y,z,qw,qx,qy,qz), pos_std3 and rot_std3 per filter. */
+int pfc_batch_reinit(void* b, const float* pose7, const float* pos_std3,
+                     const float* rot_std3);
+/* One cycle of every filter from host inputs: odom[f], nobs[f] and the
+ * concatenated observations (filter order).  est_out (may be NULL):
+ * n_filters x PFC_EST_LEN records laid out as pfc_cycle's. */
+int pfc_batch_cycle(void* b, const PfcOdom* odom, const CObservation* obs,
+                    const int* nobs, double* est_out);
+/* Same from device-resident inputs (n_filters records, n_obs observations).
+ * With est_out == NULL the call returns without waiting; pfc_batch_result
+ * then waits and copies the records. */
+int pfc_batch_cycle_device(void* b, const PfcBatchCycle* d_cycle,
+                           const CObservation* d_obs, int n_obs, double* est_out);
+int pfc_batch_result(void* b, double* est_out);
+/* 1 (default): cycles run as one CUDA-graph launch; 0: direct launches. */
+int pfc_batch_use_graph(void* b, int on);
+/* Estimate-pass tile (particles, multiple of 1024) per size bucket
+ * (n < 8192, < 32768, < 131072, larger) and the weighting variant. */
+int pfc_batch_set_tiles(void* b, const int* est_tile4, int use_packed);
+int pfc_batch_get_tiles(void* b, int* est_tile4, int* use_packed);
+/* Time the candidate tiles per bucket on the current cloud (best of reps)
+ * and keep the fastest; writes the choices. */
+int pfc_batch_autotune(void* b, int reps, int* est_tile4, int* use_packed);
+int pfc_batch_snapshot(void* b, int f, float* pos3n, float* quat4n);
+int pfc_batch_get_weights(void* b, int f, float* w);
+int pfc_batch_size(void* b, int f);
+void* pfc_batch_stream(void* b);
+/* Kernels launched by this handle so far (a graph launch counts its kernels). */
+long long pfc_batch_launches(void* b);
+
+/* ------------------------------------------------------------------------
  * Learned proposal for global localization (no counterpart in the
  * reference).  A per-map MLP maps a normalised range scan to a 32-component
  * Gaussian mixture over (x, y, cos yaw, sin yaw); queries sample hypotheses
