@@ -472,6 +472,17 @@ int gl_upload_scan(GlHandle* h, const float* scan, int nrays) {
     return ensure_scan(h, scan, nrays);
 }
 
+int gl_topk_exhaustive(GlHandle* h, int nrays, float rmax, float span, int k,
+                       float* out3k, float* caer_k, int* idx_k) {
+    if (h->nh <= 0 || k <= 0) return -1;
+    if (k > h->nh) k = h->nh;
+    if (launch_score(h, nrays, rmax, span)) return -1;
+    h->caer_valid = true;
+    const uint64_t* sorted = sort_current(h);
+    if (!sorted) return -1;
+    return copy_topk(h, sorted, k, out3k, caer_k, idx_k);
+}
+
 int gl_generate(GlHandle* h, int n_pos, int n_yaw, uint64_t seed) {
     if (h->nfree <= 0 || n_pos <= 0 || n_yaw <= 0) return -1;
     const long long n = (long long)n_pos * n_yaw;

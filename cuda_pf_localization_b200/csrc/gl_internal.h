@@ -139,6 +139,10 @@ int gl_upload_scan(GlHandle* h, const float* scan, int nrays);
 // pruned scorer; results as pfgl_localize.  Returns k written or -1.
 int gl_localize_loaded(GlHandle* h, int nrays, float rmax, float span, int k,
                        float* out3k, float* caer_k, int* idx_k);
+// Exhaustive CAER of the h->nh hypotheses in d_hyp against the loaded scan,
+// then the bottom-k (one host synchronisation).  Returns k written or -1.
+int gl_topk_exhaustive(GlHandle* h, int nrays, float rmax, float span, int k,
+                       float* out3k, float* caer_k, int* idx_k);
 // Uniform dispersion of n_pos positions x n_yaw yaws into d_hyp.
 int gl_generate(GlHandle* h, int n_pos, int n_yaw, uint64_t seed);
 

@@ -83,6 +83,7 @@ struct EpiArgs {
     const bf16* mask;   // [M][ldm] activations whose sign gates the gradient
     int ldo, ldt, ldm;
     float scale;
+    long long split_stride;  // f32 elements between split-K partial outputs
 };
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
@@ -162,6 +163,8 @@ __global__ void __launch_bounds__(128, 1)
                 const __grid_constant__ CUtensorMap tmB, int K, int a_row0,
                 int a_k0, int b_row0, int b_k0, EpiArgs ep,
                 unsigned* __restrict__ err) {
+    // Split-K: blockIdx.z takes k-blocks [kb0, kb1) and writes its partial
+    // product ep.split_stride elements after the previous split's.
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     const uint32_t s0 = smem_u32(smem_raw);
     unsigned char* base = smem_raw + ((1024u - (s0 & 1023u)) & 1023u);
@@ -174,7 +177,11 @@ __global__ void __launch_bounds__(128, 1)
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-    const int nkb = K / BK;
+    const int nkb_all = K / BK;
+    const int kb0 = (int)(((long long)blockIdx.z * nkb_all) / gridDim.z);
+    const int kb1 = (int)(((long long)(blockIdx.z + 1) * nkb_all) / gridDim.z);
+    const int nkb = kb1 - kb0;
+    if (EPI == EPI_F32) ep.out = reinterpret_cast<float*>(ep.out) + (size_t)blockIdx.z * ep.split_stride;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
@@ -206,10 +213,10 @@ __global__ void __launch_bounds__(128, 1)
                     break;
                 }
                 mbar_expect_tx(&full[s], 2 * kTileBytes);
-                tma_load_2d(sA + s * kTileBytes, &tmA, &full[s], a_k0 + kb * BK,
-                            a_row0 + m0);
-                tma_load_2d(sB + s * kTileBytes, &tmB, &full[s], b_k0 + kb * BK,
-                            b_row0 + n0);
+                tma_load_2d(sA + s * kTileBytes, &tmA, &full[s],
+                            a_k0 + (kb0 + kb) * BK, a_row0 + m0);
+                tma_load_2d(sB + s * kTileBytes, &tmB, &full[s],
+                            b_k0 + (kb0 + kb) * BK, b_row0 + n0);
             }
         }
         __syncwarp();
@@ -318,16 +325,18 @@ struct MapRef {
 
 template <int EPI>
 int gemm(cudaStream_t s, MapRef a, MapRef b, int M, int N, int K,
-         const EpiArgs& ep, unsigned* err) {
+         const EpiArgs& ep, unsigned* err, int splits = 1) {
     if (M <= 0 || N <= 0 || K <= 0 || M % BM || N % BN || K % BK ||
-        (a.k0 % 8) || (b.k0 % 8)) {
-        set_error("pf_b200: gemm shape %d x %d x %d not tileable", M, N, K);
+        (a.k0 % 8) || (b.k0 % 8) || splits < 1 || splits > K / BK ||
+        (splits > 1 && EPI != EPI_F32)) {
+        set_error("pf_b200: gemm shape %d x %d x %d (split %d) not tileable", M, N,
+                  K, splits);
         return -1;
     }
     PFB_CK(cudaFuncSetAttribute(k_gemm_bf16<EPI>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 kGemmSmem));
-    const dim3 grid(N / BN, M / BM);
+    const dim3 grid(N / BN, M / BM, splits);
     k_gemm_bf16<EPI><<<grid, 128, kGemmSmem, s>>>(*a.map, *b.map, K, a.row0,
                                                   a.k0, b.row0, b.k0, ep, err);
     PFB_KL();
@@ -437,16 +446,21 @@ __global__ void k_rowsum_bf16(const bf16* __restrict__ in, int ld, int cols,
 // With update == 0 only the bf16 copies are refreshed from the masters.
 __global__ void k_adam_w(int out, int in, float* __restrict__ w,
                          float* __restrict__ m, float* __restrict__ v,
-                         const float* __restrict__ g, bf16* __restrict__ wb,
-                         bf16* __restrict__ wtb, int update, float lr, float b1,
-                         float b2, float eps, float bc1, float bc2) {
+                         const float* __restrict__ g, int splits,
+                         bf16* __restrict__ wb, bf16* __restrict__ wtb, int update,
+                         float lr, float b1, float b2, float eps, float bc1,
+                         float bc2) {
+    // g holds `splits` partial gradients of out*in floats each, summed in
+    // split order.
+    const size_t nw = (size_t)out * in;
     __shared__ bf16 t[32][34];
     const int i0 = blockIdx.x * 32, o0 = blockIdx.y * 32;
     for (int rr = threadIdx.y; rr < 32; rr += 8) {
         const size_t idx = (size_t)(o0 + rr) * in + i0 + threadIdx.x;
         float ww = w[idx];
         if (update) {
-            const float gg = g[idx];
+            float gg = g[idx];
+            for (int sp = 1; sp < splits; ++sp) gg += g[sp * nw + idx];
             const float mm = b1 * m[idx] + (1.0f - b1) * gg;
             const float vv = b2 * v[idx] + (1.0f - b2) * gg * gg;
             m[idx] = mm;
@@ -461,6 +475,15 @@ __global__ void k_adam_w(int out, int in, float* __restrict__ w,
     __syncthreads();
     for (int cc = threadIdx.y; cc < 32; cc += 8)
         wtb[(size_t)(i0 + cc) * out + o0 + threadIdx.x] = t[threadIdx.x][cc];
+}
+
+// Sum split-K partial gradients into split 0 (split order).
+__global__ void k_sum_splits(float* __restrict__ g, int splits, long long nw) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nw) return;
+    float acc = g[i];
+    for (int sp = 1; sp < splits; ++sp) acc += g[sp * nw + i];
+    g[i] = acc;
 }
 
 __global__ void k_adam_b(int n, float* __restrict__ b, float* __restrict__ m,
@@ -690,7 +713,8 @@ struct Layer {
     float* vw = nullptr;
     float* mb = nullptr;
     float* vb = nullptr;
-    float* gw = nullptr;  // gradients
+    float* gw = nullptr;  // weight gradient: `splits` partials of out*in
+    int splits = 1;
     float* gb = nullptr;
     bf16* wb = nullptr;   // [out][in]
     bf16* wtb = nullptr;  // [in][out]
@@ -778,8 +802,8 @@ int round_weights(LpHandle* h) {
     for (int l = 0; l < kLayers; ++l) {
         Layer& L = h->L[l];
         k_adam_w<<<dim3(L.in / 32, L.out / 32), dim3(32, 8), 0, h->stream>>>(
-            L.out, L.in, L.w, L.mw, L.vw, L.gw, L.wb, L.wtb, 0, 0.f, 0.f, 0.f,
-            0.f, 1.f, 1.f);
+            L.out, L.in, L.w, L.mw, L.vw, L.gw, L.splits, L.wb, L.wtb, 0, 0.f, 0.f,
+            0.f, 0.f, 1.f, 1.f);
     }
     PFB_KL();
     return 0;
@@ -827,9 +851,10 @@ int backward(LpHandle* h, MapRef xt, const float* Y, float* d_loss_slot) {
         eg.out = L.gw;
         eg.ldo = L.in;
         eg.scale = 1.0f;
+        eg.split_stride = (long long)L.out * L.in;
         const MapRef bt = l == 0 ? xt : MapRef{&h->tm_HT[l - 1], 0, 0};
         if (gemm<EPI_F32>(s, MapRef{&h->tm_dZT[l], 0, 0}, bt, L.out, L.in, B, eg,
-                          h->d_err))
+                          h->d_err, L.splits))
             return -1;
         k_rowsum_bf16<<<ceil_div(L.out * 32, 256), 256, 0, s>>>(h->dZT[l], B, B,
                                                                  L.out, L.gb);
@@ -859,8 +884,8 @@ int adam_update(LpHandle* h, float lr) {
     for (int l = 0; l < kLayers; ++l) {
         Layer& L = h->L[l];
         k_adam_w<<<dim3(L.in / 32, L.out / 32), dim3(32, 8), 0, h->stream>>>(
-            L.out, L.in, L.w, L.mw, L.vw, L.gw, L.wb, L.wtb, 1, lr, b1, b2, eps,
-            bc1, bc2);
+            L.out, L.in, L.w, L.mw, L.vw, L.gw, L.splits, L.wb, L.wtb, 1, lr, b1, b2,
+            eps, bc1, bc2);
         k_adam_b<<<ceil_div(L.out, 256), 256, 0, h->stream>>>(
             L.out, L.b, L.mb, L.vb, L.gb, lr, b1, b2, eps, bc1, bc2);
     }
@@ -940,6 +965,10 @@ int learned_pass(LpHandle* h, int nrays, float rmax, float span, int n_samples,
     PFB_KL();
     g->nh = n_samples;
     g->caer_valid = false;
+    // Small hypothesis sets: one exhaustive scoring pass and one bottom-k
+    // (one host synchronisation); large ones go through the pruned localizer.
+    if (n_samples <= 65536)
+        return gl_topk_exhaustive(g, nrays, rmax, span, k, out3k, caer_k, idx_k);
     return gl_localize_loaded(g, nrays, rmax, span, k, out3k, caer_k, idx_k);
 }
 
@@ -978,9 +1007,15 @@ void* pfgl_learned_create(void* glv, int batch, unsigned long long seed) {
             L.in = layer_in(l);
             L.out = layer_out(l);
             const size_t nw = (size_t)L.in * L.out;
+            // split-K for the narrow weight gradients (384 x 1024 and
+            // 1024 x 384: 24 output tiles); the 1024 x 1024 ones already
+            // have 64 tiles and would pay more in partial traffic than they
+            // gain in parallelism
+            const int tiles = (L.out / BM) * (L.in / BN);
+            L.splits = tiles < 64 ? std::max(1, std::min(batch / BK, 4)) : 1;
             bad = dalloc(&L.w, nw) || dalloc(&L.b, L.out) || dalloc(&L.mw, nw) ||
                   dalloc(&L.vw, nw) || dalloc(&L.mb, L.out) ||
-                  dalloc(&L.vb, L.out) || dalloc(&L.gw, nw) ||
+                  dalloc(&L.vb, L.out) || dalloc(&L.gw, nw * L.splits) ||
                   dalloc(&L.gb, L.out) || dalloc(&L.wb, nw) || dalloc(&L.wtb, nw) ||
                   dalloc(&h->dZ[l], (size_t)batch * L.out) ||
                   dalloc(&h->dZT[l], (size_t)batch * L.out);
@@ -1259,6 +1294,11 @@ int pfgl_learned_grad(void* p, const float* x, const float* y, float* loss,
     for (int l = 0; l < kLayers; ++l) {
         Layer& L = h->L[l];
         const size_t nw = (size_t)L.in * L.out;
+        if (L.splits > 1) {
+            k_sum_splits<<<(unsigned)((nw + 255) / 256), 256, 0, h->stream>>>(
+                L.gw, L.splits, (long long)nw);
+            PFB_KL();
+        }
         PFB_CK(cudaMemcpyAsync(grad + off, L.gw, sizeof(float) * nw,
                                cudaMemcpyDeviceToHost, h->stream));
         off += nw;
