@@ -220,7 +220,7 @@ def reference_arm(args):
 
 # ------------------------------------------------------------ our GPU arm
 
-def run_value(args, sc, torch, dev):
+def run_value(args, sc, torch, dev, dist=None):
     """Fused cycles with observations resident in HBM; per-step CUDA events."""
     import cuda_pf_localization_b200 as pkg
     lib = pkg.kernels()
@@ -263,7 +263,8 @@ def run_value(args, sc, torch, dev):
                for _ in range(K)]
         lib.pfc_reset_stats(h)
         lib.pfc_profile(h, 1)
-        torch.cuda.synchronize(dev)
+        from cuda_pf_localization_b200 import multi
+        multi.sync_all(dist, dev)
         with ClockSampler(gpu_id_for(dev.index)) as clk:
             t_wall = time.perf_counter()
             with torch.cuda.stream(stream):
@@ -278,6 +279,7 @@ def run_value(args, sc, torch, dev):
                         raise RuntimeError(pkg.last_error())
             stream.synchronize()
             t_wall = time.perf_counter() - t_wall
+            multi.sync_all(dist, dev)
         ms = np.zeros(10)
         cnt = np.zeros(10, dtype=np.int64)
         lib.pfc_profile_read(h, pkg.dptr(ms), cnt.ctypes.data_as(C.POINTER(C.c_longlong)))
@@ -293,7 +295,7 @@ def run_value(args, sc, torch, dev):
         lib.pfc_destroy(h)
 
 
-def run_e2e(args, sc, torch, dev):
+def run_e2e(args, sc, torch, dev, dist=None):
     """ParticleFilter::update through the drop-in C-ABI with host buffers."""
     import cuda_pf_localization_b200 as pkg
     lib = pkg.kernels()
@@ -316,6 +318,8 @@ def run_e2e(args, sc, torch, dev):
         flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
         h = pf.handle
         lib.pfc_reset_stats(h)
+        from cuda_pf_localization_b200 import multi
+        multi.sync_all(dist, dev)
         times, errs, resampled = [], [], 0
         for k in range(K):
             flush.fill_(k & 0xFF)
@@ -329,6 +333,7 @@ def run_e2e(args, sc, torch, dev):
             times.append(t1 - t0)
             errs.append(float(np.linalg.norm(np.array(est.position[:]) - sc.steps[W + k].truth_p)))
             resampled += int(est.resampled)
+        multi.sync_all(dist, dev)
         stats = pkg.PfcStats()
         lib.pfc_get_stats(h, C.byref(stats))
         return dict(times=np.array(times), errs=np.array(errs), resampled=resampled,
@@ -625,27 +630,19 @@ def main():
         if rank == 0:
             print(json.dumps({"batched": run_batched(args, torch, dev)}), flush=True)
         return
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from cuda_pf_localization_b200 import multi
+    dist = multi.init("nccl") if world > 1 else None
 
     sc = scenario(args, args.warmup + args.steps + 1)
     n = args.particles
-    val = run_value(args, sc, torch, dev)
-    e2e = run_e2e(args, sc, torch, dev)
-    t_value = float(val["step_ms"].sum()) / 1e3
-    t_e2e = float(e2e["times"].sum())
-    if dist is not None:
-        tt = torch.tensor([t_value, t_e2e], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_value, t_e2e = float(tt[0]), float(tt[1])
-        dist.barrier()
+    val = run_value(args, sc, torch, dev, dist)
+    e2e = run_e2e(args, sc, torch, dev, dist)
+    t_value, t_e2e = multi.max_over_ranks(
+        [float(val["step_ms"].sum()) / 1e3, float(e2e["times"].sum())], dist, dev)
 
     K = args.steps
-    value = world * n * K / t_value
-    e2e_value = world * n * K / t_e2e
+    value = multi.weak_scaling_rate(world, n * K, t_value)
+    e2e_value = multi.weak_scaling_rate(world, n * K, t_e2e)
 
     # dominant kernel: gated weighting (fused with the motion update)
     hbm, peak_kind = peaks()
@@ -716,9 +713,7 @@ def main():
                                 "within 0.5 m and 0.1 rad")
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    multi.finish(dist)
 
 
 if __name__ == "__main__":
