@@ -456,6 +456,8 @@ def run_gl(args):
             if lp is not None:
                 lp.close()
             lib.pfgl_destroy(h)
+    if args.gl_maps <= 0:
+        return res
     learned_sps = tot_q / t_learn
     uniform_sps = uni_q / t_uni
     res["learned"] = dict(

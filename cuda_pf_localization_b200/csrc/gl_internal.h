@@ -64,8 +64,15 @@ struct GridView {
 // 2-D DDA from the padded start index with in-cell fractions (frx, fry):
 // distance to the first occupied cell, rmax when the ray passes rmax or
 // leaves the map.  The f32 arithmetic follows src/cuda/pf_kernels.cu:784-808
-// (tMax/tDelta stepping, x step on ties, 8192-step limit); stepping onto the
-// border byte (2) is the reference's out-of-grid test.
+// (tMax/tDelta stepping, x step on ties); stepping onto the border byte (2)
+// is the reference's out-of-grid test.
+//
+// The reference tests dist > rmax and an 8192-step limit after every step.
+// Both leave the loop here without changing any result: the step distances
+// never decrease, so "the first hit, then rmax if its distance exceeds rmax"
+// equals "rmax as soon as a step exceeds rmax"; the border ends every ray,
+// and the number of steps taken (one cell in x or y per step) is recovered
+// from the hit cell to apply the step limit.
 __device__ __forceinline__ float cast_ray(const unsigned char* __restrict__ g,
                                           int Wp, int start, float frx,
                                           float fry, float dirx, float diry,
@@ -78,22 +85,22 @@ __device__ __forceinline__ float cast_ray(const unsigned char* __restrict__ g,
     float tmx = adx > 1e-9f ? ((dirx > 0 ? 1.f - frx : frx) * tdx) : INFINITY;
     float tmy = ady > 1e-9f ? ((diry > 0 ? 1.f - fry : fry) * tdy) : INFINITY;
     int idx = start;
-    for (int step = 0; step < 8192; ++step) {
-        float dist;
-        if (tmx <= tmy) {
-            dist = tmx;
+    float dist;
+    unsigned v;
+    do {
+        const bool px = tmx <= tmy;
+        dist = px ? tmx : tmy;
+        if (px)
             tmx += tdx;
-            idx += sx;
-        } else {
-            dist = tmy;
+        else
             tmy += tdy;
-            idx += sy;
-        }
-        if (dist > rmax) return rmax;
-        const unsigned char v = g[idx];
-        if (v) return v == 1 ? dist : rmax;
-    }
-    return rmax;
+        idx += px ? sx : sy;
+        v = g[idx];
+    } while (v == 0);
+    if (v != 1 || dist > rmax) return rmax;
+    const int dy = idx / Wp - start / Wp;  // cells moved in y
+    const int dx = idx - start - dy * Wp;  // cells moved in x
+    return (abs(dx) + abs(dy) > 8192) ? rmax : dist;
 }
 
 // Start cell of a pose (floor of the f32 cell coordinate, as
