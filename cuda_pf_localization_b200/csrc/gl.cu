@@ -75,54 +75,136 @@ __global__ void k_gl_gen(int n, int n_yaw, int nfree, const int2* __restrict__ f
 
 // ------------------------------------------------------------------ raycast
 
-// Copy the padded grid and the scan into shared memory.
-__device__ __forceinline__ void load_smem(unsigned char* s_grid, int grid_bytes,
-                                          const unsigned char* __restrict__ g,
-                                          float* s_scan, const float* scan,
-                                          int nrays) {
-    const int nv = grid_bytes / 16;
-    const uint4* src = reinterpret_cast<const uint4*>(g);
-    uint4* dst = reinterpret_cast<uint4*>(s_grid);
-    for (int k = threadIdx.x; k < nv; k += blockDim.x) dst[k] = __ldg(&src[k]);
+// CAER of one hypothesis by one warp, with rays handed out dynamically: a
+// lane whose ray has ended takes the next unstarted ray of the hypothesis
+// (restarts are batched until kRestart lanes are free), so the warp is not
+// held by its longest ray.  The ray directions are computed first with all
+// lanes busy; each ray's term |scan - raycast| then replaces its direction in
+// the ray's shared-memory slot, and the total is summed in the fixed
+// lane-sequential order
+// (lane l adds rays l, l + 32, ..., then an xor butterfly), which does not
+// depend on the assignment.
+// With kPrune, the sum of the terms finished so far (any order) is compared
+// with `bound` at every restart and -1 is returned once it exceeds it; the
+// caller's bound includes a margin for the rounding difference between that
+// partial order and the final one.
+constexpr int kScoreThreads = 512;
+constexpr int kScoreWarps = kScoreThreads / 32;
+constexpr int kChunk = 8;    // DDA steps between warp votes
+constexpr int kRestart = 8;  // free lanes that trigger a restart round
+
+template <bool kPrune>
+__device__ __forceinline__ float warp_caer(const unsigned char* __restrict__ g,
+                                           const GridView& gv, int Hp, float x,
+                                           float y, float th,
+                                           const float* __restrict__ sc, int nrays,
+                                           float rmax, float span,
+                                           float* __restrict__ term,
+                                           float2* __restrict__ dirs, float bound) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    int start = 0;
+    float frx = 0.f, fry = 0.f;
+    if (!start_cell(gv, x, y, start, frx, fry)) {
+        float acc = 0.f;
+        for (int r = lane; r < nrays; r += 32) acc += fabsf(sc[r] - rmax);
+        return warp_sum_f(acc);
+    }
+    const bool long_rays = gv.Wp + Hp > 8192;
+    // ray directions of this hypothesis, all lanes busy
+    for (int r = lane; r < nrays; r += 32) {
+        float dx, dy;
+        sincosf(ray_angle(th, r, nrays, span), &dy, &dx);
+        dirs[r] = make_float2(dx, dy);
+    }
+    __syncwarp();
+    Ray ray;
+    int r = lane;
+    bool active = r < nrays;
+    ray.v = 1u;
+    if (active) {
+        const float2 d = dirs[r];
+        ray_init(ray, gv.Wp, start, frx, fry, d.x, d.y, gv.res);
+    }
+    float lane_acc = 0.f;
+    int next = 32;
+    for (;;) {
+#pragma unroll
+        for (int k = 0; k < kChunk; ++k)
+            if (ray.v == 0u) ray_step(ray, g);
+        const unsigned done = __ballot_sync(~0u, active && ray.v != 0u);
+        const unsigned moving = __ballot_sync(~0u, active && ray.v == 0u);
+        if (moving != 0u && __popc(done) < kRestart) continue;
+        if (active && ray.v != 0u) {
+            const float t =
+                fabsf(sc[r] - ray_result(ray, gv.Wp, start, rmax, long_rays));
+            term[2 * r] = t;  // the ray's direction slot, no longer needed
+            lane_acc += t;
+            const int nr = next + __popc(done & lt);
+            if (nr < nrays) {
+                r = nr;
+                const float2 d = dirs[r];
+                ray_init(ray, gv.Wp, start, frx, fry, d.x, d.y, gv.res);
+            } else {
+                active = false;
+            }
+        }
+        next += __popc(done);
+        if (kPrune && warp_sum_f(lane_acc) > bound) return -1.0f;
+        if (!__any_sync(~0u, active)) break;
+    }
+    __syncwarp();
+    float acc = 0.f;
+    for (int rr = lane; rr < nrays; rr += 32) acc += term[2 * rr];
+    return warp_sum_f(acc);
+}
+
+// Shared memory of the scorers: [padded grid (kSmem)] [scan] [per-warp ray
+// slots: the direction of each ray, then its CAER term once it has ended].
+template <bool kSmem>
+__device__ __forceinline__ void score_setup(const GridView& gv, int grid_bytes,
+                                            const float* scan, int nrays,
+                                            const unsigned char*& g,
+                                            const float*& sc, float*& term,
+                                            float2*& dirs) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int gbytes = kSmem ? grid_bytes : 0;
+    float* s_scan = reinterpret_cast<float*>(smem + gbytes);
+    if (kSmem) {
+        const int nv = grid_bytes / 16;
+        const uint4* src = reinterpret_cast<const uint4*>(gv.cells);
+        uint4* dst = reinterpret_cast<uint4*>(smem);
+        for (int k = threadIdx.x; k < nv; k += blockDim.x) dst[k] = __ldg(&src[k]);
+    }
     for (int k = threadIdx.x; k < nrays; k += blockDim.x) s_scan[k] = scan[k];
     __syncthreads();
+    g = kSmem ? smem : gv.cells;
+    sc = s_scan;
+    float2* slots = reinterpret_cast<float2*>(s_scan + ((nrays + 1) & ~1));
+    dirs = slots + (size_t)(threadIdx.x >> 5) * nrays;
+    term = reinterpret_cast<float*>(dirs);
 }
 
 // CAER of hypotheses [0, nh): one warp per hypothesis, static striding.
 template <bool kSmem>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kScoreThreads, 3)
     k_gl_score(GridView gv, int grid_bytes, const float* __restrict__ hyp,
                int nh, const float* __restrict__ scan, int nrays, float rmax,
                float span, float* __restrict__ caer) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const unsigned char* g = gv.cells;
-    const float* sc = scan;
-    if (kSmem) {
-        float* s_scan = reinterpret_cast<float*>(smem + grid_bytes);
-        load_smem(smem, grid_bytes, gv.cells, s_scan, scan, nrays);
-        g = smem;
-        sc = s_scan;
-    }
-    const int lane = threadIdx.x & 31;
-    const int gw = blockIdx.x * kWarps + (threadIdx.x >> 5);
-    const int nw = gridDim.x * kWarps;
+    const unsigned char* g;
+    const float* sc;
+    float* term;
+    float2* dirs;
+    score_setup<kSmem>(gv, grid_bytes, scan, nrays, g, sc, term, dirs);
+    const int Hp = gv.H + 2;
+    const int gw = blockIdx.x * kScoreWarps + (threadIdx.x >> 5);
+    const int nw = gridDim.x * kScoreWarps;
     for (int h = gw; h < nh; h += nw) {
-        const float x = hyp[3 * h], y = hyp[3 * h + 1], th = hyp[3 * h + 2];
-        int start = 0;
-        float frx = 0.f, fry = 0.f;
-        const bool inside = start_cell(gv, x, y, start, frx, fry);
-        float acc = 0.f;
-        for (int r = lane; r < nrays; r += 32) {
-            float vm = rmax;
-            if (inside) {
-                float dx, dy;
-                sincosf(ray_angle(th, r, nrays, span), &dy, &dx);
-                vm = cast_ray(g, gv.Wp, start, frx, fry, dx, dy, gv.res, rmax);
-            }
-            acc += fabsf(sc[r] - vm);
-        }
-        acc = warp_sum_f(acc);
-        if (lane == 0) caer[h] = acc;
+        const float c = warp_caer<false>(g, gv, Hp, hyp[3 * h], hyp[3 * h + 1],
+                                         hyp[3 * h + 2], sc, nrays, rmax, span,
+                                         term, dirs, 0.f);
+        if ((threadIdx.x & 31) == 0) caer[h] = c;
+        __syncwarp();
     }
 }
 
@@ -132,70 +214,45 @@ __device__ __forceinline__ float key_to_float(uint64_t key) {
     return __int_as_float(o >= 0 ? o : (o ^ 0x7FFFFFFF));
 }
 
-// Pruned scorer for hypotheses [h0, h1): rays are cast in rounds of 32; after
-// each round the warp's partial CAER (same lane-sequential order as the final
-// sum, so partial <= final) is compared with the bound.  Survivors (final key
-// <= tau) are appended to cand.
+// Pruned scorer for hypotheses [h0, h1).  A hypothesis is dropped once the
+// sum of its finished terms exceeds tau_f (1 + margin): with n non-negative
+// terms, any two summation orders agree to within about 2 n 2^-24 relative,
+// so such a hypothesis ends above tau_f and can never enter the bottom-k.
+// The CAER of every hypothesis that is not dropped is the exhaustive
+// scorer's value; survivors (final key <= tau) are appended to cand.
 template <bool kSmem>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kScoreThreads, 3)
     k_gl_score_pruned(GridView gv, int grid_bytes, const float* __restrict__ hyp,
                       int h0, int h1, const float* __restrict__ scan, int nrays,
                       float rmax, float span, float* __restrict__ caer,
                       uint64_t* __restrict__ cand, GlCtl* ctl, int cand_cap) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const unsigned char* g = gv.cells;
-    const float* sc = scan;
-    if (kSmem) {
-        float* s_scan = reinterpret_cast<float*>(smem + grid_bytes);
-        load_smem(smem, grid_bytes, gv.cells, s_scan, scan, nrays);
-        g = smem;
-        sc = s_scan;
-    }
+    const unsigned char* g;
+    const float* sc;
+    float* term;
+    float2* dirs;
+    score_setup<kSmem>(gv, grid_bytes, scan, nrays, g, sc, term, dirs);
+    const int Hp = gv.H + 2;
     const unsigned long long tau = ctl->tau;
     const float tau_f = key_to_float(tau);
+    const float bound = tau_f * (1.0f + 4.0f * (float)nrays * 5.9604645e-8f + 1e-6f);
     const int lane = threadIdx.x & 31;
-    const int gw = blockIdx.x * kWarps + (threadIdx.x >> 5);
-    const int nw = gridDim.x * kWarps;
+    const int gw = blockIdx.x * kScoreWarps + (threadIdx.x >> 5);
+    const int nw = gridDim.x * kScoreWarps;
     for (int h = h0 + gw; h < h1; h += nw) {
-        const float x = hyp[3 * h], y = hyp[3 * h + 1], th = hyp[3 * h + 2];
-        int start = 0;
-        float frx = 0.f, fry = 0.f;
-        const bool inside = start_cell(gv, x, y, start, frx, fry);
-        float acc = 0.f;
-        bool pruned = false;
-        for (int r0 = 0; r0 < nrays; r0 += 32) {
-            const int r = r0 + lane;
-            if (r < nrays) {
-                float vm = rmax;
-                if (inside) {
-                    float dx, dy;
-                    sincosf(ray_angle(th, r, nrays, span), &dy, &dx);
-                    vm = cast_ray(g, gv.Wp, start, frx, fry, dx, dy, gv.res,
-                                  rmax);
-                }
-                acc += fabsf(sc[r] - vm);
-            }
-            if (r0 + 32 < nrays) {
-                const float part = warp_sum_f(acc);
-                if (part > tau_f) {
-                    pruned = true;
-                    break;
-                }
-            }
-        }
-        if (pruned) {
-            if (lane == 0) caer[h] = -1.0f;  // not scored
-            continue;
-        }
-        const float total = warp_sum_f(acc);
+        const float total = warp_caer<true>(g, gv, Hp, hyp[3 * h], hyp[3 * h + 1],
+                                            hyp[3 * h + 2], sc, nrays, rmax, span,
+                                            term, dirs, bound);
         if (lane == 0) {
-            caer[h] = total;
-            const uint64_t key = composite_key(total, (uint32_t)h);
-            if (key <= tau) {
-                const unsigned slot = atomicAdd(&ctl->n_cand, 1u);
-                if ((int)slot < cand_cap) cand[slot] = key;
+            caer[h] = total;  // -1 when dropped (not scored)
+            if (total >= 0.f) {
+                const uint64_t key = composite_key(total, (uint32_t)h);
+                if (key <= tau) {
+                    const unsigned slot = atomicAdd(&ctl->n_cand, 1u);
+                    if ((int)slot < cand_cap) cand[slot] = key;
+                }
             }
         }
+        __syncwarp();
     }
 }
 
@@ -383,28 +440,45 @@ int score_grid_size(size_t smem) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gl_score<kSmem>,
-                                                  kThreads, smem);
+                                                  kScoreThreads, smem);
     if (per_sm < 1) per_sm = 1;
     return sms * per_sm;
 }
 
+// Dynamic shared memory of a scorer launch; kSmem when the padded grid fits.
+size_t score_smem(const GlHandle* h, int nrays, bool* grid_in_smem) {
+    const size_t rest =
+        sizeof(float) * (size_t)((nrays + 1) & ~1) + sizeof(float2) * (size_t)nrays * kScoreWarps;
+    const size_t with_grid = (size_t)grid_bytes_padded(h) + rest;
+    *grid_in_smem = with_grid <= (size_t)kMaxSmem;
+    return *grid_in_smem ? with_grid : rest;
+}
+
 int launch_score(GlHandle* h, int nrays, float rmax, float span) {
     const int gb = grid_bytes_padded(h);
-    const size_t smem = (size_t)gb + sizeof(float) * (size_t)nrays;
+    bool in_smem = false;
+    const size_t smem = score_smem(h, nrays, &in_smem);
+    if (smem > (size_t)kMaxSmem) {
+        set_error("pf_b200: pfgl_score: %d rays need too much shared memory", nrays);
+        return -1;
+    }
     const GridView gv = grid_view(h);
     const int warps_needed = h->nh;
-    if (smem <= (size_t)kMaxSmem) {
+    if (in_smem) {
         PFB_CK(cudaFuncSetAttribute(k_gl_score<true>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem));
         int grid = score_grid_size<true>(smem);
-        grid = std::min(grid, ceil_div(warps_needed, kWarps));
-        k_gl_score<true><<<grid, kThreads, smem, h->stream>>>(
+        grid = std::min(grid, ceil_div(warps_needed, kScoreWarps));
+        k_gl_score<true><<<grid, kScoreThreads, smem, h->stream>>>(
             gv, gb, h->d_hyp, h->nh, h->d_scan, nrays, rmax, span, h->d_caer);
     } else {
-        int grid = score_grid_size<false>(0);
-        grid = std::min(grid, ceil_div(warps_needed, kWarps));
-        k_gl_score<false><<<grid, kThreads, 0, h->stream>>>(
+        PFB_CK(cudaFuncSetAttribute(k_gl_score<false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+        int grid = score_grid_size<false>(smem);
+        grid = std::min(grid, ceil_div(warps_needed, kScoreWarps));
+        k_gl_score<false><<<grid, kScoreThreads, smem, h->stream>>>(
             gv, gb, h->d_hyp, h->nh, h->d_scan, nrays, rmax, span, h->d_caer);
     }
     PFB_KL();
@@ -414,22 +488,30 @@ int launch_score(GlHandle* h, int nrays, float rmax, float span) {
 int launch_score_pruned(GlHandle* h, int h0, int h1, int nrays, float rmax,
                         float span) {
     const int gb = grid_bytes_padded(h);
-    const size_t smem = (size_t)gb + sizeof(float) * (size_t)nrays;
+    bool in_smem = false;
+    const size_t smem = score_smem(h, nrays, &in_smem);
+    if (smem > (size_t)kMaxSmem) {
+        set_error("pf_b200: pfgl_localize: %d rays need too much shared memory", nrays);
+        return -1;
+    }
     const GridView gv = grid_view(h);
     const int warps_needed = h1 - h0;
-    if (smem <= (size_t)kMaxSmem) {
+    if (in_smem) {
         PFB_CK(cudaFuncSetAttribute(k_gl_score_pruned<true>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem));
         int grid = score_grid_size<true>(smem);
-        grid = std::min(grid, ceil_div(warps_needed, kWarps));
-        k_gl_score_pruned<true><<<grid, kThreads, smem, h->stream>>>(
+        grid = std::min(grid, ceil_div(warps_needed, kScoreWarps));
+        k_gl_score_pruned<true><<<grid, kScoreThreads, smem, h->stream>>>(
             gv, gb, h->d_hyp, h0, h1, h->d_scan, nrays, rmax, span, h->d_caer,
             h->d_cand, h->d_ctl, h->cap_hyp);
     } else {
-        int grid = score_grid_size<false>(0);
-        grid = std::min(grid, ceil_div(warps_needed, kWarps));
-        k_gl_score_pruned<false><<<grid, kThreads, 0, h->stream>>>(
+        PFB_CK(cudaFuncSetAttribute(k_gl_score_pruned<false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+        int grid = score_grid_size<false>(smem);
+        grid = std::min(grid, ceil_div(warps_needed, kScoreWarps));
+        k_gl_score_pruned<false><<<grid, kScoreThreads, smem, h->stream>>>(
             gv, gb, h->d_hyp, h0, h1, h->d_scan, nrays, rmax, span, h->d_caer,
             h->d_cand, h->d_ctl, h->cap_hyp);
     }

@@ -73,34 +73,59 @@ struct GridView {
 // equals "rmax as soon as a step exceeds rmax"; the border ends every ray,
 // and the number of steps taken (one cell in x or y per step) is recovered
 // from the hit cell to apply the step limit.
+struct Ray {
+    float tmx, tmy, tdx, tdy, dist;
+    int sx, sy, idx;
+    unsigned v;  // 0 while the ray is travelling, else the cell value it hit
+};
+
+__device__ __forceinline__ void ray_init(Ray& r, int Wp, int start, float frx,
+                                         float fry, float dirx, float diry,
+                                         float res) {
+    r.sx = dirx > 0 ? 1 : -1;
+    r.sy = diry > 0 ? Wp : -Wp;
+    const float adx = fabsf(dirx), ady = fabsf(diry);
+    r.tdx = adx > 1e-9f ? res / adx : INFINITY;
+    r.tdy = ady > 1e-9f ? res / ady : INFINITY;
+    r.tmx = adx > 1e-9f ? ((dirx > 0 ? 1.f - frx : frx) * r.tdx) : INFINITY;
+    r.tmy = ady > 1e-9f ? ((diry > 0 ? 1.f - fry : fry) * r.tdy) : INFINITY;
+    r.idx = start;
+    r.dist = 0.f;
+    r.v = 0u;
+}
+
+__device__ __forceinline__ void ray_step(Ray& r, const unsigned char* __restrict__ g) {
+    const bool px = r.tmx <= r.tmy;
+    r.dist = px ? r.tmx : r.tmy;
+    if (px)
+        r.tmx += r.tdx;
+    else
+        r.tmy += r.tdy;
+    r.idx += px ? r.sx : r.sy;
+    r.v = g[r.idx];
+}
+
+// Result of an ended ray.  The step limit can only bind when a ray can take
+// more than 8192 steps before reaching the border (Wp + Hp > 8192).
+__device__ __forceinline__ float ray_result(const Ray& r, int Wp, int start,
+                                            float rmax, bool long_rays = true) {
+    if (r.v != 1u || r.dist > rmax) return rmax;
+    if (!long_rays) return r.dist;
+    const int dy = r.idx / Wp - start / Wp;  // cells moved in y
+    const int dx = r.idx - start - dy * Wp;  // cells moved in x
+    return (abs(dx) + abs(dy) > 8192) ? rmax : r.dist;
+}
+
 __device__ __forceinline__ float cast_ray(const unsigned char* __restrict__ g,
                                           int Wp, int start, float frx,
                                           float fry, float dirx, float diry,
                                           float res, float rmax) {
-    const int sx = dirx > 0 ? 1 : -1;
-    const int sy = diry > 0 ? Wp : -Wp;
-    const float adx = fabsf(dirx), ady = fabsf(diry);
-    const float tdx = adx > 1e-9f ? res / adx : INFINITY;
-    const float tdy = ady > 1e-9f ? res / ady : INFINITY;
-    float tmx = adx > 1e-9f ? ((dirx > 0 ? 1.f - frx : frx) * tdx) : INFINITY;
-    float tmy = ady > 1e-9f ? ((diry > 0 ? 1.f - fry : fry) * tdy) : INFINITY;
-    int idx = start;
-    float dist;
-    unsigned v;
+    Ray r;
+    ray_init(r, Wp, start, frx, fry, dirx, diry, res);
     do {
-        const bool px = tmx <= tmy;
-        dist = px ? tmx : tmy;
-        if (px)
-            tmx += tdx;
-        else
-            tmy += tdy;
-        idx += px ? sx : sy;
-        v = g[idx];
-    } while (v == 0);
-    if (v != 1 || dist > rmax) return rmax;
-    const int dy = idx / Wp - start / Wp;  // cells moved in y
-    const int dx = idx - start - dy * Wp;  // cells moved in x
-    return (abs(dx) + abs(dy) > 8192) ? rmax : dist;
+        ray_step(r, g);
+    } while (r.v == 0u);
+    return ray_result(r, Wp, start, rmax);
 }
 
 // Start cell of a pose (floor of the f32 cell coordinate, as
