@@ -701,6 +701,16 @@ def main():
         line["cpu_baseline"] = {"value": n * done / secs, "unit": UNIT,
                                 "cores": int(oracle.lib().orc_threads()), "kind": "port",
                                 "sample": f"{done} cycles at N={n} (time-bounded)"}
+        # the same workload at the other particle counts of the at-scale config
+        sizes = {}
+        for n_other in (100_000, 4_000_000):
+            a2 = argparse.Namespace(**vars(args))
+            a2.particles, a2.steps = n_other, min(args.steps, 200)
+            v2 = run_value(a2, sc, torch, dev)
+            t2 = float(v2["step_ms"].sum()) / 1e3
+            sizes[str(n_other)] = {"value": n_other * a2.steps / t2, "unit": UNIT,
+                                   "ms_per_step": 1e3 * t2 / a2.steps, "steps": a2.steps}
+        line["other_sizes"] = sizes
         line["batched"] = run_batched(args, torch, dev)
         line["batched"]["config"] = ("512 filters, N log-uniform in [1k, 200k], 8-64 landmarks "
                                      "in 20x20x5 m each, own helix, 4-64 obs per cycle, "
