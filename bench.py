@@ -69,7 +69,9 @@ def parse():
     ap.add_argument("--gl-maps", type=int, default=16)
     ap.add_argument("--gl-queries", type=int, default=1000)
     ap.add_argument("--gl-pairs", type=int, default=2_000_000)
-    ap.add_argument("--gl-train-steps", type=int, default=3000)
+    ap.add_argument("--gl-train-steps", type=int, default=1200)
+    ap.add_argument("--gl-batch", type=int, default=8192)
+    ap.add_argument("--gl-lr", type=float, default=2e-3)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     return ap.parse_args()
 
@@ -421,11 +423,11 @@ def run_gl(args):
         h = lib.pfgl_create(200, 200, 0.05, 0.0, 0.0, pkg.u8ptr(g), max(args.gl_hyps, 200_000))
         lp = None
         try:
-            lp = pkg.LearnedProposal(h, batch=2048, seed=gseed)
+            lp = pkg.LearnedProposal(h, batch=args.gl_batch, seed=gseed)
             t0 = time.perf_counter()
             lp.make_data(args.gl_pairs, seed=gseed + 1)
             t1 = time.perf_counter()
-            loss = lp.train(args.gl_train_steps, lr=1e-3)
+            loss = lp.train(args.gl_train_steps, lr=args.gl_lr)
             t2 = time.perf_counter()
             t_train += t2 - t0
             t_steps += t2 - t1
@@ -467,7 +469,8 @@ def run_gl(args):
         train_pairs_per_map=args.gl_pairs, train_steps_per_map=args.gl_train_steps,
         train_seconds_per_map=t_train / args.gl_maps, final_loss_mean=float(np.mean(losses)),
         train_step_ms=1e3 * t_steps / (args.gl_maps * args.gl_train_steps),
-        train_tflops=LP_FLOPS_PER_SAMPLE * 2048 * args.gl_train_steps * args.gl_maps
+        train_batch=args.gl_batch,
+        train_tflops=LP_FLOPS_PER_SAMPLE * args.gl_batch * args.gl_train_steps * args.gl_maps
         / t_steps / 1e12,
         tau_mean=float(np.mean(taus)))
     res["uniform_same_maps"] = dict(hyps=args.gl_hyps, queries=uni_q,

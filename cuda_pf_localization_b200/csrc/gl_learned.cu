@@ -64,9 +64,22 @@ constexpr int layer_in(int l) { return l == 0 ? kIn : kHid; }
 constexpr int layer_out(int l) { return l == kLayers - 1 ? kOut : kHid; }
 
 // ------------------------------------------------------------------ GEMM
-constexpr int BM = 128, BN = 128, BK = 64, kStages = 4;
-constexpr int kTileBytes = BM * BK * 2;  // 16 KiB per operand tile
-constexpr int kGemmSmem = kStages * 2 * kTileBytes + 1024 + 256;
+constexpr int BM = 128, BK = 64;
+// Output tile 128 x BN (BN = 128 or 256; the widest tcgen05 shape of one CTA
+// is 128 x 256).  Per k-block of 64 a 128 x 256 tile moves 48 KiB of
+// operands for 4.2 MFLOP, against 32 KiB for 2.1 MFLOP at 128 x 128: the
+// wider tile needs 30 % fewer operand bytes per flop from L2.
+// Pipeline depth is sized so that two CTAs fit on an SM (96 KiB of operand
+// ring each, 2 x BN <= 512 TMEM columns): one CTA's epilogue then overlaps
+// the other's MMAs.
+template <int BN>
+struct Tile {
+    static constexpr int kStages = BN == 256 ? 2 : 3;
+    static constexpr int kABytes = BM * BK * 2;  // 16 KiB
+    static constexpr int kBBytes = BN * BK * 2;  // 16 or 32 KiB
+    static constexpr int kSmem =
+        kStages * (kABytes + kBBytes) + 1024 + 256 + BN * 4;  // + bias slice
+};
 constexpr uint32_t kWaitLimit = 1u << 24;
 
 enum Epi : int {
@@ -94,13 +107,14 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
 // Epilogue of 32 consecutive columns [col0, col0 + 32) of one output row.
 template <int EPI>
 __device__ __forceinline__ void epilogue_chunk(const uint32_t (&r)[32], int row,
-                                               int col0, const EpiArgs& ep) {
+                                               int col0, const float* bias,
+                                               const EpiArgs& ep) {
     float v[32];
 #pragma unroll
     for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
     if (EPI == EPI_RELU_BF16 || EPI == EPI_BIAS_F32) {
 #pragma unroll
-        for (int j = 0; j < 32; ++j) v[j] += __ldg(&ep.bias[col0 + j]);
+        for (int j = 0; j < 32; ++j) v[j] += bias[j];  // shared memory
     }
     if (EPI == EPI_RELU_BF16) {
 #pragma unroll
@@ -157,23 +171,28 @@ __device__ __forceinline__ void epilogue_chunk(const uint32_t (&r)[32], int row,
 
 // D[M][N] = A[M][K] . B[N][K]^T for one 128 x 128 tile per CTA.  Operand
 // tiles are read through tensor maps at (k0 + k, row0 + tile row).
-template <int EPI>
-__global__ void __launch_bounds__(128, 1)
+template <int EPI, int BN>
+__global__ void __launch_bounds__(128, 2)
     k_gemm_bf16(const __grid_constant__ CUtensorMap tmA,
                 const __grid_constant__ CUtensorMap tmB, int K, int a_row0,
                 int a_k0, int b_row0, int b_k0, EpiArgs ep,
                 unsigned* __restrict__ err) {
     // Split-K: blockIdx.z takes k-blocks [kb0, kb1) and writes its partial
     // product ep.split_stride elements after the previous split's.
+    constexpr int kStages = Tile<BN>::kStages;
+    constexpr int kABytes = Tile<BN>::kABytes, kBBytes = Tile<BN>::kBBytes;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     const uint32_t s0 = smem_u32(smem_raw);
     unsigned char* base = smem_raw + ((1024u - (s0 & 1023u)) & 1023u);
     unsigned char* sA = base;
-    unsigned char* sB = base + kStages * kTileBytes;
-    uint64_t* full = reinterpret_cast<uint64_t*>(base + 2 * kStages * kTileBytes);
+    unsigned char* sB = base + kStages * kABytes;
+    uint64_t* full =
+        reinterpret_cast<uint64_t*>(base + kStages * (kABytes + kBBytes));
     uint64_t* empty = full + kStages;
     uint64_t* accb = empty + kStages;
     uint32_t* tslot = reinterpret_cast<uint32_t*>(accb + 1);
+    float* s_bias = reinterpret_cast<float*>(
+        base + kStages * (kABytes + kBBytes) + 256);  // BN floats
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
@@ -197,6 +216,8 @@ __global__ void __launch_bounds__(128, 1)
         tmem_alloc(tslot, BN);
         tmem_relinquish();
     }
+    if (EPI == EPI_RELU_BF16 || EPI == EPI_BIAS_F32)
+        for (int j = threadIdx.x; j < BN; j += 128) s_bias[j] = ep.bias[n0 + j];
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -212,10 +233,10 @@ __global__ void __launch_bounds__(128, 1)
                     fail = true;
                     break;
                 }
-                mbar_expect_tx(&full[s], 2 * kTileBytes);
-                tma_load_2d(sA + s * kTileBytes, &tmA, &full[s],
+                mbar_expect_tx(&full[s], kABytes + kBBytes);
+                tma_load_2d(sA + s * kABytes, &tmA, &full[s],
                             a_k0 + (kb0 + kb) * BK, a_row0 + m0);
-                tma_load_2d(sB + s * kTileBytes, &tmB, &full[s],
+                tma_load_2d(sB + s * kBBytes, &tmB, &full[s],
                             b_k0 + (kb0 + kb) * BK, b_row0 + n0);
             }
         }
@@ -230,8 +251,8 @@ __global__ void __launch_bounds__(128, 1)
                     break;
                 }
                 tc_fence_after();
-                const uint64_t ad = desc_kmajor_sw128(smem_u32(sA + s * kTileBytes));
-                const uint64_t bd = desc_kmajor_sw128(smem_u32(sB + s * kTileBytes));
+                const uint64_t ad = desc_kmajor_sw128(smem_u32(sA + s * kABytes));
+                const uint64_t bd = desc_kmajor_sw128(smem_u32(sB + s * kBBytes));
 #pragma unroll
                 for (int k = 0; k < BK / 16; ++k)
                     mma_bf16(tmem, ad + 2 * k, bd + 2 * k, idesc,
@@ -259,7 +280,7 @@ __global__ void __launch_bounds__(128, 1)
             uint32_t r[32];
             tmem_ld32(trow + (uint32_t)(c * 32), r);
             tmem_wait_ld();
-            epilogue_chunk<EPI>(r, row, n0 + c * 32, ep);
+            epilogue_chunk<EPI>(r, row, n0 + c * 32, s_bias + c * 32, ep);
         }
     }
     tc_fence_before();
@@ -289,9 +310,10 @@ EncodeTiledFn encode_fn() {
     return fn;
 }
 
-// Tensor map of a row-major rows x cols bf16 matrix with 128 x 64 boxes and
-// the 128-byte swizzle.
-int make_map(CUtensorMap* m, const void* ptr, long long rows, long long cols) {
+// Tensor map of a row-major rows x cols bf16 matrix with box_rows x 64 boxes
+// and the 128-byte swizzle.
+int make_map(CUtensorMap* m, const void* ptr, long long rows, long long cols,
+             int box_rows) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) {
         set_error("pf_b200: cuTensorMapEncodeTiled is unavailable");
@@ -303,7 +325,7 @@ int make_map(CUtensorMap* m, const void* ptr, long long rows, long long cols) {
     }
     const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
     const cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
-    const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)BM};
+    const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
     const cuuint32_t es[2] = {1, 1};
     const CUresult r =
         fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims,
@@ -317,30 +339,56 @@ int make_map(CUtensorMap* m, const void* ptr, long long rows, long long cols) {
     return 0;
 }
 
+// A bf16 matrix as a GEMM operand: tensor maps with 128-row and (when the
+// matrix has at least 256 rows) 256-row boxes.
+struct Mat {
+    CUtensorMap m128, m256;
+    bool has256 = false;
+};
+
+int make_mat(Mat* m, const void* ptr, long long rows, long long cols) {
+    if (make_map(&m->m128, ptr, rows, cols, 128)) return -1;
+    m->has256 = rows >= 256;
+    if (m->has256 && make_map(&m->m256, ptr, rows, cols, 256)) return -1;
+    return 0;
+}
+
 struct MapRef {
-    const CUtensorMap* map;
+    const Mat* map;
     int row0;
     int k0;
 };
 
+template <int EPI, int BN>
+int gemm_bn(cudaStream_t s, MapRef a, MapRef b, int M, int N, int K,
+            const EpiArgs& ep, unsigned* err, int splits) {
+    constexpr int smem = Tile<BN>::kSmem;
+    PFB_CK(cudaFuncSetAttribute(k_gemm_bf16<EPI, BN>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const dim3 grid(N / BN, M / BM, splits);
+    const CUtensorMap& tb = BN == 256 ? b.map->m256 : b.map->m128;
+    k_gemm_bf16<EPI, BN><<<grid, 128, smem, s>>>(a.map->m128, tb, K, a.row0, a.k0,
+                                                 b.row0, b.k0, ep, err);
+    PFB_KL();
+    return 0;
+}
+
+// D = A B^T.  The 128 x 256 tile is used when N allows it and it still gives
+// at least one CTA per SM; otherwise 128 x 128.
 template <int EPI>
 int gemm(cudaStream_t s, MapRef a, MapRef b, int M, int N, int K,
          const EpiArgs& ep, unsigned* err, int splits = 1) {
-    if (M <= 0 || N <= 0 || K <= 0 || M % BM || N % BN || K % BK ||
+    if (M <= 0 || N <= 0 || K <= 0 || M % BM || N % 128 || K % BK ||
         (a.k0 % 8) || (b.k0 % 8) || splits < 1 || splits > K / BK ||
         (splits > 1 && EPI != EPI_F32)) {
         set_error("pf_b200: gemm shape %d x %d x %d (split %d) not tileable", M, N,
                   K, splits);
         return -1;
     }
-    PFB_CK(cudaFuncSetAttribute(k_gemm_bf16<EPI>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                kGemmSmem));
-    const dim3 grid(N / BN, M / BM, splits);
-    k_gemm_bf16<EPI><<<grid, 128, kGemmSmem, s>>>(*a.map, *b.map, K, a.row0,
-                                                  a.k0, b.row0, b.k0, ep, err);
-    PFB_KL();
-    return 0;
+    const bool wide = N % 256 == 0 && b.map->has256 &&
+                      (long long)(M / BM) * (N / 256) * splits >= 148;
+    return wide ? gemm_bn<EPI, 256>(s, a, b, M, N, K, ep, err, splits)
+                : gemm_bn<EPI, 128>(s, a, b, M, N, K, ep, err, splits);
 }
 
 // ------------------------------------------------------- elementwise kernels
@@ -718,7 +766,7 @@ struct Layer {
     float* gb = nullptr;
     bf16* wb = nullptr;   // [out][in]
     bf16* wtb = nullptr;  // [in][out]
-    CUtensorMap tm_w, tm_wt;
+    Mat tm_w, tm_wt;
 };
 
 struct LpHandle {
@@ -732,14 +780,13 @@ struct LpHandle {
     bf16* dZ[kLayers] = {};
     bf16* dZT[kLayers] = {};
     float* Z4 = nullptr;
-    CUtensorMap tm_H[kLayers - 1], tm_HT[kLayers - 1], tm_dZ[kLayers],
-        tm_dZT[kLayers];
+    Mat tm_H[kLayers - 1], tm_HT[kLayers - 1], tm_dZ[kLayers], tm_dZT[kLayers];
     // training pairs
     bf16* X = nullptr;
     bf16* XT = nullptr;
     float* Y = nullptr;
     long long n_pairs = 0;
-    CUtensorMap tm_X, tm_XT;
+    Mat tm_X, tm_XT;
     int data_nrays = 360;
     float data_rmax = 10.0f;
     // caller inputs (gradient check, forward, queries): batch rows
@@ -747,7 +794,7 @@ struct LpHandle {
     bf16* XpT = nullptr;
     float* Xp_f = nullptr;
     float* Yp = nullptr;
-    CUtensorMap tm_Xp, tm_XpT;
+    Mat tm_Xp, tm_XpT;
     // bookkeeping
     unsigned* d_err = nullptr;
     float* d_loss = nullptr;
@@ -1007,12 +1054,16 @@ void* pfgl_learned_create(void* glv, int batch, unsigned long long seed) {
             L.in = layer_in(l);
             L.out = layer_out(l);
             const size_t nw = (size_t)L.in * L.out;
-            // split-K for the narrow weight gradients (384 x 1024 and
-            // 1024 x 384: 24 output tiles); the 1024 x 1024 ones already
-            // have 64 tiles and would pay more in partial traffic than they
-            // gain in parallelism
-            const int tiles = (L.out / BM) * (L.in / BN);
-            L.splits = tiles < 64 ? std::max(1, std::min(batch / BK, 4)) : 1;
+            // split-K for the weight gradients, whose output has only
+            // (out/128) x (in/128) tiles (24 or 64) while K is the batch:
+            // enough splits to fill the SMs once the batch is long enough
+            // for the partial products' extra traffic to pay
+            const int tiles = (L.out / BM) * (L.in / 128);
+            if (tiles < 64)
+                L.splits = batch >= 4096 ? 6 : 4;
+            else
+                L.splits = batch >= 4096 ? 2 : 1;
+            L.splits = std::max(1, std::min(batch / BK, L.splits));
             bad = dalloc(&L.w, nw) || dalloc(&L.b, L.out) || dalloc(&L.mw, nw) ||
                   dalloc(&L.vw, nw) || dalloc(&L.mb, L.out) ||
                   dalloc(&L.vb, L.out) || dalloc(&L.gw, nw * L.splits) ||
@@ -1020,17 +1071,17 @@ void* pfgl_learned_create(void* glv, int batch, unsigned long long seed) {
                   dalloc(&h->dZ[l], (size_t)batch * L.out) ||
                   dalloc(&h->dZT[l], (size_t)batch * L.out);
             if (bad) break;
-            bad = make_map(&L.tm_w, L.wb, L.out, L.in) ||
-                  make_map(&L.tm_wt, L.wtb, L.in, L.out) ||
-                  make_map(&h->tm_dZ[l], h->dZ[l], batch, L.out) ||
-                  make_map(&h->tm_dZT[l], h->dZT[l], L.out, batch);
+            bad = make_mat(&L.tm_w, L.wb, L.out, L.in) ||
+                  make_mat(&L.tm_wt, L.wtb, L.in, L.out) ||
+                  make_mat(&h->tm_dZ[l], h->dZ[l], batch, L.out) ||
+                  make_mat(&h->tm_dZT[l], h->dZT[l], L.out, batch);
         }
         if (bad) break;
         for (int l = 0; l < kLayers - 1 && !bad; ++l) {
             bad = dalloc(&h->H[l], (size_t)batch * kHid) ||
                   dalloc(&h->HT[l], (size_t)batch * kHid) ||
-                  make_map(&h->tm_H[l], h->H[l], batch, kHid) ||
-                  make_map(&h->tm_HT[l], h->HT[l], kHid, batch);
+                  make_mat(&h->tm_H[l], h->H[l], batch, kHid) ||
+                  make_mat(&h->tm_HT[l], h->HT[l], kHid, batch);
         }
         if (bad) break;
         if (dalloc(&h->Z4, (size_t)batch * kOut) ||
@@ -1040,8 +1091,8 @@ void* pfgl_learned_create(void* glv, int batch, unsigned long long seed) {
             dalloc(&h->Yp, (size_t)batch * 4) || dalloc(&h->d_err, 1) ||
             dalloc(&h->d_best, 64))
             break;
-        if (make_map(&h->tm_Xp, h->Xp, batch, kIn) ||
-            make_map(&h->tm_XpT, h->XpT, kIn, batch))
+        if (make_mat(&h->tm_Xp, h->Xp, batch, kIn) ||
+            make_mat(&h->tm_XpT, h->XpT, kIn, batch))
             break;
         if (cudaMemsetAsync(h->Xp, 0, sizeof(bf16) * (size_t)batch * kIn,
                             h->stream) != cudaSuccess ||
@@ -1222,8 +1273,8 @@ int pfgl_learned_make_data(void* p, long long n_pairs, int nrays, float rmax,
                                         n_pairs, rows, kIn);
     }
     PFB_KL();
-    if (make_map(&h->tm_X, h->X, n_pairs, kIn) ||
-        make_map(&h->tm_XT, h->XT, kIn, n_pairs))
+    if (make_mat(&h->tm_X, h->X, n_pairs, kIn) ||
+        make_mat(&h->tm_XT, h->XT, kIn, n_pairs))
         return -1;
     PFB_CK(cudaStreamSynchronize(h->stream));
     h->n_pairs = n_pairs;
@@ -1446,7 +1497,7 @@ int pfgl_learned_calibrate(void* p, int n_queries, int nrays, float rmax,
 int pfgl_learned_gemm(int M, int N, int K, const unsigned short* A,
                       const unsigned short* B, float* D) {
     clear_error();
-    if (!A || !B || !D || M <= 0 || N <= 0 || K <= 0 || M % BM || N % BN || K % BK)
+    if (!A || !B || !D || M <= 0 || N <= 0 || K <= 0 || M % BM || N % 128 || K % BK)
         return -1;
     bf16* dA = nullptr;
     bf16* dB = nullptr;
@@ -1467,8 +1518,8 @@ int pfgl_learned_gemm(int M, int N, int K, const unsigned short* A,
                             s) != cudaSuccess ||
             cudaMemsetAsync(dErr, 0, sizeof(unsigned), s) != cudaSuccess)
             break;
-        CUtensorMap ta, tb;
-        if (make_map(&ta, dA, M, K) || make_map(&tb, dB, N, K)) break;
+        Mat ta, tb;
+        if (make_mat(&ta, dA, M, K) || make_mat(&tb, dB, N, K)) break;
         EpiArgs ep{};
         ep.out = dD;
         ep.ldo = N;

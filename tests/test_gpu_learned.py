@@ -24,8 +24,11 @@ def _bits_to_f32(b: np.ndarray) -> np.ndarray:
     return (b.astype(np.uint32) << 16).view(np.float32)
 
 
+# the last two shapes give at least 148 tiles of 128 x 256 and so run the
+# wide-tile kernel; the others the 128 x 128 one
 @pytest.mark.parametrize("M_, N_, K_", [(128, 128, 64), (256, 384, 320), (512, 1024, 1024),
-                                         (1024, 384, 2048)])
+                                         (1024, 384, 2048), (8192, 1024, 128),
+                                         (9472, 512, 64)])
 def test_gemm_matches_torch_fp32(kernels, M_, N_, K_):
     rng = np.random.default_rng(M_ + N_ + K_)
     a = _bf16_bits(rng.normal(0, 1, (M_, K_)))
