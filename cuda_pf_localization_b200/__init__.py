@@ -133,6 +133,7 @@ _KERNEL_SIGS = {
     "pfc_cycle_device": (c_int, [c_void_p, POINTER(PfcOdom), c_void_p, c_int,
                                  POINTER(PfcCycleParams), _dp]),
     "pfc_cycle_result": (c_int, [c_void_p, _dp]),
+    "pfc_set_graph": (c_int, [c_void_p, c_int]),
     "pfc_stream": (c_void_p, [c_void_p]),
     "pfc_size": (c_int, [c_void_p]),
     "pfc_get_weights": (c_int, [c_void_p, _fp]),

@@ -126,7 +126,15 @@ __global__ void k_unpack(PlaneSet ps, int n, const float* pos3,
 
 PfHandle* as_pf(void* h) { return static_cast<PfHandle*>(h); }
 
+void drop_cycle_graph(PfHandle* h) {
+    if (h->cyc_exec) cudaGraphExecDestroy(h->cyc_exec);
+    if (h->cyc_graph) cudaGraphDestroy(h->cyc_graph);
+    h->cyc_exec = nullptr;
+    h->cyc_graph = nullptr;
+}
+
 void free_particles(PfHandle* h) {
+    drop_cycle_graph(h);
     cudaFree(h->d_state[0]);
     cudaFree(h->d_state[1]);
     cudaFree(h->d_ll);
@@ -240,10 +248,98 @@ int ensure_stage(PfHandle* h) {
 
 bool valid_handle(PfHandle* h) { return h != nullptr && h->n > 0; }
 
+// Everything a captured cycle depends on besides the per-cycle values.
+void cycle_graph_key(const PfHandle* h, const PfcCycleParams* prm, long long k[12]) {
+    auto f2l = [](float v) { long long r = 0; memcpy(&r, &v, sizeof v); return r; };
+    long long e = 0;
+    memcpy(&e, &prm->resample_ess_ratio, sizeof e);
+    k[0] = h->n;
+    k[1] = (long long)(uintptr_t)h->d_state[0];
+    k[2] = (long long)(uintptr_t)h->d_lm;
+    k[3] = h->lm_count;
+    k[4] = f2l(prm->sigma_r);
+    k[5] = f2l(prm->sigma_b);
+    k[6] = f2l(prm->gate);
+    k[7] = e;
+    k[8] = f2l(prm->random_inject_ratio);
+    k[9] = h->weight_variant;
+    k[10] = h->record_anc ? 1 : 0;
+    k[11] = 1;
+}
+
+int enqueue_cycle(PfHandle* h, const PredictArgs& pa, const CObservation* obs_dev,
+                  int nobs, const PfcCycleParams* prm, const CycleArgs* dargs);
+
+// A fused cycle replayed from a CUDA graph (same kernels and arguments as the
+// direct launches; the per-cycle values come from d_cargs).  Used when there
+// are observations and per-kernel profiling is off.
+int run_cycle_graph(PfHandle* h, const PfcOdom* odom, const CObservation* obs_dev,
+                    int nobs, const PfcCycleParams* prm) {
+    h->gen++;
+    const int slot = h->cargs_pos;
+    h->cargs_pos = (h->cargs_pos + 1) % PfHandle::kRing;
+    PFB_CK(cudaEventSynchronize(h->cargs_ev[slot]));
+    CycleArgs& a = h->h_cargs[slot];
+    memset(&a, 0, sizeof a);
+    a.pa.enabled = 1;
+    a.pa.gen = h->gen;
+    for (int k = 0; k < 3; ++k) {
+        a.pa.t[k] = odom->t[k];
+        a.pa.tstd[k] = odom->tstd[k];
+        a.pa.rstd[k] = odom->rstd[k];
+    }
+    for (int k = 0; k < 4; ++k) a.pa.q[k] = odom->q[k];
+    a.obs = obs_dev;
+    a.nobs = nobs;
+    a.gen = h->gen;
+    a.scan_epoch = next_scan_epoch(h);
+    const int kinj = (prm->random_inject_ratio > 0.f)
+                         ? (int)(prm->random_inject_ratio * (float)h->n)
+                         : 0;
+    a.inj_epoch = kinj > 0 ? next_inj_epoch(h) : h->inj_epoch;
+    PFB_CK(cudaMemcpyAsync(h->d_cargs, &a, sizeof(CycleArgs), cudaMemcpyHostToDevice,
+                           h->stream));
+    PFB_CK(cudaEventRecord(h->cargs_ev[slot], h->stream));
+    h->stats.h2d_bytes += sizeof(CycleArgs);
+    long long key[12];
+    cycle_graph_key(h, prm, key);
+    if (h->cyc_exec && memcmp(key, h->graph_key, sizeof key) != 0) drop_cycle_graph(h);
+    if (!h->cyc_exec) {
+        const long long l0 = h->stats.launches;
+        const size_t d0 = h->stats.d2h_bytes;
+        PFB_CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = enqueue_cycle(h, a.pa, obs_dev, nobs, prm, h->d_cargs);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+        h->graph_kernels = (int)(h->stats.launches - l0);
+        h->stats.launches = l0;
+        h->stats.d2h_bytes = d0;
+        if (rc || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            set_error("pf_b200: cycle graph capture failed: %s", cudaGetErrorString(e));
+            return -1;
+        }
+        h->cyc_graph = g;
+        PFB_CK(cudaGraphInstantiate(&h->cyc_exec, g, 0));
+        memcpy(h->graph_key, key, sizeof key);
+    }
+    PFB_CK(cudaGraphLaunch(h->cyc_exec, h->stream));
+    PFB_CK(cudaEventRecord(h->est_ev, h->stream));
+    h->stats.launches += h->graph_kernels;
+    h->stats.d2h_bytes += sizeof(CycleCtl);
+    h->total_valid = false;
+    h->anc_valid = h->record_anc;
+    h->est_inflight = true;
+    h->est_valid = false;
+    return 0;
+}
+
 // One fused cycle; obs_dev points at device-resident observations.
 int run_cycle(PfHandle* h, const PfcOdom* odom, const CObservation* obs_dev,
               int nobs, const PfcCycleParams* prm) {
     if (flush_predict(h)) return -1;
+    if (h->use_graph && nobs > 0 && !h->prof.on && h->d_cargs)
+        return run_cycle_graph(h, odom, obs_dev, nobs, prm);
     h->gen++;
     PredictArgs pa{};
     pa.enabled = 1;
@@ -254,26 +350,37 @@ int run_cycle(PfHandle* h, const PfcOdom* odom, const CObservation* obs_dev,
         pa.rstd[k] = odom->rstd[k];
     }
     for (int k = 0; k < 4; ++k) pa.q[k] = odom->q[k];
-    if (nobs > 0) {
-        if (launch_weight(h, pa, obs_dev, nobs, prm->sigma_r, prm->sigma_b,
-                          prm->gate))
-            return -1;
-    } else {
+    if (nobs <= 0) {
         if (launch_predict(h, pa)) return -1;
         if (set_wmode(h, WMODE_UNIFORM)) return -1;
     }
+    if (enqueue_cycle(h, pa, obs_dev, nobs, prm, nullptr)) return -1;
+    h->est_inflight = true;
+    h->est_valid = false;
+    return 0;
+}
+
+// The kernels of a cycle after the predict / weighting decision, then the copy
+// of the control block.  With dargs (graph capture) the weighting pass runs
+// and reads its per-cycle values from dargs.
+int enqueue_cycle(PfHandle* h, const PredictArgs& pa, const CObservation* obs_dev,
+                  int nobs, const PfcCycleParams* prm, const CycleArgs* dargs) {
+    if (nobs > 0 &&
+        launch_weight(h, pa, obs_dev, nobs, prm->sigma_r, prm->sigma_b, prm->gate,
+                      dargs))
+        return -1;
     if (launch_est_sums(h, false)) return -1;
     if (launch_cycle_decide(h, prm->resample_ess_ratio)) return -1;
-    if (launch_resample(h, prm->random_inject_ratio, true, false, 0.0))
+    if (launch_resample(h, prm->random_inject_ratio, true, false, 0.0, dargs))
         return -1;
     if (launch_est_sums(h, true)) return -1;
     if (launch_covs(h, false, nullptr, nullptr, true)) return -1;
     PFB_CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(CycleCtl),
                            cudaMemcpyDeviceToHost, h->stream));
     h->stats.d2h_bytes += sizeof(CycleCtl);
-    PFB_CK(cudaEventRecord(h->est_ev, h->stream));
-    h->est_inflight = true;
-    h->est_valid = false;
+    // an event recorded inside a capture cannot be waited on afterwards: the
+    // graph path records it after the launch
+    if (!dargs) PFB_CK(cudaEventRecord(h->est_ev, h->stream));
     return 0;
 }
 
@@ -340,6 +447,15 @@ void* pfc_create(int cap_obs) {
         if (cudaEventCreateWithFlags(&h->est_ev, cudaEventDisableTiming) !=
             cudaSuccess)
             break;
+        if (cudaMalloc((void**)&h->d_cargs, sizeof(CycleArgs)) != cudaSuccess ||
+            cudaMallocHost((void**)&h->h_cargs,
+                           PfHandle::kRing * sizeof(CycleArgs)) != cudaSuccess)
+            break;
+        for (int k = 0; k < PfHandle::kRing; ++k)
+            ev_ok = ev_ok && cudaEventCreateWithFlags(&h->cargs_ev[k],
+                                                      cudaEventDisableTiming) ==
+                                 cudaSuccess;
+        if (!ev_ok) break;
         k_ctl_reset<<<1, 1, 0, h->stream>>>(h->d_ctl, 1);
         if (cudaGetLastError() != cudaSuccess) break;
         if (cudaStreamSynchronize(h->stream) != cudaSuccess) break;
@@ -365,8 +481,12 @@ int pfc_destroy(void* hv) {
     cudaFree(h->d_obs);
     cudaFreeHost(h->h_obs_ring);
     cudaFree(h->d_lm);
-    for (int k = 0; k < PfHandle::kRing; ++k)
+    cudaFree(h->d_cargs);
+    cudaFreeHost(h->h_cargs);
+    for (int k = 0; k < PfHandle::kRing; ++k) {
         if (h->ring_ev[k]) cudaEventDestroy(h->ring_ev[k]);
+        if (h->cargs_ev[k]) cudaEventDestroy(h->cargs_ev[k]);
+    }
     if (h->est_ev) cudaEventDestroy(h->est_ev);
     for (int k = 0; k < PfProfiler::kPool; ++k)
         for (int e = 0; e < 2; ++e)
@@ -613,6 +733,14 @@ int pfc_cycle_device(void* hv, const PfcOdom* odom, const void* d_obs, int nobs,
         return -1;
     if (!est_out) return 0;
     return finish_cycle(h, est_out);
+}
+
+int pfc_set_graph(void* hv, int on) {
+    PfHandle* h = as_pf(hv);
+    if (!h) return -1;
+    h->use_graph = on != 0;
+    if (!h->use_graph) drop_cycle_graph(h);
+    return 0;
 }
 
 int pfc_cycle_result(void* hv, double* est_out) {

@@ -24,6 +24,7 @@ void clear_error();
         if (e_ != cudaSuccess) {                                            \
             ::pfb::set_error("pf_b200 %s:%d %s: %s", __FILE__, __LINE__, #x, \
                              cudaGetErrorString(e_));                       \
+            (void)cudaGetLastError(); /* do not leak into later checks */   \
             return -1;                                                      \
         }                                                                   \
     } while (0)
@@ -34,6 +35,7 @@ void clear_error();
         if (e_ != cudaSuccess) {                                            \
             ::pfb::set_error("pf_b200 %s:%d %s: %s", __FILE__, __LINE__, #x, \
                              cudaGetErrorString(e_));                       \
+            (void)cudaGetLastError(); /* do not leak into later checks */   \
             return nullptr;                                                 \
         }                                                                   \
     } while (0)

@@ -153,6 +153,8 @@ struct PfProfiler {
     long long count[KK_COUNT] = {};
 };
 
+struct CycleArgs;
+
 struct PfHandle {
     int dev = 0;
     cudaStream_t stream = nullptr;
@@ -212,6 +214,18 @@ struct PfHandle {
     unsigned inj_epoch = 0;    // injection list epoch (never 0 when used)
     float* d_stage = nullptr;  // AoS staging for snapshot / set_state (7n)
 
+    // fused cycle as a CUDA graph: per-cycle values staged through a pinned
+    // ring into d_cargs; the graph is re-captured when its key changes
+    CycleArgs* d_cargs = nullptr;
+    CycleArgs* h_cargs = nullptr;  // kRing slots
+    cudaEvent_t cargs_ev[kRing] = {};
+    int cargs_pos = 0;
+    bool use_graph = true;
+    cudaGraph_t cyc_graph = nullptr;
+    cudaGraphExec_t cyc_exec = nullptr;
+    long long graph_key[12] = {};
+    int graph_kernels = 0;
+
     // accounting: kernels launched, bytes copied host<->device, host syncs
     PfcStats stats{};
     PfProfiler prof;
@@ -249,6 +263,18 @@ struct PredictArgs {
     float t[3], q[4], tstd[3], rstd[3];
 };
 
+// Per-cycle values of a fused cycle replayed as a CUDA graph: the kernels of
+// the captured cycle read them from device memory (the values passed as
+// kernel arguments at capture time are ignored when this pointer is set).
+struct CycleArgs {
+    PredictArgs pa;
+    const CObservation* obs;
+    int nobs;
+    unsigned scan_epoch;
+    unsigned inj_epoch;
+    unsigned long long gen;
+};
+
 struct WeightArgs {
     float sigma_r, sigma_b, gate;
     int nobs;
@@ -263,7 +289,8 @@ int launch_predict(PfHandle* h, const PredictArgs& pa);
 // Weighting (optionally fused with a deferred predict): writes ll, block
 // (max, sumexp) partials and the finalised M, S into the control block.
 int launch_weight(PfHandle* h, const PredictArgs& pa, const CObservation* d_obs,
-                  int nobs, float sigma_r, float sigma_b, float gate);
+                  int nobs, float sigma_r, float sigma_b, float gate,
+                  const CycleArgs* dargs = nullptr);
 // Estimate pass 1 (+ device Markley mean) and the speculative covariance pass
 // around (float)mean, (float)qmean.  When use_args is set the covariance pass
 // uses the given f32 means instead.
@@ -273,7 +300,10 @@ int launch_covs(PfHandle* h, bool use_args, const float mp[3],
 // Systematic resampling: fixed-point look-back scan, merge-path gather,
 // deterministic injection.  cond_on_ctl: skip unless ctl->resample_now.
 int launch_resample(PfHandle* h, float inject_ratio, bool cond_on_ctl,
-                    bool use_u01, double u01);
+                    bool use_u01, double u01, const CycleArgs* dargs = nullptr);
+// Look-back / injection epochs (30-bit / 32-bit counters, never 0).
+unsigned next_scan_epoch(PfHandle* h);
+unsigned next_inj_epoch(PfHandle* h);
 // Decide whether to resample (device ESS vs ratio * n) for the fused cycle.
 int launch_cycle_decide(PfHandle* h, double ess_ratio);
 // Assemble the fused-cycle output record.

@@ -55,7 +55,8 @@ __global__ void __launch_bounds__(kScanThreads)
                const float* __restrict__ ll, unsigned* flags, uint64_t* vals,
                int* __restrict__ anc, int record, HeavyRun* heavy,
                int heavy_cap, CycleCtl* ctl, int cond, unsigned epoch,
-               int use_u01, double u01_arg) {
+               int use_u01, double u01_arg, const CycleArgs* ca) {
+    if (ca) epoch = ca->scan_epoch;
     if (cond && !ctl->resample_now) return;
     const uint64_t T = ctl->w_total_fx;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -199,7 +200,11 @@ __global__ void __launch_bounds__(kThreads)
 // chains the rest; entries of older epochs read as empty.
 __global__ void k_inject_link(int n, int k, uint64_t gen, uint64_t* head,
                               int* next, CycleCtl* ctl, int cond,
-                              unsigned epoch) {
+                              unsigned epoch, const CycleArgs* ca) {
+    if (ca) {
+        gen = ca->gen;
+        epoch = ca->inj_epoch;
+    }
     if (cond && !ctl->resample_now) return;
     if (!ctl->resample_valid) return;
     const int j = blockIdx.x * kThreads + threadIdx.x;
@@ -213,7 +218,12 @@ __global__ void k_inject_link(int n, int k, uint64_t gen, uint64_t* head,
 
 __global__ void k_inject_apply(PlaneSet ps, int n, int k, uint64_t gen,
                                const uint64_t* head, const int* next,
-                               CycleCtl* ctl, int cond, unsigned epoch) {
+                               CycleCtl* ctl, int cond, unsigned epoch,
+                               const CycleArgs* ca) {
+    if (ca) {
+        gen = ca->gen;
+        epoch = ca->inj_epoch;
+    }
     if (cond && !ctl->resample_now) return;
     if (!ctl->resample_valid) return;
     const int j = blockIdx.x * kThreads + threadIdx.x;
@@ -278,17 +288,29 @@ __global__ void k_pick_from_cum(const double* __restrict__ cum, int n,
 
 }  // namespace
 
+unsigned next_scan_epoch(PfHandle* h) {
+    h->scan_epoch = (h->scan_epoch + 1u) & 0x3FFFFFFFu;
+    if (h->scan_epoch == 0u) h->scan_epoch = 1u;
+    return h->scan_epoch;
+}
+
+unsigned next_inj_epoch(PfHandle* h) {
+    h->inj_epoch = h->inj_epoch + 1u;
+    if (h->inj_epoch == 0u) h->inj_epoch = 1u;
+    return h->inj_epoch;
+}
+
+// With dargs set (graph capture) the epochs and the generation come from
+// device memory at replay time; the host counters are not advanced here.
 int launch_resample(PfHandle* h, float inject_ratio, bool cond_on_ctl,
-                    bool use_u01, double u01) {
+                    bool use_u01, double u01, const CycleArgs* dargs) {
     const int n = h->n;
     const int ntiles = ceil_div(n, kScanTile);
     // The weight total comes from the estimate pass; run one when the
     // weights changed since the last.
     if (!h->total_valid && launch_est_sums(h, false)) return -1;
     // Look-back epochs are per handle and fit in 30 bits; 0 is never used.
-    h->scan_epoch = (h->scan_epoch + 1u) & 0x3FFFFFFFu;
-    if (h->scan_epoch == 0u) h->scan_epoch = 1u;
-    const unsigned epoch = h->scan_epoch;
+    const unsigned epoch = dargs ? 0u : next_scan_epoch(h);
     const int cond = cond_on_ctl ? 1 : 0;
     const int rec = h->record_anc ? 1 : 0;
     {
@@ -296,7 +318,7 @@ int launch_resample(PfHandle* h, float inject_ratio, bool cond_on_ctl,
         k_resample<<<ntiles, kScanThreads, 0, h->stream>>>(
             plane_set(h), n, h->d_w, h->d_ll, h->d_scan_flags, h->d_scan_vals,
             h->d_anc, rec, h->d_heavy, h->heavy_cap, h->d_ctl, cond, epoch,
-            use_u01 ? 1 : 0, u01);
+            use_u01 ? 1 : 0, u01, dargs);
     }
     PFB_KL();
     {
@@ -310,21 +332,20 @@ int launch_resample(PfHandle* h, float inject_ratio, bool cond_on_ctl,
     int k = (inject_ratio > 0.f) ? (int)(inject_ratio * (float)n) : 0;
     if (k > n) k = n;
     if (k > 0) {
-        h->inj_epoch = (h->inj_epoch + 1u);
-        if (h->inj_epoch == 0u) h->inj_epoch = 1u;
+        const unsigned iepoch = dargs ? 0u : next_inj_epoch(h);
         const int ig = ceil_div(k, kThreads);
         {
             KernelScope ks(h, KK_INJECT);
             k_inject_link<<<ig, kThreads, 0, h->stream>>>(
                 n, k, h->gen, h->d_inj_head, h->d_inj_next, h->d_ctl, cond,
-                h->inj_epoch);
+                iepoch, dargs);
         }
         PFB_KL();
         {
             KernelScope ks(h, KK_INJECT);
             k_inject_apply<<<ig, kThreads, 0, h->stream>>>(
                 plane_set(h), n, k, h->gen, h->d_inj_head, h->d_inj_next,
-                h->d_ctl, cond, h->inj_epoch);
+                h->d_ctl, cond, iepoch, dargs);
         }
         PFB_KL();
     }

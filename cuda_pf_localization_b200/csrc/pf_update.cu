@@ -111,7 +111,13 @@ __global__ void __launch_bounds__(kThreads)
              const CObservation* __restrict__ obs, int nobs,
              const float* __restrict__ lm, int lm_count, float sigma_r,
              float sigma_b, float gate, float* __restrict__ ll,
-             double2* part, unsigned* done, CycleCtl* ctl, int use_packed) {
+             double2* part, unsigned* done, CycleCtl* ctl, int use_packed,
+             const CycleArgs* ca) {
+    if (ca) {  // graph replay: this cycle's values
+        pa = ca->pa;
+        obs = ca->obs;
+        nobs = ca->nobs;
+    }
     const Planes s = pick_planes(ps, ctl->live);
     const int i0 = blockIdx.x * (2 * kThreads) + threadIdx.x;
     const int i1 = i0 + kThreads;
@@ -177,7 +183,8 @@ int launch_predict(PfHandle* h, const PredictArgs& pa) {
 }
 
 int launch_weight(PfHandle* h, const PredictArgs& pa, const CObservation* d_obs,
-                  int nobs, float sigma_r, float sigma_b, float gate) {
+                  int nobs, float sigma_r, float sigma_b, float gate,
+                  const CycleArgs* dargs) {
     const int grid = ceil_div(h->n, 2 * kThreads);
     double2* part = reinterpret_cast<double2*>(h->d_part);
     KernelScope ks(h, KK_WEIGHT);
@@ -185,12 +192,12 @@ int launch_weight(PfHandle* h, const PredictArgs& pa, const CObservation* d_obs,
         k_weight<true><<<grid, kThreads, 0, h->stream>>>(
             plane_set(h), h->n, h->seed, pa, d_obs, nobs, h->d_lm, h->lm_count,
             sigma_r, sigma_b, gate, h->d_ll, part, h->d_done + 0, h->d_ctl,
-            h->weight_variant == 0 ? 1 : 0);
+            h->weight_variant == 0 ? 1 : 0, dargs);
     } else {
         k_weight<false><<<grid, kThreads, 0, h->stream>>>(
             plane_set(h), h->n, h->seed, pa, d_obs, nobs, h->d_lm, h->lm_count,
             sigma_r, sigma_b, gate, h->d_ll, part, h->d_done + 0, h->d_ctl,
-            h->weight_variant == 0 ? 1 : 0);
+            h->weight_variant == 0 ? 1 : 0, dargs);
     }
     PFB_KL();
     return 0;

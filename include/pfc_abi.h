@@ -198,6 +198,13 @@ int pfc_cycle_device(void* h, const PfcOdom* odom, const void* d_obs, int nobs,
 /* Wait for the last asynchronous cycle and copy its estimate. */
 int pfc_cycle_result(void* h, double* est_out);
 
+/* 1 (default): a fused cycle with observations is replayed from a CUDA graph
+ * captured on first use (re-captured when n, the landmark table, the cycle
+ * parameters or the weighting variant change); 0: direct kernel launches.
+ * Both give identical results.  Cycles run with per-kernel profiling
+ * (pfc_profile) always use direct launches. */
+int pfc_set_graph(void* h, int on);
+
 /* The CUDA stream (cudaStream_t) the handle runs on. */
 void* pfc_stream(void* h);
 
