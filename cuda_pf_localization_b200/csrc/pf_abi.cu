@@ -143,8 +143,7 @@ void free_particles(PfHandle* h) {
     cudaFree(h->d_anc);
     cudaFree(h->d_inj_head);
     cudaFree(h->d_inj_next);
-    cudaFree(h->d_scan_flags);
-    cudaFree(h->d_scan_vals);
+    cudaFree(h->d_wprefix);
     cudaFree(h->d_part);
     cudaFree(h->d_part_u64);
     cudaFree(h->d_heavy);
@@ -155,8 +154,7 @@ void free_particles(PfHandle* h) {
     h->d_anc = nullptr;
     h->d_inj_head = nullptr;
     h->d_inj_next = nullptr;
-    h->d_scan_flags = nullptr;
-    h->d_scan_vals = nullptr;
+    h->d_wprefix = nullptr;
     h->d_part = nullptr;
     h->d_part_u64 = nullptr;
     h->d_heavy = nullptr;
@@ -198,7 +196,7 @@ int device_error(PfHandle* h) {
 // Queue estimate pass 1 + Markley + speculative covariance pass + the copy
 // of the control block.
 int queue_estimate(PfHandle* h) {
-    if (launch_est_sums(h, false)) return -1;
+    if (launch_est_sums(h)) return -1;
     if (launch_covs(h, false, nullptr, nullptr, false)) return -1;
     PFB_CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(CycleCtl),
                            cudaMemcpyDeviceToHost, h->stream));
@@ -237,6 +235,7 @@ int set_wmode(PfHandle* h, int mode) {
     KernelScope ks(h, KK_MISC);
     k_set_wmode<<<1, 1, 0, h->stream>>>(h->d_ctl, mode);
     PFB_KL();
+    h->prefix_valid = false;
     return 0;
 }
 
@@ -292,7 +291,6 @@ int run_cycle_graph(PfHandle* h, const PfcOdom* odom, const CObservation* obs_de
     a.obs = obs_dev;
     a.nobs = nobs;
     a.gen = h->gen;
-    a.scan_epoch = next_scan_epoch(h);
     const int kinj = (prm->random_inject_ratio > 0.f)
                          ? (int)(prm->random_inject_ratio * (float)h->n)
                          : 0;
@@ -327,8 +325,8 @@ int run_cycle_graph(PfHandle* h, const PfcOdom* odom, const CObservation* obs_de
     PFB_CK(cudaEventRecord(h->est_ev, h->stream));
     h->stats.launches += h->graph_kernels;
     h->stats.d2h_bytes += sizeof(CycleCtl);
-    h->total_valid = false;
-    h->anc_valid = h->record_anc;
+    h->prefix_valid = false;
+    h->anc_valid = true;
     h->est_inflight = true;
     h->est_valid = false;
     return 0;
@@ -369,11 +367,10 @@ int enqueue_cycle(PfHandle* h, const PredictArgs& pa, const CObservation* obs_de
         launch_weight(h, pa, obs_dev, nobs, prm->sigma_r, prm->sigma_b, prm->gate,
                       dargs))
         return -1;
-    if (launch_est_sums(h, false)) return -1;
     if (launch_cycle_decide(h, prm->resample_ess_ratio)) return -1;
     if (launch_resample(h, prm->random_inject_ratio, true, false, 0.0, dargs))
         return -1;
-    if (launch_est_sums(h, true)) return -1;
+    if (launch_est_sums(h)) return -1;
     if (launch_covs(h, false, nullptr, nullptr, true)) return -1;
     PFB_CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(CycleCtl),
                            cudaMemcpyDeviceToHost, h->stream));
@@ -508,9 +505,9 @@ int pfc_init(void* hv, int n, unsigned int seed) {
     h->pending_predict = false;
     h->est_valid = h->est_inflight = false;
     h->anc_valid = false;
-    h->total_valid = false;
+    h->prefix_valid = false;
     const size_t np = (size_t)h->n_pad;
-    const int ntiles = ceil_div(n, 4096);
+    const int nprefix = ceil_div(n, kPrefixBlock);
     const int part = std::max(2 * ceil_div(n, kThreads), 1184 * 16);
     PFB_CK(cudaMalloc((void**)&h->d_state[0], 7 * np * sizeof(float)));
     PFB_CK(cudaMalloc((void**)&h->d_state[1], 7 * np * sizeof(float)));
@@ -518,21 +515,19 @@ int pfc_init(void* hv, int n, unsigned int seed) {
     PFB_CK(cudaMalloc((void**)&h->d_w, np * sizeof(float)));
     h->heavy_cap = n / 32 + n / 4096 + 2;  // runs > 32 outputs, in pieces of <= 4096
     PFB_CK(cudaMalloc((void**)&h->d_heavy, (size_t)h->heavy_cap * sizeof(HeavyRun)));
-    PFB_CK(cudaMalloc((void**)&h->d_part_u64, 2 * 1184 * sizeof(unsigned long long)));
+    PFB_CK(cudaMalloc((void**)&h->d_part_u64,
+                      2 * (size_t)std::max(nprefix, 1184) * sizeof(unsigned long long)));
     PFB_CK(cudaMalloc((void**)&h->d_anc, (size_t)n * sizeof(int)));
     PFB_CK(cudaMalloc((void**)&h->d_inj_head, (size_t)n * sizeof(uint64_t)));
     PFB_CK(cudaMalloc((void**)&h->d_inj_next, (size_t)n * sizeof(int)));
-    PFB_CK(cudaMalloc((void**)&h->d_scan_flags, (size_t)ntiles * sizeof(unsigned)));
-    PFB_CK(cudaMalloc((void**)&h->d_scan_vals, 2 * (size_t)ntiles * sizeof(uint64_t)));
+    PFB_CK(cudaMalloc((void**)&h->d_wprefix, (size_t)nprefix * sizeof(uint64_t)));
     PFB_CK(cudaMalloc((void**)&h->d_part, (size_t)part * sizeof(double)));
     h->part_cap = part;
     PFB_CK(cudaMemsetAsync(h->d_state[0], 0, 7 * np * sizeof(float), h->stream));
     PFB_CK(cudaMemsetAsync(h->d_state[1], 0, 7 * np * sizeof(float), h->stream));
     PFB_CK(cudaMemsetAsync(h->d_ll, 0, np * sizeof(float), h->stream));
     PFB_CK(cudaMemsetAsync(h->d_inj_head, 0, (size_t)n * sizeof(uint64_t), h->stream));
-    PFB_CK(cudaMemsetAsync(h->d_scan_flags, 0, (size_t)ntiles * sizeof(unsigned), h->stream));
     PFB_CK(cudaMemsetAsync(h->d_done, 0, 8 * sizeof(unsigned), h->stream));
-    h->scan_epoch = 0;
     h->inj_epoch = 0;
     k_ctl_reset<<<1, 1, 0, h->stream>>>(h->d_ctl, 0);
     PFB_KL();
@@ -575,7 +570,7 @@ int pfc_reinit(void* hv, float x, float y, float z, float qw, float qx,
     if (launch_reinit(h, p0, q0, pos_std, rot_std)) return -1;
     if (set_wmode(h, WMODE_UNIFORM)) return -1;
     h->est_valid = h->est_inflight = false;
-    h->total_valid = false;
+    h->prefix_valid = false;
     return 0;
 }
 
@@ -589,7 +584,7 @@ int pfc_reinit_poses(void* hv, const float* d_pose3k, int k, float z,
     if (launch_reinit_poses(h, d_pose3k, k, z, pos_std, rot_std)) return -1;
     if (set_wmode(h, WMODE_UNIFORM)) return -1;
     h->est_valid = h->est_inflight = false;
-    h->total_valid = false;
+    h->prefix_valid = false;
     return 0;
 }
 
@@ -631,6 +626,9 @@ int pfc_weight(void* hv, const CObservation* obs, int nobs, float sigma_r,
     PredictArgs pa = pending_args(h);
     h->pending_predict = false;
     if (launch_weight(h, pa, h->d_obs, nobs, sigma_r, sigma_b, gate)) return -1;
+    // materialise the weights with the resampler's prefixes now: the estimate
+    // pass then reads them instead of re-deriving them from ll
+    if (launch_weight_prefix(h, false, 0.0)) return -1;
     return queue_estimate(h);
 }
 
@@ -820,7 +818,7 @@ int pfc_set_state(void* hv, const float* pos3n, const float* quat4n,
     }
     PFB_CK(cudaStreamSynchronize(h->stream));
     h->est_valid = h->est_inflight = false;
-    h->total_valid = false;
+    h->prefix_valid = false;
     return 0;
 }
 
@@ -835,7 +833,7 @@ int pfc_get_ancestors(void* hv, int* anc) {
     PfHandle* h = as_pf(hv);
     if (!valid_handle(h) || !anc) return -1;
     if (!h->anc_valid) {
-        set_error("pf_b200: no recorded resample (call pfc_record_ancestors first)");
+        set_error("pf_b200: no resample has run on this particle set");
         return -1;
     }
     PFB_CK(cudaStreamSynchronize(h->stream));

@@ -466,7 +466,7 @@ __device__ __forceinline__ void est_add(double (&acc)[kEstN], float wf, float x,
     for (int r = 0; r < 4; ++r)
 #pragma unroll
         for (int cc = r; cc < 4; ++cc) acc[e++] += wd * q[r] * q[cc];
-    acc[13] += wd * wd;
+    acc[13] = __fma_rn(wd, wd, acc[13]);
 }
 
 // Accumulate one particle into the 12 covariance sums of the reference's

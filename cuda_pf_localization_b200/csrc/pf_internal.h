@@ -22,6 +22,7 @@
 namespace pfb {
 
 constexpr int kEstN = 14;  // pfc_est_sums layout
+constexpr int kPrefixBlock = 1024;  // particles per fixed-point prefix entry
 constexpr int kCovN = 12;  // pfc_covs layout
 
 // Weight plane semantics.
@@ -70,7 +71,6 @@ struct CycleCtl {
     int resample_valid;      // total finite and > 0
     // diagnostics
     unsigned err;            // ERR_* bits
-    unsigned tile_counter;   // dynamic tile ids for the look-back scan
     int live;                // which ping-pong particle set is current
     // exact fixed-point weight total of the current weights (by-product of
     // the estimate pass) and whether any weight is outside [0,1] / NaN
@@ -172,14 +172,14 @@ struct PfHandle {
     int* d_anc = nullptr;
     uint64_t* d_inj_head = nullptr;
     int* d_inj_next = nullptr;
-    unsigned* d_scan_flags = nullptr;   // look-back tile status words
-    uint64_t* d_scan_vals = nullptr;    // look-back tile values (agg, incl)
+    uint64_t* d_wprefix = nullptr;      // fixed-point weight prefix per block
     double* d_part = nullptr;           // per-block partials (max over uses)
     int part_cap = 0;                   // doubles in d_part
     unsigned long long* d_part_u64 = nullptr;  // per-block integer partials
     HeavyRun* d_heavy = nullptr;        // deferred copy runs (n/32 + 1)
     int heavy_cap = 0;
-    bool total_valid = false;  // ctl w_total_fx describes the current weights
+    bool prefix_valid = false;  // ctl w_total_fx and d_wprefix describe the
+                                // current weights
     unsigned* d_done = nullptr;         // last-block counters
     CycleCtl* d_ctl = nullptr;
     CycleCtl* h_ctl = nullptr;          // pinned mirror
@@ -210,7 +210,6 @@ struct PfHandle {
     int weight_variant = 0;
     bool record_anc = false;
     bool anc_valid = false;
-    unsigned scan_epoch = 0;   // look-back flag epoch (never 0 when used)
     unsigned inj_epoch = 0;    // injection list epoch (never 0 when used)
     float* d_stage = nullptr;  // AoS staging for snapshot / set_state (7n)
 
@@ -270,7 +269,6 @@ struct CycleArgs {
     PredictArgs pa;
     const CObservation* obs;
     int nobs;
-    unsigned scan_epoch;
     unsigned inj_epoch;
     unsigned long long gen;
 };
@@ -293,21 +291,23 @@ int launch_weight(PfHandle* h, const PredictArgs& pa, const CObservation* d_obs,
                   const CycleArgs* dargs = nullptr);
 // Estimate pass 1 (+ device Markley mean) and the speculative covariance pass
 // around (float)mean, (float)qmean.  When use_args is set the covariance pass
-// uses the given f32 means instead.
-int launch_est_sums(PfHandle* h, bool cycle_second);
+// uses the given f32 means instead; cycle_output also assembles the fused
+// cycle's output record.
+int launch_est_sums(PfHandle* h);
 int launch_covs(PfHandle* h, bool use_args, const float mp[3],
-                const float mq[4], bool cycle_second);
+                const float mq[4], bool cycle_output);
 // Systematic resampling: fixed-point look-back scan, merge-path gather,
 // deterministic injection.  cond_on_ctl: skip unless ctl->resample_now.
 int launch_resample(PfHandle* h, float inject_ratio, bool cond_on_ctl,
                     bool use_u01, double u01, const CycleArgs* dargs = nullptr);
-// Look-back / injection epochs (30-bit / 32-bit counters, never 0).
-unsigned next_scan_epoch(PfHandle* h);
+// Injection list epoch (32-bit counter, never 0).
 unsigned next_inj_epoch(PfHandle* h);
-// Decide whether to resample (device ESS vs ratio * n) for the fused cycle.
+// Weight pass before a resample: materialises the weights, their ESS, the
+// fixed-point total and the per-block prefixes (kPrefixBlock particles per
+// block); with decide set it also takes the fused cycle's resample decision
+// (device ESS vs ratio * n).
+int launch_weight_prefix(PfHandle* h, bool decide, double ess_ratio);
 int launch_cycle_decide(PfHandle* h, double ess_ratio);
-// Assemble the fused-cycle output record.
-int launch_cycle_output(PfHandle* h);
 int launch_materialize_weights(PfHandle* h);
 int launch_pick_from_cum(PfHandle* h, const double* d_cum, int n, double u0,
                          double total, int* d_anc);

@@ -15,18 +15,20 @@
 //   anc_i = min(first j with C_j >= ceil(t_i * 2^62), n - 1)
 // Because C_j is an integer, C_j >= ceil(t * 2^62) is exactly C_j * 2^-62 >= t.
 //
-// Single pass.  The estimate pass that precedes every resample already holds
-// T (it forms sum_j W_j), so thresholds are known before the scan starts.
-// A decoupled look-back scan (Merrill & Garland, "Single-pass parallel prefix
-// scan with decoupled look-back", 2016; dynamic tile ids, warp-parallel
-// look-back, bounded spins) gives each particle j its C_{j-1} and C_j; the
+// The weight pass that precedes every resample (k_ess) forms T and the
+// exclusive fixed-point prefix of every block of kPrefixBlock particles, so
+// thresholds and each tile's starting sum are known before the resampler
+// starts; a tile then scans its own weights in shared registers (no
+// inter-block look-back) and gives each particle j its C_{j-1} and C_j.  The
 // outputs whose ancestor is j are exactly the run [cnt(C_{j-1}), cnt(C_j)),
-// cnt(X) = #{i : T_i <= X} computed in closed form from the arithmetic
-// threshold sequence and corrected against the exact T_i.  So each source
-// particle is read once, in order, and copied to its run; no cumulative
-// array is stored.  Runs longer than kHeavy (one particle holding most of
-// the weight) are appended to a list and expanded by a second, output-
-// parallel kernel, so no thread copies more than kHeavy outputs.
+// cnt(X) = #{i : T_i <= X}: a thread finds its first run start in closed form
+// from the arithmetic threshold sequence (corrected against the exact T_i)
+// and then steps the thresholds run by run, writing the ancestor of each
+// output of the run; no cumulative array is stored.  Runs longer than kHeavy
+// (one particle holding most of the weight) are appended to a list and
+// filled by a second, output-parallel kernel.  A third, output-parallel
+// kernel then gathers the particles (coalesced 16-byte stores), so the copy
+// work does not pile up on the few tiles that hold most of the weight.
 //
 // Injection uses the reference's splitmix64 streams
 // (src/cuda/pf_kernels.cu:323-352), applied per particle in ascending draw
@@ -43,20 +45,19 @@ namespace {
 using namespace pfb::dev;
 
 constexpr int kScanThreads = 256;
-constexpr int kScanItems = 16;
-constexpr int kScanTile = kScanThreads * kScanItems;  // 4096
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;  // 2048
+static_assert(kScanTile % kPrefixBlock == 0, "tiles start on prefix blocks");
 constexpr int kHeavy = 32;  // longest copy run a scan thread performs
 constexpr int kThreads = kBlk;
 
 PlaneSet plane_set(const PfHandle* h) { return {h->planes(0), h->planes(1)}; }
 
 __global__ void __launch_bounds__(kScanThreads)
-    k_resample(PlaneSet ps, int n, const float* __restrict__ w,
-               const float* __restrict__ ll, unsigned* flags, uint64_t* vals,
-               int* __restrict__ anc, int record, HeavyRun* heavy,
-               int heavy_cap, CycleCtl* ctl, int cond, unsigned epoch,
-               int use_u01, double u01_arg, const CycleArgs* ca) {
-    if (ca) epoch = ca->scan_epoch;
+    k_resample(int n, const float* __restrict__ w, const float* __restrict__ ll,
+               const uint64_t* __restrict__ prefix, int* __restrict__ anc,
+               HeavyRun* heavy, int heavy_cap, CycleCtl* ctl, int cond,
+               int use_u01, double u01_arg) {
     if (cond && !ctl->resample_now) return;
     const uint64_t T = ctl->w_total_fx;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -73,54 +74,40 @@ __global__ void __launch_bounds__(kScanThreads)
     const double total = (double)T * 0x1p-62;
     const double step = total / (double)n;
     const double u0 = u01 * step;
-    __shared__ unsigned s_tile;
-    __shared__ uint64_t s_warp[kScanThreads / 32];
-    __shared__ uint64_t s_prefix, s_agg;
-    if (tid == 0) {
-        s_tile = atomicAdd(&ctl->tile_counter, 1u);
-        if (blockIdx.x == 0) {
-            ctl->lcg_next = lcg1;
-            ctl->resample_valid = 1;
-            ctl->total_fx = T;
-            ctl->total = total;
-            ctl->step = step;
-            ctl->u0 = u0;
-        }
+    if (blockIdx.x == 0 && tid == 0) {
+        ctl->lcg_next = lcg1;
+        ctl->resample_valid = 1;
+        ctl->total_fx = T;
+        ctl->total = total;
+        ctl->step = step;
+        ctl->u0 = u0;
     }
-    __syncthreads();
-    const int tile = (int)s_tile;
+    __shared__ uint64_t s_warp[kScanThreads / 32];
+    const int tile = blockIdx.x;
+    // the tile's starting sum, fetched early (it is needed after the scan)
+    const uint64_t tile_base =
+        tid == 0 ? __ldcg(&prefix[(size_t)tile * (kScanTile / kPrefixBlock)]) : 0ull;
     const int wmode = ctl->wmode;
     const double M = ctl->ll_max, S = ctl->ll_sumexp;
-    const int live = ctl->live;
-    const Planes src = pick_planes(ps, live), dst = pick_planes(ps, 1 - live);
 
-    // This thread's 16 consecutive weights -> inclusive fixed-point sums.
+    // This thread's total over its kScanItems consecutive weights.
     const long long j0 = (long long)tile * kScanTile + tid * kScanItems;
-    uint64_t v[kScanItems];
     uint64_t run = 0;
     if (wmode == WMODE_STORED && j0 + kScanItems <= n) {
         const float4* w4 = reinterpret_cast<const float4*>(w + j0);
 #pragma unroll
         for (int q = 0; q < kScanItems / 4; ++q) {
             const float4 a = w4[q];
-            run += weight_fx(a.x);
-            v[4 * q] = run;
-            run += weight_fx(a.y);
-            v[4 * q + 1] = run;
-            run += weight_fx(a.z);
-            v[4 * q + 2] = run;
-            run += weight_fx(a.w);
-            v[4 * q + 3] = run;
+            run += weight_fx(a.x) + weight_fx(a.y) + weight_fx(a.z) + weight_fx(a.w);
         }
     } else {
-#pragma unroll
         for (int k = 0; k < kScanItems; ++k) {
             const long long j = j0 + k;
             if (j < n) run += weight_fx(weight_of(wmode, j, n, w, ll, M, S));
-            v[k] = run;
         }
     }
-    // Block scan of the thread totals.
+    // Block scan of the thread totals; the tile's own start comes from the
+    // prefix pass.
     uint64_t x = run;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
@@ -130,69 +117,95 @@ __global__ void __launch_bounds__(kScanThreads)
     if (lane == 31) s_warp[warp] = x;
     __syncthreads();
     if (tid == 0) {
-        uint64_t acc = 0;
+        uint64_t acc = tile_base;
         for (int k = 0; k < kScanThreads / 32; ++k) {
             const uint64_t t = s_warp[k];
             s_warp[k] = acc;
             acc += t;
         }
-        s_agg = acc;
-        if (tile == 0) {
-            vals[1] = acc;
-            __threadfence();
-            st_release(&flags[0], (epoch << 2) | TILE_INCL);
-            s_prefix = 0;
-        } else {
-            vals[2 * (size_t)tile] = acc;
-            __threadfence();
-            st_release(&flags[tile], (epoch << 2) | TILE_AGG);
-        }
-    }
-    __syncthreads();
-    if (tile > 0 && warp == 0) {
-        const uint64_t prefix = look_back(flags, vals, tile, epoch, &ctl->err);
-        if (lane == 0) {
-            vals[2 * (size_t)tile + 1] = prefix + s_agg;
-            __threadfence();
-            st_release(&flags[tile], (epoch << 2) | TILE_INCL);
-            s_prefix = prefix;
-        }
     }
     __syncthreads();
 
-    // Copy runs.  C_{j0-1} = prefix + exclusive offset of this thread.
-    const uint64_t c_prev = s_prefix + s_warp[warp] + (x - run);
-    long long s = (j0 == 0) ? 0 : count_le(c_prev, n, u0, step);
-#pragma unroll
+    // Ancestor runs.  C_{j0-1} = tile prefix + exclusive offset of this
+    // thread.  The end of each run, cnt(C_j), is found by stepping the
+    // thresholds from the end of the previous run (one threshold per output
+    // plus one), switching to the closed form once a run exceeds kHeavy
+    // outputs; such runs are filled by the output-parallel expansion.
+    uint64_t C = s_warp[warp] + (x - run);
+    long long s = (j0 == 0) ? 0 : count_le(C, n, u0, step);
+#pragma unroll 1
     for (int k = 0; k < kScanItems; ++k) {
         const long long j = j0 + k;
         if (j >= n) break;
-        const long long e =
-            (j == n - 1) ? (long long)n : count_le(c_prev + v[k], n, u0, step);
-        const long long cnt = e - s;
-        if (cnt > kHeavy) {
+        C += weight_fx(weight_of(wmode, j, n, w, ll, M, S));
+        long long e;
+        if (j == n - 1) {
+            e = n;
+        } else {
+            e = s;
+            while (e < n && e - s <= kHeavy && threshold_fx(e, u0, step) <= C) ++e;
+            if (e - s > kHeavy) e = count_le(C, n, u0, step);
+        }
+        if (e - s > kHeavy) {
             push_run(heavy, heavy_cap, &ctl->heavy_count, &ctl->err, (int)j, s, e, 0);
-        } else if (cnt > 0) {
-            copy_particle(src, dst, (int)j, s, e, anc, record);
+        } else {
+            for (long long i = s; i < e; ++i) anc[i] = (int)j;
         }
         s = e;
     }
 }
 
-// Output-parallel expansion of the long runs: each recorded piece (at most
-// kSplit outputs) is copied by one block.
+// Output-parallel ancestors of the long runs: each recorded piece (at most
+// kSplit outputs) is filled by one block.
 __global__ void __launch_bounds__(kThreads)
-    k_expand_runs(PlaneSet ps, const HeavyRun* heavy, int heavy_cap,
-                  int* __restrict__ anc, int record, CycleCtl* ctl, int cond) {
+    k_expand_runs(const HeavyRun* heavy, int heavy_cap, int* __restrict__ anc,
+                  CycleCtl* ctl, int cond) {
     if (cond && !ctl->resample_now) return;
     if (!ctl->resample_valid) return;
     const int count = min(ctl->heavy_count, heavy_cap);
-    const int live = ctl->live;
-    const Planes src = pick_planes(ps, live), dst = pick_planes(ps, 1 - live);
     for (int r = blockIdx.x; r < count; r += gridDim.x) {
         const HeavyRun h = heavy[r];
-        fill_range(src, dst, h.j, h.start + (int)threadIdx.x, h.end, kThreads, anc,
-                   record);
+        for (int i = h.start + (int)threadIdx.x; i < h.end; i += kThreads) anc[i] = h.j;
+    }
+}
+
+// Output-parallel gather: output i takes particle anc[i] of the live set
+// (four outputs per thread, 16-byte stores on every plane; the ancestors are
+// non-decreasing, so the loads walk the source planes in order).
+__global__ void __launch_bounds__(kThreads)
+    k_gather(PlaneSet ps, int n, const int* __restrict__ anc, CycleCtl* ctl,
+             int cond) {
+    if (cond && !ctl->resample_now) return;
+    if (!ctl->resample_valid) return;
+    const int live = ctl->live;
+    const Planes src = pick_planes(ps, live), dst = pick_planes(ps, 1 - live);
+    const int i4 = blockIdx.x * kThreads + threadIdx.x;
+    const int i = 4 * i4;
+    if (i >= n) return;
+    if (i + 3 < n) {
+        const int4 a = reinterpret_cast<const int4*>(anc)[i4];
+#define PFB_GATHER_PLANE(P)                                                  \
+    reinterpret_cast<float4*>(dst.P)[i4] =                                   \
+        make_float4(src.P[a.x], src.P[a.y], src.P[a.z], src.P[a.w])
+        PFB_GATHER_PLANE(px);
+        PFB_GATHER_PLANE(py);
+        PFB_GATHER_PLANE(pz);
+        PFB_GATHER_PLANE(qw);
+        PFB_GATHER_PLANE(qx);
+        PFB_GATHER_PLANE(qy);
+        PFB_GATHER_PLANE(qz);
+#undef PFB_GATHER_PLANE
+    } else {
+        for (int o = i; o < n; ++o) {
+            const int j = anc[o];
+            dst.px[o] = src.px[j];
+            dst.py[o] = src.py[j];
+            dst.pz[o] = src.pz[j];
+            dst.qw[o] = src.qw[j];
+            dst.qx[o] = src.qx[j];
+            dst.qy[o] = src.qy[j];
+            dst.qz[o] = src.qz[j];
+        }
     }
 }
 
@@ -262,7 +275,6 @@ __global__ void k_commit(CycleCtl* ctl, int cond) {
         }
         ctl->wmode = WMODE_UNIFORM;
     }
-    ctl->tile_counter = 0u;
     ctl->heavy_count = 0;
     ctl->err &= ~ERR_SCAN_OVERFLOW;
 }
@@ -288,12 +300,6 @@ __global__ void k_pick_from_cum(const double* __restrict__ cum, int n,
 
 }  // namespace
 
-unsigned next_scan_epoch(PfHandle* h) {
-    h->scan_epoch = (h->scan_epoch + 1u) & 0x3FFFFFFFu;
-    if (h->scan_epoch == 0u) h->scan_epoch = 1u;
-    return h->scan_epoch;
-}
-
 unsigned next_inj_epoch(PfHandle* h) {
     h->inj_epoch = h->inj_epoch + 1u;
     if (h->inj_epoch == 0u) h->inj_epoch = 1u;
@@ -306,25 +312,27 @@ int launch_resample(PfHandle* h, float inject_ratio, bool cond_on_ctl,
                     bool use_u01, double u01, const CycleArgs* dargs) {
     const int n = h->n;
     const int ntiles = ceil_div(n, kScanTile);
-    // The weight total comes from the estimate pass; run one when the
-    // weights changed since the last.
-    if (!h->total_valid && launch_est_sums(h, false)) return -1;
-    // Look-back epochs are per handle and fit in 30 bits; 0 is never used.
-    const unsigned epoch = dargs ? 0u : next_scan_epoch(h);
+    // The weight total and the block prefixes come from the weight pass; run
+    // one when the weights changed since the last.
+    if (!h->prefix_valid && launch_weight_prefix(h, false, 0.0)) return -1;
     const int cond = cond_on_ctl ? 1 : 0;
-    const int rec = h->record_anc ? 1 : 0;
     {
         KernelScope ks(h, KK_SCAN);
         k_resample<<<ntiles, kScanThreads, 0, h->stream>>>(
-            plane_set(h), n, h->d_w, h->d_ll, h->d_scan_flags, h->d_scan_vals,
-            h->d_anc, rec, h->d_heavy, h->heavy_cap, h->d_ctl, cond, epoch,
-            use_u01 ? 1 : 0, u01, dargs);
+            n, h->d_w, h->d_ll, h->d_wprefix, h->d_anc, h->d_heavy, h->heavy_cap,
+            h->d_ctl, cond, use_u01 ? 1 : 0, u01);
+    }
+    PFB_KL();
+    {
+        KernelScope ks(h, KK_SCAN);
+        k_expand_runs<<<2 * 148, kThreads, 0, h->stream>>>(
+            h->d_heavy, h->heavy_cap, h->d_anc, h->d_ctl, cond);
     }
     PFB_KL();
     {
         KernelScope ks(h, KK_GATHER);
-        k_expand_runs<<<2 * 148, kThreads, 0, h->stream>>>(
-            plane_set(h), h->d_heavy, h->heavy_cap, h->d_anc, rec, h->d_ctl, cond);
+        k_gather<<<ceil_div(n, 4 * kThreads), kThreads, 0, h->stream>>>(
+            plane_set(h), n, h->d_anc, h->d_ctl, cond);
     }
     PFB_KL();
     // k = floor(ratio * n) with the reference's f32 product
@@ -354,10 +362,10 @@ int launch_resample(PfHandle* h, float inject_ratio, bool cond_on_ctl,
         k_commit<<<1, 1, 0, h->stream>>>(h->d_ctl, cond);
     }
     PFB_KL();
-    h->anc_valid = h->record_anc;
+    h->anc_valid = true;
     // The weights are uniform afterwards; the next estimate pass recomputes
     // their fixed-point total.
-    h->total_valid = false;
+    h->prefix_valid = false;
     return 0;
 }
 

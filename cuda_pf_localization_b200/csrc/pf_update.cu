@@ -200,6 +200,7 @@ int launch_weight(PfHandle* h, const PredictArgs& pa, const CObservation* d_obs,
             h->weight_variant == 0 ? 1 : 0, dargs);
     }
     PFB_KL();
+    h->prefix_valid = false;
     return 0;
 }
 

@@ -236,11 +236,11 @@ int pfc_reinit_poses(void* h, const float* d_pose3k, int k, float z,
  * handle's LCG draw (the LCG is left untouched); injection as pfc_resample. */
 int pfc_resample_u01(void* h, double u01, float random_inject_ratio);
 
-/* Record ancestor indices in later resamples (off by default: 4 B/particle
- * of extra HBM writes). */
+/* Accepted for compatibility and has no effect: every resample forms the
+ * ancestor indices (its gather reads them), so they are always available. */
 int pfc_record_ancestors(void* h, int on);
 
-/* Ancestor index of every particle in the last recorded resample (n ints). */
+/* Ancestor index of every particle in the last resample (n ints). */
 int pfc_get_ancestors(void* h, int* anc);
 
 /* The reference's pick rule (pf_kernels.cu:304-321) applied to a caller
