@@ -8,9 +8,9 @@
 // of one filter.  Per-filter reductions are finished by the last tile of that
 // filter to complete (an atomic counter per filter), so a cycle is a fixed
 // chain of kernels whatever the filter sizes:
-//   begin -> weight (+ predict) -> estimate -> covariances + ESS decision ->
-//   resample (look-back scan + run copy) -> long runs -> injection (link,
-//   apply) -> commit -> estimate / covariances of the resampled filters.
+//   begin -> weight (+ predict) -> weights + ESS decision -> resample
+//   (look-back scan + run copy) -> long runs -> injection (link, apply) ->
+//   commit -> estimate -> covariances (output record).
 // The chain is captured once into a CUDA graph; a cycle is one graph launch
 // fed by one copy of the per-filter inputs.
 //
@@ -71,7 +71,7 @@ struct BCtl {
     double M, S;
     int wmode, wvalid;
     double est[kEstN], qmean[4], covs[kCovN];
-    double ess;
+    double ess, ess_pre;
     float cmp[3], cmq[4];
     int resample_now, resampled, resample_valid, w_bad;
     unsigned long long w_total_fx;
@@ -272,18 +272,104 @@ __device__ __forceinline__ void tiles_combine(const double* part, int ntiles,
     __syncthreads();
 }
 
-// Estimate pass over one estimate tile: 14 FP64 sums, the exact fixed-point
-// weight total and the weight materialisation; the filter's last tile
-// combines, runs the Markley mean and stores the f32 covariance means.
-// second: only filters that resample this cycle (after the resample).
-__global__ void __launch_bounds__(kThreads, 2)
-    k_b_est(Arena A, const BFilter* __restrict__ F, const BTile* __restrict__ T,
+// Weight pass over one estimate tile before the resample decision: the
+// weights materialised from the log-likelihoods, sum w^2 in FP64, the exact
+// fixed-point weight total and the bad-weight flag; the filter's last tile
+// combines them and takes ParticleFilter::update's decision
+// ratio > 0 && ess < ratio * N (crates/pf_core/src/particle_filter.rs:115-117).
+// Reads 4 B per particle where the estimate pass reads 32 B.
+__global__ void __launch_bounds__(kThreads)
+    k_b_ess(Arena A, const BFilter* __restrict__ F, const BTile* __restrict__ T,
             BCtl* C, double* __restrict__ epart,
-            unsigned long long* __restrict__ eupart, int second) {
+            unsigned long long* __restrict__ eupart, double* __restrict__ out) {
     const BTile t = T[blockIdx.x];
     const BFilter& fl = F[t.f];
     BCtl* c = C + t.f;
-    if (second && !c->resample_now) return;
+    const int wmode = c->wmode;
+    const double M = c->M, S = c->S;
+    const float wuni = 1.0f / (float)fl.n;
+    float* w = A.w + fl.off;
+    const float* ll = A.ll + fl.off;
+    double acc[1] = {0.0};
+    unsigned long long tfx = 0;
+    int bad = 0;
+    const int q0 = t.start >> 2, q1 = (t.start + t.count + 3) >> 2;
+    for (int i4 = q0 + threadIdx.x; i4 < q1; i4 += kThreads) {
+        float4 W;
+        if (wmode == WMODE_STORED) {
+            W = reinterpret_cast<const float4*>(w)[i4];
+        } else if (wmode == WMODE_UNIFORM) {
+            W = make_float4(wuni, wuni, wuni, wuni);
+        } else {
+            const float4 L = reinterpret_cast<const float4*>(ll)[i4];
+            W = make_float4((float)(exp((double)L.x - M) / S),
+                            (float)(exp((double)L.y - M) / S),
+                            (float)(exp((double)L.z - M) / S),
+                            (float)(exp((double)L.w - M) / S));
+            reinterpret_cast<float4*>(w)[i4] = W;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (4 * i4 + k >= fl.n) break;
+            const float wf = comp(W, k);
+            bad |= weight_bad(wf) ? 1 : 0;
+            tfx += weight_bad(wf) ? 0ull : weight_fx(wf);
+            const double wd = (double)wf;
+            acc[0] = __fma_rn(wd, wd, acc[0]);
+        }
+    }
+    // integer total and bad flag of the tile
+    __shared__ unsigned long long s_u[kThreads / 32];
+    const unsigned long long u = warp_sum_u64(tfx);
+    if ((threadIdx.x & 31) == 0) s_u[threadIdx.x >> 5] = u;
+    const int any_bad = __syncthreads_or(bad);
+    if (threadIdx.x == 0) {
+        unsigned long long tot = 0;
+        for (int k = 0; k < kThreads / 32; ++k) tot += s_u[k];
+        eupart[2 * (size_t)(fl.etile0 + t.local)] = tot;
+        eupart[2 * (size_t)(fl.etile0 + t.local) + 1] = any_bad ? 1ull : 0ull;
+    }
+    if (!tile_partial<1>(acc, epart + (size_t)(fl.etile0 + t.local) * kEstN,
+                         &c->done_e, fl.netiles))
+        return;
+    double sq = 0.0;
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        for (int b = lane; b < fl.netiles; b += 32)
+            sq += __ldcg(&epart[(size_t)(fl.etile0 + b) * kEstN]);
+        sq = warp_sum_d(sq);
+    }
+    if (threadIdx.x == 0) {
+        unsigned long long tot = 0, fb = 0;
+        for (int b = 0; b < fl.netiles; ++b) {
+            tot += __ldcg(&eupart[2 * (size_t)(fl.etile0 + b)]);
+            fb |= __ldcg(&eupart[2 * (size_t)(fl.etile0 + b) + 1]);
+        }
+        const double ess = sq > 0.0 ? 1.0 / sq : 0.0;
+        c->ess = ess;
+        c->ess_pre = ess;
+        double* o = out + (size_t)t.f * PFC_EST_LEN;
+        o[PFC_EST_ESS_PRE] = ess;
+        c->resample_now = (fl.ess_ratio > 0.0 && ess < fl.ess_ratio * (double)fl.n) ? 1 : 0;
+        c->resampled = 0;
+        o[PFC_EST_RESAMPLED] = 0.0;
+        c->w_total_fx = tot;
+        c->w_bad = fb ? 1 : 0;
+        if (wmode == WMODE_LL) c->wmode = WMODE_STORED;
+        c->done_e = 0u;
+    }
+}
+
+// Estimate pass over one estimate tile: 14 FP64 sums (and the weight
+// materialisation when the weights are still log-likelihoods); the filter's
+// last tile combines, runs the Markley mean and stores the f32 covariance
+// means.
+__global__ void __launch_bounds__(kThreads, 2)
+    k_b_est(Arena A, const BFilter* __restrict__ F, const BTile* __restrict__ T,
+            BCtl* C, double* __restrict__ epart) {
+    const BTile t = T[blockIdx.x];
+    const BFilter& fl = F[t.f];
+    BCtl* c = C + t.f;
     const Planes s = filter_planes(A, c->live, fl.off);
     const int wmode = c->wmode;
     const double M = c->M, S = c->S;
@@ -293,8 +379,6 @@ __global__ void __launch_bounds__(kThreads, 2)
     double acc[kEstN];
 #pragma unroll
     for (int k = 0; k < kEstN; ++k) acc[k] = 0.0;
-    unsigned long long tfx = 0;
-    int bad = 0;
     const int q0 = t.start >> 2, q1 = (t.start + t.count + 3) >> 2;
     const float4* px = reinterpret_cast<const float4*>(s.px);
     const float4* py = reinterpret_cast<const float4*>(s.py);
@@ -323,22 +407,9 @@ __global__ void __launch_bounds__(kThreads, 2)
         for (int k = 0; k < 4; ++k) {
             if (4 * i4 + k >= fl.n) break;
             const float wf = comp(W, k);
-            bad |= weight_bad(wf) ? 1 : 0;
-            tfx += weight_bad(wf) ? 0ull : weight_fx(wf);
             est_add(acc, wf, comp(X, k), comp(Y, k), comp(Z, k), comp(QW, k),
                     comp(QX, k), comp(QY, k), comp(QZ, k));
         }
-    }
-    // integer total and bad flag of the tile
-    __shared__ unsigned long long s_u[kThreads / 32];
-    const unsigned long long u = warp_sum_u64(tfx);
-    if ((threadIdx.x & 31) == 0) s_u[threadIdx.x >> 5] = u;
-    const int any_bad = __syncthreads_or(bad);
-    if (threadIdx.x == 0) {
-        unsigned long long tot = 0;
-        for (int k = 0; k < kThreads / 32; ++k) tot += s_u[k];
-        eupart[2 * (size_t)(fl.etile0 + t.local)] = tot;
-        eupart[2 * (size_t)(fl.etile0 + t.local) + 1] = any_bad ? 1ull : 0ull;
     }
     if (!tile_partial<kEstN>(acc, epart + (size_t)(fl.etile0 + t.local) * kEstN,
                              &c->done_e, fl.netiles))
@@ -346,11 +417,6 @@ __global__ void __launch_bounds__(kThreads, 2)
     __shared__ double s_out[kEstN];
     tiles_combine<kEstN>(epart + (size_t)fl.etile0 * kEstN, fl.netiles, s_out);
     if (threadIdx.x == 0) {
-        unsigned long long tot = 0, fb = 0;
-        for (int b = 0; b < fl.netiles; ++b) {
-            tot += __ldcg(&eupart[2 * (size_t)(fl.etile0 + b)]);
-            fb |= __ldcg(&eupart[2 * (size_t)(fl.etile0 + b) + 1]);
-        }
         for (int k = 0; k < kEstN; ++k) c->est[k] = s_out[k];
         c->ess = s_out[13] > 0.0 ? 1.0 / s_out[13] : 0.0;
         double qm[4];
@@ -358,23 +424,18 @@ __global__ void __launch_bounds__(kThreads, 2)
         for (int k = 0; k < 4; ++k) c->qmean[k] = qm[k];
         for (int k = 0; k < 3; ++k) c->cmp[k] = (float)s_out[k];
         for (int k = 0; k < 4; ++k) c->cmq[k] = (float)qm[k];
-        c->w_total_fx = tot;
-        c->w_bad = fb ? 1 : 0;
         if (wmode == WMODE_LL) c->wmode = WMODE_STORED;
         c->done_e = 0u;
     }
 }
 
-// Covariance pass; mode 1: first pass of the cycle (output record + the
-// ESS decision), mode 2: resampled filters only (output record again).
+// Covariance pass and the filter's output record.
 __global__ void __launch_bounds__(kThreads, 2)
     k_b_covs(Arena A, const BFilter* __restrict__ F, const BTile* __restrict__ T,
-             BCtl* C, double* __restrict__ cpart, double* __restrict__ out,
-             int mode) {
+             BCtl* C, double* __restrict__ cpart, double* __restrict__ out) {
     const BTile t = T[blockIdx.x];
     const BFilter& fl = F[t.f];
     BCtl* c = C + t.f;
-    if (mode == 2 && !c->resample_now) return;
     const Planes s = filter_planes(A, c->live, fl.off);
     const int wmode = c->wmode;
     const double M = c->M, S = c->S;
@@ -429,19 +490,10 @@ __global__ void __launch_bounds__(kThreads, 2)
         for (int k = 0; k < 4; ++k) o[PFC_EST_QUAT + k] = c->qmean[k];
         for (int k = 0; k < 6; ++k) o[PFC_EST_POSCOV + k] = s_out[k];
         for (int k = 0; k < 6; ++k) o[PFC_EST_ATTCOV + k] = s_out[6 + k];
-        o[PFC_EST_ESS] = c->ess;
-        if (mode == 1) {
-            // ParticleFilter::update's trigger: ratio > 0 && ess < ratio * N
-            // (crates/pf_core/src/particle_filter.rs:115-117)
-            o[PFC_EST_ESS_PRE] = c->ess;
-            const int go =
-                (fl.ess_ratio > 0.0 && c->ess < fl.ess_ratio * (double)fl.n) ? 1 : 0;
-            c->resample_now = go;
-            c->resampled = 0;
-            o[PFC_EST_RESAMPLED] = 0.0;
-        } else {
-            o[PFC_EST_RESAMPLED] = c->resampled ? 1.0 : 0.0;
-        }
+        // without a resample the record carries the ESS the decision used,
+        // as ParticleFilter::update returns its first estimate
+        o[PFC_EST_ESS] = c->resampled ? c->ess : c->ess_pre;
+        o[PFC_EST_RESAMPLED] = c->resampled ? 1.0 : 0.0;
         c->done_c = 0u;
     }
 }
@@ -811,12 +863,11 @@ int rebuild_est_tiles(BatchHandle* h) {
     return 0;
 }
 
-int launch_est_covs(BatchHandle* h, int second) {
+int launch_est_covs(BatchHandle* h) {
     k_b_est<<<h->n_et, kThreads, 0, h->stream>>>(h->A, h->d_F, h->d_et, h->d_C,
-                                                 h->d_epart, h->d_eupart, second);
+                                                 h->d_epart);
     k_b_covs<<<h->n_et, kThreads, 0, h->stream>>>(h->A, h->d_F, h->d_et, h->d_C,
-                                                  h->d_cpart, h->d_out,
-                                                  second ? 2 : 1);
+                                                  h->d_cpart, h->d_out);
     h->launches += 2;
     PFB_KL();
     return 0;
@@ -829,9 +880,10 @@ int enqueue_cycle(BatchHandle* h) {
     k_b_weight<<<h->n_wt, kThreads, 0, s>>>(h->A, h->d_F, h->d_wt, h->d_C, h->d_cyc,
                                             h->d_obs, h->d_lm, h->d_wpart,
                                             h->use_packed);
-    h->launches += 2;
+    k_b_ess<<<h->n_et, kThreads, 0, s>>>(h->A, h->d_F, h->d_et, h->d_C, h->d_epart,
+                                         h->d_eupart, h->d_out);
+    h->launches += 3;
     PFB_KL();
-    if (launch_est_covs(h, 0)) return -1;
     k_b_resample<<<h->n_rt, kThreads, 0, s>>>(h->A, h->d_F, h->d_rt, h->d_C, h->d_G,
                                               h->d_flags, h->d_vals, h->d_heavy,
                                               h->heavy_cap);
@@ -851,7 +903,7 @@ int enqueue_cycle(BatchHandle* h) {
     k_b_commit<<<ceil_div(h->nf, kThreads), kThreads, 0, s>>>(h->d_C, h->d_G, h->nf);
     h->launches += 1;
     PFB_KL();
-    if (launch_est_covs(h, 1)) return -1;
+    if (launch_est_covs(h)) return -1;
     PFB_CK(cudaMemcpyAsync(h->h_G, h->d_G, sizeof(BGlobal), cudaMemcpyDeviceToHost, s));
     return 0;
 }
@@ -1255,7 +1307,7 @@ int pfc_batch_autotune(void* p, int reps, int* est_tile_out, int* packed_out) {
         *best = 1e30f;
         for (int r = 0; r < reps; ++r) {
             if (cudaEventRecord(e0, h->stream) != cudaSuccess) return -1;
-            if (launch_est_covs(h, 0)) return -1;
+            if (launch_est_covs(h)) return -1;
             if (cudaEventRecord(e1, h->stream) != cudaSuccess) return -1;
             if (cudaEventSynchronize(e1) != cudaSuccess) return -1;
             float ms = 0.f;
