@@ -424,7 +424,8 @@ __device__ __forceinline__ void weight_two(
 }
 
 // Attitude residual of q about qm as a canonical rotation vector
-// (w >= 0, angle = 2 atan2(|v|, w)), in FP64 — the form of
+// (w >= 0, angle = 2 atan2(|v|, w)), in FP64 (a series for angles below about
+// 11 degrees, atan2 above) — the form of
 // src/cuda/pf_kernels.cu:435-447 and crates/pf_core/src/cpu.rs:346-366.
 __device__ __forceinline__ void att_residual(const double qm[4],
                                              const double q[4], double aav[3]) {
@@ -440,15 +441,36 @@ __device__ __forceinline__ void att_residual(const double qm[4],
         dy = -dy;
         dz = -dz;
     }
-    const double hv = sqrt(dx * dx + dy * dy + dz * dz);
-    if (hv > 1e-12) {
-        const double f = 2.0 * atan2(hv, dw) / hv;
-        aav[0] = dx * f;
-        aav[1] = dy * f;
-        aav[2] = dz * f;
-    } else {
+    const double h2 = dx * dx + dy * dy + dz * dz;
+    if (!(h2 > 1e-24)) {  // |v| <= 1e-12: no rotation
         aav[0] = aav[1] = aav[2] = 0.0;
+        return;
     }
+    double f;
+    if (h2 < 0.01 * dw * dw) {
+        // z = |v| / w < 0.1: 2 atan(z) / |v| = (2 / w) atan(z) / z with the
+        // Taylor series of atan(z) / z in u = z^2 (terms to u^8; the
+        // remainder is below u^9 / 19 < 1e-19), which needs neither the
+        // square root nor atan2.
+        const double r = 1.0 / dw;
+        const double u = h2 * r * r;
+        double p = 1.0 / 17.0;
+        p = fma(p, u, -1.0 / 15.0);
+        p = fma(p, u, 1.0 / 13.0);
+        p = fma(p, u, -1.0 / 11.0);
+        p = fma(p, u, 1.0 / 9.0);
+        p = fma(p, u, -1.0 / 7.0);
+        p = fma(p, u, 1.0 / 5.0);
+        p = fma(p, u, -1.0 / 3.0);
+        p = fma(p, u, 1.0);
+        f = 2.0 * r * p;
+    } else {
+        const double hv = sqrt(h2);
+        f = 2.0 * atan2(hv, dw) / hv;
+    }
+    aav[0] = dx * f;
+    aav[1] = dy * f;
+    aav[2] = dz * f;
 }
 
 // Accumulate one particle into the 14 estimate sums of the reference's
