@@ -48,7 +48,8 @@ constexpr int kScanThreads = 256;
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;  // 2048
 static_assert(kScanTile % kPrefixBlock == 0, "tiles start on prefix blocks");
-constexpr int kHeavy = 32;  // longest copy run a scan thread performs
+constexpr int kHeavy = 32;  // longest run whose ancestors a scan thread writes
+constexpr int kStep = 4;    // thresholds stepped before the closed form
 constexpr int kThreads = kBlk;
 
 PlaneSet plane_set(const PfHandle* h) { return {h->planes(0), h->planes(1)}; }
@@ -129,8 +130,9 @@ __global__ void __launch_bounds__(kScanThreads)
     // Ancestor runs.  C_{j0-1} = tile prefix + exclusive offset of this
     // thread.  The end of each run, cnt(C_j), is found by stepping the
     // thresholds from the end of the previous run (one threshold per output
-    // plus one), switching to the closed form once a run exceeds kHeavy
-    // outputs; such runs are filled by the output-parallel expansion.
+    // plus one), switching to the closed form once a run exceeds kStep
+    // outputs (the steps form a serial FP64 chain); runs longer than kHeavy
+    // are filled by the output-parallel expansion.
     uint64_t C = s_warp[warp] + (x - run);
     long long s = (j0 == 0) ? 0 : count_le(C, n, u0, step);
 #pragma unroll 1
@@ -143,8 +145,8 @@ __global__ void __launch_bounds__(kScanThreads)
             e = n;
         } else {
             e = s;
-            while (e < n && e - s <= kHeavy && threshold_fx(e, u0, step) <= C) ++e;
-            if (e - s > kHeavy) e = count_le(C, n, u0, step);
+            while (e < n && e - s < kStep && threshold_fx(e, u0, step) <= C) ++e;
+            if (e - s == kStep) e = count_le(C, n, u0, step);
         }
         if (e - s > kHeavy) {
             push_run(heavy, heavy_cap, &ctl->heavy_count, &ctl->err, (int)j, s, e, 0);
