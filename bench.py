@@ -222,6 +222,9 @@ def reference_arm(args):
 
 # ------------------------------------------------------------ our GPU arm
 
+FP32_OPS_PER_PAIR = 29  # gated Cartesian term with the reference's roundings
+
+
 def profiled_cycles(args):
     return min(args.steps, 100)
 
@@ -711,10 +714,15 @@ def main():
                                f"stream over the {val['profiled_steps']} cycles that "
                                f"continue the timed (graph-launched) cycles' trajectory "
                                f"(direct launches)"},
-        "issue_roofline": {"kernel": "k_weight", "unit": "particle-observation pairs/s",
+        # k_weight's real bound: 29 rounded FP32 operations per particle-
+        # observation pair are required for the reference's bits
+        "issue_roofline": {"kernel": "k_weight", "bound": "fp32 pipe",
+                           "unit": "particle-observation pairs/s",
                            "achieved_pairs_per_s": pair_rate,
                            "fp32_issue_peak_lane_ops_per_s": issue_peak,
                            "lane_ops_per_pair_at_peak": issue_peak / pair_rate,
+                           "required_fp32_ops_per_pair": FP32_OPS_PER_PAIR,
+                           "frac": FP32_OPS_PER_PAIR * pair_rate / issue_peak,
                            "sm_mhz": sm_mhz},
         "kernel_ms_share": {k2: v / tot_k for k2, v in kernel_share.items() if tot_k > 0},
         "clocks": val["clocks"],

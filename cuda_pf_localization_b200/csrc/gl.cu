@@ -400,6 +400,92 @@ int index_bit_width(int n) {
     return b;
 }
 
+// ---------------------------------------------------------- small bottom-k
+// For up to kSelMaxBlocks * kSelTile keys and k <= kSelK: every block sorts
+// kSelTile composite keys in shared memory (bitonic network) and keeps its
+// kSelK smallest, then one block sorts those candidates.  The composite keys
+// are unique (the low word is the index), so the k smallest are those the
+// full radix sort puts first, in the same order: two launches instead of
+// the sort's twelve.
+
+constexpr int kSelTile = 2048;
+constexpr int kSelK = 128;
+constexpr int kSelMaxBlocks = 32;
+
+// Ascending bitonic sort of m (a power of two) keys in shared memory, by the
+// whole block.
+__device__ void bitonic_sort_smem(uint64_t* s, int m) {
+    for (int size = 2; size <= m; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            __syncthreads();
+            for (int t = threadIdx.x; t < m / 2; t += blockDim.x) {
+                const int i = 2 * t - (t & (stride - 1));
+                const int j = i + stride;
+                const bool up = (i & size) == 0;
+                const uint64_t a = s[i], b = s[j];
+                if ((a > b) == up) {
+                    s[i] = b;
+                    s[j] = a;
+                }
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// kFromCaer: keys made from caer[] (index order); else read from keys[].
+template <bool kFromCaer>
+__global__ void __launch_bounds__(kThreads)
+    k_sel_block(const float* __restrict__ caer, const uint64_t* __restrict__ keys,
+                int n, uint64_t* __restrict__ cand) {
+    __shared__ uint64_t s[kSelTile];
+    const int base = blockIdx.x * kSelTile;
+    for (int t = threadIdx.x; t < kSelTile; t += kThreads) {
+        const int i = base + t;
+        uint64_t v = ~0ull;  // after every real key (indices are < 2^32 - 1)
+        if (i < n) v = kFromCaer ? composite_key(caer[i], (uint32_t)i) : keys[i];
+        s[t] = v;
+    }
+    bitonic_sort_smem(s, kSelTile);
+    for (int t = threadIdx.x; t < kSelK; t += kThreads)
+        cand[(size_t)blockIdx.x * kSelK + t] = s[t];
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_sel_merge(const uint64_t* __restrict__ cand, int m_in, int m,
+                uint64_t* __restrict__ out, int k) {
+    __shared__ uint64_t s[kSelMaxBlocks * kSelK];
+    for (int t = threadIdx.x; t < m; t += kThreads) s[t] = t < m_in ? cand[t] : ~0ull;
+    bitonic_sort_smem(s, m);
+    for (int t = threadIdx.x; t < k; t += kThreads) out[t] = s[t];
+}
+
+bool small_select_ok(int n, int k) {
+    return n > 0 && k > 0 && k <= kSelK && n <= kSelMaxBlocks * kSelTile;
+}
+
+// The k smallest composite keys, ascending, in h->d_sel + kSelMaxBlocks *
+// kSelK (needs small_select_ok(n, k)).  From caer[0, n) when keys is null.
+const uint64_t* small_select(GlHandle* h, const float* caer, const uint64_t* keys,
+                             int n, int k) {
+    const int nb = ceil_div(n, kSelTile);
+    uint64_t* cand = h->d_sel;
+    uint64_t* out = h->d_sel + kSelMaxBlocks * kSelK;
+    if (keys)
+        k_sel_block<false><<<nb, kThreads, 0, h->stream>>>(nullptr, keys, n, cand);
+    else
+        k_sel_block<true><<<nb, kThreads, 0, h->stream>>>(caer, nullptr, n, cand);
+    const int m_in = nb * kSelK;
+    int m = 1;
+    while (m < m_in) m <<= 1;
+    k_sel_merge<<<1, kThreads, 0, h->stream>>>(cand, m_in, m, out, k);
+    if (cudaGetLastError() != cudaSuccess) {
+        set_error("pf_b200: bottom-k select launch failed");
+        return nullptr;
+    }
+    return out;
+}
+
 __global__ void k_gather_topk(const uint64_t* __restrict__ keys, int k,
                               const float* __restrict__ hyp,
                               const float* __restrict__ caer, float* out3,
@@ -527,6 +613,13 @@ uint64_t* sort_current(GlHandle* h) {
     return radix_sort_keys(h, h->nh, 0);
 }
 
+// The k smallest (CAER, index) keys of the current CAERs, ascending: the
+// block select when it applies, else the full sort.
+const uint64_t* smallest_current(GlHandle* h, int k) {
+    if (small_select_ok(h->nh, k)) return small_select(h, h->d_caer, nullptr, h->nh, k);
+    return sort_current(h);
+}
+
 int copy_topk(GlHandle* h, const uint64_t* sorted, int k, float* out3k,
               float* caer_k, int* idx_k) {
     k_gather_topk<<<ceil_div(k, kThreads), kThreads, 0, h->stream>>>(
@@ -560,7 +653,7 @@ int gl_topk_exhaustive(GlHandle* h, int nrays, float rmax, float span, int k,
     if (k > h->nh) k = h->nh;
     if (launch_score(h, nrays, rmax, span)) return -1;
     h->caer_valid = true;
-    const uint64_t* sorted = sort_current(h);
+    const uint64_t* sorted = smallest_current(h, k);
     if (!sorted) return -1;
     return copy_topk(h, sorted, k, out3k, caer_k, idx_k);
 }
@@ -588,7 +681,7 @@ int gl_localize_loaded(GlHandle* h, int nrays, float rmax, float ang_span,
     const int saved = h->nh;
     h->nh = seed_n;
     if (launch_score(h, nrays, rmax, ang_span)) return -1;
-    const uint64_t* seed_sorted = sort_current(h);
+    const uint64_t* seed_sorted = smallest_current(h, k);
     h->nh = saved;
     if (!seed_sorted) return -1;
     if (seed_n == nh) {
@@ -617,7 +710,10 @@ int gl_localize_loaded(GlHandle* h, int nrays, float rmax, float ang_span,
     // Sort the survivors (their keys already carry the index).
     PFB_CK(cudaMemcpyAsync(h->d_keys, h->d_cand, sizeof(uint64_t) * (size_t)nc,
                            cudaMemcpyDeviceToDevice, h->stream));
-    const uint64_t* sorted = radix_sort_keys(h, nc, index_bit_width(nh));
+    const int kk2 = std::min(k, nc);
+    const uint64_t* sorted = small_select_ok(nc, kk2)
+                                 ? small_select(h, nullptr, h->d_keys, nc, kk2)
+                                 : radix_sort_keys(h, nc, index_bit_width(nh));
     if (!sorted) return -1;
     h->caer_valid = false;  // pruned CAERs are not computed
     return copy_topk(h, sorted, std::min(k, nc), out3k, caer_k, idx_k);
@@ -688,6 +784,10 @@ void* pfgl_create(int W, int H, float res, float ox, float oy,
         if (cudaMalloc((void**)&h->d_keys_alt, c * sizeof(uint64_t)) !=
             cudaSuccess)
             break;
+        if (cudaMalloc((void**)&h->d_sel,
+                       (size_t)(kSelMaxBlocks + 1) * kSelK * sizeof(uint64_t)) !=
+            cudaSuccess)
+            break;
         if (cudaMalloc((void**)&h->d_cand, c * sizeof(uint64_t)) != cudaSuccess)
             break;
         if (cudaMalloc((void**)&h->d_out, 3 * c * sizeof(float)) != cudaSuccess)
@@ -727,6 +827,7 @@ int pfgl_destroy(void* hv) {
     cudaFree(h->d_outc);
     cudaFree(h->d_outi);
     cudaFree(h->d_cand);
+    cudaFree(h->d_sel);
     cudaFree(h->d_ctl);
     cudaFreeHost(h->h_ctl);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -792,7 +893,7 @@ int pfgl_topk_ex(void* hv, int k, float* out3k, float* caer_k, int* idx_k) {
     GlHandle* h = as_gl(hv);
     if (!h || k <= 0 || h->nh <= 0 || !h->caer_valid) return -1;
     if (k > h->nh) k = h->nh;
-    const uint64_t* sorted = sort_current(h);
+    const uint64_t* sorted = smallest_current(h, k);
     if (!sorted) return -1;
     return copy_topk(h, sorted, k, out3k, caer_k, idx_k);
 }

@@ -207,3 +207,34 @@ def test_start_outside_map_scores_rmax(kernels):
         assert abs(c[2] - (10.0 - d)) < 1e-4
     finally:
         gl.close()
+
+
+@pytest.mark.parametrize("n", [1, 100, 2048, 2049, 20_000, 65_536])
+def test_small_bottom_k_select_equals_full_sort(kernels, n):
+    """pfgl_topk_ex picks the block select for n <= 65536 and k <= 128 and
+    the radix sort otherwise; both must return the same (CAER, index) order,
+    ties included (each hypothesis appears three times, so equal CAERs are
+    common and the lower index must come first)."""
+    g, _, scan, hyp = _scene(seed=9, n_hyp=max(16, (n + 2) // 3 + 16))
+    fed = np.repeat(hyp[: (n + 2) // 3], 3, axis=0)[:n]
+    gl = Gl(kernels, g, 70_000)
+    try:
+        assert kernels.pfgl_set_hyps(gl.h, f32p(np.ascontiguousarray(fed, np.float32)), n) == 0
+        assert kernels.pfgl_score(gl.h, f32p(scan), 360, 10.0, TAU) == 0
+        caer = np.zeros(n, np.float32)
+        assert kernels.pfgl_get_caer(gl.h, f32p(caer)) == 0
+        for k in (1, 7, 64, 128, 129):
+            kk = min(k, n)
+            out = np.zeros(3 * kk, np.float32)
+            cs = np.zeros(kk, np.float32)
+            idx = np.zeros(kk, np.int32)
+            assert kernels.pfgl_topk_ex(gl.h, k, f32p(out), f32p(cs), i32p(idx)) == kk
+            ref = np.zeros(kk, np.int32)
+            assert kernels.pfgl_topk_from_scores(gl.h, f32p(caer), n, kk, i32p(ref)) == kk
+            assert np.array_equal(idx, ref), (n, k)
+            assert np.array_equal(cs, caer[ref])
+            assert np.array_equal(out.reshape(-1, 3), fed[ref].astype(np.float32))
+            # pfgl_topk_from_scores left caller scores in place of the CAERs
+            assert kernels.pfgl_score(gl.h, f32p(scan), 360, 10.0, TAU) == 0
+    finally:
+        gl.close()

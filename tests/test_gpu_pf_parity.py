@@ -147,9 +147,12 @@ def _weighted_state(kernels, n, seed, sr=1.0):
 
 
 # sr = 0.05 m puts (nearly) all weight on one particle: one scan tile then owns
-# every output, the load-imbalance case of the merge-path gather.
+# every output, the load-imbalance case of the ancestor runs.  4M is the
+# largest size of the at-scale workload; beyond 4096 * 1024 particles the
+# weight pass forms its block prefixes without staging them in shared memory.
 @pytest.mark.parametrize("n,sr", [(1, 1.0), (7, 1.0), (4096, 1.0), (4097, 1.0), (50_000, 1.0),
-                                  (1_000_000, 1.0), (1_000_000, 0.05)])
+                                  (1_000_000, 1.0), (1_000_000, 0.05), (4_000_000, 1.0),
+                                  (4_500_000, 0.05)])
 def test_resample_ancestors_bit_exact_vs_spec(kernels, n, sr):
     pf = _weighted_state(kernels, n, 21, sr)
     try:
