@@ -434,7 +434,9 @@ __device__ void bitonic_sort_smem(uint64_t* s, int m) {
 }
 
 // kFromCaer: keys made from caer[] (index order); else read from keys[].
-template <bool kFromCaer>
+// kDroppedLast: a negative CAER marks a hypothesis the pruned scorer dropped;
+// its key sorts after every scored one (high word all ones, then index).
+template <bool kFromCaer, bool kDroppedLast>
 __global__ void __launch_bounds__(kThreads)
     k_sel_block(const float* __restrict__ caer, const uint64_t* __restrict__ keys,
                 int n, uint64_t* __restrict__ cand) {
@@ -443,7 +445,15 @@ __global__ void __launch_bounds__(kThreads)
     for (int t = threadIdx.x; t < kSelTile; t += kThreads) {
         const int i = base + t;
         uint64_t v = ~0ull;  // after every real key (indices are < 2^32 - 1)
-        if (i < n) v = kFromCaer ? composite_key(caer[i], (uint32_t)i) : keys[i];
+        if (i < n) {
+            if (kFromCaer) {
+                const float c = caer[i];
+                v = (kDroppedLast && c < 0.f) ? (0xFFFFFFFFull << 32) | (uint32_t)i
+                                              : composite_key(c, (uint32_t)i);
+            } else {
+                v = keys[i];
+            }
+        }
         s[t] = v;
     }
     bitonic_sort_smem(s, kSelTile);
@@ -466,15 +476,18 @@ bool small_select_ok(int n, int k) {
 
 // The k smallest composite keys, ascending, in h->d_sel + kSelMaxBlocks *
 // kSelK (needs small_select_ok(n, k)).  From caer[0, n) when keys is null.
+// dropped_last: negative CAERs (hypotheses the pruned scorer dropped) last.
 const uint64_t* small_select(GlHandle* h, const float* caer, const uint64_t* keys,
-                             int n, int k) {
+                             int n, int k, bool dropped_last = false) {
     const int nb = ceil_div(n, kSelTile);
     uint64_t* cand = h->d_sel;
     uint64_t* out = h->d_sel + kSelMaxBlocks * kSelK;
     if (keys)
-        k_sel_block<false><<<nb, kThreads, 0, h->stream>>>(nullptr, keys, n, cand);
+        k_sel_block<false, false><<<nb, kThreads, 0, h->stream>>>(nullptr, keys, n, cand);
+    else if (dropped_last)
+        k_sel_block<true, true><<<nb, kThreads, 0, h->stream>>>(caer, nullptr, n, cand);
     else
-        k_sel_block<true><<<nb, kThreads, 0, h->stream>>>(caer, nullptr, n, cand);
+        k_sel_block<true, false><<<nb, kThreads, 0, h->stream>>>(caer, nullptr, n, cand);
     const int m_in = nb * kSelK;
     int m = 1;
     while (m < m_in) m <<= 1;
@@ -671,10 +684,42 @@ int gl_generate(GlHandle* h, int n_pos, int n_yaw, uint64_t seed) {
     return 0;
 }
 
+// Up to 64k hypotheses: a seed batch scored exhaustively, the bound set from
+// its k-th best key on the device, the rest scored by the pruned scorer
+// (dropped ones keep CAER -1), then the k smallest over all of them.  Every
+// hypothesis whose CAER can reach the bottom-k is scored exactly, so the
+// result equals exhaustive scoring; one host synchronisation.
+int localize_small(GlHandle* h, int nrays, float rmax, float ang_span, int k,
+                   float* out3k, float* caer_k, int* idx_k) {
+    const int nh = h->nh;
+    const int seed_n = std::min(nh, std::max(4 * k, 4096));
+    h->nh = seed_n;
+    const int rc = launch_score(h, nrays, rmax, ang_span);
+    h->nh = nh;
+    if (rc) return -1;
+    if (seed_n == nh) {
+        h->caer_valid = true;
+        const uint64_t* sorted = small_select(h, h->d_caer, nullptr, nh, k);
+        if (!sorted) return -1;
+        return copy_topk(h, sorted, k, out3k, caer_k, idx_k);
+    }
+    const uint64_t* seed_sorted = small_select(h, h->d_caer, nullptr, seed_n, k);
+    if (!seed_sorted) return -1;
+    k_set_tau<<<1, 1, 0, h->stream>>>(seed_sorted, k, h->d_ctl);
+    PFB_KL();
+    if (launch_score_pruned(h, seed_n, nh, nrays, rmax, ang_span)) return -1;
+    const uint64_t* sorted = small_select(h, h->d_caer, nullptr, nh, k, true);
+    if (!sorted) return -1;
+    h->caer_valid = false;  // dropped hypotheses have no CAER
+    return copy_topk(h, sorted, k, out3k, caer_k, idx_k);
+}
+
 int gl_localize_loaded(GlHandle* h, int nrays, float rmax, float ang_span,
                        int k, float* out3k, float* caer_k, int* idx_k) {
     if (h->nh <= 0 || k <= 0) return -1;
     if (k > h->nh) k = h->nh;
+    if (small_select_ok(h->nh, k))
+        return localize_small(h, nrays, rmax, ang_span, k, out3k, caer_k, idx_k);
     const int nh = h->nh;
     // Seed batch scored exhaustively, then pruned chunks.
     const int seed_n = std::min(nh, std::max(4 * k, 8192));

@@ -1012,10 +1012,7 @@ int learned_pass(LpHandle* h, int nrays, float rmax, float span, int n_samples,
     PFB_KL();
     g->nh = n_samples;
     g->caer_valid = false;
-    // Small hypothesis sets: one exhaustive scoring pass and one bottom-k
-    // (one host synchronisation); large ones go through the pruned localizer.
-    if (n_samples <= 65536)
-        return gl_topk_exhaustive(g, nrays, rmax, span, k, out3k, caer_k, idx_k);
+    // the pruned localizer (one host synchronisation up to 64k samples)
     return gl_localize_loaded(g, nrays, rmax, span, k, out3k, caer_k, idx_k);
 }
 
