@@ -187,7 +187,7 @@ int flush_predict(PfHandle* h) {
 
 int device_error(PfHandle* h) {
     if (h->h_ctl->err & ERR_SPIN_TIMEOUT) {
-        set_error("pf_b200: device look-back wait timed out");
+        set_error("pf_b200: a device wait timed out");
         return -1;
     }
     return 0;

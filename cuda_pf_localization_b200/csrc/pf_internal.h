@@ -296,8 +296,10 @@ int launch_weight(PfHandle* h, const PredictArgs& pa, const CObservation* d_obs,
 int launch_est_sums(PfHandle* h);
 int launch_covs(PfHandle* h, bool use_args, const float mp[3],
                 const float mq[4], bool cycle_output);
-// Systematic resampling: fixed-point look-back scan, merge-path gather,
-// deterministic injection.  cond_on_ctl: skip unless ctl->resample_now.
+// Systematic resampling: tile scan from the weight pass's fixed-point block
+// prefixes (the pass runs first when the weights changed since), ancestors,
+// long runs, output-parallel gather, deterministic injection.  cond_on_ctl:
+// skip unless ctl->resample_now.
 int launch_resample(PfHandle* h, float inject_ratio, bool cond_on_ctl,
                     bool use_u01, double u01, const CycleArgs* dargs = nullptr);
 // Injection list epoch (32-bit counter, never 0).
