@@ -425,9 +425,18 @@ def run_gl(args):
                     ok_p += dp <= 0.5
                     ok_pt += dp <= 0.5 and dth <= 0.1
                 dt = time.perf_counter() - t0
+                # algorithmic work: DDA cell visits of exhaustive scoring of the
+                # last trial's hypotheses (counted by an untimed replay kernel)
+                visits = lib.pfgl_count_visits(h, 360, span)
+                sps = len(poses) / dt
                 res["uniform"][f"{nh}_{mode}"] = dict(
-                    solves_per_s=len(poses) / dt, success_pos=ok_p / len(poses),
-                    success_pos_yaw=ok_pt / len(poses), trials=len(poses))
+                    solves_per_s=sps, success_pos=ok_p / len(poses),
+                    success_pos_yaw=ok_pt / len(poses), trials=len(poses),
+                    hyps_per_s=nh * sps, dda_visits_per_solve=int(visits),
+                    dda_visits_per_s=visits * sps,
+                    visits_note="exhaustive-scoring visits x solves/s" +
+                                ("" if mode == "abi" else
+                                 " (the pruned scorer visits fewer cells)"))
     finally:
         lib.pfgl_destroy(h)
 

@@ -154,6 +154,7 @@ _KERNEL_SIGS = {
     "pfgl_set_hyps": (c_int, [c_void_p, _fp, c_int]),
     "pfgl_get_hyps": (c_int, [c_void_p, _fp]),
     "pfgl_get_caer": (c_int, [c_void_p, _fp]),
+    "pfgl_count_visits": (C.c_longlong, [c_void_p, c_int, c_float]),
     "pfgl_topk_ex": (c_int, [c_void_p, c_int, _fp, _fp, _ip]),
     "pfgl_topk_from_scores": (c_int, [c_void_p, _fp, c_int, c_int, _ip]),
     "pfgl_localize": (c_int, [c_void_p, _fp, c_int, c_float, c_float, c_int, _fp, _fp, _ip]),

@@ -208,6 +208,43 @@ __global__ void __launch_bounds__(kScoreThreads, 3)
     }
 }
 
+// DDA cell visits of every (hypothesis, ray) pair, one thread each: the
+// scorer's start cell, ray directions and stepping, so the count is exactly
+// the number of cell steps the scorer takes for these hypotheses (the
+// algorithmic work unit of CAER scoring).  Diagnostic, not timed.
+__global__ void __launch_bounds__(kThreads)
+    k_gl_count_visits(GridView gv, const float* __restrict__ hyp, int nh, int nrays,
+                      float span, unsigned long long* total) {
+    const long long t = (long long)blockIdx.x * kThreads + threadIdx.x;
+    unsigned long long steps = 0;
+    if (t < (long long)nh * nrays) {
+        const int h = (int)(t / nrays), r = (int)(t % nrays);
+        int start = 0;
+        float frx = 0.f, fry = 0.f;
+        if (start_cell(gv, hyp[3 * h], hyp[3 * h + 1], start, frx, fry)) {
+            float dx, dy;
+            sincosf(ray_angle(hyp[3 * h + 2], r, nrays, span), &dy, &dx);
+            Ray ray;
+            ray_init(ray, gv.Wp, start, frx, fry, dx, dy, gv.res);
+            do {
+                ray_step(ray, gv.cells);
+                ++steps;
+            } while (ray.v == 0u);
+        }
+    }
+    __shared__ unsigned long long s_w[kWarps];
+    unsigned long long v = steps;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(~0u, v, o);
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long b = 0;
+        for (int k = 0; k < kWarps; ++k) b += s_w[k];
+        atomicAdd(total, b);
+    }
+}
+
 // CAER value of a composite key (inverse of composite_key's high word).
 __device__ __forceinline__ float key_to_float(uint64_t key) {
     const int o = (int)((uint32_t)(key >> 32) ^ 0x80000000u);
@@ -923,6 +960,23 @@ int pfgl_score(void* hv, const float* scan, int nrays, float rmax,
     if (launch_score(h, nrays, rmax, ang_span)) return -1;
     h->caer_valid = true;
     return 0;
+}
+
+long long pfgl_count_visits(void* hv, int nrays, float ang_span) {
+    GlHandle* h = as_gl(hv);
+    if (!h || h->nh <= 0 || nrays <= 0) return -1;
+    const GridView gv = grid_view(h);
+    PFB_CK(cudaMemsetAsync(&h->d_ctl->visits, 0, sizeof(unsigned long long), h->stream));
+    const long long pairs = (long long)h->nh * nrays;
+    k_gl_count_visits<<<(unsigned)((pairs + kThreads - 1) / kThreads), kThreads, 0,
+                        h->stream>>>(gv, h->d_hyp, h->nh, nrays, ang_span,
+                                     &h->d_ctl->visits);
+    PFB_KL();
+    unsigned long long v = 0;
+    PFB_CK(cudaMemcpyAsync(&v, &h->d_ctl->visits, sizeof v, cudaMemcpyDeviceToHost,
+                           h->stream));
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    return (long long)v;
 }
 
 int pfgl_get_caer(void* hv, float* caer) {

@@ -24,6 +24,7 @@ struct GlCtl {
     unsigned long long tau;   // pruning bound on the composite key
     unsigned n_cand;          // survivors appended by the pruned scorer
     unsigned err;
+    unsigned long long visits;  // DDA cell visits counted by pfgl_count_visits
 };
 
 struct GlHandle {

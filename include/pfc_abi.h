@@ -301,6 +301,12 @@ int pfgl_get_hyps(void* h, float* hyp3n);
 /* CAER of every current hypothesis (n floats) from the last pfgl_score. */
 int pfgl_get_caer(void* h, float* caer);
 
+/* DDA cell visits that scoring the current hypotheses with nrays rays over
+ * ang_span takes (the work unit of CAER scoring), counted by a separate,
+ * untimed kernel that replays the scorer's ray stepping; -1 on error.  No
+ * reference counterpart (a measurement aid). */
+long long pfgl_count_visits(void* h, int nrays, float ang_span);
+
 /* Bottom-k with scores and indices: out3k may be NULL; caer_k / idx_k may be
  * NULL.  Returns the count written or -1. */
 int pfgl_topk_ex(void* h, int k, float* out3k, float* caer_k, int* idx_k);

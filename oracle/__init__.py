@@ -316,6 +316,17 @@ def caer(cells, res, origin, scan, span, rmax, hyp3) -> np.ndarray:
     return out
 
 
+def dda_visits(cells, res, origin, hyp3, nrays, span) -> int:
+    """DDA cell steps of every ray of the hypotheses (see orc_dda_visits)."""
+    c, cp = u8(cells)
+    h, w = c.shape
+    hy, hp = f32(np.asarray(hyp3, dtype=np.float32).reshape(-1))
+    fn = lib().orc_dda_visits
+    fn.restype = C.c_longlong
+    return int(fn(w, h, C.c_float(res), C.c_float(origin[0]), C.c_float(origin[1]), cp, hp,
+                  hy.size // 3, nrays, C.c_float(span)))
+
+
 def caer_f32(cells, res, origin, scan, span, rmax, hyp3) -> np.ndarray:
     c, cp = u8(cells)
     h, w = c.shape

@@ -837,6 +837,49 @@ float orc_cast_ray_f32(int W, int H, float res, float ox, float oy,
     return rmax;
 }
 
+// DDA cell steps of every ray of n hypotheses until the first occupied cell
+// or the step that leaves the grid, as the GPU scorer's loop takes them (no
+// range or step limit inside the loop); directions from cos/sin of the f32
+// ray angle.  Hypotheses outside the grid cast no ray.
+long long orc_dda_visits(int W, int H, float res, float ox, float oy,
+                         const unsigned char* cells, const float* hyp3, int n,
+                         int nrays, float span) {
+    long long total = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : total)
+    for (int i = 0; i < n; ++i) {
+        const float px = hyp3[3 * i], py = hyp3[3 * i + 1], th = hyp3[3 * i + 2];
+        const float fx = (px - ox) / res, fy = (py - oy) / res;
+        const int cx0 = (int)std::floor(fx), cy0 = (int)std::floor(fy);
+        if (!(cx0 >= 0 && cy0 >= 0 && cx0 < W && cy0 < H)) continue;
+        for (int r = 0; r < nrays; ++r) {
+            const float a = th + (nrays > 1 ? span * (float)r / (float)(nrays - 1) : 0.f);
+            const float dirx = std::cos(a), diry = std::sin(a);
+            int cx = cx0, cy = cy0;
+            const int sx = dirx > 0 ? 1 : -1, sy = diry > 0 ? 1 : -1;
+            const float adx = std::fabs(dirx), ady = std::fabs(diry);
+            const float tdx = adx > 1e-9f ? res / adx : INFINITY;
+            const float tdy = ady > 1e-9f ? res / ady : INFINITY;
+            const float frx = (px - ox) / res - (float)cx;
+            const float fry = (py - oy) / res - (float)cy;
+            float tmx = adx > 1e-9f ? ((dirx > 0 ? 1.f - frx : frx) * tdx) : INFINITY;
+            float tmy = ady > 1e-9f ? ((diry > 0 ? 1.f - fry : fry) * tdy) : INFINITY;
+            for (;;) {
+                ++total;
+                if (tmx <= tmy) {
+                    tmx += tdx;
+                    cx += sx;
+                } else {
+                    tmy += tdy;
+                    cy += sy;
+                }
+                if (cx < 0 || cy < 0 || cx >= W || cy >= H) break;
+                if (cells[(size_t)cy * W + cx]) break;
+            }
+        }
+    }
+    return total;
+}
+
 // f32 CAER mirror (directions from sinf/cosf of the f32 ray angle).
 void orc_caer_f32(int W, int H, float res, float ox, float oy,
                   const unsigned char* cells, const float* scan, int nrays,

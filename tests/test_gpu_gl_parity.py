@@ -238,3 +238,22 @@ def test_small_bottom_k_select_equals_full_sort(kernels, n):
             assert kernels.pfgl_score(gl.h, f32p(scan), 360, 10.0, TAU) == 0
     finally:
         gl.close()
+
+
+def test_visit_count_matches_oracle_dda(kernels):
+    """pfgl_count_visits replays the scorer's DDA: its count of cell steps
+    agrees with the oracle's f32 DDA.  The oracle takes its ray directions
+    from host cos/sin, which can differ from the device's sincosf in the last
+    bit and so, rarely, send a ray through a different cell; the bar is
+    1e-3 of the total."""
+    g, _, scan, hyp = _scene(seed=13, n_hyp=2000)
+    n = len(hyp)
+    gl = Gl(kernels, g, 4000)
+    try:
+        assert kernels.pfgl_set_hyps(gl.h, f32p(np.ascontiguousarray(hyp, np.float32)), n) == 0
+        got = kernels.pfgl_count_visits(gl.h, 360, TAU)
+        ref = oracle.dda_visits(g, 0.05, (0, 0), hyp, 360, TAU)
+        print(f"\nDDA visits: device {got}, oracle {ref}")
+        assert ref > 0 and abs(got - ref) <= 1e-3 * ref
+    finally:
+        gl.close()
