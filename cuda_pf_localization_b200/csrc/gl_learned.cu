@@ -698,6 +698,46 @@ __global__ void k_query_row(const float* __restrict__ scan, int nrays,
         x[r] = __float2bfloat16_rn(r < nrays ? scan[r] * inv_rmax : 0.0f);
 }
 
+// One row through one layer (a query's forward pass): warp w of the block
+// computes output n = 8 blockIdx + w as the f32 dot product of the bf16
+// weight row n (16-byte loads) with the bf16 input row, then the GEMM
+// epilogue: bf16 relu(acc + bias) for hidden layers, f32 acc + bias for the
+// output layer.  Same arithmetic as the tiled GEMM up to the f32 summation
+// order; eight warps stream 16 KB of weights where a 128-row tcgen05 tile
+// would run almost empty.
+template <bool kRelu>
+__global__ void __launch_bounds__(256)
+    k_gemv_bf16(const bf16* __restrict__ W, const bf16* __restrict__ x,
+                const float* __restrict__ b, int in, int out, bf16* __restrict__ yb,
+                float* __restrict__ yf) {
+    const int n = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (n >= out) return;
+    const uint4* w4 = reinterpret_cast<const uint4*>(W + (size_t)n * in);
+    const uint4* x4 = reinterpret_cast<const uint4*>(x);
+    float acc = 0.f;
+    for (int q = lane; q < in / 8; q += 32) {
+        const uint4 a = __ldg(&w4[q]), c = x4[q];
+        const uint32_t aw[4] = {a.x, a.y, a.z, a.w}, cw[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const float2 fa = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&aw[t]));
+            const float2 fc = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&cw[t]));
+            acc = fmaf(fa.x, fc.x, acc);
+            acc = fmaf(fa.y, fc.y, acc);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(~0u, acc, o);
+    if (lane == 0) {
+        const float v = acc + b[n];
+        if (kRelu)
+            yb[n] = __float2bfloat16_rn(fmaxf(v, 0.0f));
+        else
+            yf[n] = v;
+    }
+}
+
 // n hypotheses from the mixture in Z row 0: component by inverse CDF of
 // softmax(logits), then a diagonal Gaussian draw in (x_n, y_n, c, s); yaw =
 // atan2(s, c).  Sample i uses Philox counters (i, query, 0/1, LP_SAMPLE).
@@ -880,6 +920,24 @@ int forward(LpHandle* h, MapRef x, int rows, bool write_t) {
                               kHid, ep, h->d_err);
 }
 
+// Forward pass of the single query row in Xp row 0 (rows 0 of H[] and Z4).
+int forward_one(LpHandle* h) {
+    cudaStream_t s = h->stream;
+    const bf16* x = h->Xp;
+    for (int l = 0; l < kLayers - 1; ++l) {
+        const Layer& L = h->L[l];
+        k_gemv_bf16<true><<<ceil_div(L.out, 8), 256, 0, s>>>(L.wb, x, L.b, L.in, L.out,
+                                                             h->H[l], nullptr);
+        PFB_KL();
+        x = h->H[l];
+    }
+    const Layer& L = h->L[kLayers - 1];
+    k_gemv_bf16<false><<<ceil_div(L.out, 8), 256, 0, s>>>(L.wb, x, L.b, L.in, L.out,
+                                                          nullptr, h->Z4);
+    PFB_KL();
+    return 0;
+}
+
 // Loss + backward over one batch (after forward); the loss is accumulated
 // into *d_loss_slot.  xt: the transposed input rows (columns = samples); Y:
 // the batch's targets.
@@ -1005,7 +1063,7 @@ int learned_pass(LpHandle* h, int nrays, float rmax, float span, int n_samples,
     GlHandle* g = h->gl;
     k_query_row<<<1, 128, 0, h->stream>>>(g->d_scan, nrays, 1.0f / rmax, h->Xp);
     PFB_KL();
-    if (forward(h, MapRef{&h->tm_Xp, 0, 0}, BM, false)) return -1;
+    if (forward_one(h)) return -1;
     k_lp_sample<<<ceil_div(n_samples, 256), 256, 0, h->stream>>>(
         h->Z4, n_samples, h->seed ^ 0x5DEECE66DULL, h->query_count++, h->cx,
         h->cy, h->sx, h->sy, g->d_hyp);
