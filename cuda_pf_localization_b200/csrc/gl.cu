@@ -448,6 +448,7 @@ int index_bit_width(int n) {
 constexpr int kSelTile = 2048;
 constexpr int kSelK = 128;
 constexpr int kSelMaxBlocks = 32;
+constexpr int kSelThreads = 1024;  // one compare-exchange per thread and phase
 
 // Ascending bitonic sort of m (a power of two) keys in shared memory, by the
 // whole block.
@@ -474,12 +475,12 @@ __device__ void bitonic_sort_smem(uint64_t* s, int m) {
 // kDroppedLast: a negative CAER marks a hypothesis the pruned scorer dropped;
 // its key sorts after every scored one (high word all ones, then index).
 template <bool kFromCaer, bool kDroppedLast>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kSelThreads)
     k_sel_block(const float* __restrict__ caer, const uint64_t* __restrict__ keys,
                 int n, uint64_t* __restrict__ cand) {
     __shared__ uint64_t s[kSelTile];
     const int base = blockIdx.x * kSelTile;
-    for (int t = threadIdx.x; t < kSelTile; t += kThreads) {
+    for (int t = threadIdx.x; t < kSelTile; t += kSelThreads) {
         const int i = base + t;
         uint64_t v = ~0ull;  // after every real key (indices are < 2^32 - 1)
         if (i < n) {
@@ -494,17 +495,17 @@ __global__ void __launch_bounds__(kThreads)
         s[t] = v;
     }
     bitonic_sort_smem(s, kSelTile);
-    for (int t = threadIdx.x; t < kSelK; t += kThreads)
+    for (int t = threadIdx.x; t < kSelK; t += kSelThreads)
         cand[(size_t)blockIdx.x * kSelK + t] = s[t];
 }
 
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kSelThreads)
     k_sel_merge(const uint64_t* __restrict__ cand, int m_in, int m,
                 uint64_t* __restrict__ out, int k) {
     __shared__ uint64_t s[kSelMaxBlocks * kSelK];
-    for (int t = threadIdx.x; t < m; t += kThreads) s[t] = t < m_in ? cand[t] : ~0ull;
+    for (int t = threadIdx.x; t < m; t += kSelThreads) s[t] = t < m_in ? cand[t] : ~0ull;
     bitonic_sort_smem(s, m);
-    for (int t = threadIdx.x; t < k; t += kThreads) out[t] = s[t];
+    for (int t = threadIdx.x; t < k; t += kSelThreads) out[t] = s[t];
 }
 
 bool small_select_ok(int n, int k) {
@@ -520,15 +521,15 @@ const uint64_t* small_select(GlHandle* h, const float* caer, const uint64_t* key
     uint64_t* cand = h->d_sel;
     uint64_t* out = h->d_sel + kSelMaxBlocks * kSelK;
     if (keys)
-        k_sel_block<false, false><<<nb, kThreads, 0, h->stream>>>(nullptr, keys, n, cand);
+        k_sel_block<false, false><<<nb, kSelThreads, 0, h->stream>>>(nullptr, keys, n, cand);
     else if (dropped_last)
-        k_sel_block<true, true><<<nb, kThreads, 0, h->stream>>>(caer, nullptr, n, cand);
+        k_sel_block<true, true><<<nb, kSelThreads, 0, h->stream>>>(caer, nullptr, n, cand);
     else
-        k_sel_block<true, false><<<nb, kThreads, 0, h->stream>>>(caer, nullptr, n, cand);
+        k_sel_block<true, false><<<nb, kSelThreads, 0, h->stream>>>(caer, nullptr, n, cand);
     const int m_in = nb * kSelK;
     int m = 1;
     while (m < m_in) m <<= 1;
-    k_sel_merge<<<1, kThreads, 0, h->stream>>>(cand, m_in, m, out, k);
+    k_sel_merge<<<1, kSelThreads, 0, h->stream>>>(cand, m_in, m, out, k);
     if (cudaGetLastError() != cudaSuccess) {
         set_error("pf_b200: bottom-k select launch failed");
         return nullptr;
