@@ -196,6 +196,7 @@ _KERNEL_SIGS = {
     "pfgl_learned_calibrate": (c_int, [c_void_p, c_int, c_int, c_float, c_float, c_float,
                                        c_int, c_float, c_ulonglong, _fp, _fp]),
     "pfgl_learned_set_threshold": (c_int, [c_void_p, c_float]),
+    "pfgl_learned_set_graph": (c_int, [c_void_p, c_int]),
     "pfgl_learned_gemm": (c_int, [c_int, c_int, c_int, POINTER(C.c_ushort),
                                   POINTER(C.c_ushort), _fp]),
 }
@@ -544,6 +545,9 @@ class LearnedProposal:
                                                  n_samples, quantile, int(seed), fptr(tau),
                                                  fptr(ok)), "calibrate")
         return float(tau[0]), float(ok[0])
+
+    def use_graph(self, on: bool = True):
+        self._ok(self.lib.pfgl_learned_set_graph(self._h, 1 if on else 0), "set_graph")
 
     def set_threshold(self, tau: float):
         self._ok(self.lib.pfgl_learned_set_threshold(self._h, float(tau)), "set_threshold")

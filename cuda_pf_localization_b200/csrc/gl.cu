@@ -726,29 +726,46 @@ int gl_generate(GlHandle* h, int n_pos, int n_yaw, uint64_t seed) {
 // its k-th best key on the device, the rest scored by the pruned scorer
 // (dropped ones keep CAER -1), then the k smallest over all of them.  Every
 // hypothesis whose CAER can reach the bottom-k is scored exactly, so the
-// result equals exhaustive scoring; one host synchronisation.
-int localize_small(GlHandle* h, int nrays, float rmax, float ang_span, int k,
-                   float* out3k, float* caer_k, int* idx_k) {
+// result equals exhaustive scoring.  Enqueued only; localize_small then
+// copies the result with the one host synchronisation.
+const uint64_t* gl_localize_small_keys(GlHandle* h, int nrays, float rmax,
+                                       float ang_span, int k) {
     const int nh = h->nh;
     const int seed_n = std::min(nh, std::max(4 * k, 4096));
     h->nh = seed_n;
     const int rc = launch_score(h, nrays, rmax, ang_span);
     h->nh = nh;
-    if (rc) return -1;
+    if (rc) return nullptr;
     if (seed_n == nh) {
         h->caer_valid = true;
-        const uint64_t* sorted = small_select(h, h->d_caer, nullptr, nh, k);
-        if (!sorted) return -1;
-        return copy_topk(h, sorted, k, out3k, caer_k, idx_k);
+        return small_select(h, h->d_caer, nullptr, nh, k);
     }
     const uint64_t* seed_sorted = small_select(h, h->d_caer, nullptr, seed_n, k);
-    if (!seed_sorted) return -1;
+    if (!seed_sorted) return nullptr;
     k_set_tau<<<1, 1, 0, h->stream>>>(seed_sorted, k, h->d_ctl);
-    PFB_KL();
-    if (launch_score_pruned(h, seed_n, nh, nrays, rmax, ang_span)) return -1;
-    const uint64_t* sorted = small_select(h, h->d_caer, nullptr, nh, k, true);
-    if (!sorted) return -1;
+    if (cudaGetLastError() != cudaSuccess) {
+        set_error("pf_b200: bound launch failed");
+        return nullptr;
+    }
+    if (launch_score_pruned(h, seed_n, nh, nrays, rmax, ang_span)) return nullptr;
     h->caer_valid = false;  // dropped hypotheses have no CAER
+    return small_select(h, h->d_caer, nullptr, nh, k, true);
+}
+
+bool gl_small_select_ok(int n, int k) { return small_select_ok(n, k); }
+
+int gl_gather_topk(GlHandle* h, const uint64_t* sorted, int k) {
+    k_gather_topk<<<ceil_div(k, kThreads), kThreads, 0, h->stream>>>(
+        sorted, k, h->d_hyp, h->d_caer, h->d_out, h->d_outc, h->d_outi);
+    PFB_KL();
+    h->last_k = k;
+    return 0;
+}
+
+int localize_small(GlHandle* h, int nrays, float rmax, float ang_span, int k,
+                   float* out3k, float* caer_k, int* idx_k) {
+    const uint64_t* sorted = gl_localize_small_keys(h, nrays, rmax, ang_span, k);
+    if (!sorted) return -1;
     return copy_topk(h, sorted, k, out3k, caer_k, idx_k);
 }
 

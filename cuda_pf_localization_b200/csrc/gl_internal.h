@@ -179,5 +179,14 @@ int gl_topk_exhaustive(GlHandle* h, int nrays, float rmax, float span, int k,
                        float* out3k, float* caer_k, int* idx_k);
 // Uniform dispersion of n_pos positions x n_yaw yaws into d_hyp.
 int gl_generate(GlHandle* h, int n_pos, int n_yaw, uint64_t seed);
+// The small-set localizer (n <= 65536 hypotheses, k <= 128, see
+// gl_small_select_ok) enqueued without host synchronisation: returns the
+// device buffer that will hold the k smallest (CAER, index) keys, or nullptr.
+const uint64_t* gl_localize_small_keys(GlHandle* h, int nrays, float rmax, float span,
+                                       int k);
+bool gl_small_select_ok(int n, int k);
+// Gathers the poses, CAERs and indices of the k keys into d_out / d_outc /
+// d_outi (asynchronous).
+int gl_gather_topk(GlHandle* h, const uint64_t* sorted, int k);
 
 }  // namespace pfb

@@ -743,7 +743,9 @@ __global__ void __launch_bounds__(256)
 // atan2(s, c).  Sample i uses Philox counters (i, query, 0/1, LP_SAMPLE).
 __global__ void k_lp_sample(const float* __restrict__ Z, int n, uint64_t seed,
                             uint32_t query, float cx, float cy, float sx,
-                            float sy, float* __restrict__ hyp) {
+                            float sy, float* __restrict__ hyp,
+                            const uint32_t* __restrict__ query_dev) {
+    if (query_dev) query = *query_dev;  // graph replay: this query's counter
     __shared__ float s_cum[kComp];
     __shared__ float s_mu[4 * kComp], s_sig[4 * kComp];
     const int t = threadIdx.x;
@@ -845,7 +847,21 @@ struct LpHandle {
     float tau = INFINITY;
     uint32_t query_count = 0;
     float* d_best = nullptr;
+    // a query replayed from a CUDA graph: the query counter in device memory,
+    // the results copied to pinned memory, the graph keyed on the query's
+    // static parameters
+    uint32_t* d_query = nullptr;
+    float* h_res = nullptr;  // 3 kSelKMax poses, kSelKMax CAERs, kSelKMax indices
+    cudaGraph_t q_graph = nullptr;
+    cudaGraphExec_t q_exec = nullptr;
+    int q_n = 0, q_k = 0, q_nrays = 0;
+    float q_rmax = 0.f, q_span = 0.f;
+    const float* q_scan = nullptr;
+    bool q_caer_valid = false;
+    bool q_off = false;  // capture failed once: direct launches from then on
 };
+
+constexpr int kSelKMax = 128;  // largest k of the small-set localizer
 
 LpHandle* as_lp(void* p) { return static_cast<LpHandle*>(p); }
 
@@ -1008,9 +1024,14 @@ int train_one(LpHandle* h, long long row0, float lr, float* d_loss_slot) {
     return adam_update(h, lr);
 }
 
+void drop_query_graph(LpHandle* h);
+
 void free_lp(LpHandle* h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    drop_query_graph(h);
+    cudaFree(h->d_query);
+    if (h->h_res) cudaFreeHost(h->h_res);
     for (int l = 0; l < kLayers; ++l) {
         Layer& L = h->L[l];
         cudaFree(L.w);
@@ -1057,16 +1078,111 @@ long long num_params() {
     return n;
 }
 
+void drop_query_graph(LpHandle* h) {
+    if (h->q_exec) cudaGraphExecDestroy(h->q_exec);
+    if (h->q_graph) cudaGraphDestroy(h->q_graph);
+    h->q_exec = nullptr;
+    h->q_graph = nullptr;
+}
+
+// The kernels of a query up to the gathered bottom-k (asynchronous).  With
+// query_dev the sampling counter is read from device memory.
+int enqueue_query(LpHandle* h, int nrays, float rmax, float span, int n_samples,
+                  int k, const uint32_t* query_dev, const uint64_t** sorted) {
+    GlHandle* g = h->gl;
+    k_query_row<<<1, 128, 0, h->stream>>>(g->d_scan, nrays, 1.0f / rmax, h->Xp);
+    PFB_KL();
+    if (forward_one(h)) return -1;
+    k_lp_sample<<<ceil_div(n_samples, 256), 256, 0, h->stream>>>(
+        h->Z4, n_samples, h->seed ^ 0x5DEECE66DULL, h->query_count, h->cx, h->cy,
+        h->sx, h->sy, g->d_hyp, query_dev);
+    PFB_KL();
+    g->nh = n_samples;
+    g->caer_valid = false;
+    *sorted = gl_localize_small_keys(g, nrays, rmax, span, k);
+    if (!*sorted) return -1;
+    return gl_gather_topk(g, *sorted, k);
+}
+
+// A query of the small-set localizer replayed from a CUDA graph (captured on
+// first use and again when n, k, the ray geometry or the scan buffer change):
+// one launch and one synchronisation instead of about fifteen launches and
+// pageable copies.  Same kernels and arguments as the direct path, so the
+// same results.  Returns -2 when the graph cannot be used.
+int learned_pass_graph(LpHandle* h, int nrays, float rmax, float span, int n_samples,
+                       int k, float* out3k, float* caer_k, int* idx_k) {
+    GlHandle* g = h->gl;
+    if (h->q_off || !h->h_res || !gl_small_select_ok(n_samples, k) || k > kSelKMax)
+        return -2;
+    const bool same = h->q_exec && h->q_n == n_samples && h->q_k == k &&
+                      h->q_nrays == nrays && h->q_rmax == rmax && h->q_span == span &&
+                      h->q_scan == g->d_scan;
+    if (!same) {
+        drop_query_graph(h);
+        if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeRelaxed) !=
+            cudaSuccess) {
+            (void)cudaGetLastError();
+            h->q_off = true;
+            return -2;
+        }
+        const uint64_t* sorted = nullptr;
+        int rc = enqueue_query(h, nrays, rmax, span, n_samples, k, h->d_query, &sorted);
+        if (rc == 0) {
+            const size_t kk = (size_t)k;
+            rc |= cudaMemcpyAsync(h->h_res, g->d_out, sizeof(float) * 3 * kk,
+                                  cudaMemcpyDeviceToHost, h->stream) != cudaSuccess;
+            rc |= cudaMemcpyAsync(h->h_res + 3 * kSelKMax, g->d_outc, sizeof(float) * kk,
+                                  cudaMemcpyDeviceToHost, h->stream) != cudaSuccess;
+            rc |= cudaMemcpyAsync(h->h_res + 4 * kSelKMax, g->d_outi, sizeof(int) * kk,
+                                  cudaMemcpyDeviceToHost, h->stream) != cudaSuccess;
+        }
+        cudaGraph_t gr = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(h->stream, &gr);
+        if (rc || e != cudaSuccess || !gr ||
+            cudaGraphInstantiate(&h->q_exec, gr, 0) != cudaSuccess) {
+            if (gr) cudaGraphDestroy(gr);
+            h->q_exec = nullptr;
+            (void)cudaGetLastError();
+            h->q_off = true;
+            return -2;
+        }
+        h->q_graph = gr;
+        h->q_n = n_samples;
+        h->q_k = k;
+        h->q_nrays = nrays;
+        h->q_rmax = rmax;
+        h->q_span = span;
+        h->q_scan = g->d_scan;
+        h->q_caer_valid = g->caer_valid;
+    }
+    // the counter is staged from pageable memory before the call returns
+    PFB_CK(cudaMemcpyAsync(h->d_query, &h->query_count, sizeof(uint32_t),
+                           cudaMemcpyHostToDevice, h->stream));
+    PFB_CK(cudaGraphLaunch(h->q_exec, h->stream));
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    h->query_count++;
+    g->nh = n_samples;
+    g->caer_valid = h->q_caer_valid;
+    g->last_k = k;
+    if (out3k) memcpy(out3k, h->h_res, sizeof(float) * 3 * (size_t)k);
+    if (caer_k) memcpy(caer_k, h->h_res + 3 * kSelKMax, sizeof(float) * (size_t)k);
+    if (idx_k) memcpy(idx_k, h->h_res + 4 * kSelKMax, sizeof(int) * (size_t)k);
+    return k;
+}
+
 // Localize against the scan already in gl->d_scan with n learned samples.
 int learned_pass(LpHandle* h, int nrays, float rmax, float span, int n_samples,
                  int k, float* out3k, float* caer_k, int* idx_k) {
+    const int rg = learned_pass_graph(h, nrays, rmax, span, n_samples, k, out3k,
+                                      caer_k, idx_k);
+    if (rg != -2) return rg;
     GlHandle* g = h->gl;
     k_query_row<<<1, 128, 0, h->stream>>>(g->d_scan, nrays, 1.0f / rmax, h->Xp);
     PFB_KL();
     if (forward_one(h)) return -1;
     k_lp_sample<<<ceil_div(n_samples, 256), 256, 0, h->stream>>>(
         h->Z4, n_samples, h->seed ^ 0x5DEECE66DULL, h->query_count++, h->cx,
-        h->cy, h->sx, h->sy, g->d_hyp);
+        h->cy, h->sx, h->sy, g->d_hyp, nullptr);
     PFB_KL();
     g->nh = n_samples;
     g->caer_valid = false;
@@ -1144,8 +1260,13 @@ void* pfgl_learned_create(void* glv, int batch, unsigned long long seed) {
             dalloc(&h->XpT, (size_t)batch * kIn) ||
             dalloc(&h->Xp_f, (size_t)batch * kIn) ||
             dalloc(&h->Yp, (size_t)batch * 4) || dalloc(&h->d_err, 1) ||
-            dalloc(&h->d_best, 64))
+            dalloc(&h->d_best, 64) || dalloc(&h->d_query, 1))
             break;
+        if (cudaMallocHost((void**)&h->h_res, sizeof(float) * 5 * kSelKMax) !=
+            cudaSuccess) {
+            h->h_res = nullptr;  // queries then use direct launches
+            (void)cudaGetLastError();
+        }
         if (make_mat(&h->tm_Xp, h->Xp, batch, kIn) ||
             make_mat(&h->tm_XpT, h->XpT, kIn, batch))
             break;
@@ -1433,6 +1554,14 @@ int pfgl_learned_forward(void* p, const float* x, int rows, float* out) {
                              sizeof(float) * kOut, sizeof(float) * kUsedOut, rows,
                              cudaMemcpyDeviceToHost, h->stream));
     return check_err(h);
+}
+
+int pfgl_learned_set_graph(void* p, int on) {
+    LpHandle* h = as_lp(p);
+    if (!h) return -1;
+    h->q_off = on == 0;
+    if (h->q_off) drop_query_graph(h);
+    return 0;
 }
 
 int pfgl_learned_set_threshold(void* p, float tau) {

@@ -478,6 +478,11 @@ int pfgl_learned_calibrate(void* lp, int n_queries, int nrays, float rmax,
                            float quantile, unsigned long long seed,
                            float* tau_out, float* success_out);
 int pfgl_learned_set_threshold(void* lp, float tau);
+
+/* 1 (default): a query of up to 65536 samples and k <= 128 is replayed from a
+ * CUDA graph captured on first use (again when its sizes, ray geometry or
+ * scan buffer change); 0: direct launches.  Both give the same results. */
+int pfgl_learned_set_graph(void* lp, int on);
 /* Plain tcgen05 GEMM D = A * B^T (A: M x K, B: N x K, bf16 bit patterns,
  * row-major; D: M x N f32) for numerics tests.  M, N multiples of 128, K a
  * multiple of 64. */

@@ -169,3 +169,34 @@ def test_learned_proposal_beats_uniform_at_equal_budget(kernels):
     finally:
         lp.close()
         lib.pfgl_destroy(h)
+
+
+def test_learned_query_graph_equals_direct(kernels):
+    """A learned query replayed from its CUDA graph gives the same poses,
+    CAERs and indices as the same query launched kernel by kernel (two
+    proposals with identical weights, seed and query counter), including
+    after a change of sample count and k (re-capture)."""
+    lib, g, h = _gl(seed=21, cap=200_000)
+    lp1 = pkg.LearnedProposal(h, batch=1024, seed=3)
+    lp2 = None
+    try:
+        lp1.make_data(65_536, seed=17)
+        lp1.train(200, lr=1e-3)
+        lp2 = pkg.LearnedProposal(h, batch=1024, seed=3)
+        lp2.set_params(lp1.params())
+        lp2.use_graph(False)
+        rng = np.random.default_rng(5)
+        poses = np.array([sim.free_pose(g, rng) for _ in range(6)], np.float32)
+        scans = pkg.render_scans(h, poses, noise=0.01, seed=99)
+        for n_samples, k in ((20_000, 64), (5_000, 8)):
+            for q in range(len(poses)):
+                a = lp1.localize(scans[q], n_samples=n_samples, n_fallback=0, k=k)
+                b = lp2.localize(scans[q], n_samples=n_samples, n_fallback=0, k=k)
+                for x, y in zip(a[:3], b[:3]):
+                    assert np.array_equal(x, y), (n_samples, k, q)
+                assert a[3] == b[3]
+    finally:
+        if lp2 is not None:
+            lp2.close()
+        lp1.close()
+        lib.pfgl_destroy(h)
