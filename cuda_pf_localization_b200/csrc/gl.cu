@@ -474,10 +474,12 @@ __device__ void bitonic_sort_smem(uint64_t* s, int m) {
 // kFromCaer: keys made from caer[] (index order); else read from keys[].
 // kDroppedLast: a negative CAER marks a hypothesis the pruned scorer dropped;
 // its key sorts after every scored one (high word all ones, then index).
+// n_dev (optional): the key count in device memory, at most n.
 template <bool kFromCaer, bool kDroppedLast>
 __global__ void __launch_bounds__(kSelThreads)
     k_sel_block(const float* __restrict__ caer, const uint64_t* __restrict__ keys,
-                int n, uint64_t* __restrict__ cand) {
+                int n, uint64_t* __restrict__ cand, const unsigned* n_dev) {
+    if (n_dev) n = min(n, (int)min(*n_dev, 0x7FFFFFFFu));
     __shared__ uint64_t s[kSelTile];
     const int base = blockIdx.x * kSelTile;
     for (int t = threadIdx.x; t < kSelTile; t += kSelThreads) {
@@ -521,11 +523,14 @@ const uint64_t* small_select(GlHandle* h, const float* caer, const uint64_t* key
     uint64_t* cand = h->d_sel;
     uint64_t* out = h->d_sel + kSelMaxBlocks * kSelK;
     if (keys)
-        k_sel_block<false, false><<<nb, kSelThreads, 0, h->stream>>>(nullptr, keys, n, cand);
+        k_sel_block<false, false><<<nb, kSelThreads, 0, h->stream>>>(nullptr, keys, n, cand,
+                                                                    nullptr);
     else if (dropped_last)
-        k_sel_block<true, true><<<nb, kSelThreads, 0, h->stream>>>(caer, nullptr, n, cand);
+        k_sel_block<true, true><<<nb, kSelThreads, 0, h->stream>>>(caer, nullptr, n, cand,
+                                                                  nullptr);
     else
-        k_sel_block<true, false><<<nb, kSelThreads, 0, h->stream>>>(caer, nullptr, n, cand);
+        k_sel_block<true, false><<<nb, kSelThreads, 0, h->stream>>>(caer, nullptr, n, cand,
+                                                                   nullptr);
     const int m_in = nb * kSelK;
     int m = 1;
     while (m < m_in) m <<= 1;
@@ -664,6 +669,37 @@ uint64_t* sort_current(GlHandle* h) {
     return radix_sort_keys(h, h->nh, 0);
 }
 
+// Bound tightening between chunks of the pruned scorer: when the candidates
+// (ctl->n_cand keys in cand) fit the block select, their k smallest (best)
+// become the candidate list and the k-th of them the bound.  A hypothesis
+// outside these k has k better ones and cannot reach the final bottom-k,
+// and the new bound is still at least the final k-th best key.
+__global__ void k_tighten(const uint64_t* __restrict__ best, int k,
+                          uint64_t* __restrict__ cand, GlCtl* ctl, unsigned cap) {
+    const unsigned nc = ctl->n_cand;
+    __syncthreads();  // every thread has read n_cand before it changes
+    if (nc > cap || nc < (unsigned)k) return;
+    for (int t = threadIdx.x; t < k; t += blockDim.x) cand[t] = best[t];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ctl->n_cand = (unsigned)k;
+        ctl->tau = best[k - 1];
+    }
+}
+
+int tighten_bound(GlHandle* h, int k) {
+    const int cap = kSelMaxBlocks * kSelTile;
+    uint64_t* cand = h->d_sel;
+    uint64_t* out = h->d_sel + kSelMaxBlocks * kSelK;
+    k_sel_block<false, false><<<kSelMaxBlocks, kSelThreads, 0, h->stream>>>(
+        nullptr, h->d_cand, cap, cand, &h->d_ctl->n_cand);
+    k_sel_merge<<<1, kSelThreads, 0, h->stream>>>(cand, kSelMaxBlocks * kSelK,
+                                                  kSelMaxBlocks * kSelK, out, k);
+    k_tighten<<<1, 128, 0, h->stream>>>(out, k, h->d_cand, h->d_ctl, (unsigned)cap);
+    PFB_KL();
+    return 0;
+}
+
 // The k smallest (CAER, index) keys of the current CAERs, ascending: the
 // block select when it applies, else the full sort.
 const uint64_t* smallest_current(GlHandle* h, int k) {
@@ -797,8 +833,14 @@ int gl_localize_loaded(GlHandle* h, int nrays, float rmax, float ang_span,
     unsigned kk = (unsigned)k;
     PFB_CK(cudaMemcpyAsync(&h->d_ctl->n_cand, &kk, sizeof(unsigned),
                            cudaMemcpyHostToDevice, h->stream));
-    PFB_CK(cudaStreamSynchronize(h->stream));
-    if (launch_score_pruned(h, seed_n, nh, nrays, rmax, ang_span)) return -1;
+    // Chunks of the rest; between chunks the bound is tightened to the k-th
+    // best key found so far (on the device, no host synchronisation).
+    const int chunk = std::max(65536, ceil_div(nh - seed_n, 8));
+    for (int c0 = seed_n; c0 < nh; c0 += chunk) {
+        const int c1 = std::min(nh, c0 + chunk);
+        if (launch_score_pruned(h, c0, c1, nrays, rmax, ang_span)) return -1;
+        if (c1 < nh && k <= kSelK && tighten_bound(h, k)) return -1;
+    }
     PFB_CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(GlCtl),
                            cudaMemcpyDeviceToHost, h->stream));
     PFB_CK(cudaStreamSynchronize(h->stream));
