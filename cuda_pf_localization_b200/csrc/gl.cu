@@ -835,7 +835,7 @@ int gl_localize_loaded(GlHandle* h, int nrays, float rmax, float ang_span,
                            cudaMemcpyHostToDevice, h->stream));
     // Chunks of the rest; between chunks the bound is tightened to the k-th
     // best key found so far (on the device, no host synchronisation).
-    const int chunk = std::max(65536, ceil_div(nh - seed_n, 8));
+    const int chunk = std::max(131072, ceil_div(nh - seed_n, 4));
     for (int c0 = seed_n; c0 < nh; c0 += chunk) {
         const int c1 = std::min(nh, c0 + chunk);
         if (launch_score_pruned(h, c0, c1, nrays, rmax, ang_span)) return -1;

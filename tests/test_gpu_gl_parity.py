@@ -147,8 +147,9 @@ def test_topk_full_path_and_clamps(kernels):
         gl.close()
 
 
-# 200k and 1M run the pruned scorer in chunks with the bound tightened between
-# them (k <= 128); k = 200 keeps the seed batch's bound throughout.
+# 200k (two chunks) and 1M (four) run the pruned scorer in chunks with the
+# bound tightened between them (k <= 128); k = 200 keeps the seed batch's
+# bound throughout.
 @pytest.mark.parametrize("n_hyp,k", [(20_000, 64), (200_000, 64), (200_000, 10),
                                      (1_000_000, 64), (1_000_000, 200)])
 def test_pruned_localize_equals_exhaustive(kernels, n_hyp, k):
