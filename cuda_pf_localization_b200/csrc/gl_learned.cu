@@ -21,12 +21,13 @@
 // The forward and input-gradient epilogues write their bf16 result in both
 // orientations, so no separate transposes are needed for the next GEMMs.
 //
-// GEMM kernel (sm_100a): one 128 x 128 output tile per CTA, 4-stage TMA ring
-// of 128 x 64 bf16 tiles (128-byte swizzle), one thread issuing
-// tcgen05.mma (128 x 128 x 16, f32 accumulator in 128 TMEM columns), one
-// thread issuing the TMA loads, and all four warps draining TMEM through
-// tcgen05.ld in the fused epilogue.  Every mbarrier wait is bounded; a wait
-// that runs out sets an error word the host turns into -1.
+// GEMM kernel (sm_100a): persistent, one CTA per SM over 128 x BN output
+// tiles (BN = 256 or 128), a 4- or 6-stage TMA ring of 64-element k-slices
+// (128-byte swizzle), one thread issuing tcgen05.mma into two TMEM
+// accumulators in turn, one thread issuing the TMA loads, and four epilogue
+// warps draining the idle accumulator through tcgen05.ld.  Every mbarrier
+// wait is bounded; a wait that runs out sets an error word the host turns
+// into -1.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -69,17 +70,6 @@ constexpr int BM = 128, BK = 64;
 // is 128 x 256).  Per k-block of 64 a 128 x 256 tile moves 48 KiB of
 // operands for 4.2 MFLOP, against 32 KiB for 2.1 MFLOP at 128 x 128: the
 // wider tile needs 30 % fewer operand bytes per flop from L2.
-// Pipeline depth is sized so that two CTAs fit on an SM (96 KiB of operand
-// ring each, 2 x BN <= 512 TMEM columns): one CTA's epilogue then overlaps
-// the other's MMAs.
-template <int BN>
-struct Tile {
-    static constexpr int kStages = BN == 256 ? 2 : 3;
-    static constexpr int kABytes = BM * BK * 2;  // 16 KiB
-    static constexpr int kBBytes = BN * BK * 2;  // 16 or 32 KiB
-    static constexpr int kSmem =
-        kStages * (kABytes + kBBytes) + 1024 + 256 + BN * 4;  // + bias slice
-};
 constexpr uint32_t kWaitLimit = 1u << 24;
 
 enum Epi : int {
@@ -169,123 +159,212 @@ __device__ __forceinline__ void epilogue_chunk(const uint32_t (&r)[32], int row,
     }
 }
 
-// D[M][N] = A[M][K] . B[N][K]^T for one 128 x 128 tile per CTA.  Operand
-// tiles are read through tensor maps at (k0 + k, row0 + tile row).
+// D[M][N] = A[M][K] . B[N][K]^T, persistent and warp-specialised: one CTA
+// per SM walks the output tiles t = blockIdx.x, blockIdx.x + gridDim.x, ...
+// (tile t = split z, row block, column block; column blocks fastest so
+// consecutive tiles share their A rows in L2).
+//   warp 0 (one thread): TMA producer over a PTile<BN>::kStages-deep ring
+//                        that runs on across tile boundaries;
+//   warp 1 (one thread): MMA issuer into one of two TMEM accumulators
+//                        (columns [0, BN) and [BN, 2 BN)), alternating per
+//                        tile;
+//   warps 2-5:           the epilogue of the other accumulator, so tile i's
+//                        epilogue overlaps tile i + 1's MMAs.  Warp w reads
+//                        TMEM lanes [32 (w % 4), 32 (w % 4) + 32), the lane
+//                        quarter its warp may access.
+// Barriers: full/empty per ring stage, acc_full (MMA commit) and acc_empty
+// (one arrival per epilogue warp) per accumulator.  Every wait is bounded
+// and gives up early once another role has failed; the producer then waits
+// for its own loads in flight and the MMA thread for its MMAs before the
+// TMEM is freed.
+template <int BN>
+struct PTile {
+    static constexpr int kStages = BN == 256 ? 4 : 6;
+    static constexpr int kABytes = BM * BK * 2;
+    static constexpr int kBBytes = BN * BK * 2;
+    static constexpr int kRing = kStages * (kABytes + kBBytes);
+    static constexpr int kSmem = kRing + 1024 + 256;  // + alignment, barriers
+};
+constexpr int kPThreads = 192;
+
+struct TileGrid {
+    int tn;      // column blocks (N / BN)
+    int tmn;     // row blocks x column blocks
+    int tiles;   // tmn x splits
+    int splits;
+};
+
 template <int EPI, int BN>
-__global__ void __launch_bounds__(128, 2)
-    k_gemm_bf16(const __grid_constant__ CUtensorMap tmA,
-                const __grid_constant__ CUtensorMap tmB, int K, int a_row0,
-                int a_k0, int b_row0, int b_k0, EpiArgs ep,
-                unsigned* __restrict__ err) {
-    // Split-K: blockIdx.z takes k-blocks [kb0, kb1) and writes its partial
-    // product ep.split_stride elements after the previous split's.
-    constexpr int kStages = Tile<BN>::kStages;
-    constexpr int kABytes = Tile<BN>::kABytes, kBBytes = Tile<BN>::kBBytes;
+__global__ void __launch_bounds__(kPThreads, 1)
+    k_gemm_bf16_ws(const __grid_constant__ CUtensorMap tmA,
+                   const __grid_constant__ CUtensorMap tmB, int K, int a_row0,
+                   int a_k0, int b_row0, int b_k0, TileGrid tg, EpiArgs ep,
+                   unsigned* __restrict__ err) {
+    constexpr int S = PTile<BN>::kStages;
+    constexpr int kABytes = PTile<BN>::kABytes, kBBytes = PTile<BN>::kBBytes;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     const uint32_t s0 = smem_u32(smem_raw);
     unsigned char* base = smem_raw + ((1024u - (s0 & 1023u)) & 1023u);
     unsigned char* sA = base;
-    unsigned char* sB = base + kStages * kABytes;
-    uint64_t* full =
-        reinterpret_cast<uint64_t*>(base + kStages * (kABytes + kBBytes));
-    uint64_t* empty = full + kStages;
-    uint64_t* accb = empty + kStages;
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(accb + 1);
-    float* s_bias = reinterpret_cast<float*>(
-        base + kStages * (kABytes + kBBytes) + 256);  // BN floats
+    unsigned char* sB = base + S * kABytes;
+    uint64_t* full = reinterpret_cast<uint64_t*>(base + PTile<BN>::kRing);
+    uint64_t* empty = full + S;
+    uint64_t* acc_full = empty + S;   // [2]
+    uint64_t* acc_empty = acc_full + 2;  // [2]
+    uint64_t* fin = acc_empty + 2;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(fin + 1);
+    volatile int* abort = reinterpret_cast<volatile int*>(tslot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     const int nkb_all = K / BK;
-    const int kb0 = (int)(((long long)blockIdx.z * nkb_all) / gridDim.z);
-    const int kb1 = (int)(((long long)(blockIdx.z + 1) * nkb_all) / gridDim.z);
-    const int nkb = kb1 - kb0;
-    if (EPI == EPI_F32) ep.out = reinterpret_cast<float*>(ep.out) + (size_t)blockIdx.z * ep.split_stride;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kStages; ++s) {
+        for (int s = 0; s < S; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(accb, 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], 4);
+        }
+        mbar_init(fin, 1);
+        *abort = 0;
         fence_mbar_init();
         tma_prefetch_map(&tmA);
         tma_prefetch_map(&tmB);
     }
-    if (warp == 0) {
-        tmem_alloc(tslot, BN);
+    if (warp == 1) {
+        tmem_alloc(tslot, 2 * BN);
         tmem_relinquish();
     }
-    if (EPI == EPI_RELU_BF16 || EPI == EPI_BIAS_F32)
-        for (int j = threadIdx.x; j < BN; j += 128) s_bias[j] = ep.bias[n0 + j];
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tslot;
 
-    bool fail = false;
     if (warp == 0) {
         if (lane == 0) {  // TMA producer
-            for (int kb = 0; kb < nkb; ++kb) {
-                const int s = kb % kStages;
-                if (kb >= kStages &&
-                    !mbar_wait(&empty[s], ((kb / kStages) - 1) & 1, kWaitLimit)) {
-                    fail = true;
-                    break;
+            uint32_t it = 0;  // k-slices issued so far (all tiles)
+            bool ok = true;
+            for (int t = blockIdx.x; ok && t < tg.tiles; t += gridDim.x) {
+                const int z = t / tg.tmn, r = t - z * tg.tmn;
+                const int m0 = (r / tg.tn) * BM, n0 = (r % tg.tn) * BN;
+                const int kb0 = (int)(((long long)z * nkb_all) / tg.splits);
+                const int kb1 = (int)(((long long)(z + 1) * nkb_all) / tg.splits);
+                for (int kb = kb0; kb < kb1; ++kb, ++it) {
+                    const uint32_t s = it % S, use = it / S;
+                    if (use > 0 &&
+                        !mbar_wait_abort(&empty[s], (use - 1) & 1, kWaitLimit, abort)) {
+                        ok = false;
+                        break;
+                    }
+                    mbar_expect_tx(&full[s], kABytes + kBBytes);
+                    tma_load_2d(sA + s * kABytes, &tmA, &full[s], a_k0 + kb * BK,
+                                a_row0 + m0);
+                    tma_load_2d(sB + s * kBBytes, &tmB, &full[s], b_k0 + kb * BK,
+                                b_row0 + n0);
                 }
-                mbar_expect_tx(&full[s], kABytes + kBBytes);
-                tma_load_2d(sA + s * kABytes, &tmA, &full[s],
-                            a_k0 + (kb0 + kb) * BK, a_row0 + m0);
-                tma_load_2d(sB + s * kBBytes, &tmB, &full[s],
-                            b_k0 + (kb0 + kb) * BK, b_row0 + n0);
+            }
+            if (!ok) {
+                *abort = 1;
+                atomicOr(err, ERR_SPIN_TIMEOUT);
+            }
+            // Wait for the last load issued into each stage (already consumed
+            // on the normal path), so no copy lands after the CTA ends.
+            for (uint32_t s = 0; s < (uint32_t)S && s < it; ++s) {
+                const uint32_t last_use = (it - 1 - s) / S;
+                if (!mbar_wait(&full[s], last_use & 1, kWaitLimit))
+                    atomicOr(err, ERR_SPIN_TIMEOUT);
             }
         }
         __syncwarp();
     } else if (warp == 1) {
         if (lane == 0) {  // MMA issuer
             constexpr uint32_t idesc = idesc_bf16_f32(BM, BN);
-            for (int kb = 0; kb < nkb; ++kb) {
-                const int s = kb % kStages;
-                if (!mbar_wait(&full[s], (kb / kStages) & 1, kWaitLimit)) {
-                    fail = true;
+            uint32_t it = 0;
+            int i = 0;  // tiles of this CTA so far
+            bool ok = true;
+            for (int t = blockIdx.x; ok && t < tg.tiles; t += gridDim.x, ++i) {
+                const int z = t / tg.tmn;
+                const int kb0 = (int)(((long long)z * nkb_all) / tg.splits);
+                const int kb1 = (int)(((long long)(z + 1) * nkb_all) / tg.splits);
+                const int b = i & 1, use = i >> 1;
+                if (use > 0 &&
+                    !mbar_wait_abort(&acc_empty[b], (use - 1) & 1, kWaitLimit, abort)) {
+                    ok = false;
                     break;
                 }
                 tc_fence_after();
-                const uint64_t ad = desc_kmajor_sw128(smem_u32(sA + s * kABytes));
-                const uint64_t bd = desc_kmajor_sw128(smem_u32(sB + s * kBBytes));
+                const uint32_t d = tmem + (uint32_t)(b * BN);
+                for (int kb = kb0; kb < kb1; ++kb, ++it) {
+                    const uint32_t s = it % S;
+                    if (!mbar_wait_abort(&full[s], (it / S) & 1, kWaitLimit, abort)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint64_t ad = desc_kmajor_sw128(smem_u32(sA + s * kABytes));
+                    const uint64_t bd = desc_kmajor_sw128(smem_u32(sB + s * kBBytes));
 #pragma unroll
-                for (int k = 0; k < BK / 16; ++k)
-                    mma_bf16(tmem, ad + 2 * k, bd + 2 * k, idesc,
-                             (kb | k) != 0 ? 1u : 0u);
-                mma_commit(&empty[s]);
+                    for (int k = 0; k < BK / 16; ++k)
+                        mma_bf16(d, ad + 2 * k, bd + 2 * k, idesc,
+                                 (kb != kb0 || k != 0) ? 1u : 0u);
+                    mma_commit(&empty[s]);
+                }
+                if (ok) mma_commit(&acc_full[b]);
             }
-            // Arrives once every MMA issued above has completed (also after a
-            // failed wait, so the epilogue never reads a live accumulator).
-            mma_commit(accb);
+            if (!ok) {
+                *abort = 1;
+                atomicOr(err, ERR_SPIN_TIMEOUT);
+            }
+            // Every MMA issued above has completed once fin's phase 0 ends.
+            mma_commit(fin);
+            if (!mbar_wait(fin, 0, kWaitLimit)) atomicOr(err, ERR_SPIN_TIMEOUT);
         }
         __syncwarp();
-    }
-    if (fail) atomicOr(err, ERR_SPIN_TIMEOUT);
-
-    // Epilogue: warp w drains TMEM lanes [32w, 32w + 32) = tile rows.
-    const bool got = __all_sync(~0u, mbar_wait(accb, 0, kWaitLimit));
-    tc_fence_after();
-    if (!got) {
-        if (lane == 0) atomicOr(err, ERR_SPIN_TIMEOUT);
-    } else {
-        const int row = m0 + warp * 32 + lane;
-        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    } else {  // epilogue warps 2..5
+        const int q = warp & 3;
+        int i = 0;
+        for (int t = blockIdx.x; t < tg.tiles; t += gridDim.x, ++i) {
+            const int z = t / tg.tmn, r = t - z * tg.tmn;
+            const int m0 = (r / tg.tn) * BM, n0 = (r % tg.tn) * BN;
+            const int b = i & 1, use = i >> 1;
+            const bool got = __all_sync(
+                ~0u, mbar_wait_abort(&acc_full[b], use & 1, kWaitLimit, abort));
+            if (!got) {
+                if (lane == 0) {
+                    *abort = 1;
+                    atomicOr(err, ERR_SPIN_TIMEOUT);
+                }
+                break;
+            }
+            tc_fence_after();
+            EpiArgs et = ep;
+            if (EPI == EPI_F32)
+                et.out = reinterpret_cast<float*>(ep.out) + (size_t)z * ep.split_stride;
+            const int row = m0 + q * 32 + lane;
+            const uint32_t trow = tmem + (uint32_t)(b * BN) + ((uint32_t)(q * 32) << 16);
 #pragma unroll 1
-        for (int c = 0; c < BN / 32; ++c) {
-            uint32_t r[32];
-            tmem_ld32(trow + (uint32_t)(c * 32), r);
-            tmem_wait_ld();
-            epilogue_chunk<EPI>(r, row, n0 + c * 32, s_bias + c * 32, ep);
+            for (int c = 0; c < BN / 32; ++c) {
+                uint32_t v[32];
+                tmem_ld32(trow + (uint32_t)(c * 32), v);
+                tmem_wait_ld();
+                if (c == BN / 32 - 1) {  // accumulator drained: hand it back
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&acc_empty[b]);
+                }
+                epilogue_chunk<EPI>(v, row, n0 + c * 32,
+                                    ep.bias ? ep.bias + n0 + c * 32 : nullptr, et);
+            }
         }
     }
     tc_fence_before();
     __syncthreads();
-    if (warp == 0) tmem_dealloc(tmem, BN);
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem, 2 * BN);
+    }
 }
 
 // ------------------------------------------------------------ tensor maps
@@ -359,16 +438,35 @@ struct MapRef {
     int k0;
 };
 
+int sm_count() {
+    static std::once_flag once;
+    static int n = 148;
+    std::call_once(once, [] {
+        int dev = 0, v = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) ==
+                cudaSuccess &&
+            v > 0)
+            n = v;
+    });
+    return n;
+}
+
 template <int EPI, int BN>
 int gemm_bn(cudaStream_t s, MapRef a, MapRef b, int M, int N, int K,
             const EpiArgs& ep, unsigned* err, int splits) {
-    constexpr int smem = Tile<BN>::kSmem;
-    PFB_CK(cudaFuncSetAttribute(k_gemm_bf16<EPI, BN>,
+    constexpr int smem = PTile<BN>::kSmem;
+    PFB_CK(cudaFuncSetAttribute(k_gemm_bf16_ws<EPI, BN>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    const dim3 grid(N / BN, M / BM, splits);
+    TileGrid tg;
+    tg.tn = N / BN;
+    tg.tmn = (M / BM) * tg.tn;
+    tg.tiles = tg.tmn * splits;
+    tg.splits = splits;
+    const int grid = std::min(tg.tiles, sm_count());
     const CUtensorMap& tb = BN == 256 ? b.map->m256 : b.map->m128;
-    k_gemm_bf16<EPI, BN><<<grid, 128, smem, s>>>(a.map->m128, tb, K, a.row0, a.k0,
-                                                 b.row0, b.k0, ep, err);
+    k_gemm_bf16_ws<EPI, BN><<<grid, kPThreads, smem, s>>>(
+        a.map->m128, tb, K, a.row0, a.k0, b.row0, b.k0, tg, ep, err);
     PFB_KL();
     return 0;
 }

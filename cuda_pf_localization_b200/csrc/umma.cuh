@@ -64,6 +64,34 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
     return false;
 }
 
+// As mbar_wait, but also gives up as soon as *abort is nonzero (another role
+// of the CTA has failed), so one failed wait does not leave the others
+// polling until their own limits run out.
+__device__ __forceinline__ bool mbar_wait_abort(uint64_t* bar, uint32_t parity,
+                                                uint32_t limit,
+                                                const volatile int* abort) {
+    const uint32_t a = smem_u32(bar);
+    for (uint32_t it = 0; it < limit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (*abort) return false;
+    }
+    return false;
+}
+
+// One plain arrival on the mbarrier.
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
 // ------------------------------------------------------------------ TMA
 // 2-D tiled load of the box at element coordinates (x = inner, y = row) into
 // shared memory, completing `bytes` on the mbarrier.  x * 2 bytes must be a
