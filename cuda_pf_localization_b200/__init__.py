@@ -157,6 +157,7 @@ _KERNEL_SIGS = {
     "pfgl_count_visits": (C.c_longlong, [c_void_p, c_int, c_float]),
     "pfgl_topk_ex": (c_int, [c_void_p, c_int, _fp, _fp, _ip]),
     "pfgl_topk_from_scores": (c_int, [c_void_p, _fp, c_int, c_int, _ip]),
+    "pfgl_select_from_scores": (c_int, [c_void_p, _fp, c_int, c_int, c_int, _ip]),
     "pfgl_localize": (c_int, [c_void_p, _fp, c_int, c_float, c_float, c_int, _fp, _fp, _ip]),
     "pfgl_cell": (c_int, [c_void_p, c_int, c_int]),
     "pfc_reinit_poses": (c_int, [c_void_p, c_void_p, c_int, c_float, _fp, _fp]),

@@ -438,17 +438,28 @@ int index_bit_width(int n) {
 }
 
 // ---------------------------------------------------------- small bottom-k
-// For up to kSelMaxBlocks * kSelTile keys and k <= kSelK: every block sorts
-// kSelTile composite keys in shared memory (bitonic network) and keeps its
-// kSelK smallest, then one block sorts those candidates.  The composite keys
-// are unique (the low word is the index), so the k smallest are those the
-// full radix sort puts first, in the same order: two launches instead of
-// the sort's twelve.
+// For up to kSelMaxN keys and k <= kSelK, one block finds the k smallest
+// composite keys by radix selection on the key range:
+//   1. min and max of the keys (the max over scored keys only when dropped
+//      hypotheses sort last and at least k are scored);
+//   2. a 1024-bin histogram of (key - lo) >> sh over the current range
+//      [lo, hi], with sh the smallest shift that maps the range onto 1024
+//      bins; the prefix of the counts gives the bin b that holds the
+//      remaining k-th smallest key;
+//   3. when the keys of bins <= b (and those accepted at earlier levels) fit
+//      the 2048-key buffer, they are sorted (bitonic network in shared
+//      memory) and the first k written; otherwise the keys of bins < b are
+//      accepted and the range narrows to bin b (at least 2^9 times smaller,
+//      so at most eight levels: at shift 0 a bin holds one distinct key).
+// The binning is monotone in the key, so the result is the k smallest keys
+// in ascending order exactly, ties of CAER broken by the index word: the
+// order the full radix sort gives, in one launch.
 
-constexpr int kSelTile = 2048;
 constexpr int kSelK = 128;
-constexpr int kSelMaxBlocks = 32;
-constexpr int kSelThreads = 1024;  // one compare-exchange per thread and phase
+constexpr int kSelMaxN = 65536;
+constexpr int kSelThreads = 1024;
+constexpr int kSelBins = 1024;  // one per thread
+constexpr int kSelCap = 2048;   // keys sorted at the end
 
 // Ascending bitonic sort of m (a power of two) keys in shared memory, by the
 // whole block.
@@ -471,70 +482,185 @@ __device__ void bitonic_sort_smem(uint64_t* s, int m) {
     __syncthreads();
 }
 
-// kFromCaer: keys made from caer[] (index order); else read from keys[].
+// kFromCaer: the key of hypothesis i made from caer[i]; else keys[i].
 // kDroppedLast: a negative CAER marks a hypothesis the pruned scorer dropped;
 // its key sorts after every scored one (high word all ones, then index).
-// n_dev (optional): the key count in device memory, at most n.
 template <bool kFromCaer, bool kDroppedLast>
-__global__ void __launch_bounds__(kSelThreads)
-    k_sel_block(const float* __restrict__ caer, const uint64_t* __restrict__ keys,
-                int n, uint64_t* __restrict__ cand, const unsigned* n_dev) {
-    if (n_dev) n = min(n, (int)min(*n_dev, 0x7FFFFFFFu));
-    __shared__ uint64_t s[kSelTile];
-    const int base = blockIdx.x * kSelTile;
-    for (int t = threadIdx.x; t < kSelTile; t += kSelThreads) {
-        const int i = base + t;
-        uint64_t v = ~0ull;  // after every real key (indices are < 2^32 - 1)
-        if (i < n) {
-            if (kFromCaer) {
-                const float c = caer[i];
-                v = (kDroppedLast && c < 0.f) ? (0xFFFFFFFFull << 32) | (uint32_t)i
-                                              : composite_key(c, (uint32_t)i);
-            } else {
-                v = keys[i];
-            }
-        }
-        s[t] = v;
+__device__ __forceinline__ uint64_t sel_key(const float* __restrict__ caer,
+                                            const uint64_t* __restrict__ keys, int i) {
+    if (kFromCaer) {
+        const float c = caer[i];
+        return (kDroppedLast && c < 0.f) ? (0xFFFFFFFFull << 32) | (uint32_t)i
+                                         : composite_key(c, (uint32_t)i);
     }
-    bitonic_sort_smem(s, kSelTile);
-    for (int t = threadIdx.x; t < kSelK; t += kSelThreads)
-        cand[(size_t)blockIdx.x * kSelK + t] = s[t];
+    return keys[i];
 }
 
+// Exclusive prefix of one count per thread over a 1024-thread block.
+__device__ __forceinline__ unsigned block_excl_scan(unsigned v, unsigned* s_w) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(~0u, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_w[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        unsigned t = s_w[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(~0u, t, o);
+            if (lane >= o) t += y;
+        }
+        s_w[lane] = t;
+    }
+    __syncthreads();
+    return (w > 0 ? s_w[w - 1] : 0u) + x - v;
+}
+
+__device__ __forceinline__ uint64_t warp_min_u64(uint64_t v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = min(v, (uint64_t)__shfl_xor_sync(~0u, v, o));
+    return v;
+}
+
+__device__ __forceinline__ uint64_t warp_max_u64(uint64_t v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, (uint64_t)__shfl_xor_sync(~0u, v, o));
+    return v;
+}
+
+// The k smallest of n keys, ascending, into out[0, k) (out[j] = ~0 for
+// j >= n).  n_dev (optional): the key count in device memory, at most n.
+template <bool kFromCaer, bool kDroppedLast>
 __global__ void __launch_bounds__(kSelThreads)
-    k_sel_merge(const uint64_t* __restrict__ cand, int m_in, int m,
-                uint64_t* __restrict__ out, int k) {
-    __shared__ uint64_t s[kSelMaxBlocks * kSelK];
-    for (int t = threadIdx.x; t < m; t += kSelThreads) s[t] = t < m_in ? cand[t] : ~0ull;
-    bitonic_sort_smem(s, m);
-    for (int t = threadIdx.x; t < k; t += kSelThreads) out[t] = s[t];
+    k_select_small(const float* __restrict__ caer, const uint64_t* __restrict__ keys,
+                   int n, const unsigned* n_dev, int k, uint64_t* __restrict__ out) {
+    __shared__ unsigned s_hist[kSelBins];
+    __shared__ uint64_t s_list[kSelCap];
+    __shared__ uint64_t s_red[3][32];
+    __shared__ unsigned s_w[32], s_nv[32];
+    __shared__ uint64_t s_lo, s_hi;
+    __shared__ unsigned s_b, s_cb, s_hb, s_n;
+    if (n_dev) n = min(n, (int)min(*n_dev, 0x7FFFFFFFu));
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int kk = max(0, min(k, n));
+
+    // 1. key range
+    uint64_t mn = ~0ull, mx = 0, mxv = 0;
+    unsigned nv = 0;
+    for (int i = tid; i < n; i += kSelThreads) {
+        const uint64_t key = sel_key<kFromCaer, kDroppedLast>(caer, keys, i);
+        mn = min(mn, key);
+        mx = max(mx, key);
+        if (!kDroppedLast || (uint32_t)(key >> 32) != 0xFFFFFFFFu) {
+            mxv = max(mxv, key);
+            ++nv;
+        }
+    }
+    mn = warp_min_u64(mn);
+    mx = warp_max_u64(mx);
+    mxv = warp_max_u64(mxv);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) nv += __shfl_xor_sync(~0u, nv, o);
+    if (lane == 0) {
+        s_red[0][w] = mn;
+        s_red[1][w] = mx;
+        s_red[2][w] = mxv;
+        s_nv[w] = nv;
+    }
+    __syncthreads();
+    if (w == 0) {
+        mn = warp_min_u64(s_red[0][lane]);
+        mx = warp_max_u64(s_red[1][lane]);
+        mxv = warp_max_u64(s_red[2][lane]);
+        nv = s_nv[lane];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) nv += __shfl_xor_sync(~0u, nv, o);
+        if (lane == 0) {
+            s_lo = mn;
+            s_hi = nv >= (unsigned)kk ? mxv : mx;  // at least kk keys <= s_hi
+        }
+    }
+    __syncthreads();
+
+    // 2. narrow the range until the candidates fit the sort buffer
+    uint64_t lo = s_lo, hi = s_hi;
+    unsigned krem = (unsigned)kk, acc_n = 0, m = 0;
+    bool done = kk == 0;
+    for (int level = 0; level < 10 && !done; ++level) {
+        const uint64_t range = hi - lo;
+        const int sh = range < (uint64_t)kSelBins ? 0 : 54 - __clzll((long long)range);
+        s_hist[tid] = 0u;
+        __syncthreads();
+        for (int i = tid; i < n; i += kSelThreads) {
+            const uint64_t key = sel_key<kFromCaer, kDroppedLast>(caer, keys, i);
+            if (key >= lo && key <= hi) atomicAdd(&s_hist[(unsigned)((key - lo) >> sh)], 1u);
+        }
+        __syncthreads();
+        const unsigned hc = s_hist[tid];
+        const unsigned cb = block_excl_scan(hc, s_w);
+        if (cb < krem && krem <= cb + hc) {  // exactly one bin
+            s_b = (unsigned)tid;
+            s_cb = cb;
+            s_hb = hc;
+        }
+        if (tid == 0) s_n = acc_n;
+        __syncthreads();
+        const unsigned b = s_b, cbb = s_cb, hb = s_hb;
+        const bool last = acc_n + cbb + hb <= (unsigned)kSelCap;
+        for (int i = tid; i < n; i += kSelThreads) {
+            const uint64_t key = sel_key<kFromCaer, kDroppedLast>(caer, keys, i);
+            if (key >= lo && key <= hi) {
+                const unsigned bin = (unsigned)((key - lo) >> sh);
+                if (bin < b || (last && bin == b)) s_list[atomicAdd(&s_n, 1u)] = key;
+            }
+        }
+        __syncthreads();
+        if (last) {
+            m = acc_n + cbb + hb;
+            done = true;
+        } else {  // sh > 0 here: a bin of one key would have fitted
+            acc_n += cbb;
+            krem -= cbb;
+            lo += (uint64_t)b << sh;
+            const uint64_t top = lo + (((uint64_t)1 << sh) - 1);  // end of bin b
+            if (top >= lo) hi = min(hi, top);  // else it wrapped: hi stays
+        }
+    }
+
+    // 3. sort the candidates and write the first k
+    int p = 2;
+    while (p < (int)m) p <<= 1;
+    for (int t = (int)m + tid; t < p; t += kSelThreads) s_list[t] = ~0ull;
+    bitonic_sort_smem(s_list, p);
+    for (int t = tid; t < k; t += kSelThreads)
+        out[t] = (done && t < kk) ? s_list[t] : ~0ull;
 }
 
 bool small_select_ok(int n, int k) {
-    return n > 0 && k > 0 && k <= kSelK && n <= kSelMaxBlocks * kSelTile;
+    return n > 0 && k > 0 && k <= kSelK && n <= kSelMaxN;
 }
 
-// The k smallest composite keys, ascending, in h->d_sel + kSelMaxBlocks *
-// kSelK (needs small_select_ok(n, k)).  From caer[0, n) when keys is null.
+// The k smallest composite keys, ascending, in h->d_sel (needs
+// small_select_ok(n, k)).  From caer[0, n) when keys is null.
 // dropped_last: negative CAERs (hypotheses the pruned scorer dropped) last.
+// n_dev: the key count in device memory (at most n), for keys only.
 const uint64_t* small_select(GlHandle* h, const float* caer, const uint64_t* keys,
-                             int n, int k, bool dropped_last = false) {
-    const int nb = ceil_div(n, kSelTile);
-    uint64_t* cand = h->d_sel;
-    uint64_t* out = h->d_sel + kSelMaxBlocks * kSelK;
+                             int n, int k, bool dropped_last = false,
+                             const unsigned* n_dev = nullptr) {
+    uint64_t* out = h->d_sel;
     if (keys)
-        k_sel_block<false, false><<<nb, kSelThreads, 0, h->stream>>>(nullptr, keys, n, cand,
-                                                                    nullptr);
+        k_select_small<false, false><<<1, kSelThreads, 0, h->stream>>>(nullptr, keys, n,
+                                                                      n_dev, k, out);
     else if (dropped_last)
-        k_sel_block<true, true><<<nb, kSelThreads, 0, h->stream>>>(caer, nullptr, n, cand,
-                                                                  nullptr);
+        k_select_small<true, true><<<1, kSelThreads, 0, h->stream>>>(caer, nullptr, n,
+                                                                    nullptr, k, out);
     else
-        k_sel_block<true, false><<<nb, kSelThreads, 0, h->stream>>>(caer, nullptr, n, cand,
-                                                                   nullptr);
-    const int m_in = nb * kSelK;
-    int m = 1;
-    while (m < m_in) m <<= 1;
-    k_sel_merge<<<1, kSelThreads, 0, h->stream>>>(cand, m_in, m, out, k);
+        k_select_small<true, false><<<1, kSelThreads, 0, h->stream>>>(caer, nullptr, n,
+                                                                     nullptr, k, out);
     if (cudaGetLastError() != cudaSuccess) {
         set_error("pf_b200: bottom-k select launch failed");
         return nullptr;
@@ -556,10 +682,16 @@ __global__ void k_gather_topk(const uint64_t* __restrict__ keys, int k,
     outi[j] = src;
 }
 
-// k-th smallest key of a sorted array -> pruning bound.
-__global__ void k_set_tau(const uint64_t* sorted, int k, GlCtl* ctl) {
-    ctl->tau = sorted[k - 1];
-    ctl->n_cand = 0;
+// Start of the pruned passes: the k smallest keys of the seed batch (sorted)
+// become the first k candidates and the k-th of them the pruning bound; the
+// pruned scorer appends its survivors after them.
+__global__ void k_seed_cand(const uint64_t* __restrict__ sorted, int k,
+                            uint64_t* __restrict__ cand, GlCtl* ctl) {
+    for (int t = threadIdx.x; t < k; t += blockDim.x) cand[t] = sorted[t];
+    if (threadIdx.x == 0) {
+        ctl->tau = sorted[k - 1];
+        ctl->n_cand = (unsigned)k;
+    }
 }
 
 // ------------------------------------------------------------ host helpers
@@ -688,14 +820,11 @@ __global__ void k_tighten(const uint64_t* __restrict__ best, int k,
 }
 
 int tighten_bound(GlHandle* h, int k) {
-    const int cap = kSelMaxBlocks * kSelTile;
-    uint64_t* cand = h->d_sel;
-    uint64_t* out = h->d_sel + kSelMaxBlocks * kSelK;
-    k_sel_block<false, false><<<kSelMaxBlocks, kSelThreads, 0, h->stream>>>(
-        nullptr, h->d_cand, cap, cand, &h->d_ctl->n_cand);
-    k_sel_merge<<<1, kSelThreads, 0, h->stream>>>(cand, kSelMaxBlocks * kSelK,
-                                                  kSelMaxBlocks * kSelK, out, k);
-    k_tighten<<<1, 128, 0, h->stream>>>(out, k, h->d_cand, h->d_ctl, (unsigned)cap);
+    const int cap = std::min(kSelMaxN, h->cap_hyp);
+    const uint64_t* best = small_select(h, nullptr, h->d_cand, cap, k, false,
+                                        &h->d_ctl->n_cand);
+    if (!best) return -1;
+    k_tighten<<<1, 128, 0, h->stream>>>(best, k, h->d_cand, h->d_ctl, (unsigned)cap);
     PFB_KL();
     return 0;
 }
@@ -760,9 +889,11 @@ int gl_generate(GlHandle* h, int n_pos, int n_yaw, uint64_t seed) {
 
 // Up to 64k hypotheses: a seed batch scored exhaustively, the bound set from
 // its k-th best key on the device, the rest scored by the pruned scorer
-// (dropped ones keep CAER -1), then the k smallest over all of them.  Every
-// hypothesis whose CAER can reach the bottom-k is scored exactly, so the
-// result equals exhaustive scoring.  Enqueued only; localize_small then
+// (dropped ones keep CAER -1), then the k smallest of the candidates: the
+// seed's k best and the pruned scorer's survivors (key <= bound).  Every
+// hypothesis whose CAER can reach the bottom-k is scored exactly and is a
+// candidate (a hypothesis above the bound has the seed's k better ones), so
+// the result equals exhaustive scoring.  Enqueued only; localize_small then
 // copies the result with the one host synchronisation.
 const uint64_t* gl_localize_small_keys(GlHandle* h, int nrays, float rmax,
                                        float ang_span, int k) {
@@ -778,14 +909,15 @@ const uint64_t* gl_localize_small_keys(GlHandle* h, int nrays, float rmax,
     }
     const uint64_t* seed_sorted = small_select(h, h->d_caer, nullptr, seed_n, k);
     if (!seed_sorted) return nullptr;
-    k_set_tau<<<1, 1, 0, h->stream>>>(seed_sorted, k, h->d_ctl);
+    k_seed_cand<<<1, kSelK, 0, h->stream>>>(seed_sorted, k, h->d_cand, h->d_ctl);
     if (cudaGetLastError() != cudaSuccess) {
         set_error("pf_b200: bound launch failed");
         return nullptr;
     }
     if (launch_score_pruned(h, seed_n, nh, nrays, rmax, ang_span)) return nullptr;
     h->caer_valid = false;  // dropped hypotheses have no CAER
-    return small_select(h, h->d_caer, nullptr, nh, k, true);
+    // at most k + (nh - seed_n) <= nh candidates
+    return small_select(h, nullptr, h->d_cand, nh, k, false, &h->d_ctl->n_cand);
 }
 
 bool gl_small_select_ok(int n, int k) { return small_select_ok(n, k); }
@@ -826,13 +958,8 @@ int gl_localize_loaded(GlHandle* h, int nrays, float rmax, float ang_span,
     }
     // Pruning bound = k-th best key of the seed batch; candidates start with
     // the seed batch's best k.
-    k_set_tau<<<1, 1, 0, h->stream>>>(seed_sorted, k, h->d_ctl);
+    k_seed_cand<<<1, kSelK, 0, h->stream>>>(seed_sorted, k, h->d_cand, h->d_ctl);
     PFB_KL();
-    PFB_CK(cudaMemcpyAsync(h->d_cand, seed_sorted, sizeof(uint64_t) * (size_t)k,
-                           cudaMemcpyDeviceToDevice, h->stream));
-    unsigned kk = (unsigned)k;
-    PFB_CK(cudaMemcpyAsync(&h->d_ctl->n_cand, &kk, sizeof(unsigned),
-                           cudaMemcpyHostToDevice, h->stream));
     // Chunks of the rest; between chunks the bound is tightened to the k-th
     // best key found so far (on the device, no host synchronisation).
     const int chunk = std::max(131072, ceil_div(nh - seed_n, 4));
@@ -926,8 +1053,7 @@ void* pfgl_create(int W, int H, float res, float ox, float oy,
         if (cudaMalloc((void**)&h->d_keys_alt, c * sizeof(uint64_t)) !=
             cudaSuccess)
             break;
-        if (cudaMalloc((void**)&h->d_sel,
-                       (size_t)(kSelMaxBlocks + 1) * kSelK * sizeof(uint64_t)) !=
+        if (cudaMalloc((void**)&h->d_sel, (size_t)kSelK * sizeof(uint64_t)) !=
             cudaSuccess)
             break;
         if (cudaMalloc((void**)&h->d_cand, c * sizeof(uint64_t)) != cudaSuccess)
@@ -1074,6 +1200,29 @@ int pfgl_topk_from_scores(void* hv, const float* caer, int n, int k,
         h->d_caer, n, h->d_keys);
     PFB_KL();
     const uint64_t* sorted = radix_sort_keys(h, n, 0);
+    if (!sorted) return -1;
+    std::vector<uint64_t> keys((size_t)k);
+    PFB_CK(cudaMemcpyAsync(keys.data(), sorted, sizeof(uint64_t) * (size_t)k,
+                           cudaMemcpyDeviceToHost, h->stream));
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    for (int j = 0; j < k; ++j) idx_out[j] = (int)(uint32_t)keys[(size_t)j];
+    h->caer_valid = false;  // d_caer now holds caller scores
+    return k;
+}
+
+int pfgl_select_from_scores(void* hv, const float* caer, int n, int k,
+                            int dropped_last, int* idx_out) {
+    GlHandle* h = as_gl(hv);
+    if (!h || !caer || !idx_out || n <= 0 || k <= 0 || n > h->cap_hyp) return -1;
+    if (k > n) k = n;
+    if (!small_select_ok(n, k)) {
+        set_error("pf_b200: pfgl_select_from_scores: needs n <= %d and k <= %d",
+                  kSelMaxN, kSelK);
+        return -1;
+    }
+    PFB_CK(cudaMemcpyAsync(h->d_caer, caer, sizeof(float) * (size_t)n,
+                           cudaMemcpyHostToDevice, h->stream));
+    const uint64_t* sorted = small_select(h, h->d_caer, nullptr, n, k, dropped_last != 0);
     if (!sorted) return -1;
     std::vector<uint64_t> keys((size_t)k);
     PFB_CK(cudaMemcpyAsync(keys.data(), sorted, sizeof(uint64_t) * (size_t)k,

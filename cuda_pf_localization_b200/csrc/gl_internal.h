@@ -49,7 +49,7 @@ struct GlHandle {
     float* d_outc = nullptr;  // k CAER
     int* d_outi = nullptr;    // k indices
     uint64_t* d_cand = nullptr;  // pruned-scorer survivors (cap_hyp)
-    uint64_t* d_sel = nullptr;   // small bottom-k select: candidates + result
+    uint64_t* d_sel = nullptr;   // small bottom-k select: the k smallest keys
     GlCtl* d_ctl = nullptr;
     GlCtl* h_ctl = nullptr;
     std::vector<unsigned char> host_grid;  // unpadded 0/1 copy

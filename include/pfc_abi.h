@@ -316,6 +316,15 @@ int pfgl_topk_ex(void* h, int k, float* out3k, float* caer_k, int* idx_k);
 int pfgl_topk_from_scores(void* h, const float* caer, int n, int k,
                           int* idx_out);
 
+/* Bottom-k of caller scores by the one-block radix select that the fused
+ * localizers use (no reference counterpart): n <= 65536 and k <= 128.  Same
+ * order as pfgl_topk_from_scores; when dropped_last is nonzero, negative
+ * scores (hypotheses a pruned pass dropped) sort after every other one, in
+ * index order.  The scores replace the handle's CAERs.  Writes min(k,n)
+ * indices; returns that count or -1. */
+int pfgl_select_from_scores(void* h, const float* caer, int n, int k,
+                            int dropped_last, int* idx_out);
+
 /* Fused global localization over the current hypotheses: raycast + CAER with
  * exact early termination against the running k-th best, and bottom-k
  * selection.  Same results as pfgl_score + pfgl_topk_ex for those k.  CAERs

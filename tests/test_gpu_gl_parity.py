@@ -244,6 +244,56 @@ def test_small_bottom_k_select_equals_full_sort(kernels, n):
         gl.close()
 
 
+def _select_cases(rng, n):
+    """Score arrays that stress the radix select's range narrowing: spread,
+    all equal (ties resolved by the index word alone), two values, 60 decades,
+    infinities, negative scores."""
+    yield "uniform", rng.uniform(50, 3000, n)
+    yield "equal", np.full(n, 7.0)
+    yield "two", rng.choice([1.0, 2.0], n)
+    yield "decades", 10.0 ** rng.uniform(-30, 30, n)
+    c = rng.uniform(0, 1, n)
+    c[::7] = np.inf
+    yield "inf", c
+    yield "signed", rng.normal(0, 100, n)
+
+
+@pytest.mark.parametrize("n", [1, 2, 100, 2048, 2049, 20_000, 65_536])
+def test_select_from_scores_equals_oracle_order(kernels, n):
+    """pfgl_select_from_scores (the one-block radix select of the fused
+    localizers) against the oracle's stable sort of the same scores, with and
+    without dropped (negative) scores sorted last."""
+    g, _, _, _ = _scene(seed=9, n_hyp=16)
+    gl = Gl(kernels, g, 70_000)
+    rng = np.random.default_rng(n)
+    try:
+        for name, c in _select_cases(rng, n):
+            s = np.ascontiguousarray(c, np.float32)
+            for k in (1, 64, 128):
+                kk = min(k, n)
+                got = np.zeros(kk, np.int32)
+                assert kernels.pfgl_select_from_scores(gl.h, f32p(s), n, k, 0, i32p(got)) == kk
+                assert np.array_equal(got, oracle.topk_from_scores(s, k)), (name, n, k)
+        # dropped last: the oracle sees a dropped score as NaN (after +inf)
+        for frac in (0.0, 0.5, 0.97):
+            s = rng.uniform(50, 3000, n).astype(np.float32)
+            s[rng.random(n) < frac] = -1.0
+            if n >= 3:
+                s[: n // 3] = np.where(s[: n // 3] < 0, -1.0, 9.0)  # ties among valid
+            ref_s = np.where(s < 0, np.float32(np.nan), s).astype(np.float32)
+            for k in (1, 64, 128):
+                kk = min(k, n)
+                got = np.zeros(kk, np.int32)
+                assert kernels.pfgl_select_from_scores(gl.h, f32p(s), n, k, 1, i32p(got)) == kk
+                assert np.array_equal(got, oracle.topk_from_scores(ref_s, k)), (frac, n, k)
+        # k above the select's limit of 128 is refused
+        if n >= 129:
+            big = np.zeros(129, np.int32)
+            assert kernels.pfgl_select_from_scores(gl.h, f32p(s), n, 129, 0, i32p(big)) == -1
+    finally:
+        gl.close()
+
+
 def test_visit_count_matches_oracle_dda(kernels):
     """pfgl_count_visits replays the scorer's DDA: its count of cell steps
     agrees with the oracle's f32 DDA.  The oracle takes its ray directions
