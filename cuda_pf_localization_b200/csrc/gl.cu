@@ -78,8 +78,9 @@ __global__ void k_gl_gen(int n, int n_yaw, int nfree, const int2* __restrict__ f
 // CAER of one hypothesis by one warp, with rays handed out dynamically: a
 // lane whose ray has ended takes the next unstarted ray of the hypothesis
 // (restarts are batched until kRestart lanes are free), so the warp is not
-// held by its longest ray.  The ray directions are computed first with all
-// lanes busy; each ray's term |scan - raycast| then replaces its direction in
+// held by its longest ray.  The rays' crossing distances (ray_deltas: the
+// sincos and the divisions) are computed first with all lanes busy, so a
+// restart does neither; each ray's term |scan - raycast| then replaces them in
 // the ray's shared-memory slot, and the total is summed in the fixed
 // lane-sequential order
 // (lane l adds rays l, l + 32, ..., then an xor butterfly), which does not
@@ -111,21 +112,19 @@ __device__ __forceinline__ float warp_caer(const unsigned char* __restrict__ g,
         return warp_sum_f(acc);
     }
     const bool long_rays = gv.Wp + Hp > 8192;
-    // ray directions of this hypothesis, all lanes busy
+    // ray directions of this hypothesis as signed crossing distances, all
+    // lanes busy
     for (int r = lane; r < nrays; r += 32) {
         float dx, dy;
         sincosf(ray_angle(th, r, nrays, span), &dy, &dx);
-        dirs[r] = make_float2(dx, dy);
+        dirs[r] = ray_deltas(dx, dy, gv.res);
     }
     __syncwarp();
     Ray ray;
     int r = lane;
     bool active = r < nrays;
     ray.v = 1u;
-    if (active) {
-        const float2 d = dirs[r];
-        ray_init(ray, gv.Wp, start, frx, fry, d.x, d.y, gv.res);
-    }
+    if (active) ray_init_deltas(ray, gv.Wp, start, frx, fry, dirs[r]);
     float lane_acc = 0.f;
     int next = 32;
     for (;;) {
@@ -143,8 +142,7 @@ __device__ __forceinline__ float warp_caer(const unsigned char* __restrict__ g,
             const int nr = next + __popc(done & lt);
             if (nr < nrays) {
                 r = nr;
-                const float2 d = dirs[r];
-                ray_init(ray, gv.Wp, start, frx, fry, d.x, d.y, gv.res);
+                ray_init_deltas(ray, gv.Wp, start, frx, fry, dirs[r]);
             } else {
                 active = false;
             }

@@ -96,6 +96,33 @@ __device__ __forceinline__ void ray_init(Ray& r, int Wp, int start, float frx,
     r.v = 0u;
 }
 
+// The distances between x and between y cell crossings of a ray, each signed
+// by its step direction (+ for dirx > 0, resp. diry > 0; an axis the ray does
+// not cross holds +-INFINITY): ray_init's divisions, done once per ray ahead
+// of the stepping so that a lane restarting on a new ray does no division.
+__device__ __forceinline__ float2 ray_deltas(float dirx, float diry, float res) {
+    const float adx = fabsf(dirx), ady = fabsf(diry);
+    const float tdx = adx > 1e-9f ? res / adx : INFINITY;
+    const float tdy = ady > 1e-9f ? res / ady : INFINITY;
+    return make_float2(dirx > 0 ? tdx : -tdx, diry > 0 ? tdy : -tdy);
+}
+
+// ray_init from ray_deltas: the same Ray, field for field (res / |dir| is
+// finite exactly when |dir| > 1e-9, and its sign carries dir > 0).
+__device__ __forceinline__ void ray_init_deltas(Ray& r, int Wp, int start, float frx,
+                                                float fry, float2 d) {
+    const bool px = d.x > 0.f, py = d.y > 0.f;
+    r.sx = px ? 1 : -1;
+    r.sy = py ? Wp : -Wp;
+    r.tdx = fabsf(d.x);
+    r.tdy = fabsf(d.y);
+    r.tmx = r.tdx != INFINITY ? ((px ? 1.f - frx : frx) * r.tdx) : INFINITY;
+    r.tmy = r.tdy != INFINITY ? ((py ? 1.f - fry : fry) * r.tdy) : INFINITY;
+    r.idx = start;
+    r.dist = 0.f;
+    r.v = 0u;
+}
+
 __device__ __forceinline__ void ray_step(Ray& r, const unsigned char* __restrict__ g) {
     const bool px = r.tmx <= r.tmy;
     r.dist = px ? r.tmx : r.tmy;
