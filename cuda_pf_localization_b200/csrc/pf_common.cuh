@@ -236,4 +236,33 @@ __host__ __device__ __forceinline__ long long ceil_div_ll(long long a,
     return (a + b - 1) / b;
 }
 
+// ------------------------------------------------- programmatic dependent launch
+// The kernels of a filter cycle are launched with programmatic stream
+// serialisation: a kernel's blocks may be scheduled as soon as every block
+// of its predecessor has exited, before the predecessor grid is retired, and
+// wait at pdl_wait() until the predecessor grid has completed and its memory
+// is visible.  Every such kernel calls pdl_wait() first, before any early
+// return, so completion stays transitive along the chain (a kernel that ended
+// without waiting could finish before the kernel two back).  A no-op for a
+// plain launch.
+__device__ __forceinline__ void pdl_wait() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block,
+                              size_t smem, cudaStream_t stream, Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 }  // namespace pfb

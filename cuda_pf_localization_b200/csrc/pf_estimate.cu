@@ -98,6 +98,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     k_est_sums(PlaneSet ps, int n, const float* __restrict__ ll,
                float* __restrict__ w, double* part, unsigned* done,
                CycleCtl* ctl) {
+    pdl_wait();
     const Planes s = pick_planes(ps, ctl->live);
     const int wmode = ctl->wmode;
     const double M = ctl->ll_max, S = ctl->ll_sumexp;
@@ -158,6 +159,7 @@ __global__ void __launch_bounds__(kThreads, 2)
            const float* __restrict__ w, double* part, unsigned* done,
            CycleCtl* ctl, int use_args, float3 mp_arg, float4 mq_arg,
            int mode) {
+    pdl_wait();
     const Planes s = pick_planes(ps, ctl->live);
     const int wmode = ctl->wmode;
     const double M = ctl->ll_max, S = ctl->ll_sumexp;
@@ -249,6 +251,7 @@ __global__ void __launch_bounds__(kThreads)
     k_ess(int n, const float* __restrict__ ll, float* __restrict__ w,
           double* part, unsigned long long* partu, uint64_t* prefix,
           unsigned* done, CycleCtl* ctl, int decide, double ess_ratio) {
+    pdl_wait();
     static_assert(kPrefixBlock == 4 * kThreads, "one float4 per thread");
     const int wmode = ctl->wmode;
     const double M = ctl->ll_max, S = ctl->ll_sumexp;
@@ -395,8 +398,8 @@ int est_grid(int n) {
 
 int launch_est_sums(PfHandle* h) {
     KernelScope ks(h, KK_EST);
-    k_est_sums<<<est_grid(h->n), kThreads, 0, h->stream>>>(
-        plane_set(h), h->n, h->d_ll, h->d_w, h->d_part, h->d_done + 1, h->d_ctl);
+    PFB_CK(launch_pdl(k_est_sums, est_grid(h->n), kThreads, 0, h->stream, plane_set(h),
+                      h->n, h->d_ll, h->d_w, h->d_part, h->d_done + 1, h->d_ctl));
     PFB_KL();
     return 0;
 }
@@ -408,18 +411,18 @@ int launch_covs(PfHandle* h, bool use_args, const float mp[3],
     float4 b = use_args ? make_float4(mq[0], mq[1], mq[2], mq[3])
                         : make_float4(1.f, 0.f, 0.f, 0.f);
     KernelScope ks(h, KK_COVS);
-    k_covs<<<est_grid(h->n), kThreads, 0, h->stream>>>(
-        plane_set(h), h->n, h->d_ll, h->d_w, h->d_part, h->d_done + 2, h->d_ctl,
-        use_args ? 1 : 0, a, b, cycle_output ? 1 : 0);
+    PFB_CK(launch_pdl(k_covs, est_grid(h->n), kThreads, 0, h->stream, plane_set(h), h->n,
+                      h->d_ll, h->d_w, h->d_part, h->d_done + 2, h->d_ctl,
+                      use_args ? 1 : 0, a, b, cycle_output ? 1 : 0));
     PFB_KL();
     return 0;
 }
 
 int launch_weight_prefix(PfHandle* h, bool decide, double ess_ratio) {
     KernelScope ks(h, KK_EST);
-    k_ess<<<ceil_div(h->n, kPrefixBlock), kThreads, 0, h->stream>>>(
-        h->n, h->d_ll, h->d_w, h->d_part, h->d_part_u64, h->d_wprefix,
-        h->d_done + 3, h->d_ctl, decide ? 1 : 0, ess_ratio);
+    PFB_CK(launch_pdl(k_ess, ceil_div(h->n, kPrefixBlock), kThreads, 0, h->stream, h->n,
+                      h->d_ll, h->d_w, h->d_part, h->d_part_u64, h->d_wprefix,
+                      h->d_done + 3, h->d_ctl, decide ? 1 : 0, ess_ratio));
     PFB_KL();
     h->prefix_valid = true;
     return 0;

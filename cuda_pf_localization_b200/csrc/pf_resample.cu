@@ -59,6 +59,7 @@ __global__ void __launch_bounds__(kScanThreads)
                const uint64_t* __restrict__ prefix, int* __restrict__ anc,
                HeavyRun* heavy, int heavy_cap, CycleCtl* ctl, int cond,
                int use_u01, double u01_arg) {
+    pdl_wait();
     if (cond && !ctl->resample_now) return;
     const uint64_t T = ctl->w_total_fx;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -162,6 +163,7 @@ __global__ void __launch_bounds__(kScanThreads)
 __global__ void __launch_bounds__(kThreads)
     k_expand_runs(const HeavyRun* heavy, int heavy_cap, int* __restrict__ anc,
                   CycleCtl* ctl, int cond) {
+    pdl_wait();
     if (cond && !ctl->resample_now) return;
     if (!ctl->resample_valid) return;
     const int count = min(ctl->heavy_count, heavy_cap);
@@ -177,6 +179,7 @@ __global__ void __launch_bounds__(kThreads)
 __global__ void __launch_bounds__(kThreads)
     k_gather(PlaneSet ps, int n, const int* __restrict__ anc, CycleCtl* ctl,
              int cond) {
+    pdl_wait();
     if (cond && !ctl->resample_now) return;
     if (!ctl->resample_valid) return;
     const int live = ctl->live;
@@ -216,6 +219,7 @@ __global__ void __launch_bounds__(kThreads)
 __global__ void k_inject_link(int n, int k, uint64_t gen, uint64_t* head,
                               int* next, CycleCtl* ctl, int cond,
                               unsigned epoch, const CycleArgs* ca) {
+    pdl_wait();
     if (ca) {
         gen = ca->gen;
         epoch = ca->inj_epoch;
@@ -235,6 +239,7 @@ __global__ void k_inject_apply(PlaneSet ps, int n, int k, uint64_t gen,
                                const uint64_t* head, const int* next,
                                CycleCtl* ctl, int cond, unsigned epoch,
                                const CycleArgs* ca) {
+    pdl_wait();
     if (ca) {
         gen = ca->gen;
         epoch = ca->inj_epoch;
@@ -269,6 +274,7 @@ __global__ void k_inject_apply(PlaneSet ps, int n, int k, uint64_t gen,
 }
 
 __global__ void k_commit(CycleCtl* ctl, int cond) {
+    pdl_wait();
     if (!(cond && !ctl->resample_now)) {
         if (ctl->resample_valid) {
             ctl->live = 1 - ctl->live;
@@ -320,21 +326,21 @@ int launch_resample(PfHandle* h, float inject_ratio, bool cond_on_ctl,
     const int cond = cond_on_ctl ? 1 : 0;
     {
         KernelScope ks(h, KK_SCAN);
-        k_resample<<<ntiles, kScanThreads, 0, h->stream>>>(
-            n, h->d_w, h->d_ll, h->d_wprefix, h->d_anc, h->d_heavy, h->heavy_cap,
-            h->d_ctl, cond, use_u01 ? 1 : 0, u01);
+        PFB_CK(launch_pdl(k_resample, ntiles, kScanThreads, 0, h->stream, n, h->d_w,
+                          h->d_ll, h->d_wprefix, h->d_anc, h->d_heavy, h->heavy_cap,
+                          h->d_ctl, cond, use_u01 ? 1 : 0, u01));
     }
     PFB_KL();
     {
         KernelScope ks(h, KK_SCAN);
-        k_expand_runs<<<2 * 148, kThreads, 0, h->stream>>>(
-            h->d_heavy, h->heavy_cap, h->d_anc, h->d_ctl, cond);
+        PFB_CK(launch_pdl(k_expand_runs, 2 * 148, kThreads, 0, h->stream, h->d_heavy,
+                          h->heavy_cap, h->d_anc, h->d_ctl, cond));
     }
     PFB_KL();
     {
         KernelScope ks(h, KK_GATHER);
-        k_gather<<<ceil_div(n, 4 * kThreads), kThreads, 0, h->stream>>>(
-            plane_set(h), n, h->d_anc, h->d_ctl, cond);
+        PFB_CK(launch_pdl(k_gather, ceil_div(n, 4 * kThreads), kThreads, 0, h->stream,
+                          plane_set(h), n, h->d_anc, h->d_ctl, cond));
     }
     PFB_KL();
     // k = floor(ratio * n) with the reference's f32 product
@@ -346,22 +352,22 @@ int launch_resample(PfHandle* h, float inject_ratio, bool cond_on_ctl,
         const int ig = ceil_div(k, kThreads);
         {
             KernelScope ks(h, KK_INJECT);
-            k_inject_link<<<ig, kThreads, 0, h->stream>>>(
-                n, k, h->gen, h->d_inj_head, h->d_inj_next, h->d_ctl, cond,
-                iepoch, dargs);
+            PFB_CK(launch_pdl(k_inject_link, ig, kThreads, 0, h->stream, n, k, h->gen,
+                              h->d_inj_head, h->d_inj_next, h->d_ctl, cond, iepoch,
+                              dargs));
         }
         PFB_KL();
         {
             KernelScope ks(h, KK_INJECT);
-            k_inject_apply<<<ig, kThreads, 0, h->stream>>>(
-                plane_set(h), n, k, h->gen, h->d_inj_head, h->d_inj_next,
-                h->d_ctl, cond, iepoch, dargs);
+            PFB_CK(launch_pdl(k_inject_apply, ig, kThreads, 0, h->stream, plane_set(h), n,
+                              k, h->gen, h->d_inj_head, h->d_inj_next, h->d_ctl, cond,
+                              iepoch, dargs));
         }
         PFB_KL();
     }
     {
         KernelScope ks(h, KK_COMMIT);
-        k_commit<<<1, 1, 0, h->stream>>>(h->d_ctl, cond);
+        PFB_CK(launch_pdl(k_commit, 1, 1, 0, h->stream, h->d_ctl, cond));
     }
     PFB_KL();
     h->anc_valid = true;

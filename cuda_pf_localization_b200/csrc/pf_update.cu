@@ -113,6 +113,7 @@ __global__ void __launch_bounds__(kThreads)
              float sigma_b, float gate, float* __restrict__ ll,
              double2* part, unsigned* done, CycleCtl* ctl, int use_packed,
              const CycleArgs* ca) {
+    pdl_wait();
     if (ca) {  // graph replay: this cycle's values
         pa = ca->pa;
         obs = ca->obs;
@@ -189,15 +190,15 @@ int launch_weight(PfHandle* h, const PredictArgs& pa, const CObservation* d_obs,
     double2* part = reinterpret_cast<double2*>(h->d_part);
     KernelScope ks(h, KK_WEIGHT);
     if (pa.enabled) {
-        k_weight<true><<<grid, kThreads, 0, h->stream>>>(
-            plane_set(h), h->n, h->seed, pa, d_obs, nobs, h->d_lm, h->lm_count,
-            sigma_r, sigma_b, gate, h->d_ll, part, h->d_done + 0, h->d_ctl,
-            h->weight_variant == 0 ? 1 : 0, dargs);
+        PFB_CK(launch_pdl(k_weight<true>, grid, kThreads, 0, h->stream, plane_set(h),
+                          h->n, h->seed, pa, d_obs, nobs, h->d_lm, h->lm_count,
+                          sigma_r, sigma_b, gate, h->d_ll, part, h->d_done + 0,
+                          h->d_ctl, h->weight_variant == 0 ? 1 : 0, dargs));
     } else {
-        k_weight<false><<<grid, kThreads, 0, h->stream>>>(
-            plane_set(h), h->n, h->seed, pa, d_obs, nobs, h->d_lm, h->lm_count,
-            sigma_r, sigma_b, gate, h->d_ll, part, h->d_done + 0, h->d_ctl,
-            h->weight_variant == 0 ? 1 : 0, dargs);
+        PFB_CK(launch_pdl(k_weight<false>, grid, kThreads, 0, h->stream, plane_set(h),
+                          h->n, h->seed, pa, d_obs, nobs, h->d_lm, h->lm_count,
+                          sigma_r, sigma_b, gate, h->d_ll, part, h->d_done + 0,
+                          h->d_ctl, h->weight_variant == 0 ? 1 : 0, dargs));
     }
     PFB_KL();
     h->prefix_valid = false;
