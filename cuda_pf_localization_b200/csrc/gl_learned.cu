@@ -510,117 +510,227 @@ __device__ __forceinline__ float sigmoidf_(float x) { return 1.0f / (1.0f + expf
 //   dloss/draw = r (1 - z^2) (LS_HI - LS_LO) s (1 - s)
 // Gradients are scaled by inv_b (mean over the batch) and written as bf16
 // (padding columns 288..383 zero).
-__global__ void k_gmm_loss(const float* __restrict__ Z, const float* __restrict__ Y,
-                           int y_row0, int rows, float inv_b,
-                           bf16* __restrict__ dZ, float* __restrict__ loss_acc) {
+__global__ void __launch_bounds__(256)
+    k_gmm_loss(const float* __restrict__ Z, const float* __restrict__ Y, int y_row0,
+               int rows, float inv_b, bf16* __restrict__ dZ, float* __restrict__ loss_acc) {
+    __shared__ float s_loss[8];
     const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (wid >= rows) return;
-    const float* z = Z + (size_t)wid * kOut;
-    const float* y = Y + (size_t)(y_row0 + wid) * 4;
-    const float logit = z[lane];
-    const float yv[4] = {y[0], y[1], y[2], y[3]};
-    const float mx = warp_max_f(logit);
-    const float lse_l = mx + logf(warp_sum_f(expf(logit - mx)));
-    const float logpi = logit - lse_l;
-    const float pi = expf(logpi);
-    float zz[4], sg[4], sig[4], mu[4];
-    float nll = 4.0f * kHalfLog2Pi;
+    float loss = 0.0f;
+    if (wid < rows) {
+        const float* z = Z + (size_t)wid * kOut;
+        const float* y = Y + (size_t)(y_row0 + wid) * 4;
+        const float logit = z[lane];
+        const float yv[4] = {y[0], y[1], y[2], y[3]};
+        // component `lane`: its 4 means and 4 log-sigma pre-activations are
+        // consecutive (one 16-byte load each)
+        const float4 mu4 = reinterpret_cast<const float4*>(z + kMeanOff)[lane];
+        const float4 raw4 = reinterpret_cast<const float4*>(z + kSigOff)[lane];
+        const float mu[4] = {mu4.x, mu4.y, mu4.z, mu4.w};
+        const float raw[4] = {raw4.x, raw4.y, raw4.z, raw4.w};
+        const float mx = warp_max_f(logit);
+        const float lse_l = mx + logf(warp_sum_f(expf(logit - mx)));
+        const float logpi = logit - lse_l;
+        const float pi = expf(logpi);
+        float zz[4], sg[4], sig[4];
+        float nll = 4.0f * kHalfLog2Pi;
 #pragma unroll
-    for (int d = 0; d < 4; ++d) {
-        mu[d] = z[kMeanOff + 4 * lane + d];
-        const float s = sigmoidf_(z[kSigOff + 4 * lane + d]);
-        const float ls = kLsLo + (kLsHi - kLsLo) * s;
-        sg[d] = s;
-        sig[d] = expf(ls);
-        zz[d] = (yv[d] - mu[d]) / sig[d];
-        nll += 0.5f * zz[d] * zz[d] + ls;
-    }
-    const float a = logpi - nll;
-    const float amx = warp_max_f(a);
-    const float logp = amx + logf(warp_sum_f(expf(a - amx)));
-    const float r = expf(a - logp);
-    if (lane == 0) atomicAdd(loss_acc, -logp * inv_b);
-    bf16* o = dZ + (size_t)wid * kOut;
-    o[lane] = __float2bfloat16_rn((pi - r) * inv_b);
+        for (int d = 0; d < 4; ++d) {
+            const float sgm = sigmoidf_(raw[d]);
+            const float ls = kLsLo + (kLsHi - kLsLo) * sgm;
+            sg[d] = sgm;
+            sig[d] = expf(ls);
+            zz[d] = (yv[d] - mu[d]) / sig[d];
+            nll += 0.5f * zz[d] * zz[d] + ls;
+        }
+        const float a = logpi - nll;
+        const float amx = warp_max_f(a);
+        const float logp = amx + logf(warp_sum_f(expf(a - amx)));
+        const float r = expf(a - logp);
+        loss = -logp * inv_b;
+        bf16* o = dZ + (size_t)wid * kOut;
+        o[lane] = __float2bfloat16_rn((pi - r) * inv_b);
+        bf16 gm[4], gs[4];
 #pragma unroll
-    for (int d = 0; d < 4; ++d) {
-        o[kMeanOff + 4 * lane + d] = __float2bfloat16_rn(-r * zz[d] / sig[d] * inv_b);
-        o[kSigOff + 4 * lane + d] = __float2bfloat16_rn(
-            r * (1.0f - zz[d] * zz[d]) * (kLsHi - kLsLo) * sg[d] * (1.0f - sg[d]) *
-            inv_b);
+        for (int d = 0; d < 4; ++d) {
+            gm[d] = __float2bfloat16_rn(-r * zz[d] / sig[d] * inv_b);
+            gs[d] = __float2bfloat16_rn(r * (1.0f - zz[d] * zz[d]) * (kLsHi - kLsLo) *
+                                        sg[d] * (1.0f - sg[d]) * inv_b);
+        }
+        uint2 pm, ps;
+        pm.x = (uint32_t)__bfloat16_as_ushort(gm[0]) | ((uint32_t)__bfloat16_as_ushort(gm[1]) << 16);
+        pm.y = (uint32_t)__bfloat16_as_ushort(gm[2]) | ((uint32_t)__bfloat16_as_ushort(gm[3]) << 16);
+        ps.x = (uint32_t)__bfloat16_as_ushort(gs[0]) | ((uint32_t)__bfloat16_as_ushort(gs[1]) << 16);
+        ps.y = (uint32_t)__bfloat16_as_ushort(gs[2]) | ((uint32_t)__bfloat16_as_ushort(gs[3]) << 16);
+        reinterpret_cast<uint2*>(o + kMeanOff)[lane] = pm;
+        reinterpret_cast<uint2*>(o + kSigOff)[lane] = ps;
+        for (int p = kUsedOut + lane; p < kOut; p += 32) o[p] = __float2bfloat16_rn(0.0f);
     }
-    for (int p = kUsedOut + lane; p < kOut; p += 32) o[p] = __float2bfloat16_rn(0.0f);
+    // one atomic per block: the block's samples in warp order
+    if (lane == 0) s_loss[threadIdx.x >> 5] = loss;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.0f;
+        for (int k = 0; k < 8; ++k) t += s_loss[k];
+        atomicAdd(loss_acc, t);
+    }
 }
 
-// out[c][r] = in[r][c] for an R x C bf16 matrix; 32 x 32 tiles, block 32 x 8.
+// out[c][r] = in[r][c] for an R x C bf16 matrix, in 64 x 64 tiles through
+// shared memory; tile rows are read and written as bf16 pairs (4-byte
+// accesses, 128 bytes per warp) where the strides and base addresses allow.
 __global__ void k_transpose_bf16(const bf16* __restrict__ in, long long ld_in,
                                  bf16* __restrict__ out, long long ld_out,
                                  long long R, long long C) {
-    __shared__ bf16 t[32][34];
-    const long long c0 = (long long)blockIdx.x * 32, r0 = (long long)blockIdx.y * 32;
-    for (int i = threadIdx.y; i < 32; i += 8) {
-        const long long r = r0 + i, c = c0 + threadIdx.x;
-        if (r < R && c < C) t[i][threadIdx.x] = in[r * ld_in + c];
+    __shared__ bf16 t[64][66];
+    const long long c0 = (long long)blockIdx.x * 64, r0 = (long long)blockIdx.y * 64;
+    const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+    const bool vin = (ld_in & 1) == 0 && (reinterpret_cast<uintptr_t>(in) & 3) == 0;
+    const bool vout = (ld_out & 1) == 0 && (reinterpret_cast<uintptr_t>(out) & 3) == 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int i = ty + 8 * k;
+        const long long r = r0 + i, c = c0 + 2 * tx;
+        if (r >= R) continue;
+        const bf16* src = in + r * ld_in + c;
+        if (vin && c + 1 < C) {
+            const __nv_bfloat162 v = *reinterpret_cast<const __nv_bfloat162*>(src);
+            t[i][2 * tx] = v.x;
+            t[i][2 * tx + 1] = v.y;
+        } else {
+            if (c < C) t[i][2 * tx] = src[0];
+            if (c + 1 < C) t[i][2 * tx + 1] = src[1];
+        }
     }
     __syncthreads();
-    for (int i = threadIdx.y; i < 32; i += 8) {
-        const long long c = c0 + i, r = r0 + threadIdx.x;
-        if (r < R && c < C) out[c * ld_out + r] = t[threadIdx.x][i];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int i = ty + 8 * k;
+        const long long c = c0 + i, r = r0 + 2 * tx;
+        if (c >= C) continue;
+        bf16* dst = out + c * ld_out + r;
+        if (vout && r + 1 < R) {
+            __nv_bfloat162 v;
+            v.x = t[2 * tx][i];
+            v.y = t[2 * tx + 1][i];
+            *reinterpret_cast<__nv_bfloat162*>(dst) = v;
+        } else {
+            if (r < R) dst[0] = t[2 * tx][i];
+            if (r + 1 < R) dst[1] = t[2 * tx + 1][i];
+        }
     }
 }
 
-// out[o] = sum over cols of in[o][*] (bf16 rows, f32 sum), one warp per row.
-__global__ void k_rowsum_bf16(const bf16* __restrict__ in, int ld, int cols,
-                              int rows, float* __restrict__ out) {
-    const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (wid >= rows) return;
-    const __nv_bfloat162* p =
-        reinterpret_cast<const __nv_bfloat162*>(in + (size_t)wid * ld);
+// out[o] = sum over cols of in[o][*] (bf16 rows, f32 sum), one 256-thread
+// block per row: thread t sums the 8-element chunks t, t + 256, ... (16-byte
+// loads, all issued together), then the block adds the threads in a fixed
+// order.
+__device__ __forceinline__ float bf16x2_sum(uint32_t u) {
+    const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u));
+    return f.x + f.y;
+}
+
+__global__ void __launch_bounds__(256)
+    k_rowsum_bf16(const bf16* __restrict__ in, int ld, int cols, int rows,
+                  float* __restrict__ out) {
+    __shared__ float s_w[8];
+    const int row = blockIdx.x;
+    if (row >= rows) return;
+    const bf16* p = in + (size_t)row * ld;
     float acc = 0.0f;
-    for (int c = lane; c < cols / 2; c += 32) {
-        const float2 f = __bfloat1622float2(p[c]);
-        acc += f.x + f.y;
+    if ((cols & 7) == 0 && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+        const uint4* q = reinterpret_cast<const uint4*>(p);
+        const int nq = cols >> 3;
+#pragma unroll 4
+        for (int c = threadIdx.x; c < nq; c += 256) {
+            const uint4 u = q[c];
+            acc += (bf16x2_sum(u.x) + bf16x2_sum(u.y)) + (bf16x2_sum(u.z) + bf16x2_sum(u.w));
+        }
+    } else {
+        for (int c = threadIdx.x; c < cols; c += 256) acc += __bfloat162float(p[c]);
     }
     acc = warp_sum_f(acc);
-    if (lane == 0) out[wid] = acc;
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.0f;
+        for (int k = 0; k < 8; ++k) t += s_w[k];
+        out[row] = t;
+    }
 }
 
 // Adam on one weight matrix [out][in] (f32 master, moments) followed by the
-// bf16 copies W [out][in] and W^T [in][out]; 32 x 32 tiles, block 32 x 8.
+// bf16 copies W [out][in] and W^T [in][out]; 32 x 32 tiles, 256 threads, one
+// float4 of a tile row per thread (every load of the tile issued at once),
+// the transposed copy through shared memory in 8-byte stores.  The blocks of
+// tile column 0 also update the 32 biases of their rows (b, mb, vb from gb).
 // With update == 0 only the bf16 copies are refreshed from the masters.
-__global__ void k_adam_w(int out, int in, float* __restrict__ w,
-                         float* __restrict__ m, float* __restrict__ v,
-                         const float* __restrict__ g, int splits,
-                         bf16* __restrict__ wb, bf16* __restrict__ wtb, int update,
-                         float lr, float b1, float b2, float eps, float bc1,
-                         float bc2) {
+__device__ __forceinline__ void adam_one(float& w, float& m, float& v, float g, float lr,
+                                         float b1, float b2, float eps, float bc1,
+                                         float bc2) {
+    m = b1 * m + (1.0f - b1) * g;
+    v = b2 * v + (1.0f - b2) * g * g;
+    w -= lr * (m / bc1) / (sqrtf(v / bc2) + eps);
+}
+
+__global__ void __launch_bounds__(256)
+    k_adam_w(int out, int in, float* __restrict__ w, float* __restrict__ m,
+             float* __restrict__ v, const float* __restrict__ g, int splits,
+             bf16* __restrict__ wb, bf16* __restrict__ wtb, float* __restrict__ b,
+             float* __restrict__ mb, float* __restrict__ vb, const float* __restrict__ gb,
+             int update, float lr, float b1, float b2, float eps, float bc1, float bc2) {
     // g holds `splits` partial gradients of out*in floats each, summed in
     // split order.
     const size_t nw = (size_t)out * in;
-    __shared__ bf16 t[32][34];
+    __shared__ bf16 t[32][36];
     const int i0 = blockIdx.x * 32, o0 = blockIdx.y * 32;
-    for (int rr = threadIdx.y; rr < 32; rr += 8) {
-        const size_t idx = (size_t)(o0 + rr) * in + i0 + threadIdx.x;
-        float ww = w[idx];
-        if (update) {
-            float gg = g[idx];
-            for (int sp = 1; sp < splits; ++sp) gg += g[sp * nw + idx];
-            const float mm = b1 * m[idx] + (1.0f - b1) * gg;
-            const float vv = b2 * v[idx] + (1.0f - b2) * gg * gg;
-            m[idx] = mm;
-            v[idx] = vv;
-            ww -= lr * (mm / bc1) / (sqrtf(vv / bc2) + eps);
-            w[idx] = ww;
+    const int rr = threadIdx.x >> 3, q = threadIdx.x & 7;
+    const size_t idx = (size_t)(o0 + rr) * in + i0 + 4 * q;
+    float4 ww = *reinterpret_cast<const float4*>(w + idx);
+    if (update) {
+        float4 gg = *reinterpret_cast<const float4*>(g + idx);
+        for (int sp = 1; sp < splits; ++sp) {
+            const float4 o = *reinterpret_cast<const float4*>(g + sp * nw + idx);
+            gg.x += o.x;
+            gg.y += o.y;
+            gg.z += o.z;
+            gg.w += o.w;
         }
-        const bf16 h = __float2bfloat16_rn(ww);
-        wb[idx] = h;
-        t[rr][threadIdx.x] = h;
+        float4 mm = *reinterpret_cast<const float4*>(m + idx);
+        float4 vv = *reinterpret_cast<const float4*>(v + idx);
+        adam_one(ww.x, mm.x, vv.x, gg.x, lr, b1, b2, eps, bc1, bc2);
+        adam_one(ww.y, mm.y, vv.y, gg.y, lr, b1, b2, eps, bc1, bc2);
+        adam_one(ww.z, mm.z, vv.z, gg.z, lr, b1, b2, eps, bc1, bc2);
+        adam_one(ww.w, mm.w, vv.w, gg.w, lr, b1, b2, eps, bc1, bc2);
+        *reinterpret_cast<float4*>(m + idx) = mm;
+        *reinterpret_cast<float4*>(v + idx) = vv;
+        *reinterpret_cast<float4*>(w + idx) = ww;
+        if (blockIdx.x == 0 && threadIdx.x < 32) {
+            const int o = o0 + threadIdx.x;
+            float bb = b[o], bm = mb[o], bv = vb[o];
+            adam_one(bb, bm, bv, gb[o], lr, b1, b2, eps, bc1, bc2);
+            b[o] = bb;
+            mb[o] = bm;
+            vb[o] = bv;
+        }
     }
+    const bf16 h[4] = {__float2bfloat16_rn(ww.x), __float2bfloat16_rn(ww.y),
+                       __float2bfloat16_rn(ww.z), __float2bfloat16_rn(ww.w)};
+    uint2 pk;
+    pk.x = (uint32_t)__bfloat16_as_ushort(h[0]) | ((uint32_t)__bfloat16_as_ushort(h[1]) << 16);
+    pk.y = (uint32_t)__bfloat16_as_ushort(h[2]) | ((uint32_t)__bfloat16_as_ushort(h[3]) << 16);
+    *reinterpret_cast<uint2*>(wb + idx) = pk;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) t[rr][4 * q + j] = h[j];
     __syncthreads();
-    for (int cc = threadIdx.y; cc < 32; cc += 8)
-        wtb[(size_t)(i0 + cc) * out + o0 + threadIdx.x] = t[threadIdx.x][cc];
+    // transposed row i0 + c, columns o0 + 4 q .. + 3
+    const int c = threadIdx.x >> 3;
+    uint2 pt;
+    pt.x = (uint32_t)__bfloat16_as_ushort(t[4 * q][c]) |
+           ((uint32_t)__bfloat16_as_ushort(t[4 * q + 1][c]) << 16);
+    pt.y = (uint32_t)__bfloat16_as_ushort(t[4 * q + 2][c]) |
+           ((uint32_t)__bfloat16_as_ushort(t[4 * q + 3][c]) << 16);
+    *reinterpret_cast<uint2*>(wtb + (size_t)(i0 + c) * out + o0 + 4 * q) = pt;
 }
 
 // Sum split-K partial gradients into split 0 (split order).
@@ -630,20 +740,6 @@ __global__ void k_sum_splits(float* __restrict__ g, int splits, long long nw) {
     float acc = g[i];
     for (int sp = 1; sp < splits; ++sp) acc += g[sp * nw + i];
     g[i] = acc;
-}
-
-__global__ void k_adam_b(int n, float* __restrict__ b, float* __restrict__ m,
-                         float* __restrict__ v, const float* __restrict__ g,
-                         float lr, float b1, float b2, float eps, float bc1,
-                         float bc2) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float gg = g[i];
-    const float mm = b1 * m[i] + (1.0f - b1) * gg;
-    const float vv = b2 * v[i] + (1.0f - b2) * gg * gg;
-    m[i] = mm;
-    v[i] = vv;
-    b[i] -= lr * (mm / bc1) / (sqrtf(vv / bc2) + eps);
 }
 
 // He-uniform initialisation from Philox (counter (i, layer, part, INIT)).
@@ -1002,9 +1098,9 @@ int check_err(LpHandle* h) {
 int round_weights(LpHandle* h) {
     for (int l = 0; l < kLayers; ++l) {
         Layer& L = h->L[l];
-        k_adam_w<<<dim3(L.in / 32, L.out / 32), dim3(32, 8), 0, h->stream>>>(
-            L.out, L.in, L.w, L.mw, L.vw, L.gw, L.splits, L.wb, L.wtb, 0, 0.f, 0.f,
-            0.f, 0.f, 1.f, 1.f);
+        k_adam_w<<<dim3(L.in / 32, L.out / 32), 256, 0, h->stream>>>(
+            L.out, L.in, L.w, L.mw, L.vw, L.gw, L.splits, L.wb, L.wtb, L.b, L.mb, L.vb,
+            L.gb, 0, 0.f, 0.f, 0.f, 0.f, 1.f, 1.f);
     }
     PFB_KL();
     return 0;
@@ -1061,7 +1157,7 @@ int backward(LpHandle* h, MapRef xt, const float* Y, float* d_loss_slot) {
     k_gmm_loss<<<ceil_div(B * 32, 256), 256, 0, s>>>(
         h->Z4, Y, 0, B, 1.0f / (float)B, h->dZ[kLayers - 1], d_loss_slot);
     PFB_KL();
-    k_transpose_bf16<<<dim3(kOut / 32, B / 32), dim3(32, 8), 0, s>>>(
+    k_transpose_bf16<<<dim3(ceil_div(kOut, 64), ceil_div(B, 64)), dim3(32, 8), 0, s>>>(
         h->dZ[kLayers - 1], kOut, h->dZT[kLayers - 1], B, B, kOut);
     PFB_KL();
     for (int l = kLayers - 1; l >= 0; --l) {
@@ -1075,8 +1171,7 @@ int backward(LpHandle* h, MapRef xt, const float* Y, float* d_loss_slot) {
         if (gemm<EPI_F32>(s, MapRef{&h->tm_dZT[l], 0, 0}, bt, L.out, L.in, B, eg,
                           h->d_err, L.splits))
             return -1;
-        k_rowsum_bf16<<<ceil_div(L.out * 32, 256), 256, 0, s>>>(h->dZT[l], B, B,
-                                                                 L.out, L.gb);
+        k_rowsum_bf16<<<L.out, 256, 0, s>>>(h->dZT[l], B, B, L.out, L.gb);
         PFB_KL();
         if (l > 0) {
             EpiArgs ed{};
@@ -1102,11 +1197,10 @@ int adam_update(LpHandle* h, float lr) {
     const float bc2 = 1.0f - powf(b2, (float)h->adam_t);
     for (int l = 0; l < kLayers; ++l) {
         Layer& L = h->L[l];
-        k_adam_w<<<dim3(L.in / 32, L.out / 32), dim3(32, 8), 0, h->stream>>>(
-            L.out, L.in, L.w, L.mw, L.vw, L.gw, L.splits, L.wb, L.wtb, 1, lr, b1, b2,
-            eps, bc1, bc2);
-        k_adam_b<<<ceil_div(L.out, 256), 256, 0, h->stream>>>(
-            L.out, L.b, L.mb, L.vb, L.gb, lr, b1, b2, eps, bc1, bc2);
+        // weights and biases of the layer in one launch
+        k_adam_w<<<dim3(L.in / 32, L.out / 32), 256, 0, h->stream>>>(
+            L.out, L.in, L.w, L.mw, L.vw, L.gw, L.splits, L.wb, L.wtb, L.b, L.mb, L.vb,
+            L.gb, 1, lr, b1, b2, eps, bc1, bc2);
     }
     PFB_KL();
     return 0;
@@ -1542,7 +1636,7 @@ int pfgl_learned_make_data(void* p, long long n_pairs, int nrays, float rmax,
     const long long chunk = 65535ll * 32;
     for (long long r0 = 0; r0 < n_pairs; r0 += chunk) {
         const long long rows = std::min(chunk, n_pairs - r0);
-        k_transpose_bf16<<<dim3(kIn / 32, (unsigned)((rows + 31) / 32)), dim3(32, 8), 0,
+        k_transpose_bf16<<<dim3(ceil_div(kIn, 64), (unsigned)((rows + 63) / 64)), dim3(32, 8), 0,
                            h->stream>>>(h->X + (size_t)r0 * kIn, kIn, h->XT + r0,
                                         n_pairs, rows, kIn);
     }
@@ -1604,7 +1698,7 @@ int pfgl_learned_grad(void* p, const float* x, const float* y, float* loss,
                            h->stream));
     k_f32_to_bf16<<<(unsigned)((nx + 255) / 256), 256, 0, h->stream>>>(h->Xp_f, h->Xp,
                                                                       (long long)nx);
-    k_transpose_bf16<<<dim3(kIn / 32, B / 32), dim3(32, 8), 0, h->stream>>>(
+    k_transpose_bf16<<<dim3(ceil_div(kIn, 64), ceil_div(B, 64)), dim3(32, 8), 0, h->stream>>>(
         h->Xp, kIn, h->XpT, B, B, kIn);
     PFB_KL();
     if (h->loss_cap < 1) {
