@@ -24,7 +24,7 @@
 // GEMM kernel (sm_100a): persistent, one CTA per SM over 128 x BN output
 // tiles (BN = 256 or 128), a 4- or 6-stage TMA ring of 64-element k-slices
 // (128-byte swizzle), one thread issuing tcgen05.mma into two TMEM
-// accumulators in turn, one thread issuing the TMA loads, and four epilogue
+// accumulators in turn, one thread issuing the TMA loads, and eight epilogue
 // warps draining the idle accumulator through tcgen05.ld.  Every mbarrier
 // wait is bounded; a wait that runs out sets an error word the host turns
 // into -1.
@@ -168,12 +168,13 @@ __device__ __forceinline__ void epilogue_chunk(const uint32_t (&r)[32], int row,
 //   warp 1 (one thread): MMA issuer into one of two TMEM accumulators
 //                        (columns [0, BN) and [BN, 2 BN)), alternating per
 //                        tile;
-//   warps 2-5:           the epilogue of the other accumulator, so tile i's
+//   warps 2-9:           the epilogue of the other accumulator, so tile i's
 //                        epilogue overlaps tile i + 1's MMAs.  Warp w reads
 //                        TMEM lanes [32 (w % 4), 32 (w % 4) + 32), the lane
-//                        quarter its warp may access.
+//                        quarter its warp may access; the two warps of a
+//                        quarter take alternate 32-column chunks.
 // Barriers: full/empty per ring stage, acc_full (MMA commit) and acc_empty
-// (one arrival per epilogue warp) per accumulator.  Every wait is bounded
+// (one arrival per epilogue warp, after its last chunk) per accumulator.  Every wait is bounded
 // and gives up early once another role has failed; the producer then waits
 // for its own loads in flight and the MMA thread for its MMAs before the
 // TMEM is freed.
@@ -185,7 +186,8 @@ struct PTile {
     static constexpr int kRing = kStages * (kABytes + kBBytes);
     static constexpr int kSmem = kRing + 1024 + 256;  // + alignment, barriers
 };
-constexpr int kPThreads = 192;
+constexpr int kEpiWarps = 8;  // two per TMEM lane quarter
+constexpr int kPThreads = 64 + 32 * kEpiWarps;
 
 struct TileGrid {
     int tn;      // column blocks (N / BN)
@@ -225,7 +227,7 @@ __global__ void __launch_bounds__(kPThreads, 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&acc_full[b], 1);
-            mbar_init(&acc_empty[b], 4);
+            mbar_init(&acc_empty[b], kEpiWarps);
         }
         mbar_init(fin, 1);
         *abort = 0;
@@ -322,8 +324,11 @@ __global__ void __launch_bounds__(kPThreads, 1)
             if (!mbar_wait(fin, 0, kWaitLimit)) atomicOr(err, ERR_SPIN_TIMEOUT);
         }
         __syncwarp();
-    } else {  // epilogue warps 2..5
+    } else {  // epilogue warps 2 .. kEpiWarps + 1
         const int q = warp & 3;
+        constexpr int kPerQ = kEpiWarps / 4;  // warps sharing a lane quarter
+        const int part = (warp - 2) / 4;      // which of them: chunks part, part + kPerQ, ...
+        constexpr int kChunks = BN / 32;
         int i = 0;
         for (int t = blockIdx.x; t < tg.tiles; t += gridDim.x, ++i) {
             const int z = t / tg.tmn, r = t - z * tg.tmn;
@@ -345,11 +350,11 @@ __global__ void __launch_bounds__(kPThreads, 1)
             const int row = m0 + q * 32 + lane;
             const uint32_t trow = tmem + (uint32_t)(b * BN) + ((uint32_t)(q * 32) << 16);
 #pragma unroll 1
-            for (int c = 0; c < BN / 32; ++c) {
+            for (int c = part; c < kChunks; c += kPerQ) {
                 uint32_t v[32];
                 tmem_ld32(trow + (uint32_t)(c * 32), v);
                 tmem_wait_ld();
-                if (c == BN / 32 - 1) {  // accumulator drained: hand it back
+                if (c + kPerQ >= kChunks) {  // this warp's last chunk: hand it back
                     tc_fence_before();
                     __syncwarp();
                     if (lane == 0) mbar_arrive(&acc_empty[b]);

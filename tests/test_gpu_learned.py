@@ -64,9 +64,12 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
 
 
-def test_learned_grad_matches_fp64_oracle(kernels):
+# batch 8192 (the training batch) runs the forward and input-gradient GEMMs
+# on 128 x 256 tiles over every SM, batch 128 on 128 x 128 tiles
+@pytest.mark.parametrize("batch", [128, 8192])
+def test_learned_grad_matches_fp64_oracle(kernels, batch):
     lib, _, h = _gl()
-    lp = pkg.LearnedProposal(h, batch=128, seed=5)
+    lp = pkg.LearnedProposal(h, batch=batch, seed=5)
     try:
         rng = np.random.default_rng(11)
         flat = lp.params()
@@ -78,7 +81,7 @@ def test_learned_grad_matches_fp64_oracle(kernels):
         flat = M.flatten(layers).astype(np.float32)
         lp.set_params(flat)
         assert np.array_equal(lp.params(), flat)
-        x, y = _batch(rng, 128)
+        x, y = _batch(rng, batch)
         loss, g = lp.grad(x, y)
         ref_loss, ref = M.loss_and_grad(M.unflatten(flat.astype(np.float64)),
                                         x.astype(np.float64), y.astype(np.float64))
