@@ -89,7 +89,7 @@ __global__ void k_gl_gen(int n, int n_yaw, int nfree, const int2* __restrict__ f
 // with `bound` at every restart and -1 is returned once it exceeds it; the
 // caller's bound includes a margin for the rounding difference between that
 // partial order and the final one.
-constexpr int kScoreThreads = 512;
+constexpr int kScoreThreads = 768;
 constexpr int kScoreWarps = kScoreThreads / 32;
 constexpr int kChunk = 8;    // DDA steps between warp votes
 constexpr int kRestart = 8;  // free lanes that trigger a restart round
@@ -185,7 +185,7 @@ __device__ __forceinline__ void score_setup(const GridView& gv, int grid_bytes,
 
 // CAER of hypotheses [0, nh): one warp per hypothesis, static striding.
 template <bool kSmem>
-__global__ void __launch_bounds__(kScoreThreads, 3)
+__global__ void __launch_bounds__(kScoreThreads, 2)
     k_gl_score(GridView gv, int grid_bytes, const float* __restrict__ hyp,
                int nh, const float* __restrict__ scan, int nrays, float rmax,
                float span, float* __restrict__ caer) {
@@ -256,7 +256,7 @@ __device__ __forceinline__ float key_to_float(uint64_t key) {
 // The CAER of every hypothesis that is not dropped is the exhaustive
 // scorer's value; survivors (final key <= tau) are appended to cand.
 template <bool kSmem>
-__global__ void __launch_bounds__(kScoreThreads, 3)
+__global__ void __launch_bounds__(kScoreThreads, 2)
     k_gl_score_pruned(GridView gv, int grid_bytes, const float* __restrict__ hyp,
                       int h0, int h1, const float* __restrict__ scan, int nrays,
                       float rmax, float span, float* __restrict__ caer,
