@@ -91,6 +91,10 @@ __global__ void k_gl_gen(int n, int n_yaw, int nfree, const int2* __restrict__ f
 // partial order and the final one.
 constexpr int kScoreThreads = 768;
 constexpr int kScoreWarps = kScoreThreads / 32;
+// a launch keeps at least this many hypotheses per block on average, so a
+// small batch still reaches every SM without each block copying the grid
+// for a handful of warps
+constexpr int kMinScoreWarps = 8;
 constexpr int kChunk = 8;    // DDA steps between warp votes
 constexpr int kRestart = 8;  // free lanes that trigger a restart round
 
@@ -195,7 +199,10 @@ __global__ void __launch_bounds__(kScoreThreads, 2)
     float2* dirs;
     score_setup<kSmem>(gv, grid_bytes, scan, nrays, g, sc, term, dirs);
     const int Hp = gv.H + 2;
-    const int gw = blockIdx.x * kScoreWarps + (threadIdx.x >> 5);
+    // hypotheses striped across the blocks first (warp w of block b takes
+    // b + w * gridDim.x, ...), so a batch smaller than the grid's warps is
+    // spread evenly over the SMs
+    const int gw = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;
     const int nw = gridDim.x * kScoreWarps;
     for (int h = gw; h < nh; h += nw) {
         const float c = warp_caer<false>(g, gv, Hp, hyp[3 * h], hyp[3 * h + 1],
@@ -271,7 +278,10 @@ __global__ void __launch_bounds__(kScoreThreads, 2)
     const float tau_f = key_to_float(tau);
     const float bound = tau_f * (1.0f + 4.0f * (float)nrays * 5.9604645e-8f + 1e-6f);
     const int lane = threadIdx.x & 31;
-    const int gw = blockIdx.x * kScoreWarps + (threadIdx.x >> 5);
+    // hypotheses striped across the blocks first (warp w of block b takes
+    // b + w * gridDim.x, ...), so a batch smaller than the grid's warps is
+    // spread evenly over the SMs
+    const int gw = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;
     const int nw = gridDim.x * kScoreWarps;
     for (int h = h0 + gw; h < h1; h += nw) {
         const float total = warp_caer<true>(g, gv, Hp, hyp[3 * h], hyp[3 * h + 1],
@@ -741,7 +751,7 @@ int launch_score(GlHandle* h, int nrays, float rmax, float span) {
                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem));
         int grid = score_grid_size<true>(smem);
-        grid = std::min(grid, ceil_div(warps_needed, kScoreWarps));
+        grid = std::min(grid, ceil_div(warps_needed, kMinScoreWarps));
         k_gl_score<true><<<grid, kScoreThreads, smem, h->stream>>>(
             gv, gb, h->d_hyp, h->nh, h->d_scan, nrays, rmax, span, h->d_caer);
     } else {
@@ -749,7 +759,7 @@ int launch_score(GlHandle* h, int nrays, float rmax, float span) {
                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem));
         int grid = score_grid_size<false>(smem);
-        grid = std::min(grid, ceil_div(warps_needed, kScoreWarps));
+        grid = std::min(grid, ceil_div(warps_needed, kMinScoreWarps));
         k_gl_score<false><<<grid, kScoreThreads, smem, h->stream>>>(
             gv, gb, h->d_hyp, h->nh, h->d_scan, nrays, rmax, span, h->d_caer);
     }
@@ -773,7 +783,7 @@ int launch_score_pruned(GlHandle* h, int h0, int h1, int nrays, float rmax,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem));
         int grid = score_grid_size<true>(smem);
-        grid = std::min(grid, ceil_div(warps_needed, kScoreWarps));
+        grid = std::min(grid, ceil_div(warps_needed, kMinScoreWarps));
         k_gl_score_pruned<true><<<grid, kScoreThreads, smem, h->stream>>>(
             gv, gb, h->d_hyp, h0, h1, h->d_scan, nrays, rmax, span, h->d_caer,
             h->d_cand, h->d_ctl, h->cap_hyp);
@@ -782,7 +792,7 @@ int launch_score_pruned(GlHandle* h, int h0, int h1, int nrays, float rmax,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem));
         int grid = score_grid_size<false>(smem);
-        grid = std::min(grid, ceil_div(warps_needed, kScoreWarps));
+        grid = std::min(grid, ceil_div(warps_needed, kMinScoreWarps));
         k_gl_score_pruned<false><<<grid, kScoreThreads, smem, h->stream>>>(
             gv, gb, h->d_hyp, h0, h1, h->d_scan, nrays, rmax, span, h->d_caer,
             h->d_cand, h->d_ctl, h->cap_hyp);
