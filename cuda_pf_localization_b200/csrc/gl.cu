@@ -95,7 +95,7 @@ constexpr int kScoreWarps = kScoreThreads / 32;
 // small batch still reaches every SM without each block copying the grid
 // for a handful of warps
 constexpr int kMinScoreWarps = 8;
-constexpr int kChunk = 8;    // DDA steps between warp votes
+constexpr int kChunk = 12;   // DDA steps between warp votes
 constexpr int kRestart = 8;  // free lanes that trigger a restart round
 
 template <bool kPrune>
