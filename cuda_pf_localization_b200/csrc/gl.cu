@@ -906,7 +906,7 @@ int gl_generate(GlHandle* h, int n_pos, int n_yaw, uint64_t seed) {
 const uint64_t* gl_localize_small_keys(GlHandle* h, int nrays, float rmax,
                                        float ang_span, int k) {
     const int nh = h->nh;
-    const int seed_n = std::min(nh, std::max(4 * k, 4096));
+    const int seed_n = std::min(nh, std::max(4 * k, 6144));
     h->nh = seed_n;
     const int rc = launch_score(h, nrays, rmax, ang_span);
     h->nh = nh;
