@@ -906,6 +906,7 @@ int gl_generate(GlHandle* h, int n_pos, int n_yaw, uint64_t seed) {
 const uint64_t* gl_localize_small_keys(GlHandle* h, int nrays, float rmax,
                                        float ang_span, int k) {
     const int nh = h->nh;
+    // seed batch: most of one round of the scorer grid's 7104 warps
     const int seed_n = std::min(nh, std::max(4 * k, 6144));
     h->nh = seed_n;
     const int rc = launch_score(h, nrays, rmax, ang_span);
@@ -952,8 +953,9 @@ int gl_localize_loaded(GlHandle* h, int nrays, float rmax, float ang_span,
     if (small_select_ok(h->nh, k))
         return localize_small(h, nrays, rmax, ang_span, k, out3k, caer_k, idx_k);
     const int nh = h->nh;
-    // Seed batch scored exhaustively, then pruned chunks.
-    const int seed_n = std::min(nh, std::max(4 * k, 8192));
+    // Seed batch scored exhaustively (two rounds of the scorer grid's 7104
+    // warps on a 148-SM B200), then pruned chunks.
+    const int seed_n = std::min(nh, std::max(4 * k, 14208));
     const int saved = h->nh;
     h->nh = seed_n;
     if (launch_score(h, nrays, rmax, ang_span)) return -1;
