@@ -244,6 +244,51 @@ def test_small_bottom_k_select_equals_full_sort(kernels, n):
         gl.close()
 
 
+def test_large_map_scoring_reads_grid_from_global_memory(kernels, ref):
+    """A 30 x 30 m room (600 x 600 cells, 356 KB padded) does not fit the
+    scorers' shared-memory grid copy, so they read the grid from global
+    memory: CAERs against the reference on fed hypotheses (1e-5 relative,
+    as on the small map) and the pruned localizer against exhaustive
+    scoring there."""
+    g = sim.rooms_grid(21, n_boxes=120, size_m=30.0)
+    rng = np.random.default_rng(21)
+    x, y, th = sim.free_pose(g, rng)
+    scan = oracle.map_scan(g, 0.05, (0, 0), x, y, th, 360, TAU, 10.0)
+    scan = (scan + rng.normal(0, 0.01, scan.size)).astype(np.float32)
+    hyp = oracle.gl_generate(g, 0.05, (0, 0), 4000 // 16, 16, 77)
+    n = len(hyp)
+    ours, theirs = Gl(kernels, g, 40_000), Gl(ref, g, n)
+    try:
+        flat = np.ascontiguousarray(hyp.reshape(-1))
+        assert kernels.pfgl_set_hyps(ours.h, f32p(flat), n) == 0
+        assert ref.ref_gl_set_hyps(theirs.h, f32p(flat), n) == 0
+        assert kernels.pfgl_score(ours.h, f32p(scan), scan.size, 10.0, TAU) == 0
+        assert ref.pfgl_score(theirs.h, f32p(scan), scan.size, 10.0, TAU) == 0
+        a = np.zeros(n, np.float32)
+        b = np.zeros(n, np.float32)
+        assert kernels.pfgl_get_caer(ours.h, f32p(a)) == 0
+        assert ref.ref_gl_get_caer(theirs.h, f32p(b)) == 0
+        rel = np.abs(a.astype(np.float64) - b) / np.maximum(np.abs(b), 1e-3)
+        assert rel.max() <= 1e-5, rel.max()
+        # pruned localizer (small-set path: seed batch, bound, survivors)
+        # against exhaustive scoring on 40 000 hypotheses of this map
+        k = 64
+        assert kernels.pfgl_generate_yaws(ours.h, 40_000 // 16, 16, 5) == 0
+        o1 = np.zeros(3 * k, np.float32)
+        c1 = np.zeros(k, np.float32)
+        i1 = np.zeros(k, np.int32)
+        assert kernels.pfgl_localize(ours.h, f32p(scan), scan.size, 10.0, TAU, k, f32p(o1),
+                                     f32p(c1), i32p(i1)) == k
+        assert kernels.pfgl_score(ours.h, f32p(scan), scan.size, 10.0, TAU) == 0
+        c2 = np.zeros(k, np.float32)
+        i2 = np.zeros(k, np.int32)
+        assert kernels.pfgl_topk_ex(ours.h, k, None, f32p(c2), i32p(i2)) == k
+        assert np.array_equal(i1, i2) and np.array_equal(c1, c2)
+    finally:
+        ours.close()
+        theirs.close()
+
+
 def _select_cases(rng, n):
     """Score arrays that stress the radix select's range narrowing: spread,
     all equal (ties resolved by the index word alone), two values, 60 decades,
