@@ -223,6 +223,11 @@ def reference_arm(args):
 # ------------------------------------------------------------ our GPU arm
 
 FP32_OPS_PER_PAIR = 29  # gated Cartesian term with the reference's roundings
+# DRAM bytes (read + write) of one k_weight launch at N = 1M, 256 observations,
+# from ncu (dram__bytes_read.sum + dram__bytes_write.sum; the capture command
+# is in profiles/pf_cycle_1M_scale.md): the poses are read from HBM, the
+# predicted poses and log-likelihoods it writes stay in L2.
+KWEIGHT_DRAM_BYTES_1M = 28.7e6 + 0.06e6
 
 
 def profiled_cycles(args):
@@ -717,7 +722,11 @@ def main():
         "gpu_launches": val["launches"],
         "roofline": {"bound": "hbm", "kernel": "k_weight (fused predict + gated weighting)",
                      "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None, "peak_source": peak_kind,
+                     "frac": achieved / hbm,
+                     "traffic": (KWEIGHT_DRAM_BYTES_1M
+                                 if (n, nobs) == (1_000_000, 256) else None),
+                     "traffic_source": "ncu capture of one k_weight launch at this workload",
+                     "peak_source": peak_kind,
                      "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": w_ms,
                      "timing": f"CUDA events around each k_weight launch on the library "
                                f"stream over the {val['profiled_steps']} cycles that "
