@@ -151,6 +151,7 @@ _KERNEL_SIGS = {
     "pfc_profile": (c_int, [c_void_p, c_int]),
     "pfc_profile_read": (c_int, [c_void_p, _dp, POINTER(C.c_longlong)]),
     "pfgl_generate_yaws": (c_int, [c_void_p, c_int, c_int, c_ulonglong]),
+    "pfgl_generate_yaws_range": (c_int, [c_void_p, c_int, c_int, c_int, c_ulonglong]),
     "pfgl_set_hyps": (c_int, [c_void_p, _fp, c_int]),
     "pfgl_get_hyps": (c_int, [c_void_p, _fp]),
     "pfgl_get_caer": (c_int, [c_void_p, _fp]),
@@ -179,6 +180,7 @@ _KERNEL_SIGS = {
     "pfc_batch_size": (c_int, [c_void_p, c_int]),
     "pfc_batch_stream": (c_void_p, [c_void_p]),
     "pfc_batch_launches": (C.c_longlong, [c_void_p]),
+    "pfc_batch_set_wait_test": (c_int, [c_void_p, c_int, c_int]),
     "pfgl_learned_create": (c_void_p, [c_void_p, c_int, c_ulonglong]),
     "pfgl_learned_destroy": (c_int, [c_void_p]),
     "pfgl_learned_num_params": (C.c_longlong, []),
@@ -210,6 +212,15 @@ _CORE_SIGS = {
     "pfcore_map_clear": (c_int, [c_void_p]),
     "pfcore_map_load_text": (c_int, [c_void_p, C.c_char_p]),
     "pfcore_map_capacity": (c_int, [c_void_p]),
+    "pfcore_landmarks_new": (c_void_p, []),
+    "pfcore_landmarks_free": (None, [c_void_p]),
+    "pfcore_landmarks_add": (c_int, [c_void_p, c_int, c_double, c_double, c_double]),
+    "pfcore_landmarks_has": (c_int, [c_void_p, c_int]),
+    "pfcore_landmarks_at": (c_int, [c_void_p, c_int, _dp]),
+    "pfcore_landmarks_capacity": (c_int, [c_void_p]),
+    "pfcore_landmarks_len_defined": (c_int, [c_void_p]),
+    "pfcore_landmarks_load_text": (c_int, [c_void_p, C.c_char_p]),
+    "pfcore_filter_set_map": (c_int, [c_void_p, c_void_p]),
     "pfcore_filter_reinitialize": (c_int, [c_void_p, _dp, _dp, _dp]),
     "pfcore_filter_update": (c_int, [c_void_p, POINTER(PfcoreOdom),
                                      POINTER(PfcoreObservation), c_int,
@@ -342,6 +353,59 @@ def estimate_dict(e: PfcoreEstimate) -> dict:
                 valid=bool(e.valid), resampled=bool(e.resampled))
 
 
+class LandmarkMap:
+    """``pf_core::LandmarkMap`` (crates/pf_core/src/landmark_map.rs:7-80):
+    dense id -> 3-D position, host only.  Where the reference panics (a
+    negative id in ``add``, an absent id in ``at``) this raises ValueError;
+    ``load_from_str`` raises ValueError at the first bad line, the lines before
+    it staying in the map as in the reference."""
+
+    def __init__(self):
+        self._m = core().pfcore_landmarks_new()
+        if not self._m:
+            raise MemoryError("pfcore_landmarks_new failed")
+
+    def close(self):
+        if getattr(self, "_m", None):
+            core().pfcore_landmarks_free(self._m)
+            self._m = None
+
+    __del__ = close
+
+    @property
+    def handle(self):
+        return self._m
+
+    def add(self, id: int, position) -> None:
+        p = [float(v) for v in position]
+        if core().pfcore_landmarks_add(self._m, int(id), p[0], p[1], p[2]) != 0:
+            raise ValueError(core().pfcore_last_error().decode())
+
+    def has(self, id: int) -> bool:
+        return core().pfcore_landmarks_has(self._m, int(id)) == 1
+
+    def at(self, id: int) -> np.ndarray:
+        out = np.zeros(3)
+        if core().pfcore_landmarks_at(self._m, int(id), dptr(out)) != 0:
+            raise ValueError(core().pfcore_last_error().decode())
+        return out
+
+    def capacity(self) -> int:
+        return int(core().pfcore_landmarks_capacity(self._m))
+
+    def len_defined(self) -> int:
+        return int(core().pfcore_landmarks_len_defined(self._m))
+
+    def is_empty(self) -> bool:
+        return self.len_defined() == 0
+
+    def load_from_str(self, text: str) -> int:
+        n = core().pfcore_landmarks_load_text(self._m, text.encode())
+        if n < 0:
+            raise ValueError(core().pfcore_last_error().decode())
+        return n
+
+
 class ParticleFilter:
     """``pf_core::ParticleFilter`` with the CUDA backend (through libpf_core)."""
 
@@ -378,11 +442,19 @@ class ParticleFilter:
     def handle(self):
         return core().pfcore_filter_handle(self._h)
 
-    def set_map(self, landmarks: dict):
+    def set_map(self, landmarks):
+        """A ``LandmarkMap`` (copied, as ``ParticleFilter::set_map``) or a
+        dict id -> (x, y, z)."""
         lib = core()
+        if isinstance(landmarks, LandmarkMap):
+            if lib.pfcore_filter_set_map(self._h, landmarks.handle) != 0:
+                raise RuntimeError("set_map failed")
+            return
         lib.pfcore_map_clear(self._h)
         for i, p in landmarks.items():
-            lib.pfcore_map_add(self._h, int(i), float(p[0]), float(p[1]), float(p[2]))
+            if lib.pfcore_map_add(self._h, int(i), float(p[0]), float(p[1]),
+                                  float(p[2])) != 0:
+                raise ValueError(lib.pfcore_last_error().decode())
 
     def load_map_text(self, text: str) -> int:
         lib = core()
@@ -674,6 +746,11 @@ class BatchPF:
 
     def use_graph(self, on: bool):
         self._ok(self.lib.pfc_batch_use_graph(self._h, 1 if on else 0), "use_graph")
+
+    def set_wait_test(self, spin_limit: int = 0, stall_filter: int = -1):
+        """Bounded-wait test hook (pfc_batch_set_wait_test)."""
+        self._ok(self.lib.pfc_batch_set_wait_test(self._h, int(spin_limit),
+                                                  int(stall_filter)), "set_wait_test")
 
     def tiles(self):
         t = np.zeros(4, np.int32)

@@ -27,6 +27,7 @@
 // never enter the bottom-k.  The bound is the k-th best composite key of a
 // fully scored seed batch, tightened after every chunk.  Selected results
 // are identical to exhaustive scoring.
+#include <limits.h>
 #include <math.h>
 #include <stdint.h>
 #include <string.h>
@@ -56,10 +57,11 @@ GlHandle* as_gl(void* h) { return static_cast<GlHandle*>(h); }
 // counter (i, 0, 0, RNG_GL).
 __global__ void k_gl_gen(int n, int n_yaw, int nfree, const int2* __restrict__ free_cells,
                          float ox, float oy, float res, uint64_t seed,
-                         float* __restrict__ hyp) {
+                         float* __restrict__ hyp, int p0) {
     const int i = blockIdx.x * kThreads + threadIdx.x;
     if (i >= n) return;
-    const int p = i / n_yaw, j = i - p * n_yaw;
+    const int pl = i / n_yaw, j = i - pl * n_yaw;
+    const int p = p0 + pl;  // global position index: the Philox counter
     const U4 r = philox4x32_10({(uint32_t)p, 0u, 0u, RNG_GL}, (uint32_t)seed,
                                (uint32_t)(seed >> 32));
     const float ux = u01_open(r.x), uy = u01_open(r.y), uz = u01_open(r.z),
@@ -882,17 +884,21 @@ int gl_topk_exhaustive(GlHandle* h, int nrays, float rmax, float span, int k,
     return copy_topk(h, sorted, k, out3k, caer_k, idx_k);
 }
 
-int gl_generate(GlHandle* h, int n_pos, int n_yaw, uint64_t seed) {
-    if (h->nfree <= 0 || n_pos <= 0 || n_yaw <= 0) return -1;
+int gl_generate_range(GlHandle* h, int p0, int n_pos, int n_yaw, uint64_t seed) {
+    if (h->nfree <= 0 || p0 < 0 || n_pos <= 0 || n_yaw <= 0) return -1;
     const long long n = (long long)n_pos * n_yaw;
-    if (n > h->cap_hyp) return -1;
+    if (n > h->cap_hyp || (long long)p0 + n_pos > INT_MAX) return -1;
     h->nh = (int)n;
     k_gl_gen<<<ceil_div(h->nh, kThreads), kThreads, 0, h->stream>>>(
         h->nh, n_yaw, h->nfree, h->d_free, h->ox, h->oy, h->res, seed,
-        h->d_hyp);
+        h->d_hyp, p0);
     PFB_KL();
     h->caer_valid = false;
     return 0;
+}
+
+int gl_generate(GlHandle* h, int n_pos, int n_yaw, uint64_t seed) {
+    return gl_generate_range(h, 0, n_pos, n_yaw, seed);
 }
 
 // Up to 64k hypotheses: a seed batch scored exhaustively, the bound set from
@@ -1126,6 +1132,13 @@ int pfgl_generate_yaws(void* hv, int n_pos, int n_yaw, unsigned long long seed) 
     GlHandle* h = as_gl(hv);
     if (!h) return -1;
     return gl_generate(h, n_pos, n_yaw, seed);
+}
+
+int pfgl_generate_yaws_range(void* hv, int p0, int n_pos, int n_yaw,
+                             unsigned long long seed) {
+    GlHandle* h = as_gl(hv);
+    if (!h) return -1;
+    return gl_generate_range(h, p0, n_pos, n_yaw, seed);
 }
 
 int pfgl_set_hyps(void* hv, const float* hyp3n, int n) {

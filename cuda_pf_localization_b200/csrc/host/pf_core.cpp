@@ -44,14 +44,44 @@ struct LandmarkMap {
                positions[(size_t)id].has_value();
     }
     size_t capacity() const { return positions.size(); }
+    size_t len_defined() const {
+        size_t n = 0;
+        for (const auto& p : positions) n += p.has_value();
+        return n;
+    }
 
-    // load_from_str: "#" comments; "[", "]", ":", "," become spaces; exactly
-    // four numbers per non-empty line; the id is parsed as f64 then cast.
+    // Rust's f64 grammar (str::parse::<f64>): optional sign, then digits with
+    // an optional '.' and exponent, or inf / infinity / nan in any case.
+    // strtod also takes hexadecimal and "nan(...)" forms, which Rust rejects.
+    static bool parse_f64(const std::string& s, double& v) {
+        if (s.empty()) return false;
+        for (char c : s)
+            if (c == 'x' || c == 'X' || c == '(' || c == ')' || isspace((unsigned char)c))
+                return false;
+        char* end = nullptr;
+        v = strtod(s.c_str(), &end);
+        return end != s.c_str() && *end == '\0';
+    }
+
+    // Rust's `f64 as i32`: truncation toward zero, saturating at the i32
+    // range, NaN -> 0.
+    static long long saturating_i32(double v) {
+        if (std::isnan(v)) return 0;
+        if (v >= 2147483647.0) return 2147483647;
+        if (v <= -2147483648.0) return -2147483648LL;
+        return (long long)v;
+    }
+
+    // load_from_str (landmark_map.rs:59-80): '#' starts a comment; '[', ']',
+    // ':' and ',' become spaces; a non-empty line must hold exactly four
+    // numbers; the id is parsed as f64 and cast.  Each line is added as it is
+    // parsed, so the lines before a bad one stay in the map, as in the
+    // reference.  A negative id is an error here (the reference's add()
+    // panics on it).
     int load_from_str(const std::string& text, std::string& err) {
         std::istringstream in(text);
         std::string line;
         int count = 0, lineno = 0;
-        std::vector<std::pair<int, Vec3>> staged;
         while (std::getline(in, line)) {
             ++lineno;
             const size_t hash = line.find('#');
@@ -70,17 +100,20 @@ struct LandmarkMap {
             }
             double v[4];
             for (int k = 0; k < 4; ++k) {
-                char* end = nullptr;
-                v[k] = strtod(toks[(size_t)k].c_str(), &end);
-                if (end == toks[(size_t)k].c_str() || *end != '\0') {
-                    err = "line " + std::to_string(lineno) + ": invalid float";
+                if (!parse_f64(toks[(size_t)k], v[k])) {
+                    err = "line " + std::to_string(lineno) + ": invalid float literal";
                     return -1;
                 }
             }
-            staged.push_back({(int)v[0], Vec3{v[1], v[2], v[3]}});
+            const long long id = saturating_i32(v[0]);
+            if (id < 0) {
+                err = "line " + std::to_string(lineno) +
+                      ": landmark ids must be non-negative";
+                return -1;
+            }
+            add((int)id, Vec3{v[1], v[2], v[3]});
             ++count;
         }
-        for (auto& s : staged) add(s.first, s.second);
         return count;
     }
 };
@@ -281,9 +314,8 @@ void pfcore_filter_free(void* p) { delete static_cast<ParticleFilter*>(p); }
 
 int pfcore_map_add(void* p, int id, double x, double y, double z) {
     ParticleFilter* pf = static_cast<ParticleFilter*>(p);
-    if (!pf || id < 0) return -1;
-    pf->map.add(id, Vec3{x, y, z});
-    return 0;
+    if (!pf) return -1;
+    return pfcore_landmarks_add(&pf->map, id, x, y, z);
 }
 
 int pfcore_map_clear(void* p) {
@@ -296,15 +328,85 @@ int pfcore_map_clear(void* p) {
 int pfcore_map_load_text(void* p, const char* text) {
     ParticleFilter* pf = static_cast<ParticleFilter*>(p);
     if (!pf || !text) return -1;
-    std::string err;
-    const int n = pf->map.load_from_str(text, err);
-    if (n < 0) set_err(err);
-    return n;
+    return pfcore_landmarks_load_text(&pf->map, text);
 }
 
 int pfcore_map_capacity(void* p) {
     ParticleFilter* pf = static_cast<ParticleFilter*>(p);
     return pf ? (int)pf->map.capacity() : -1;
+}
+
+// ---- LandmarkMap as a value of its own (landmark_map.rs:7-80), host only.
+
+void* pfcore_landmarks_new(void) { return new (std::nothrow) LandmarkMap(); }
+
+void pfcore_landmarks_free(void* m) { delete static_cast<LandmarkMap*>(m); }
+
+int pfcore_landmarks_add(void* mv, int id, double x, double y, double z) {
+    LandmarkMap* m = static_cast<LandmarkMap*>(mv);
+    if (!m) return -1;
+    if (id < 0) {
+        set_err("landmark ids must be non-negative");
+        return -1;
+    }
+    try {
+        m->add(id, Vec3{x, y, z});
+    } catch (const std::bad_alloc&) {
+        set_err("landmark id too large to allocate");
+        return -1;
+    }
+    return 0;
+}
+
+int pfcore_landmarks_has(void* mv, int id) {
+    const LandmarkMap* m = static_cast<const LandmarkMap*>(mv);
+    return m && m->has(id) ? 1 : 0;
+}
+
+int pfcore_landmarks_at(void* mv, int id, double out[3]) {
+    const LandmarkMap* m = static_cast<const LandmarkMap*>(mv);
+    if (!m || !out || !m->has(id)) {
+        set_err("landmark id not present");
+        return -1;
+    }
+    const Vec3& p = *m->positions[(size_t)id];
+    out[0] = p.x;
+    out[1] = p.y;
+    out[2] = p.z;
+    return 0;
+}
+
+int pfcore_landmarks_capacity(void* mv) {
+    const LandmarkMap* m = static_cast<const LandmarkMap*>(mv);
+    return m ? (int)m->capacity() : -1;
+}
+
+int pfcore_landmarks_len_defined(void* mv) {
+    const LandmarkMap* m = static_cast<const LandmarkMap*>(mv);
+    return m ? (int)m->len_defined() : -1;
+}
+
+int pfcore_landmarks_load_text(void* mv, const char* text) {
+    LandmarkMap* m = static_cast<LandmarkMap*>(mv);
+    if (!m || !text) return -1;
+    std::string err;
+    int n;
+    try {
+        n = m->load_from_str(text, err);
+    } catch (const std::bad_alloc&) {
+        err = "landmark id too large to allocate";
+        n = -1;
+    }
+    if (n < 0) set_err(err);
+    return n;
+}
+
+int pfcore_filter_set_map(void* p, void* mv) {
+    ParticleFilter* pf = static_cast<ParticleFilter*>(p);
+    const LandmarkMap* m = static_cast<const LandmarkMap*>(mv);
+    if (!pf || !m) return -1;
+    pf->map = *m;
+    return 0;
 }
 
 int pfcore_filter_reinitialize(void* p, const double pose[7],

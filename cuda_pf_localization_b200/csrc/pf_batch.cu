@@ -88,6 +88,12 @@ struct BGlobal {
     unsigned tile_counter;
     int heavy_count;
     unsigned err;
+    // look-back polls before a wait gives up (kSpinLimit unless the host
+    // lowers it), and the filter whose first resampling tile publishes its
+    // prefix under a stale epoch (-1: none), so that the waits of its later
+    // tiles run out: both set only by pfc_batch_set_wait_test
+    int spin_limit;
+    int stall_f;
 };
 
 struct Arena {
@@ -121,6 +127,8 @@ __global__ void k_b_init(BCtl* C, BGlobal* G, int nf) {
         G->tile_counter = 0u;
         G->heavy_count = 0;
         G->err = 0u;
+        G->spin_limit = kSpinLimit;
+        G->stall_f = -1;
     }
     if (f >= nf) return;
     BCtl c;
@@ -588,7 +596,9 @@ __global__ void __launch_bounds__(kThreads)
         if (tile == 0) {
             fvals[1] = acc;
             __threadfence();
-            st_release(&fflags[0], (epoch << 2) | TILE_INCL);
+            // a stale epoch (host-planted wait test) is a flag no waiter accepts
+            const unsigned pub = t.f == G->stall_f ? (epoch ^ 0x20000000u) : epoch;
+            st_release(&fflags[0], (pub << 2) | TILE_INCL);
             s_prefix = 0;
         } else {
             fvals[2 * (size_t)tile] = acc;
@@ -598,7 +608,8 @@ __global__ void __launch_bounds__(kThreads)
     }
     __syncthreads();
     if (tile > 0 && warp == 0) {
-        const uint64_t prefix = look_back(fflags, fvals, tile, epoch, &c->err);
+        const uint64_t prefix =
+            look_back(fflags, fvals, tile, epoch, &c->err, G->spin_limit);
         if (lane == 0) {
             fvals[2 * (size_t)tile + 1] = prefix + s_agg;
             __threadfence();
@@ -1377,6 +1388,19 @@ int pfc_batch_get_weights(void* p, int f, float* w) {
     PFB_KL();
     PFB_CK(cudaMemcpyAsync(w, h->d_tmp, sizeof(float) * (size_t)n,
                            cudaMemcpyDeviceToHost, h->stream));
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int pfc_batch_set_wait_test(void* p, int spin_limit, int stall_filter) {
+    BatchHandle* h = as_b(p);
+    if (!h || spin_limit < 0 || stall_filter < -1 || stall_filter >= h->nf) {
+        set_error("pf_b200: pfc_batch_set_wait_test: bad arguments");
+        return -1;
+    }
+    const int v[2] = {spin_limit > 0 ? spin_limit : kSpinLimit, stall_filter};
+    PFB_CK(cudaMemcpyAsync(&h->d_G->spin_limit, v, sizeof(v), cudaMemcpyHostToDevice,
+                           h->stream));
     PFB_CK(cudaStreamSynchronize(h->stream));
     return 0;
 }

@@ -581,9 +581,13 @@ __device__ __forceinline__ void copy_particle(const Planes& src, const Planes& d
 
 // Warp-parallel look-back (run by warp 0 of a tile > 0): returns the sum of
 // all predecessors' weights.  Lane l inspects tile base - l; the nearest
-// predecessor that already knows its inclusive prefix ends the walk.
+// predecessor that already knows its inclusive prefix ends the walk.  After
+// `limit` polls without progress the wait gives up: ERR_SPIN_TIMEOUT is set
+// and the partial sum returned (at most the true prefix, so every count the
+// caller derives from it stays within [0, n]).
 __device__ inline uint64_t look_back(const unsigned* flags, const uint64_t* vals,
-                              int tile, unsigned epoch, unsigned* err) {
+                              int tile, unsigned epoch, unsigned* err,
+                              int limit = kSpinLimit) {
     const int lane = threadIdx.x & 31;
     uint64_t prefix = 0;
     int base = tile - 1;
@@ -597,7 +601,7 @@ __device__ inline uint64_t look_back(const unsigned* flags, const uint64_t* vals
             ready = (f >> 2) == epoch && (f & 3u) != 0u;
         }
         if (!__all_sync(~0u, ready)) {
-            if (++spins > kSpinLimit) {
+            if (++spins > limit) {
                 if (lane == 0) atomicOr(err, ERR_SPIN_TIMEOUT);
                 return prefix;
             }

@@ -1,15 +1,23 @@
 """Host-side plumbing for one process per GPU (torch.distributed).
 
-The particle filter does not shard in this library: N GPUs run N independent
-replica filters (weak scaling).  The only cross-rank steps are the barrier
-around a timed region and the max over ranks of the measured times, which
-this module keeps in one place so that the CPU tests can exercise them with
-the gloo backend.
+The single particle filter does not shard in this library: N GPUs run N
+independent replica filters (weak scaling), and the cross-rank steps are the
+barrier around a timed region and the max over ranks of the measured times.
+A global-localization query shards by hypotheses: every rank scores a
+contiguous slice of one global hypothesis set, keeps its k best (CAER,
+global index) keys, and one all-gather of k keys and poses per rank gives the
+global bottom-k (sharded_localize).  This module keeps those steps in one
+place so that the CPU tests can exercise them with the gloo backend.
 """
 from __future__ import annotations
 
 import datetime
 import os
+import socket
+import subprocess
+import sys
+
+import numpy as np
 
 
 def world_info() -> tuple[int, int, int]:
@@ -63,3 +71,154 @@ def finish(dist):
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ------------------------------------------------------------ rank launch
+
+def launch_plan(gpus: int, env=None) -> tuple[str, int]:
+    """What a benchmark process asked for ``gpus`` GPUs should do:
+    ("run", world) when it is already one rank of a torchrun world of that
+    size (or a single process for gpus == 1), ("spawn", gpus) when gpus > 1
+    and no torchrun environment is present.  A torchrun world of another size
+    is an error."""
+    env = os.environ if env is None else env
+    if gpus < 1:
+        raise ValueError(f"--gpus must be >= 1, got {gpus}")
+    ws = env.get("WORLD_SIZE")
+    if ws is None:
+        return ("spawn", gpus) if gpus > 1 else ("run", 1)
+    if int(ws) != gpus:
+        raise ValueError(f"WORLD_SIZE={ws} but --gpus {gpus}")
+    return ("run", int(ws))
+
+
+def free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def spawn_command(script: str, argv: list[str], gpus: int, port: int) -> list[str]:
+    """torchrun command that runs ``script argv`` as ``gpus`` local ranks with
+    the rendezvous on 127.0.0.1."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+            f"--nproc-per-node={gpus}", "--master-addr=127.0.0.1",
+            f"--master-port={port}", script, *argv]
+
+
+def spawn_ranks(script: str, argv: list[str], gpus: int) -> int:
+    """Run ``script`` as ``gpus`` ranks (one process per GPU); returns the
+    launcher's exit code."""
+    return subprocess.call(spawn_command(script, argv, gpus, free_port()))
+
+
+# ------------------------------------------------- sharded global localization
+
+def shard_range(n_units: int, world: int, rank: int) -> tuple[int, int]:
+    """Contiguous slice [a, b) of n_units for this rank (sizes differ by at
+    most one)."""
+    q, r = divmod(int(n_units), int(world))
+    a = rank * q + min(rank, r)
+    return a, a + q + (1 if rank < r else 0)
+
+
+def ordered_u32(caer: np.ndarray) -> np.ndarray:
+    """Unsigned image of a float whose integer order is the float order (the
+    reference's float_as_ordered, src/cuda/pf_kernels.cu:151-155, with the
+    sign bit flipped), as the library's composite keys carry it."""
+    i = np.ascontiguousarray(caer, np.float32).view(np.int32)
+    o = np.where(i >= 0, i, i ^ np.int32(0x7FFFFFFF)).astype(np.int32)
+    return o.view(np.uint32) ^ np.uint32(0x80000000)
+
+
+def composite_keys(caer: np.ndarray, global_idx: np.ndarray) -> np.ndarray:
+    """(ordered CAER << 32) | global hypothesis index: ascending order is a
+    stable sort by CAER, ties to the lower index."""
+    return (ordered_u32(caer).astype(np.uint64) << np.uint64(32)) | \
+        np.asarray(global_idx, np.uint64)
+
+
+_NO_KEY = np.uint64(0xFFFFFFFFFFFFFFFF)
+
+
+def merge_bottom_k(keys: np.ndarray, poses: np.ndarray, k: int, dist, device=None):
+    """Global bottom-k from every rank's local candidates: the k smallest local
+    keys of each rank go through one all-gather of k (key, pose) slots per
+    rank (empty slots carry the all-ones key), then the k smallest keys of
+    the union are kept.  Keys are unique (they hold the global index), so the
+    result is the bottom-k of the union exactly.  With dist None the local
+    candidates are the union (one rank, or ranks emulated in one process).
+    Returns (keys, poses) ascending."""
+    keys = np.asarray(keys, np.uint64)
+    poses = np.asarray(poses, np.float32).reshape(-1, 3)
+    first = np.argsort(keys, kind="stable")[:k]
+    kk = np.full(k, _NO_KEY, np.uint64)
+    pp = np.zeros((k, 3), np.float32)
+    kk[:len(first)] = keys[first]
+    pp[:len(first)] = poses[first]
+    if dist is not None:
+        import torch
+        dev = device if device is not None else torch.device("cpu")
+        world = dist.get_world_size()
+        tk = torch.from_numpy(kk.view(np.int64).copy()).to(dev)
+        tp = torch.from_numpy(pp.copy()).to(dev)
+        gk = [torch.empty_like(tk) for _ in range(world)]
+        gp = [torch.empty_like(tp) for _ in range(world)]
+        dist.all_gather(gk, tk)
+        dist.all_gather(gp, tp)
+        kk = np.concatenate([g.cpu().numpy() for g in gk]).view(np.uint64)
+        pp = np.concatenate([g.cpu().numpy() for g in gp])
+    order = np.argsort(kk, kind="stable")[:k]
+    order = order[kk[order] != _NO_KEY]
+    return kk[order], pp[order]
+
+
+def key_caer(keys: np.ndarray) -> np.ndarray:
+    """CAER of composite keys (inverse of ordered_u32)."""
+    hi = (np.asarray(keys, np.uint64) >> np.uint64(32)).astype(np.uint32) ^ \
+        np.uint32(0x80000000)
+    o = hi.view(np.int32)
+    return np.where(o >= 0, o, o ^ np.int32(0x7FFFFFFF)).astype(np.int32).view(np.float32)
+
+
+def local_bottom_k(gl_handle, scan: np.ndarray, n_pos: int, n_yaw: int, seed: int,
+                   k: int, world: int, rank: int, rmax: float = 10.0,
+                   span: float = 2 * np.pi):
+    """This rank's part of a sharded CBGL query: positions shard_range(n_pos,
+    world, rank) of the dispersion pfgl_generate_yaws(n_pos, n_yaw, seed),
+    scored by the pruned localizer of this rank's GPU; returns its k best
+    (composite keys with global indices, poses)."""
+    from . import fptr, iptr, kernels, last_error
+    lib = kernels()
+    p0, p1 = shard_range(n_pos, world, rank)
+    if p1 <= p0:
+        return np.zeros(0, np.uint64), np.zeros((0, 3), np.float32)
+    if lib.pfgl_generate_yaws_range(gl_handle, p0, p1 - p0, n_yaw, seed) != 0:
+        raise RuntimeError("pfgl_generate_yaws_range failed: " + last_error())
+    kl = min(k, (p1 - p0) * n_yaw)
+    out = np.zeros(3 * kl, np.float32)
+    cs = np.zeros(kl, np.float32)
+    ids = np.zeros(kl, np.int32)
+    scan = np.ascontiguousarray(scan, np.float32)
+    r = lib.pfgl_localize(gl_handle, fptr(scan), len(scan), rmax, span, kl, fptr(out),
+                          fptr(cs), iptr(ids))
+    if r < 0:
+        raise RuntimeError("pfgl_localize failed: " + last_error())
+    keys = composite_keys(cs[:r], ids[:r].astype(np.int64) + p0 * n_yaw)
+    return keys, out[:3 * r].reshape(r, 3)
+
+
+def sharded_localize(gl_handle, scan: np.ndarray, n_pos: int, n_yaw: int, seed: int,
+                     k: int, dist, device=None, rmax: float = 10.0,
+                     span: float = 2 * np.pi):
+    """One CBGL query over n_pos positions x n_yaw yaws, its positions split
+    across the ranks of ``dist`` (None: one rank): local_bottom_k on every
+    rank, then merge_bottom_k.  Returns (keys, poses, caer, global indices)
+    of the global bottom-k, ascending: identical to localizing the whole set
+    on one GPU."""
+    world = dist.get_world_size() if dist is not None else 1
+    rank = dist.get_rank() if dist is not None else 0
+    keys, poses = local_bottom_k(gl_handle, scan, n_pos, n_yaw, seed, k, world, rank,
+                                 rmax, span)
+    kk, pp = merge_bottom_k(keys, poses, k, dist, device)
+    return kk, pp, key_caer(kk), (kk & np.uint64(0xFFFFFFFF)).astype(np.int64)

@@ -83,6 +83,25 @@ int pfcore_map_clear(void* pf);
 int pfcore_map_load_text(void* pf, const char* text);
 int pfcore_map_capacity(void* pf);
 
+/* LandmarkMap as a value of its own (crates/pf_core/src/landmark_map.rs:7-80),
+ * host only, no device needed.  new/add/has/at/capacity/len_defined/
+ * load_from_str keep the reference's meaning; where the reference panics
+ * (a negative id in add, an absent id in at) these return -1 with a message
+ * in pfcore_last_error.  load_text returns the number of lines read, or -1 at
+ * the first bad line, the lines before it staying in the map as in the
+ * reference. */
+void* pfcore_landmarks_new(void);
+void pfcore_landmarks_free(void* map);
+int pfcore_landmarks_add(void* map, int id, double x, double y, double z);
+int pfcore_landmarks_has(void* map, int id);
+int pfcore_landmarks_at(void* map, int id, double out_xyz[3]);
+int pfcore_landmarks_capacity(void* map);
+int pfcore_landmarks_len_defined(void* map);
+int pfcore_landmarks_load_text(void* map, const char* text);
+/* ParticleFilter::set_map (crates/pf_core/src/particle_filter.rs:88-90): the
+ * filter takes a copy. */
+int pfcore_filter_set_map(void* pf, void* map);
+
 /* ParticleFilter::reinitialize: pose = (x,y,z, qw,qx,qy,qz). */
 int pfcore_filter_reinitialize(void* pf, const double pose[7],
                                const double pos_std[3],

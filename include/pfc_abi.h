@@ -293,6 +293,12 @@ int pfc_set_weight_kernel(void* h, int variant);
 /* n_pos uniform free-space positions x n_yaw yaws theta0 + j*2*pi/n_yaw
  * (theta0 uniform per position); hypothesis index = pos*n_yaw + j. */
 int pfgl_generate_yaws(void* h, int n_pos, int n_yaw, unsigned long long seed);
+/* Positions [p0, p0 + n_pos) of that same dispersion (hypothesis index on
+ * this handle = (pos - p0)*n_yaw + j): one rank's slice of a global
+ * hypothesis set, identical to the corresponding rows of pfgl_generate_yaws
+ * with n_pos >= p0 + n_pos positions. */
+int pfgl_generate_yaws_range(void* h, int p0, int n_pos, int n_yaw,
+                             unsigned long long seed);
 
 /* Set / read hypotheses directly (3n floats x,y,theta). */
 int pfgl_set_hyps(void* h, const float* hyp3n, int n);
@@ -417,6 +423,16 @@ int pfc_batch_size(void* b, int f);
 void* pfc_batch_stream(void* b);
 /* Kernels launched by this handle so far (a graph launch counts its kernels). */
 long long pfc_batch_launches(void* b);
+/* Test hook for the bounded device waits (no counterpart in the reference).
+ * spin_limit: polls before a resampling look-back gives up (0 restores the
+ * default of 2^22).  stall_filter: a filter whose first resampling tile
+ * publishes its prefix under a stale epoch, a flag no waiter accepts, so the
+ * look-backs of its later tiles run out (-1: none).  A wait that runs out
+ * sets an error bit: the cycle call (or pfc_batch_result) returns -1 with
+ * "look-back wait timed out" in pfc_last_error_message(), and the handle keeps
+ * failing from then on (its particles are no longer trustworthy); other
+ * handles and the CUDA context are unaffected. */
+int pfc_batch_set_wait_test(void* b, int spin_limit, int stall_filter);
 
 /* ------------------------------------------------------------------------
  * Learned proposal for global localization (no counterpart in the

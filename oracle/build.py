@@ -1,14 +1,16 @@
 """Build the test-only checkers under oracle/ (TEST INFRASTRUCTURE ONLY).
 
-    python oracle/build.py            # liboracle.so (+ _ref/ when the reference is present)
+    python oracle/build.py                       # liboracle.so
+    PF_REFERENCE=<reference checkout> python oracle/build.py   # + _ref/
 
 * oracle/liboracle.so — the C++ restatement of the reference's CPU path
   (pf_oracle.cpp), built with g++ and OpenMP.
 * oracle/_ref/libpf_kernels_ref.so — the reference's own CUDA library,
   compiled for sm_100a from its source file where it lies (read-only, never
-  copied) together with ref_shim.cu's test accessors.  Built only when the
-  reference tree exists (PF_REFERENCE, default /root/reference); the GPU box
-  uses the prebuilt file.
+  copied) together with ref_shim.cu's test accessors.  Built only when a
+  reference checkout is named (the `reference` argument or the PF_REFERENCE
+  environment variable) and holds that file; otherwise an already built
+  library is used as it is.
 """
 from __future__ import annotations
 
@@ -18,7 +20,6 @@ import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REF_ROOT = Path(os.environ.get("PF_REFERENCE", "/root/reference"))
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 
@@ -44,10 +45,11 @@ def build_oracle(force: bool = False) -> Path:
     return out
 
 
-def build_ref(force: bool = False) -> Path | None:
-    src = REF_ROOT / "src" / "cuda" / "pf_kernels.cu"
+def build_ref(force: bool = False, reference: str | Path | None = None) -> Path | None:
     out = HERE / "_ref" / "libpf_kernels_ref.so"
-    if not src.exists():
+    root = reference or os.environ.get("PF_REFERENCE")
+    src = Path(root) / "src" / "cuda" / "pf_kernels.cu" if root else None
+    if src is None or not src.exists():
         return out if out.exists() else None
     if force or _stale(out, [src, HERE / "ref_shim.cu"]):
         out.parent.mkdir(exist_ok=True)
