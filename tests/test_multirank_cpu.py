@@ -81,10 +81,10 @@ sys.path.insert(0, {root!r})
 from cuda_pf_localization_b200 import multi
 dist = multi.init("gloo", timeout_s=30)
 m = multi.max_over_ranks([float(os.environ["RANK"])], dist, None)
-sys.stdout.write(f"rank {os.environ['RANK']} of {os.environ['WORLD_SIZE']} max {m[0]}\n")
+sys.stdout.write("rank %s of %s max %s\\n" % (os.environ["RANK"], os.environ["WORLD_SIZE"], m[0]))
 sys.stdout.flush()
 multi.finish(dist)
-"""
+"""  # one write per line: the ranks' output is unbuffered and shares one pipe
 
 
 def test_spawn_ranks_runs_one_process_per_rank(tmp_path):
