@@ -196,6 +196,10 @@ _KERNEL_SIGS = {
     "pfgl_learned_norm": (c_int, [c_void_p, _fp]),
     "pfgl_learned_localize": (c_int, [c_void_p, _fp, c_int, c_float, c_float, c_int, c_int,
                                       c_int, _fp, _fp, _ip, _ip]),
+    "pfgl_learned_localize_batch": (c_int, [c_void_p, _fp, c_int, c_int, c_float, c_float,
+                                            c_int, c_int, c_int, _fp, _fp, _ip, _ip]),
+    "pfgl_localize_batch": (c_int, [c_void_p, _fp, c_int, c_int, c_float, c_float, c_int,
+                                    c_int, POINTER(c_ulonglong), c_int, _fp, _fp, _ip]),
     "pfgl_learned_calibrate": (c_int, [c_void_p, c_int, c_int, c_float, c_float, c_float,
                                        c_int, c_float, c_ulonglong, _fp, _fp]),
     "pfgl_learned_set_threshold": (c_int, [c_void_p, c_float]),
@@ -625,6 +629,23 @@ class LearnedProposal:
     def set_threshold(self, tau: float):
         self._ok(self.lib.pfgl_learned_set_threshold(self._h, float(tau)), "set_threshold")
 
+    def localize_batch(self, scans: np.ndarray, n_samples=1000, n_fallback=200000, k=64,
+                       rmax=10.0, span=2 * np.pi):
+        """``pfgl_learned_localize_batch``: returns (poses nq x k x 3, CAERs
+        nq x k, sample indices nq x k, info nq)."""
+        scans = np.ascontiguousarray(scans, np.float32)
+        nq, nrays = scans.shape
+        kk = min(k, n_samples)
+        out = np.zeros((nq, kk, 3), np.float32)
+        cs = np.zeros((nq, kk), np.float32)
+        ids = np.zeros((nq, kk), np.int32)
+        info = np.zeros(nq, np.int32)
+        self._ok(self.lib.pfgl_learned_localize_batch(self._h, fptr(scans), nq, nrays, rmax,
+                                                      span, n_samples, n_fallback, kk,
+                                                      fptr(out), fptr(cs), iptr(ids),
+                                                      iptr(info)), "localize_batch")
+        return out, cs, ids, info
+
     def localize(self, scan: np.ndarray, n_samples=20000, n_fallback=200000, k=64,
                  rmax=10.0, span=2 * np.pi):
         scan = np.ascontiguousarray(scan, np.float32)
@@ -637,6 +658,25 @@ class LearnedProposal:
                                                     fptr(cs), iptr(ids), iptr(info)),
                      "localize")
         return out[:3 * r].reshape(r, 3), cs[:r], ids[:r], int(info[0])
+
+
+def localize_batch(gl_handle, scans: np.ndarray, n_pos: int, n_yaw: int, seeds, k=64,
+                   rmax=10.0, span=2 * np.pi):
+    """Batched uniform CBGL (``pfgl_localize_batch``): query q scored against
+    its own dispersion (n_pos x n_yaw, seeds[q]).  Returns (poses nq x k x 3,
+    CAERs nq x k, indices nq x k)."""
+    scans = np.ascontiguousarray(scans, np.float32)
+    nq, nrays = scans.shape
+    sd = np.ascontiguousarray(seeds, np.uint64)
+    out = np.zeros((nq, k, 3), np.float32)
+    cs = np.zeros((nq, k), np.float32)
+    ids = np.zeros((nq, k), np.int32)
+    r = kernels().pfgl_localize_batch(gl_handle, fptr(scans), nq, nrays, rmax, span, n_pos,
+                                      n_yaw, sd.ctypes.data_as(POINTER(c_ulonglong)), k,
+                                      fptr(out), fptr(cs), iptr(ids))
+    if r < 0:
+        raise RuntimeError("pfgl_localize_batch failed: " + last_error())
+    return out[:, :r], cs[:, :r], ids[:, :r]
 
 
 def render_scans(gl_handle, poses: np.ndarray, nrays=360, rmax=10.0, span=2 * np.pi,

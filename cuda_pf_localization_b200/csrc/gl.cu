@@ -75,6 +75,31 @@ __global__ void k_gl_gen(int n, int n_yaw, int nfree, const int2* __restrict__ f
     hyp[3 * i + 2] = th;
 }
 
+// Dispersions of many queries: query q's n_pos x n_yaw hypotheses (k_gl_gen
+// with seeds[q]) at [q * n_pos * n_yaw, ...).
+__global__ void k_gl_gen_multi(int per_q, int n_yaw, int nfree,
+                               const int2* __restrict__ free_cells, float ox, float oy,
+                               float res, const uint64_t* __restrict__ seeds,
+                               float* __restrict__ hyp) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= per_q) return;
+    const int q = blockIdx.y;
+    const uint64_t seed = seeds[q];
+    const int p = i / n_yaw, j = i - p * n_yaw;
+    const U4 r = philox4x32_10({(uint32_t)p, 0u, 0u, RNG_GL}, (uint32_t)seed,
+                               (uint32_t)(seed >> 32));
+    const float ux = u01_open(r.x), uy = u01_open(r.y), uz = u01_open(r.z),
+                uw = u01_open(r.w);
+    const int c = min((int)(uw * (float)nfree), nfree - 1);
+    const int2 cell = free_cells[c];
+    float th = -3.14159265f + 6.28318530f * uz;
+    if (n_yaw > 1) th = th + (6.28318530f / (float)n_yaw) * (float)j;
+    float* o = hyp + 3 * ((size_t)q * per_q + i);
+    o[0] = ox + ((float)cell.x + ux) * res;
+    o[1] = oy + ((float)cell.y + uy) * res;
+    o[2] = th;
+}
+
 // ------------------------------------------------------------------ raycast
 
 // CAER of one hypothesis by one warp, with rays handed out dynamically: a
@@ -299,6 +324,43 @@ __global__ void __launch_bounds__(kScoreThreads, 2)
                 }
             }
         }
+        __syncwarp();
+    }
+}
+
+// CAER of the hypotheses of many queries in one launch (exhaustive): the
+// hypotheses of query q are [q * per_q, (q + 1) * per_q) and its scan is
+// scans + q * nrays in global memory (each ray's term reads one scan value
+// when the ray ends; the scan stays L1-resident).  Per hypothesis the same
+// warp_caer as the single-query scorer, so every CAER equals the single-query
+// scorer's value bit for bit.  Shared memory: [padded grid (kSmem)] [per-warp
+// ray slots].
+template <bool kSmem>
+__global__ void __launch_bounds__(kScoreThreads, 2)
+    k_gl_score_multi(GridView gv, int grid_bytes, const float* __restrict__ hyp,
+                     int nh, int per_q, const float* __restrict__ scans, int nrays,
+                     float rmax, float span, float* __restrict__ caer) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    if (kSmem) {
+        const int nv = grid_bytes / 16;
+        const uint4* src = reinterpret_cast<const uint4*>(gv.cells);
+        uint4* dst = reinterpret_cast<uint4*>(smem);
+        for (int k = threadIdx.x; k < nv; k += blockDim.x) dst[k] = __ldg(&src[k]);
+    }
+    __syncthreads();
+    const unsigned char* g = kSmem ? smem : gv.cells;
+    float2* dirs = reinterpret_cast<float2*>(smem + (kSmem ? grid_bytes : 0)) +
+                   (size_t)(threadIdx.x >> 5) * nrays;
+    float* term = reinterpret_cast<float*>(dirs);
+    const int Hp = gv.H + 2;
+    const int gw = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;
+    const int nw = gridDim.x * kScoreWarps;
+    for (int h = gw; h < nh; h += nw) {
+        const float* sc = scans + (size_t)(h / per_q) * nrays;
+        const float c = warp_caer<false>(g, gv, Hp, hyp[3 * h], hyp[3 * h + 1],
+                                         hyp[3 * h + 2], sc, nrays, rmax, span, term,
+                                         dirs, 0.f);
+        if ((threadIdx.x & 31) == 0) caer[h] = c;
         __syncwarp();
     }
 }
@@ -544,17 +606,25 @@ __device__ __forceinline__ uint64_t warp_max_u64(uint64_t v) {
 
 // The k smallest of n keys, ascending, into out[0, k) (out[j] = ~0 for
 // j >= n).  n_dev (optional): the key count in device memory, at most n.
+// Segmented form: block b selects from the segment starting at element
+// b * seg_stride of caer / keys (counts n_dev[b]) into out[b * k, b * k + k);
+// the index word of a key is the element's index within its segment.
 template <bool kFromCaer, bool kDroppedLast>
 __global__ void __launch_bounds__(kSelThreads)
     k_select_small(const float* __restrict__ caer, const uint64_t* __restrict__ keys,
-                   int n, const unsigned* n_dev, int k, uint64_t* __restrict__ out) {
+                   int n, const unsigned* n_dev, int k, uint64_t* __restrict__ out,
+                   int seg_stride) {
     __shared__ unsigned s_hist[kSelBins];
     __shared__ uint64_t s_list[kSelCap];
     __shared__ uint64_t s_red[3][32];
     __shared__ unsigned s_w[32], s_nv[32];
     __shared__ uint64_t s_lo, s_hi;
     __shared__ unsigned s_b, s_cb, s_hb, s_n;
-    if (n_dev) n = min(n, (int)min(*n_dev, 0x7FFFFFFFu));
+    const size_t seg = blockIdx.x;
+    if (caer) caer += seg * (size_t)seg_stride;
+    if (keys) keys += seg * (size_t)seg_stride;
+    out += seg * (size_t)k;
+    if (n_dev) n = min(n, (int)min(n_dev[seg], 0x7FFFFFFFu));
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int kk = max(0, min(k, n));
 
@@ -664,13 +734,13 @@ const uint64_t* small_select(GlHandle* h, const float* caer, const uint64_t* key
     uint64_t* out = h->d_sel;
     if (keys)
         k_select_small<false, false><<<1, kSelThreads, 0, h->stream>>>(nullptr, keys, n,
-                                                                      n_dev, k, out);
+                                                                      n_dev, k, out, 0);
     else if (dropped_last)
         k_select_small<true, true><<<1, kSelThreads, 0, h->stream>>>(caer, nullptr, n,
-                                                                    nullptr, k, out);
+                                                                    nullptr, k, out, 0);
     else
         k_select_small<true, false><<<1, kSelThreads, 0, h->stream>>>(caer, nullptr, n,
-                                                                     nullptr, k, out);
+                                                                     nullptr, k, out, 0);
     if (cudaGetLastError() != cudaSuccess) {
         set_error("pf_b200: bottom-k select launch failed");
         return nullptr;
@@ -690,6 +760,32 @@ __global__ void k_gather_topk(const uint64_t* __restrict__ keys, int k,
     out3[3 * j + 2] = hyp[3 * src + 2];
     outc[j] = caer[src];
     outi[j] = src;
+}
+
+// Bottom-k of many queries: out[q * k + j] from key q * k + j, whose index
+// word is the hypothesis index within query q.  Keys beyond a query's count
+// (all ones) give index -1 and CAER +inf.
+__global__ void k_gather_topk_multi(const uint64_t* __restrict__ keys, int nq, int k,
+                                    int per_q, const float* __restrict__ hyp,
+                                    const float* __restrict__ caer, float* out3,
+                                    float* outc, int* outi) {
+    const int t = blockIdx.x * kThreads + threadIdx.x;
+    if (t >= nq * k) return;
+    const int q = t / k;
+    const uint64_t key = keys[t];
+    if (key == ~0ull) {
+        out3[3 * t] = out3[3 * t + 1] = out3[3 * t + 2] = 0.f;
+        outc[t] = INFINITY;
+        outi[t] = -1;
+        return;
+    }
+    const int loc = (int)(uint32_t)key;
+    const size_t src = (size_t)q * per_q + loc;
+    out3[3 * t] = hyp[3 * src];
+    out3[3 * t + 1] = hyp[3 * src + 1];
+    out3[3 * t + 2] = hyp[3 * src + 2];
+    outc[t] = caer[src];
+    outi[t] = loc;
 }
 
 // Start of the pruned passes: the k smallest keys of the seed batch (sorted)
@@ -865,6 +961,19 @@ int copy_topk(GlHandle* h, const uint64_t* sorted, int k, float* out3k,
     return k;
 }
 
+
+// Device scans of a batch of queries (grown on demand).
+int ensure_scans(GlHandle* h, int count) {
+    if (count > h->scans_cap) {
+        cudaFree(h->d_scans);
+        h->d_scans = nullptr;
+        h->scans_cap = 0;
+        PFB_CK(cudaMalloc((void**)&h->d_scans, sizeof(float) * (size_t)count));
+        h->scans_cap = count;
+    }
+    return 0;
+}
+
 }  // namespace
 
 // ------------------------------------------- entry points shared across units
@@ -936,6 +1045,69 @@ const uint64_t* gl_localize_small_keys(GlHandle* h, int nrays, float rmax,
 }
 
 bool gl_small_select_ok(int n, int k) { return small_select_ok(n, k); }
+
+int gl_upload_scans(GlHandle* h, const float* scans, int nq, int nrays) {
+    if (!scans || nq <= 0 || nrays <= 0) return -1;
+    if (ensure_scans(h, nq * nrays)) return -1;
+    PFB_CK(cudaMemcpyAsync(h->d_scans, scans, sizeof(float) * (size_t)nq * nrays,
+                           cudaMemcpyHostToDevice, h->stream));
+    return 0;
+}
+
+bool gl_batch_ok(const GlHandle* h, int nq, int per_q, int k) {
+    return nq > 0 && per_q > 0 && k > 0 && k <= kSelK && per_q <= kSelMaxN &&
+           (long long)nq * per_q <= h->cap_hyp && (long long)nq * k <= h->cap_hyp;
+}
+
+int gl_localize_batch_enqueue(GlHandle* h, int nq, int per_q, int nrays, float rmax,
+                              float span, int k) {
+    if (!gl_batch_ok(h, nq, per_q, k) || nq * nrays > h->scans_cap) {
+        set_error("pf_b200: batch of %d queries x %d hypotheses (k %d) not supported", nq,
+                  per_q, k);
+        return -1;
+    }
+    const int nh = nq * per_q;
+    h->nh = nh;
+    const int gb = grid_bytes_padded(h);
+    const size_t slots = sizeof(float2) * (size_t)nrays * kScoreWarps;
+    const bool in_smem = (size_t)gb + slots <= (size_t)kMaxSmem;
+    const size_t smem = in_smem ? gb + slots : slots;
+    if (smem > (size_t)kMaxSmem) {
+        set_error("pf_b200: %d rays need too much shared memory", nrays);
+        return -1;
+    }
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const GridView gv = grid_view(h);
+    if (in_smem) {
+        PFB_CK(cudaFuncSetAttribute(k_gl_score_multi<true>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gl_score_multi<true>,
+                                                      kScoreThreads, smem);
+        const int grid = std::min(sms * std::max(per_sm, 1), ceil_div(nh, kMinScoreWarps));
+        k_gl_score_multi<true><<<grid, kScoreThreads, smem, h->stream>>>(
+            gv, gb, h->d_hyp, nh, per_q, h->d_scans, nrays, rmax, span, h->d_caer);
+    } else {
+        PFB_CK(cudaFuncSetAttribute(k_gl_score_multi<false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gl_score_multi<false>,
+                                                      kScoreThreads, smem);
+        const int grid = std::min(sms * std::max(per_sm, 1), ceil_div(nh, kMinScoreWarps));
+        k_gl_score_multi<false><<<grid, kScoreThreads, smem, h->stream>>>(
+            gv, gb, h->d_hyp, nh, per_q, h->d_scans, nrays, rmax, span, h->d_caer);
+    }
+    PFB_KL();
+    h->caer_valid = true;
+    k_select_small<true, false><<<nq, kSelThreads, 0, h->stream>>>(
+        h->d_caer, nullptr, per_q, nullptr, k, h->d_keys, per_q);
+    PFB_KL();
+    k_gather_topk_multi<<<ceil_div(nq * k, kThreads), kThreads, 0, h->stream>>>(
+        h->d_keys, nq, k, per_q, h->d_hyp, h->d_caer, h->d_out, h->d_outc, h->d_outi);
+    PFB_KL();
+    h->last_k = 0;  // d_out holds a batch, not one bottom-k
+    return 0;
+}
 
 int gl_gather_topk(GlHandle* h, const uint64_t* sorted, int k) {
     k_gather_topk<<<ceil_div(k, kThreads), kThreads, 0, h->stream>>>(
@@ -1107,6 +1279,7 @@ int pfgl_destroy(void* hv) {
     cudaFree(h->d_keys_alt);
     cudaFree(h->d_hist);
     cudaFree(h->d_scan);
+    cudaFree(h->d_scans);
     cudaFree(h->d_out);
     cudaFree(h->d_outc);
     cudaFree(h->d_outi);
@@ -1139,6 +1312,66 @@ int pfgl_generate_yaws_range(void* hv, int p0, int n_pos, int n_yaw,
     GlHandle* h = as_gl(hv);
     if (!h) return -1;
     return gl_generate_range(h, p0, n_pos, n_yaw, seed);
+}
+
+int pfgl_localize_batch(void* hv, const float* scans, int nq, int nrays, float rmax,
+                        float ang_span, int n_pos, int n_yaw,
+                        const unsigned long long* seeds, int k, float* out3k,
+                        float* caer_k, int* idx_k) {
+    GlHandle* h = as_gl(hv);
+    clear_error();
+    if (!h || !scans || !seeds || nq <= 0 || nrays <= 0 || n_pos <= 0 || n_yaw <= 0 ||
+        k <= 0 || h->nfree <= 0)
+        return -1;
+    const long long per = (long long)n_pos * n_yaw;
+    if (per > INT_MAX) return -1;
+    const int per_q = (int)per;
+    if (k > per_q) k = per_q;
+    const int chunk = (int)std::min<long long>(nq, h->cap_hyp / std::max(per_q, 1));
+    if (!gl_batch_ok(h, std::max(chunk, 1), per_q, k) || chunk <= 0) {
+        set_error("pf_b200: pfgl_localize_batch: %d hypotheses per query (k %d) exceed the "
+                  "batch limits", per_q, k);
+        return -1;
+    }
+    uint64_t* d_seeds = nullptr;
+    PFB_CK(cudaMalloc((void**)&d_seeds, sizeof(uint64_t) * (size_t)chunk));
+    int rc = 0;
+    for (int q0 = 0; q0 < nq && rc == 0; q0 += chunk) {
+        const int m = std::min(chunk, nq - q0);
+        if (cudaMemcpyAsync(d_seeds, seeds + q0, sizeof(uint64_t) * (size_t)m,
+                            cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+            gl_upload_scans(h, scans + (size_t)q0 * nrays, m, nrays)) {
+            set_error("pf_b200: pfgl_localize_batch: input copy failed");
+            rc = -1;
+            break;
+        }
+        k_gl_gen_multi<<<dim3(ceil_div(per_q, kThreads), m), kThreads, 0, h->stream>>>(
+            per_q, n_yaw, h->nfree, h->d_free, h->ox, h->oy, h->res, d_seeds, h->d_hyp);
+        if (cudaGetLastError() != cudaSuccess) {
+            set_error("pf_b200: pfgl_localize_batch: dispersion launch failed");
+            rc = -1;
+            break;
+        }
+        if (gl_localize_batch_enqueue(h, m, per_q, nrays, rmax, ang_span, k)) {
+            rc = -1;
+            break;
+        }
+        const size_t o = (size_t)q0 * k, mk = (size_t)m * k;
+        if ((out3k && cudaMemcpyAsync(out3k + 3 * o, h->d_out, sizeof(float) * 3 * mk,
+                                      cudaMemcpyDeviceToHost, h->stream) != cudaSuccess) ||
+            (caer_k && cudaMemcpyAsync(caer_k + o, h->d_outc, sizeof(float) * mk,
+                                       cudaMemcpyDeviceToHost, h->stream) != cudaSuccess) ||
+            (idx_k && cudaMemcpyAsync(idx_k + o, h->d_outi, sizeof(int) * mk,
+                                      cudaMemcpyDeviceToHost, h->stream) != cudaSuccess) ||
+            cudaStreamSynchronize(h->stream) != cudaSuccess) {
+            set_error("pf_b200: pfgl_localize_batch: %s",
+                      cudaGetErrorString(cudaGetLastError()));
+            rc = -1;
+        }
+    }
+    cudaStreamSynchronize(h->stream);
+    cudaFree(d_seeds);
+    return rc ? -1 : k;
 }
 
 int pfgl_set_hyps(void* hv, const float* hyp3n, int n) {

@@ -45,6 +45,8 @@ struct GlHandle {
     int hist_cap = 0;
     float* d_scan = nullptr;
     int scan_cap = 0;
+    float* d_scans = nullptr;  // a batch of queries' scans (nq x nrays)
+    int scans_cap = 0;
     float* d_out = nullptr;   // k x 3 (cap_hyp)
     float* d_outc = nullptr;  // k CAER
     int* d_outi = nullptr;    // k indices
@@ -215,5 +217,15 @@ bool gl_small_select_ok(int n, int k);
 // Gathers the poses, CAERs and indices of the k keys into d_out / d_outc /
 // d_outi (asynchronous).
 int gl_gather_topk(GlHandle* h, const uint64_t* sorted, int k);
+// Batches of queries.  gl_upload_scans copies nq host scans into d_scans;
+// gl_localize_batch_enqueue scores the nq * per_q hypotheses in d_hyp
+// (query q's at [q * per_q, (q + 1) * per_q)) exhaustively against their
+// queries' scans in d_scans and writes each query's bottom-k (ascending,
+// indices within the query) to d_out / d_outc / d_outi at [q * k, q * k + k)
+// (asynchronous).  gl_batch_ok: the sizes this supports.
+int gl_upload_scans(GlHandle* h, const float* scans, int nq, int nrays);
+bool gl_batch_ok(const GlHandle* h, int nq, int per_q, int k);
+int gl_localize_batch_enqueue(GlHandle* h, int nq, int per_q, int nrays, float rmax,
+                              float span, int k);
 
 }  // namespace pfb

@@ -937,16 +937,14 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// n hypotheses from the mixture in Z row 0: component by inverse CDF of
-// softmax(logits), then a diagonal Gaussian draw in (x_n, y_n, c, s); yaw =
-// atan2(s, c).  Sample i uses Philox counters (i, query, 0/1, LP_SAMPLE).
-__global__ void k_lp_sample(const float* __restrict__ Z, int n, uint64_t seed,
-                            uint32_t query, float cx, float cy, float sx,
-                            float sy, float* __restrict__ hyp,
-                            const uint32_t* __restrict__ query_dev) {
-    if (query_dev) query = *query_dev;  // graph replay: this query's counter
-    __shared__ float s_cum[kComp];
-    __shared__ float s_mu[4 * kComp], s_sig[4 * kComp];
+// The mixture of one network output row Z in shared memory: cumulative
+// component weights (softmax of the logits), means and standard deviations.
+struct MixtureSmem {
+    float cum[kComp];
+    float mu[4 * kComp], sig[4 * kComp];
+};
+
+__device__ __forceinline__ void load_mixture(const float* __restrict__ Z, MixtureSmem& m) {
     const int t = threadIdx.x;
     if (t < 32) {
         const float l = Z[t];
@@ -959,37 +957,82 @@ __global__ void k_lp_sample(const float* __restrict__ Z, int n, uint64_t seed,
             if (t >= d) c += o;
         }
         const float tot = __shfl_sync(~0u, c, 31);
-        s_cum[t] = c / tot;
+        m.cum[t] = c / tot;
     }
     if (t < 4 * kComp) {
-        s_mu[t] = Z[kMeanOff + t];
+        m.mu[t] = Z[kMeanOff + t];
         const float s = sigmoidf_(Z[kSigOff + t]);
-        s_sig[t] = expf(kLsLo + (kLsHi - kLsLo) * s);
+        m.sig[t] = expf(kLsLo + (kLsHi - kLsLo) * s);
     }
     __syncthreads();
-    const int i = blockIdx.x * blockDim.x + t;
-    if (i >= n) return;
+}
+
+// Sample i of a query: component by inverse CDF, then a diagonal Gaussian
+// draw in (x_n, y_n, c, s); yaw = atan2(s, c).  Philox counters (i, query,
+// 0/1, LP_SAMPLE).
+__device__ __forceinline__ void draw_sample(const MixtureSmem& m, int i, uint64_t seed,
+                                            uint32_t query, float cx, float cy, float sx,
+                                            float sy, float* __restrict__ out3) {
     const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
     const U4 a = philox4x32_10({(uint32_t)i, query, 0u, RNG_LP_SAMPLE}, k0, k1);
     const U4 b = philox4x32_10({(uint32_t)i, query, 1u, RNG_LP_SAMPLE}, k0, k1);
     const float uc = u01_open(a.x);
     int c = kComp - 1;
     for (int j = 0; j < kComp; ++j)
-        if (s_cum[j] >= uc) {
+        if (m.cum[j] >= uc) {
             c = j;
             break;
         }
     const float2 n01 = box_muller(u01_open(a.y), u01_open(a.z));
     const float2 n23 = box_muller(u01_open(a.w), u01_open(b.x));
-    const float* mu = s_mu + 4 * c;
-    const float* sg = s_sig + 4 * c;
+    const float* mu = m.mu + 4 * c;
+    const float* sg = m.sig + 4 * c;
     const float xn = mu[0] + sg[0] * n01.x;
     const float yn = mu[1] + sg[1] * n01.y;
     const float cc = mu[2] + sg[2] * n23.x;
     const float ss = mu[3] + sg[3] * n23.y;
-    hyp[3 * i] = cx + sx * xn;
-    hyp[3 * i + 1] = cy + sy * yn;
-    hyp[3 * i + 2] = atan2f(ss, cc);
+    out3[0] = cx + sx * xn;
+    out3[1] = cy + sy * yn;
+    out3[2] = atan2f(ss, cc);
+}
+
+// n hypotheses from the mixture in Z row 0 (query counter `query`, or read
+// from query_dev on a graph replay).
+__global__ void k_lp_sample(const float* __restrict__ Z, int n, uint64_t seed,
+                            uint32_t query, float cx, float cy, float sx,
+                            float sy, float* __restrict__ hyp,
+                            const uint32_t* __restrict__ query_dev) {
+    if (query_dev) query = *query_dev;  // graph replay: this query's counter
+    __shared__ MixtureSmem m;
+    load_mixture(Z, m);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    draw_sample(m, i, seed, query, cx, cy, sx, sy, hyp + 3 * (size_t)i);
+}
+
+// A batch of queries: query q (blockIdx.y) draws its n samples from output
+// row q of Z with counter query0 + q into hyp[q * n, (q + 1) * n).
+__global__ void k_lp_sample_multi(const float* __restrict__ Z, int n, uint64_t seed,
+                                  uint32_t query0, float cx, float cy, float sx, float sy,
+                                  float* __restrict__ hyp) {
+    const int q = blockIdx.y;
+    __shared__ MixtureSmem m;
+    load_mixture(Z + (size_t)q * kOut, m);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    draw_sample(m, i, seed, query0 + (uint32_t)q, cx, cy, sx, sy,
+                hyp + 3 * ((size_t)q * n + i));
+}
+
+// Network input rows [0, rows) from a batch of device scans: bf16(scan /
+// rmax) zero padded to kIn columns; rows [nq, rows) all zero.
+__global__ void k_query_rows(const float* __restrict__ scans, int nq, int nrays,
+                             float inv_rmax, bf16* __restrict__ x, int rows) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)rows * kIn) return;
+    const int r = (int)(t / kIn), c = (int)(t - (long long)r * kIn);
+    x[t] = __float2bfloat16_rn(r < nq && c < nrays ? scans[(size_t)r * nrays + c] * inv_rmax
+                                                   : 0.0f);
 }
 
 // ------------------------------------------------------------------ handle
@@ -1385,6 +1428,113 @@ int learned_pass(LpHandle* h, int nrays, float rmax, float span, int n_samples,
     g->caer_valid = false;
     // the pruned localizer (one host synchronisation up to 64k samples)
     return gl_localize_loaded(g, nrays, rmax, span, k, out3k, caer_k, idx_k);
+}
+
+// A batch of nq queries whose scans are in gl->d_scans: the nq scan rows
+// through the network with the tiled tcgen05 GEMM (rows padded to a multiple
+// of 128), n_samples mixture samples per query (query counters query_count +
+// q), exhaustive CAER of every sample and each query's bottom-k
+// (gl_localize_batch_enqueue).  Asynchronous; query q's results land in
+// gl->d_out / d_outc / d_outi at [q * k, q * k + k).
+int learned_batch_enqueue(LpHandle* h, int nq, int nrays, float rmax, float span,
+                          int n_samples, int k) {
+    GlHandle* g = h->gl;
+    const int rows = ceil_div(nq, BM) * BM;
+    const long long nx = (long long)rows * kIn;
+    k_query_rows<<<(unsigned)((nx + 255) / 256), 256, 0, h->stream>>>(
+        g->d_scans, nq, nrays, 1.0f / rmax, h->Xp, rows);
+    PFB_KL();
+    if (forward(h, MapRef{&h->tm_Xp, 0, 0}, rows, false)) return -1;
+    k_lp_sample_multi<<<dim3(ceil_div(n_samples, 256), nq), 256, 0, h->stream>>>(
+        h->Z4, n_samples, h->seed ^ 0x5DEECE66DULL, h->query_count, h->cx, h->cy, h->sx,
+        h->sy, g->d_hyp);
+    PFB_KL();
+    h->query_count += (uint32_t)nq;
+    g->caer_valid = false;
+    return gl_localize_batch_enqueue(g, nq, n_samples, nrays, rmax, span, k);
+}
+
+// Queries per chunk of a batch: the GEMM input rows, the hypothesis and
+// result buffers of the map handle.
+int batch_chunk(const LpHandle* h, int nq, int n_samples, int k) {
+    const long long cap = h->gl->cap_hyp;
+    long long c = std::min<long long>(nq, (h->batch / BM) * BM);
+    c = std::min(c, cap / std::max(n_samples, 1));
+    c = std::min(c, cap / std::max(k, 1));
+    return (int)std::max(0LL, c);
+}
+
+// Learned localization of nq host scans in batches.  Query q's k best
+// (poses, CAERs, sample indices) go to out3k/caer_k/idx_k at [q * k, ...);
+// with n_fallback > 0 a query whose best CAER exceeds tau is localized again
+// with n_fallback uniform hypotheses (the better bottom-k is kept; info[q]
+// as pfgl_learned_localize).  best_out (optional): each query's best learned
+// CAER before any fallback.  Returns k (clamped to n_samples) or -1.
+int learned_localize_batch(LpHandle* h, const float* scans, int nq, int nrays, float rmax,
+                           float span, int n_samples, int n_fallback, int k, float tau,
+                           float* out3k, float* caer_k, int* idx_k, int* info,
+                           float* best_out) {
+    GlHandle* g = h->gl;
+    if (k > n_samples) k = n_samples;
+    const int chunk = batch_chunk(h, nq, n_samples, k);
+    if (chunk <= 0 || !gl_batch_ok(g, chunk, n_samples, k)) {
+        set_error("pf_b200: learned batch: %d samples per query (k %d) exceed the batch "
+                  "limits", n_samples, k);
+        return -1;
+    }
+    std::vector<float> o1(3 * (size_t)chunk * k), c1((size_t)chunk * k);
+    std::vector<int> i1((size_t)chunk * k);
+    for (int q0 = 0; q0 < nq; q0 += chunk) {
+        const int m = std::min(chunk, nq - q0);
+        const uint32_t qc0 = h->query_count;
+        if (gl_upload_scans(g, scans + (size_t)q0 * nrays, m, nrays)) return -1;
+        if (learned_batch_enqueue(h, m, nrays, rmax, span, n_samples, k)) return -1;
+        const size_t mk = (size_t)m * k;
+        PFB_CK(cudaMemcpyAsync(o1.data(), g->d_out, sizeof(float) * 3 * mk,
+                               cudaMemcpyDeviceToHost, h->stream));
+        PFB_CK(cudaMemcpyAsync(c1.data(), g->d_outc, sizeof(float) * mk,
+                               cudaMemcpyDeviceToHost, h->stream));
+        PFB_CK(cudaMemcpyAsync(i1.data(), g->d_outi, sizeof(int) * mk,
+                               cudaMemcpyDeviceToHost, h->stream));
+        if (check_err(h)) return -1;  // synchronises
+        for (int q = 0; q < m; ++q) {
+            const size_t o = (size_t)(q0 + q) * k, l = (size_t)q * k;
+            const float best = c1[l];
+            if (best_out) best_out[q0 + q] = best;
+            int which = 0;
+            const float* os = o1.data() + 3 * l;
+            const float* cs = c1.data() + l;
+            const int* is = i1.data() + l;
+            std::vector<float> c2, o2;
+            std::vector<int> i2;
+            if (n_fallback > 0 && !(best <= tau)) {
+                const int n_pos = std::max(1, n_fallback / 16);
+                const int kk = std::min(k, n_pos * 16);
+                c2.assign(k, INFINITY);
+                o2.assign(3 * (size_t)k, 0.f);
+                i2.assign(k, -1);
+                if (gl_upload_scan(g, scans + (size_t)(q0 + q) * nrays, nrays) ||
+                    gl_generate(g, n_pos, 16,
+                                h->seed + 0x9E3779B97F4A7C15ULL * (qc0 + (uint64_t)q + 1)))
+                    return -1;
+                if (gl_localize_loaded(g, nrays, rmax, span, kk, o2.data(), c2.data(),
+                                       i2.data()) <= 0)
+                    return -1;
+                which = 1;
+                if (c2[0] < best) {
+                    which = 2;
+                    os = o2.data();
+                    cs = c2.data();
+                    is = i2.data();
+                }
+            }
+            if (out3k) memcpy(out3k + 3 * o, os, sizeof(float) * 3 * (size_t)k);
+            if (caer_k) memcpy(caer_k + o, cs, sizeof(float) * (size_t)k);
+            if (idx_k) memcpy(idx_k + o, is, sizeof(int) * (size_t)k);
+            if (info) info[q0 + q] = which;
+        }
+    }
+    return k;
 }
 
 }  // namespace lp
@@ -1815,6 +1965,19 @@ int pfgl_learned_localize(void* p, const float* scan, int nrays, float rmax,
     return rk;
 }
 
+int pfgl_learned_localize_batch(void* p, const float* scans, int nq, int nrays,
+                                float rmax, float ang_span, int n_samples, int n_fallback,
+                                int k, float* out3k, float* caer_k, int* idx_k, int* info) {
+    LpHandle* h = as_lp(p);
+    clear_error();
+    if (!h || !scans || nq <= 0 || nrays <= 0 || nrays > kIn || n_samples <= 0 || k <= 0 ||
+        n_fallback < 0 || n_fallback > h->gl->cap_hyp)
+        return -1;
+    return learned_localize_batch(h, scans, nq, nrays, rmax, ang_span, n_samples,
+                                  n_fallback, k, h->tau, out3k, caer_k, idx_k, info,
+                                  nullptr);
+}
+
 int pfgl_learned_calibrate(void* p, int n_queries, int nrays, float rmax,
                            float ang_span, float noise_std, int n_samples,
                            float quantile, unsigned long long seed,
@@ -1841,25 +2004,38 @@ int pfgl_learned_calibrate(void* p, int n_queries, int nrays, float rmax,
     if (pfgl_render_scans(g, poses.data(), n_queries, nrays, rmax, ang_span,
                           noise_std, seed ^ 0xA5A5A5A5ULL, scans.data()))
         return -1;
+    // the held-out queries' best samples: through the batched path, or one
+    // query at a time beyond its sample limit
+    std::vector<float> best3(3 * (size_t)n_queries), bestc((size_t)n_queries);
+    if (gl_batch_ok(g, 1, n_samples, 1)) {
+        if (learned_localize_batch(h, scans.data(), n_queries, nrays, rmax, ang_span,
+                                   n_samples, 0, 1, INFINITY, best3.data(), bestc.data(),
+                                   nullptr, nullptr, nullptr) < 0)
+            return -1;
+    } else {
+        for (int q = 0; q < n_queries; ++q) {
+            int i0;
+            if (gl_upload_scan(g, scans.data() + (size_t)q * nrays, nrays)) return -1;
+            if (learned_pass(h, nrays, rmax, ang_span, n_samples, 1,
+                             best3.data() + 3 * (size_t)q, bestc.data() + q, &i0) <= 0)
+                return -1;
+        }
+        if (check_err(h)) return -1;
+    }
     std::vector<float> good;
     int n_ok = 0;
-    float out3[3], c0;
-    int i0;
     for (int q = 0; q < n_queries; ++q) {
-        if (gl_upload_scan(g, scans.data() + (size_t)q * nrays, nrays)) return -1;
-        if (learned_pass(h, nrays, rmax, ang_span, n_samples, 1, out3, &c0, &i0) <= 0)
-            return -1;
         const float* t = poses.data() + 3 * (size_t)q;
+        const float* out3 = best3.data() + 3 * (size_t)q;
         const double dp = std::hypot((double)out3[0] - t[0], (double)out3[1] - t[1]);
         double dth = std::fmod((double)out3[2] - t[2] + M_PI, 2 * M_PI);
         if (dth < 0) dth += 2 * M_PI;
         dth = std::fabs(dth - M_PI);
         if (dp <= 0.5 && dth <= 0.1) {
             ++n_ok;
-            good.push_back(c0);
+            good.push_back(bestc[(size_t)q]);
         }
     }
-    if (check_err(h)) return -1;
     float tau = INFINITY;
     if (!good.empty()) {
         std::sort(good.begin(), good.end());

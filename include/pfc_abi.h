@@ -300,6 +300,19 @@ int pfgl_generate_yaws(void* h, int n_pos, int n_yaw, unsigned long long seed);
 int pfgl_generate_yaws_range(void* h, int p0, int n_pos, int n_yaw,
                              unsigned long long seed);
 
+/* Batched uniform CBGL (no counterpart in the reference): nq queries, query
+ * q with its own scan (scans + q*nrays) and the dispersion of
+ * pfgl_generate_yaws(n_pos, n_yaw, seeds[q]); every hypothesis scored
+ * exhaustively (the CAERs equal pfgl_score's bit for bit), each query's
+ * bottom-k (stable by CAER, ties to the lower index) written to
+ * out3k/caer_k/idx_k at [q*k, q*k + k) with indices within the query.
+ * Needs n_pos*n_yaw <= 65536 and k <= 128; queries are processed in chunks
+ * of cap_hyp / (n_pos*n_yaw).  Returns k (clamped to n_pos*n_yaw) or -1. */
+int pfgl_localize_batch(void* h, const float* scans, int nq, int nrays, float rmax,
+                        float ang_span, int n_pos, int n_yaw,
+                        const unsigned long long* seeds, int k, float* out3k,
+                        float* caer_k, int* idx_k);
+
 /* Set / read hypotheses directly (3n floats x,y,theta). */
 int pfgl_set_hyps(void* h, const float* hyp3n, int n);
 int pfgl_get_hyps(void* h, float* hyp3n);
@@ -495,9 +508,24 @@ int pfgl_learned_norm(void* lp, float* c4);
 int pfgl_learned_localize(void* lp, const float* scan, int nrays, float rmax,
                           float ang_span, int n_samples, int n_fallback, int k,
                           float* out3k, float* caer_k, int* idx_k, int* info);
+/* Learned localization of nq queries in batches (no counterpart in the
+ * reference): the scans go through the network as rows of one tiled GEMM
+ * per layer, n_samples mixture samples per query are scored exhaustively in
+ * one launch across the batch, and each query's bottom-k is selected by its
+ * own block; results at [q*k, q*k + k) of out3k/caer_k/idx_k, info[q] as
+ * pfgl_learned_localize.  A query whose best CAER exceeds the calibrated
+ * threshold falls back to n_fallback uniform hypotheses (n_fallback = 0:
+ * never).  Needs n_samples <= 65536 and k <= 128.  Returns k (clamped to
+ * n_samples) or -1. */
+int pfgl_learned_localize_batch(void* lp, const float* scans, int nq, int nrays,
+                                float rmax, float ang_span, int n_samples, int n_fallback,
+                                int k, float* out3k, float* caer_k, int* idx_k, int* info);
+
 /* Calibrate the fallback threshold on n_queries held-out poses: the
  * `quantile` of the best CAER over held-out successes (within 0.5 m and
- * 0.1 rad).  Writes the threshold and the held-out success rate. */
+ * 0.1 rad), the queries run through the batched path (one at a time when
+ * n_samples exceeds its limit).  Writes the threshold and the held-out
+ * success rate. */
 int pfgl_learned_calibrate(void* lp, int n_queries, int nrays, float rmax,
                            float ang_span, float noise_std, int n_samples,
                            float quantile, unsigned long long seed,
