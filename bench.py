@@ -2,8 +2,10 @@
 """Benchmark: particle-filter cycle throughput at N = 1M particles on the
 at-scale workload (64 landmarks in a 50 x 50 x 10 m box, 256 observations per
 cycle of which 10 % are outliers, random_inject_ratio 0.01, helix trajectory),
-plus uniform CBGL global-localization solves on 10 x 10 m rooms with 30 box
-obstacles (360 rays, 1M hypotheses = 62 500 positions x 16 yaws, k = 64).
+plus the other workloads of the hot path: the tracking workload (10k
+particles, 12 landmarks, 100 cycles), range-bearing observations at scale,
+batched filters, and global localization (uniform CBGL and the learned
+proposal at iso-success on the same maps and poses).
 
 One step = one full ParticleFilter::update cycle (predict, gated weighting,
 softmax, estimate, resample when ESS < N/2 with injection, estimate) over all
@@ -19,9 +21,11 @@ N particles.  Metric: particle-updates/s = N * steps / time.
 
 --impl reference times the reference's CPU implementation of the same cycle
 (the CPU oracle port of crates/pf_core/src/cpu.rs, all host threads) on the
-same workload, a bounded number of cycles per run.
+same workload: --warmup untimed and --steps timed cycles, each over a bounded
+sample of the particles so the run ends within minutes.
 
-Multi-GPU (torchrun): every rank runs an independent filter of N particles
+Multi-GPU: --gpus N outside torchrun launches N ranks (torch.distributed.run,
+one process per GPU); every rank runs an independent filter of N particles
 (replicas, weak scaling); time = max over ranks.
 """
 from __future__ import annotations
@@ -45,6 +49,7 @@ sys.path.insert(0, str(ROOT))
 METRIC = "PF particle-updates/s @1M"
 UNIT = "particle-updates/s"
 L2_FLUSH_BYTES = 256 << 20
+CPU_RUN_SECONDS = 90.0  # budget of the reference arm's timed cycles
 
 
 def parse():
@@ -57,13 +62,13 @@ def parse():
     ap.add_argument("--seed", type=int, default=11)
     ap.add_argument("--batch-filters", type=int, default=512)
     ap.add_argument("--batch-cycles", type=int, default=200)
-    ap.add_argument("--batch-seq-cycles", type=int, default=5)
+    ap.add_argument("--batch-seq-cycles", type=int, default=20)
     ap.add_argument("--batch-only", action="store_true",
                     help="run only the batched-filter leg and print its JSON")
     ap.add_argument("--gl-only", action="store_true",
                     help="run only the global-localization legs and print their JSON")
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip the GL and CPU-baseline legs")
+                    help="skip the GL, batched, other-workload and CPU-baseline legs")
     ap.add_argument("--gl-hyps", type=int, default=1_000_000)
     ap.add_argument("--gl-trials", type=int, default=20)
     ap.add_argument("--gl-maps", type=int, default=16)
@@ -143,10 +148,12 @@ def gpu_id_for(local_rank: int) -> str:
 
 
 def peaks():
+    """HBM copy bandwidth (GB/s) and where it comes from."""
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return d.get("hbm_gbs", 6650.0), "measured"
+        if "hbm_gbs" in d:
+            return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
 
 
@@ -170,21 +177,33 @@ FILTER = dict(range_noise=0.05, bearing_noise=0.02, gate_sigma=3.0, resample_ess
               random_inject_ratio=0.01)
 
 
+def workload_config(args, world: int) -> dict:
+    """The workload both arms measure (identical dict in both JSON lines)."""
+    return {
+        "workload": "at-scale PF cycle: N=1M f32 particles, 64 landmarks in 50x50x10 m, "
+                    "256 obs/cycle (10% uniform outliers), gate 3 sigma, ESS<N/2 resample, "
+                    "random_inject_ratio 0.01, helix trajectory",
+        "particles": args.particles, "obs_per_cycle": 256,
+        "parallelism": f"replicas x{world}",
+        "l2": "flushed (256 MiB write) between timed GPU steps, outside the timed region",
+    }
+
+
 # ------------------------------------------------------- reference (CPU) arm
 
-def run_cpu_cycles(sc, n, seconds, max_cycles, warm=1):
+def run_cpu_cycles(sc, n, seconds, max_cycles, warm=1, filt=FILTER):
     """The CPU oracle's ParticleFilter::update (cpu.rs restated, OpenMP over the
     par_iter regions) for a bounded number of cycles; returns (cycles, s)."""
     import oracle
-    pf = oracle.OraclePF(n, seed=42, range_noise=FILTER["range_noise"],
-                         bearing_noise=FILTER["bearing_noise"], gate=FILTER["gate_sigma"],
-                         ess_ratio=FILTER["resample_ess_ratio"],
-                         inject=FILTER["random_inject_ratio"])
+    pf = oracle.OraclePF(n, seed=42, range_noise=filt["range_noise"],
+                         bearing_noise=filt["bearing_noise"], gate=filt["gate_sigma"],
+                         ess_ratio=filt["resample_ess_ratio"],
+                         inject=filt["random_inject_ratio"])
     pf.reinit(np.r_[sc.prior_p, sc.prior_q], [0.5] * 3, [0.2] * 3)
     tn, rn = sc.trans_noise, sc.rot_noise
     steps = sc.steps
     for k in range(warm):
-        st = steps[k]
+        st = steps[k % len(steps)]
         pf.update(st.odom_t, st.odom_q, tn, rn, sc.landmarks, st.obs)
     done, t0 = 0, time.perf_counter()
     while done < max_cycles:
@@ -196,25 +215,34 @@ def run_cpu_cycles(sc, n, seconds, max_cycles, warm=1):
     return done, time.perf_counter() - t0
 
 
-def reference_arm(args):
-    import oracle
+def reference_sample(args, sc) -> int:
+    """Particles per timed reference step: the workload's N, or fewer so that
+    warmup + steps cycles fit CPU_RUN_SECONDS (the CPU cost of a cycle is
+    linear in N; one probe cycle at 100k measures it)."""
     n = args.particles
-    # each step is one cycle; the run is capped at a bounded number of cycles
-    sc = scenario(args, max(4, min(args.steps, 64) + args.warmup + 1))
+    probe = min(n, 100_000)
+    _, secs = run_cpu_cycles(sc, probe, 1e9, 1, warm=0)
+    per_particle = secs / probe
+    budget = CPU_RUN_SECONDS / max(1, args.steps + args.warmup)
+    return int(max(10_000, min(n, budget / per_particle)))
+
+
+def reference_arm(args, world):
+    import oracle
+    sc = scenario(args, max(8, min(args.steps + args.warmup, 200)))
     threads = oracle.lib().orc_threads()
-    done, secs = run_cpu_cycles(sc, n, seconds=max(20.0, args.cpu_seconds), max_cycles=args.steps,
-                                warm=max(1, min(args.warmup, 3)))
-    v = n * done / secs
+    ns = reference_sample(args, sc)
+    done, secs = run_cpu_cycles(sc, ns, 1e9, args.steps, warm=args.warmup)
+    v = ns * done / secs
+    sample = (f"{args.warmup} untimed + {done} timed cycles of the workload over {ns} "
+              f"particles each (of N={args.particles}; the CPU cost is linear in N)")
     line = {
-        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": done, "warmup": max(1, min(args.warmup, 3)), "ms_per_step": 1e3 * secs / done,
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+        "steps": done, "warmup": args.warmup, "ms_per_step": 1e3 * secs / done,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic",
-        "config": {"workload": "at-scale PF cycle: N=1M, 64 landmarks (50x50x10 m), 256 obs/cycle "
-                               "(10% outliers), gate 3 sigma, inject 0.01, helix",
-                   "particles": n, "sample": f"{done} of {args.steps} cycles (time-bounded)"},
+        "data": "synthetic", "config": workload_config(args, world),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{done} cycles at N={n}"},
+                         "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -228,18 +256,25 @@ FP32_OPS_PER_PAIR = 29  # gated Cartesian term with the reference's roundings
 # is in profiles/pf_cycle_1M_scale.md): the poses are read from HBM, the
 # predicted poses and log-likelihoods it writes stay in L2.
 KWEIGHT_DRAM_BYTES_1M = 28.7e6 + 0.06e6
+# Algorithmic bytes per particle of each kernel of a resampling cycle, by the
+# library's kernel kinds: weight (fused predict + weighting: pose R 28 + W 28,
+# ll W 4), est (weight pass: ll R 4, w W 4), scan (run starts: w R 4), gather
+# (ancestors R 28, new cloud W 28), covs (pose R 28; uniform weights).
+STAGE_BYTES = {"weight": 60, "est": 8, "scan": 4, "gather": 56, "covs": 28}
+KINDS = ("reinit", "predict", "weight", "est", "covs", "scan", "gather", "inject",
+         "commit", "misc")
 
 
-def profiled_cycles(args):
-    return min(args.steps, 100)
-
-
-def run_value(args, sc, torch, dev, dist=None):
+def run_value(args, sc, torch, dev, dist=None, n=None, steps=None, warmup=None,
+              filt=FILTER, profile=True):
     """Fused cycles with observations resident in HBM; per-step CUDA events."""
     import cuda_pf_localization_b200 as pkg
     lib = pkg.kernels()
-    n = args.particles
-    h = lib.pfc_create(256)
+    n = n or args.particles
+    K = steps if steps is not None else args.steps
+    W = warmup if warmup is not None else args.warmup
+    nobs = len(sc.steps[0].obs)
+    h = lib.pfc_create(max(256, nobs))
     assert h
     try:
         assert lib.pfc_init(h, n, 42) == 0
@@ -249,7 +284,6 @@ def run_value(args, sc, torch, dev, dist=None):
         ps = np.full(3, 0.5, np.float32)
         rs = np.full(3, 0.2, np.float32)
         assert lib.pfc_reinit(h, *map(float, pri), pkg.fptr(ps), pkg.fptr(rs)) == 0
-        nobs = 256
         allobs = np.concatenate([obs_array(st.obs) for st in sc.steps])
         d_obs = torch.from_numpy(allobs.view(np.uint8).copy()).to(dev)
         base = d_obs.data_ptr()
@@ -262,14 +296,12 @@ def run_value(args, sc, torch, dev, dist=None):
             o.tstd[:] = list(sc.trans_noise)
             o.rstd[:] = list(sc.rot_noise)
             odoms.append(o)
-        prm = pkg.PfcCycleParams(FILTER["range_noise"], FILTER["bearing_noise"],
-                                 FILTER["gate_sigma"], FILTER["resample_ess_ratio"],
-                                 FILTER["random_inject_ratio"], 0)
+        prm = pkg.PfcCycleParams(filt["range_noise"], filt["bearing_noise"],
+                                 filt["gate_sigma"], filt["resample_ess_ratio"],
+                                 filt["random_inject_ratio"], 0)
         est = np.zeros(pkg.PFC_EST_LEN)
         stream = torch.cuda.ExternalStream(lib.pfc_stream(h), device=dev)
         flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
-        W, K = args.warmup, args.steps
-        resampled, errs = 0, []
         for k in range(W):
             assert lib.pfc_cycle_device(h, C.byref(odoms[k]), C.c_void_p(base + k * rec), nobs,
                                         C.byref(prm), pkg.dptr(est)) == 0
@@ -297,38 +329,42 @@ def run_value(args, sc, torch, dev, dist=None):
         lib.pfc_get_stats(h, C.byref(stats))
         step_ms = np.array([a.elapsed_time(b) for a, b in evs])
         assert lib.pfc_cycle_result(h, pkg.dptr(est)) == 0
-        final_err = float(np.linalg.norm(est[0:3] - sc.steps[W + K - 1].truth_p))
-        # Per-kernel CUDA-event times: the timed cycles above are graph
-        # replays (no per-kernel events), so the next cycles of the same
-        # trajectory run with the library's per-kernel events (direct
-        # launches).
-        P = profiled_cycles(args)
-        lib.pfc_profile(h, 1)
-        with torch.cuda.stream(stream):
-            for k in range(P):
-                flush.fill_(k & 0xFF)
-                assert lib.pfc_cycle_device(h, C.byref(odoms[W + K + k]),
-                                            C.c_void_p(base + (W + K + k) * rec), nobs,
-                                            C.byref(prm), None) == 0
-        stream.synchronize()
-        ms = np.zeros(10)
-        cnt = np.zeros(10, dtype=np.int64)
-        lib.pfc_profile_read(h, pkg.dptr(ms), cnt.ctypes.data_as(C.POINTER(C.c_longlong)))
-        lib.pfc_profile(h, 0)
-        return dict(step_ms=step_ms, wall=t_wall, kernel_ms=ms, kernel_count=cnt,
-                    launches=int(stats.launches), clocks=clk.summary(), final_err=final_err,
-                    profiled_steps=P)
+        out = dict(step_ms=step_ms, wall=t_wall, launches=int(stats.launches),
+                   clocks=clk.summary(), resampled_last=bool(est[pkg.PFC_EST_RESAMPLED]))
+        if profile:
+            # Per-kernel CUDA-event times: the timed cycles above are graph
+            # replays (no per-kernel events), so the next cycles of the same
+            # trajectory run with the library's per-kernel events (direct
+            # launches).
+            P = min(K, 100)
+            lib.pfc_profile(h, 1)
+            with torch.cuda.stream(stream):
+                for k in range(P):
+                    flush.fill_(k & 0xFF)
+                    assert lib.pfc_cycle_device(h, C.byref(odoms[W + K + k]),
+                                                C.c_void_p(base + (W + K + k) * rec), nobs,
+                                                C.byref(prm), None) == 0
+            stream.synchronize()
+            ms = np.zeros(10)
+            cnt = np.zeros(10, dtype=np.int64)
+            lib.pfc_profile_read(h, pkg.dptr(ms), cnt.ctypes.data_as(C.POINTER(C.c_longlong)))
+            lib.pfc_profile(h, 0)
+            out.update(kernel_ms=ms, kernel_count=cnt, profiled_steps=P)
+        return out
     finally:
         lib.pfc_destroy(h)
 
 
-def run_e2e(args, sc, torch, dev, dist=None):
+def run_e2e(args, sc, torch, dev, dist=None, n=None, steps=None, warmup=None, filt=FILTER,
+            truth_offset=0):
     """ParticleFilter::update through the drop-in C-ABI with host buffers."""
     import cuda_pf_localization_b200 as pkg
     lib = pkg.kernels()
-    n = args.particles
+    n = n or args.particles
+    K = steps if steps is not None else args.steps
+    W = warmup if warmup is not None else args.warmup
     pf = pkg.ParticleFilter(n, seed=42, trans_noise=sc.trans_noise, rot_noise=sc.rot_noise,
-                            **FILTER)
+                            **filt)
     try:
         pf.set_map(sc.landmark_dict())
         pf.reinitialize(np.r_[sc.prior_p, sc.prior_q], [0.5] * 3, [0.2] * 3)
@@ -338,7 +374,6 @@ def run_e2e(args, sc, torch, dev, dist=None):
         nob = [len(st.obs) for st in sc.steps]
         core = pkg.core()
         est = pkg.PfcoreEstimate()
-        W, K = args.warmup, args.steps
         for k in range(W):
             assert core.pfcore_filter_update(pf._h, C.byref(odoms[k]), obs[k], nob[k],
                                              C.byref(est)) == 0
@@ -370,6 +405,47 @@ def run_e2e(args, sc, torch, dev, dist=None):
         pf.close()
 
 
+def run_tracking(args, torch, dev):
+    """The tracking workload (N=10k, 12 landmarks in 20x20x5 m, every landmark
+    observed, 3-sigma gate, 100 cycles of the helix): the fused device path,
+    the drop-in path with host arrays, and the CPU port, each over the 100
+    cycles after a warm-up run of the same trajectory."""
+    from cuda_pf_localization_b200 import sim
+    sc = sim.tracking_config(cycles=200, seed=7)
+    filt = dict(FILTER, random_inject_ratio=0.0)
+    n, K, W = 10_000, 100, 100
+    v = run_value(args, sc, torch, dev, n=n, steps=K, warmup=W, filt=filt, profile=False)
+    e = run_e2e(args, sc, torch, dev, n=n, steps=K, warmup=W, filt=filt)
+    done, secs = run_cpu_cycles(sc, n, args.cpu_seconds, K, warm=3, filt=filt)
+    import oracle
+    t_v = float(v["step_ms"].sum()) / 1e3
+    return {"workload": "tracking: N=10k, 12 landmarks in 20x20x5 m, all observed, "
+                        "gate 3 sigma, helix, 100 cycles",
+            "value": n * K / t_v, "unit": UNIT, "ms_per_step": 1e3 * t_v / K,
+            "e2e": {"value": n * K / float(e["times"].sum()),
+                    "ms_per_step": 1e3 * float(e["times"].mean()),
+                    "host_syncs_per_step": float(e["syncs"])},
+            "cpu_baseline": {"value": n * done / secs, "unit": UNIT,
+                             "cores": int(oracle.lib().orc_threads()), "kind": "port",
+                             "sample": f"{done} cycles at N={n}"},
+            "mean_track_err_m": float(e["errs"].mean())}
+
+
+def run_range_bearing(args, sc, torch, dev):
+    """The at-scale workload with every observation range-bearing (mode 1:
+    range and unit direction, the gated acos bearing term)."""
+    from cuda_pf_localization_b200 import sim
+    rb = sim.as_range_bearing(sc)
+    K = min(args.steps, 200)
+    v = run_value(args, rb, torch, dev, steps=K, warmup=args.warmup, profile=True)
+    t = float(v["step_ms"].sum()) / 1e3
+    w_ms = v["kernel_ms"][KINDS.index("weight")] / max(1, v["kernel_count"][KINDS.index("weight")])
+    return {"workload": "at-scale PF cycle with all 256 observations range-bearing",
+            "value": args.particles * K / t, "unit": UNIT, "ms_per_step": 1e3 * t / K,
+            "steps": K, "k_weight_ms": float(w_ms),
+            "pairs_per_s": args.particles * 256 / (w_ms * 1e-3)}
+
+
 # Tensor-core work of one training sample: forward (2 * sum in*out) + weight
 # gradients (the same) + input gradients of layers 1..4.
 LP_FLOPS_PER_SAMPLE = 2 * (2 * (384 * 1024 + 3 * 1024 * 1024 + 1024 * 384)
@@ -382,30 +458,52 @@ def _pose_err(top, truth):
     return dp, dth
 
 
+def _success(top, poses):
+    top, poses = np.asarray(top, np.float64), np.asarray(poses, np.float64)
+    dp = np.hypot(top[:, 0] - poses[:, 0], top[:, 1] - poses[:, 1])
+    dth = np.abs((top[:, 2] - poses[:, 2] + np.pi) % (2 * np.pi) - np.pi)
+    return (dp <= 0.5) & (dth <= 0.1)
+
+
+# uniform hypothesis counts of the iso-success sweep (positions x 16 yaws), the
+# learned configurations (samples per query, calibration quantile), the one
+# quoted in the headline ratio
+UNIFORM_SWEEP = (50_000, 56_000, 64_000, 100_000, 200_000)
+LEARNED_SWEEP = ((250, 0.995), (1000, 0.995), (20_000, 0.98))
+LEARNED_HEADLINE = (1000, 0.995)
+UNIFORM_1M_POSES = 20   # poses per map of the 1M-hypothesis uniform leg
+
+
 def run_gl(args):
     """CBGL on 10 x 10 m rooms with 30 boxes (200 x 200 at 0.05 m), 360-ray
     scans (rmax 10 m, N(0, 0.01 m) noise) rendered by the library's raycaster.
 
-    uniform: free positions x 16 yaws at each hypothesis count, k = 64, the
-             fused pruned localizer and the reference's call pattern
-             (pfgl_score + pfgl_topk).
-    learned: per map, 2M (scan, pose) pairs generated on the device, the MLP
-             trained by the library's tcgen05 kernels, the fallback threshold
-             calibrated on held-out poses; then unseen poses localized from
-             20k mixture samples (200k uniform fallback), and the same poses
-             with uniform CBGL at the largest hypothesis count."""
+    c3:       uniform CBGL on one room, 20 trials at 50k / 200k / 1M
+              hypotheses (positions x 16 yaws), k = 64: the fused pruned
+              localizer and the reference's call pattern (pfgl_score +
+              pfgl_topk).
+    iso:      16 maps x 1000 unseen poses.  Uniform CBGL (pruned localizer,
+              one query at a time) at every count of UNIFORM_SWEEP, and the
+              same queries batched; the learned proposal (per map: 2M
+              (scan, pose) pairs generated on the device, the MLP trained by
+              the library's tcgen05 kernels, the fallback threshold calibrated
+              on 1000 held-out poses) localizing the same poses in batches at
+              each of LEARNED_SWEEP's sample counts with a 200k uniform
+              fallback.  The headline ratio compares the learned rate at
+              LEARNED_HEADLINE with the cheapest uniform count whose success
+              within 0.5 m and 0.1 rad is at least 95 %."""
     import cuda_pf_localization_b200 as pkg
     from cuda_pf_localization_b200 import sim
     lib = pkg.kernels()
     span, rmax, k = 2 * math.pi, 10.0, 64
-    res = {"uniform": {}, "learned": {}}
+    res = {"c3": {}, "iso": {}}
     out = np.zeros(3 * k, np.float32)
 
     def trials_for(g, rng, n, h):
         poses = np.array([sim.free_pose(g, rng) for _ in range(n)], np.float32)
         return poses, pkg.render_scans(h, poses, noise=0.01, seed=int(rng.integers(1 << 31)))
 
-    # ---- uniform CBGL, the reference method (config sizes, 20 trials each)
+    # ---- config 3: uniform CBGL, the reference method, 20 trials per size
     g = np.ascontiguousarray(sim.rooms_grid(args.seed))
     h = lib.pfgl_create(200, 200, 0.05, 0.0, 0.0, pkg.u8ptr(g), max(args.gl_hyps, 200_000))
     try:
@@ -434,7 +532,7 @@ def run_gl(args):
                 # last trial's hypotheses (counted by an untimed replay kernel)
                 visits = lib.pfgl_count_visits(h, 360, span)
                 sps = len(poses) / dt
-                res["uniform"][f"{nh}_{mode}"] = dict(
+                res["c3"][f"{nh}_{mode}"] = dict(
                     solves_per_s=sps, success_pos=ok_p / len(poses),
                     success_pos_yaw=ok_pt / len(poses), trials=len(poses),
                     hyps_per_s=nh * sps, dda_visits_per_solve=int(visits),
@@ -445,12 +543,12 @@ def run_gl(args):
     finally:
         lib.pfgl_destroy(h)
 
-    # ---- learned proposal vs uniform at the largest size on the same poses
-    tot_q = ok_q = fb_q = 0
-    t_learn = t_train = t_steps = 0.0
-    uni_q = uni_ok = 0
-    t_uni = 0.0
-    losses, taus = [], []
+    # ---- iso-success: learned vs uniform on the same maps and poses
+    uni = {u: dict(ok=0, n=0, t=0.0) for u in UNIFORM_SWEEP + (args.gl_hyps,)}
+    uni_b = {u: dict(ok=0, n=0, t=0.0) for u in UNIFORM_SWEEP[:3]}
+    lrn = {c: dict(ok=0, n=0, t=0.0, fb=0, tau=[], held=[]) for c in LEARNED_SWEEP}
+    t_train = t_steps = 0.0
+    losses = []
     for m in range(args.gl_maps):
         gseed = 1000 + 17 * m
         g = np.ascontiguousarray(sim.rooms_grid(gseed))
@@ -466,51 +564,87 @@ def run_gl(args):
             t_train += t2 - t0
             t_steps += t2 - t1
             losses.append(float(loss[-50:].mean()))
-            tau, _ = lp.calibrate(n_queries=200, n_samples=20000, seed=gseed + 2)
-            taus.append(tau)
             poses, scans = trials_for(g, np.random.default_rng(gseed + 3), args.gl_queries, h)
-            lp.localize(scans[0], n_samples=20000, n_fallback=200_000, k=k)  # warm-up
-            t0 = time.perf_counter()
-            for q in range(len(poses)):
-                top, _, _, info = lp.localize(scans[q], n_samples=20000, n_fallback=200_000, k=k)
-                dp, dth = _pose_err(top[0], poses[q])
-                ok_q += dp <= 0.5 and dth <= 0.1
-                fb_q += info > 0
-            t_learn += time.perf_counter() - t0
-            tot_q += len(poses)
-            nu = min(args.gl_trials, len(poses))
-            t0 = time.perf_counter()
-            for q in range(nu):
-                lib.pfgl_generate_yaws(h, args.gl_hyps // 16, 16, 7000 + q)
-                lib.pfgl_localize(h, pkg.fptr(scans[q]), 360, rmax, span, k, pkg.fptr(out),
-                                  None, None)
-                dp, dth = _pose_err(out[:3], poses[q])
-                uni_ok += dp <= 0.5 and dth <= 0.1
-            t_uni += time.perf_counter() - t0
-            uni_q += nu
+            for (S, ql), a in lrn.items():
+                tau, held = lp.calibrate(n_queries=1000, n_samples=S, quantile=ql,
+                                         seed=gseed + 2)
+                a["tau"].append(tau)
+                a["held"].append(held)
+                lp.localize_batch(scans[:4], n_samples=S, n_fallback=200_000, k=k)  # warm-up
+                t0 = time.perf_counter()
+                top, _, _, info = lp.localize_batch(scans, n_samples=S, n_fallback=200_000, k=k)
+                a["t"] += time.perf_counter() - t0
+                a["ok"] += int(_success(top[:, 0], poses).sum())
+                a["n"] += len(poses)
+                a["fb"] += int((info > 0).sum())
+            for u, a in uni.items():
+                nq = len(poses) if u in UNIFORM_SWEEP else min(UNIFORM_1M_POSES, len(poses))
+                lib.pfgl_generate_yaws(h, u // 16, 16, 1)
+                lib.pfgl_localize(h, pkg.fptr(scans[0]), 360, rmax, span, k, pkg.fptr(out),
+                                  None, None)  # warm-up
+                tops = np.zeros((nq, 3), np.float32)
+                t0 = time.perf_counter()
+                for q in range(nq):
+                    lib.pfgl_generate_yaws(h, u // 16, 16, 7000 + q)
+                    lib.pfgl_localize(h, pkg.fptr(scans[q]), 360, rmax, span, k, pkg.fptr(out),
+                                      None, None)
+                    tops[q] = out[:3]
+                a["t"] += time.perf_counter() - t0
+                a["ok"] += int(_success(tops, poses[:nq]).sum())
+                a["n"] += nq
+            for u, a in uni_b.items():
+                seeds = np.arange(7000, 7000 + len(poses), dtype=np.uint64)
+                pkg.localize_batch(h, scans[:2], u // 16, 16, seeds[:2], k)  # warm-up
+                t0 = time.perf_counter()
+                bp, _, _ = pkg.localize_batch(h, scans, u // 16, 16, seeds, k)
+                a["t"] += time.perf_counter() - t0
+                a["ok"] += int(_success(bp[:, 0], poses).sum())
+                a["n"] += len(poses)
         finally:
             if lp is not None:
                 lp.close()
             lib.pfgl_destroy(h)
     if args.gl_maps <= 0:
         return res
-    learned_sps = tot_q / t_learn
-    uniform_sps = uni_q / t_uni
-    res["learned"] = dict(
-        maps=args.gl_maps, queries=tot_q, success_pos_yaw=ok_q / tot_q,
-        fallback_rate=fb_q / tot_q, solves_per_s=learned_sps,
-        samples_per_query=20000, fallback_hyps=200_000,
-        train_pairs_per_map=args.gl_pairs, train_steps_per_map=args.gl_train_steps,
-        train_seconds_per_map=t_train / args.gl_maps, final_loss_mean=float(np.mean(losses)),
-        train_step_ms=1e3 * t_steps / (args.gl_maps * args.gl_train_steps),
-        train_batch=args.gl_batch,
-        train_tflops=LP_FLOPS_PER_SAMPLE * args.gl_batch * args.gl_train_steps * args.gl_maps
-        / t_steps / 1e12,
-        tau_mean=float(np.mean(taus)))
-    res["uniform_same_maps"] = dict(hyps=args.gl_hyps, queries=uni_q,
-                                    success_pos_yaw=uni_ok / max(1, uni_q),
-                                    solves_per_s=uniform_sps)
-    res["learned_vs_uniform_solves_ratio"] = learned_sps / uniform_sps
+    iso = res["iso"]
+    iso["uniform"] = {str(u): dict(hyps=u, queries=a["n"], success_pos_yaw=a["ok"] / a["n"],
+                                   solves_per_s=a["n"] / a["t"],
+                                   mode="pruned localizer, one query at a time")
+                      for u, a in uni.items() if a["n"]}
+    iso["uniform_batched"] = {str(u): dict(hyps=u, queries=a["n"],
+                                           success_pos_yaw=a["ok"] / a["n"],
+                                           solves_per_s=a["n"] / a["t"],
+                                           mode="pfgl_localize_batch (exhaustive)")
+                              for u, a in uni_b.items() if a["n"]}
+    iso["learned"] = {f"{S}_q{ql}": dict(samples_per_query=S, calibration_quantile=ql,
+                                         queries=a["n"], success_pos_yaw=a["ok"] / a["n"],
+                                         solves_per_s=a["n"] / a["t"],
+                                         fallback_rate=a["fb"] / a["n"],
+                                         fallback_hyps=200_000, tau_mean=float(np.mean(a["tau"])),
+                                         held_out_success=float(np.mean(a["held"])),
+                                         mode="pfgl_learned_localize_batch")
+                      for (S, ql), a in lrn.items()}
+    iso["training"] = dict(pairs_per_map=args.gl_pairs, steps_per_map=args.gl_train_steps,
+                           batch=args.gl_batch, seconds_per_map=t_train / args.gl_maps,
+                           step_ms=1e3 * t_steps / (args.gl_maps * args.gl_train_steps),
+                           tflops=LP_FLOPS_PER_SAMPLE * args.gl_batch * args.gl_train_steps
+                           * args.gl_maps / t_steps / 1e12,
+                           final_loss_mean=float(np.mean(losses)))
+    # the comparator: the cheapest uniform count reaching 95 % (pos + yaw)
+    cands = sorted((u, d) for u, d in ((int(k2), d2) for k2, d2 in iso["uniform"].items())
+                   if d["success_pos_yaw"] >= 0.95 and d["queries"] >= args.gl_queries)
+    head = iso["learned"][f"{LEARNED_HEADLINE[0]}_q{LEARNED_HEADLINE[1]}"]
+    if cands:
+        u, d = cands[0]
+        best_uni = max(d["solves_per_s"],
+                       iso["uniform_batched"].get(str(u), {}).get("solves_per_s", 0.0))
+        iso["comparator"] = dict(hyps=u, success_pos_yaw=d["success_pos_yaw"],
+                                 solves_per_s=best_uni,
+                                 rule="cheapest uniform count of the sweep with success "
+                                      "within 0.5 m / 0.1 rad >= 0.95 on the same poses; "
+                                      "its faster mode")
+        iso["learned_headline"] = dict(head, samples_per_query=LEARNED_HEADLINE[0])
+        iso["learned_vs_uniform_solves_ratio"] = head["solves_per_s"] / best_uni
     return res
 
 
@@ -539,7 +673,7 @@ def run_batched(args, torch, dev):
     total_cycles = cycles + args.warmup
     # device-resident inputs of every cycle
     rec = np.zeros((total_cycles, F), np.dtype((np.void, C.sizeof(pkg.PfcBatchCycle))))
-    obs_blocks, obs_off, n_obs = [], [], []
+    obs_blocks, n_obs = [], []
     for k in range(total_cycles):
         recs = (pkg.PfcBatchCycle * F)()
         off = 0
@@ -578,7 +712,6 @@ def run_batched(args, torch, dev):
                for _ in range(cycles)]
         l0 = lib.pfc_batch_launches(b.handle)
         torch.cuda.synchronize(dev)
-        resampled = 0
         for i in range(cycles):
             k = args.warmup + i
             evs[i][0].record(stream)
@@ -595,7 +728,7 @@ def run_batched(args, torch, dev):
                 for f in range(F)]
     finally:
         b.close()
-    # sequential single-filter cycles (the same filters, host inputs, a few cycles)
+    # sequential single-filter cycles (the same filters, host inputs)
     seq_cycles = min(args.batch_seq_cycles, cycles)
     hs = []
     seq_ms = float("nan")
@@ -647,15 +780,65 @@ def run_batched(args, torch, dev):
         mean_track_err_m=float(np.mean(errs)), n_min=int(sizes.min()), n_max=int(sizes.max()))
 
 
+def rooflines(val, n, nobs, t_cycle_s, hbm, peak_kind):
+    """The dominant kernel's roofline (k_weight: FP32 issue bound) and the
+    cycle's per-stage roofline sum_s max(B_s / BW, I_s / issue) / t_cycle."""
+    ms, cnt = val["kernel_ms"], val["kernel_count"]
+    per = {k: (ms[i] / cnt[i] if cnt[i] else 0.0) for i, k in enumerate(KINDS)}
+    sm_mhz = val["clocks"]["sm_mhz"] or 1965.0
+    issue_peak = 148 * 128 * sm_mhz * 1e6  # FP32 lane operations / s
+    w_ms = per["weight"]
+    pair_rate = n * nobs / (w_ms * 1e-3)
+    achieved_ops = FP32_OPS_PER_PAIR * pair_rate
+    hbm_bytes = STAGE_BYTES["weight"] * n
+    roof = {"bound": "fp32 issue", "kernel": "k_weight (fused predict + gated weighting)",
+            "achieved": achieved_ops / 1e12, "peak": issue_peak / 1e12,
+            "unit": "T FP32 lane-ops/s", "frac": achieved_ops / issue_peak,
+            "traffic": (KWEIGHT_DRAM_BYTES_1M if (n, nobs) == (1_000_000, 256) else None),
+            "traffic_source": "ncu capture of one k_weight launch at this workload "
+                              "(dram__bytes_read.sum + dram__bytes_write.sum)",
+            "ops_per_launch": FP32_OPS_PER_PAIR * n * nobs,
+            "ops_note": f"{FP32_OPS_PER_PAIR} rounded FP32 operations per particle-observation "
+                        "pair are required for the reference's bits (an FMA counts once); "
+                        "peak = 148 SM x 128 lanes x sampled SM clock",
+            "avg_launch_ms": w_ms, "sm_mhz": sm_mhz,
+            "hbm": {"achieved": hbm_bytes / (w_ms * 1e-3) / 1e9, "peak": hbm,
+                    "unit": "GB/s", "frac": hbm_bytes / (w_ms * 1e-3) / 1e9 / hbm,
+                    "alg_bytes_per_launch": hbm_bytes, "peak_source": peak_kind},
+            "timing": f"CUDA events around each k_weight launch on the library stream over "
+                      f"the {val['profiled_steps']} cycles that continue the timed "
+                      f"(graph-launched) cycles' trajectory (direct launches)"}
+    stages = {}
+    t_roof = 0.0
+    for name, b in STAGE_BYTES.items():
+        t_b = b * n / (hbm * 1e9)
+        t_i = (FP32_OPS_PER_PAIR * n * nobs / issue_peak) if name == "weight" else 0.0
+        t_s = max(t_b, t_i)
+        t_roof += t_s
+        stages[name] = {"alg_bytes_per_particle": b, "roof_us": 1e6 * t_s,
+                        "measured_us": 1e3 * per[name],
+                        "bound": "fp32 issue" if t_i > t_b else "hbm"}
+    cycle = {"frac": t_roof / t_cycle_s, "roof_us": 1e6 * t_roof,
+             "measured_cycle_us": 1e6 * t_cycle_s, "stages": stages,
+             "rule": "sum over the cycle's kernels of max(alg bytes / measured HBM copy "
+                     "bandwidth, FP32 ops / FP32 issue peak), divided by the measured "
+                     "(graph-replayed) cycle time; a resampling cycle"}
+    return roof, cycle
+
+
 def main():
     args = parse()
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from cuda_pf_localization_b200 import multi
+    try:
+        plan, world = multi.launch_plan(args.gpus)
+    except ValueError as e:
+        sys.exit(f"bench.py: {e}")
+    if plan == "spawn":
+        sys.exit(multi.spawn_ranks(str(Path(__file__).resolve()), sys.argv[1:], world))
+    _, rank, local = multi.world_info()
     if args.impl == "reference":
-        if rank != 0:
-            return
-        reference_arm(args)
+        if rank == 0:
+            reference_arm(args, world)
         return
 
     import torch
@@ -669,11 +852,10 @@ def main():
         if rank == 0:
             print(json.dumps({"batched": run_batched(args, torch, dev)}), flush=True)
         return
-    from cuda_pf_localization_b200 import multi
     dist = multi.init("nccl") if world > 1 else None
 
     # the profiled pass after the timed cycles continues the same trajectory
-    sc = scenario(args, args.warmup + args.steps + profiled_cycles(args) + 1)
+    sc = scenario(args, args.warmup + args.steps + min(args.steps, 100) + 1)
     n = args.particles
     val = run_value(args, sc, torch, dev, dist)
     e2e = run_e2e(args, sc, torch, dev, dist)
@@ -683,65 +865,27 @@ def main():
     K = args.steps
     value = multi.weak_scaling_rate(world, n * K, t_value)
     e2e_value = multi.weak_scaling_rate(world, n * K, t_e2e)
-
-    # dominant kernel: gated weighting (fused with the motion update)
-    hbm, peak_kind = peaks()
-    kk = dict(zip(("reinit", "predict", "weight", "est", "covs", "scan", "gather", "inject",
-                   "commit", "misc"), range(10)))
-    w_ms = val["kernel_ms"][kk["weight"]] / max(1, val["kernel_count"][kk["weight"]])
-    # algorithmic bytes per particle of the fused predict+weight pass:
-    # read pose 28 B, write pose 28 B, write log-likelihood 4 B
-    alg_bytes = 60.0 * n
-    achieved = alg_bytes / (w_ms * 1e-3) / 1e9
     nobs = 256
-    sm_mhz = val["clocks"]["sm_mhz"] or 1965.0
-    issue_peak = 148 * 128 * sm_mhz * 1e6  # FP32 lane-ops/s
-    pair_rate = n * nobs / (w_ms * 1e-3)
-    kernel_share = {name: float(val["kernel_ms"][i]) for name, i in kk.items()}
+    hbm, peak_kind = peaks()
+    roof, cycle_roof = rooflines(val, n, nobs, t_value / K, hbm, peak_kind)
+    kernel_share = {name: float(val["kernel_ms"][i]) for i, name in enumerate(KINDS)}
     tot_k = sum(kernel_share.values())
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_value / K, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic",
-        "config": {
-            "workload": "at-scale PF cycle: N=1M f32 particles, 64 landmarks in 50x50x10 m, "
-                        "256 obs/cycle (10% uniform outliers), gate 3 sigma, ESS<N/2 resample, "
-                        "random_inject_ratio 0.01, helix trajectory",
-            "particles": n, "obs_per_cycle": nobs, "parallelism": f"replicas x{world}",
-            "launch": "each cycle replayed from a CUDA graph (pfc_cycle_device)",
-            "l2": "flushed (256 MiB write) between timed steps, outside the events",
-            "mean_track_err_m": float(e2e["errs"].mean()),
-            "resamples_in_e2e": int(e2e["resampled"]),
-        },
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(args, world),
+        "launch": "each cycle replayed from a CUDA graph (pfc_cycle_device)",
+        "accuracy": {"mean_track_err_m": float(e2e["errs"].mean()),
+                     "resamples_in_e2e": int(e2e["resampled"])},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": float(e2e["h2d"]),
                 "d2h_bytes_per_step": float(e2e["d2h"]),
                 "ms_per_step": 1e3 * t_e2e / K, "host_syncs_per_step": float(e2e["syncs"]),
                 "path": "pf_core ParticleFilter::update mirror -> pfc_* C-ABI"},
         "gpu_launches": val["launches"],
-        "roofline": {"bound": "hbm", "kernel": "k_weight (fused predict + gated weighting)",
-                     "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm,
-                     "traffic": (KWEIGHT_DRAM_BYTES_1M
-                                 if (n, nobs) == (1_000_000, 256) else None),
-                     "traffic_source": "ncu capture of one k_weight launch at this workload",
-                     "peak_source": peak_kind,
-                     "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": w_ms,
-                     "timing": f"CUDA events around each k_weight launch on the library "
-                               f"stream over the {val['profiled_steps']} cycles that "
-                               f"continue the timed (graph-launched) cycles' trajectory "
-                               f"(direct launches)"},
-        # k_weight's real bound: 29 rounded FP32 operations per particle-
-        # observation pair are required for the reference's bits
-        "issue_roofline": {"kernel": "k_weight", "bound": "fp32 pipe",
-                           "unit": "particle-observation pairs/s",
-                           "achieved_pairs_per_s": pair_rate,
-                           "fp32_issue_peak_lane_ops_per_s": issue_peak,
-                           "lane_ops_per_pair_at_peak": issue_peak / pair_rate,
-                           "required_fp32_ops_per_pair": FP32_OPS_PER_PAIR,
-                           "frac": FP32_OPS_PER_PAIR * pair_rate / issue_peak,
-                           "sm_mhz": sm_mhz},
+        "roofline": roof,
+        "cycle_roofline": cycle_roof,
         "kernel_ms_share": {k2: v / tot_k for k2, v in kernel_share.items() if tot_k > 0},
         "clocks": val["clocks"],
     }
@@ -753,15 +897,18 @@ def main():
         line["cpu_baseline"] = {"value": n * done / secs, "unit": UNIT,
                                 "cores": int(oracle.lib().orc_threads()), "kind": "port",
                                 "sample": f"{done} cycles at N={n} (time-bounded)"}
-        # the same workload at the other particle counts of the at-scale config
+        # the same workload at the other particle counts of the at-scale config,
+        # the tracking workload, and range-bearing observations at scale
         sizes = {}
         for n_other in (100_000, 4_000_000):
             a2 = argparse.Namespace(**vars(args))
             a2.particles, a2.steps = n_other, min(args.steps, 200)
-            v2 = run_value(a2, sc, torch, dev)
+            v2 = run_value(a2, sc, torch, dev, profile=False)
             t2 = float(v2["step_ms"].sum()) / 1e3
             sizes[str(n_other)] = {"value": n_other * a2.steps / t2, "unit": UNIT,
                                    "ms_per_step": 1e3 * t2 / a2.steps, "steps": a2.steps}
+        sizes["10000_tracking"] = run_tracking(args, torch, dev)
+        sizes["1000000_range_bearing"] = run_range_bearing(args, sc, torch, dev)
         line["other_sizes"] = sizes
         line["batched"] = run_batched(args, torch, dev)
         line["batched"]["config"] = ("512 filters, N log-uniform in [1k, 200k], 8-64 landmarks "
@@ -771,10 +918,10 @@ def main():
                                      "another")
         line["gl"] = run_gl(args)
         line["gl"]["config"] = ("10x10 m rooms at 0.05 m (200x200), 30 boxes 0.2-1.0 m, 360 rays, "
-                                "rmax 10, scan noise N(0, 0.01 m); uniform: positions x 16 yaws, "
-                                f"k=64, {args.gl_trials} trials per size; learned: "
+                                "rmax 10, scan noise N(0, 0.01 m); c3: positions x 16 yaws, k=64, "
+                                f"{args.gl_trials} trials per size on one room; iso: "
                                 f"{args.gl_maps} maps x {args.gl_queries} unseen poses, success "
-                                "within 0.5 m and 0.1 rad")
+                                "within 0.5 m and 0.1 rad, learned and uniform on the same poses")
     if rank == 0:
         print(json.dumps(line), flush=True)
     multi.finish(dist)

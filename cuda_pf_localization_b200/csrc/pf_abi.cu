@@ -141,24 +141,24 @@ void free_particles(PfHandle* h) {
     cudaFree(h->d_w);
     cudaFree(h->d_cum);
     cudaFree(h->d_anc);
-    cudaFree(h->d_inj_head);
-    cudaFree(h->d_inj_next);
     cudaFree(h->d_wprefix);
+    cudaFree(h->d_marker);
+    cudaFree(h->d_inj_cnt);
+    cudaFree(h->d_inj_bucket);
     cudaFree(h->d_part);
     cudaFree(h->d_part_u64);
-    cudaFree(h->d_heavy);
     cudaFree(h->d_stage);
     h->d_state[0] = h->d_state[1] = nullptr;
     h->d_ll = h->d_w = nullptr;
     h->d_cum = nullptr;
     h->d_anc = nullptr;
-    h->d_inj_head = nullptr;
-    h->d_inj_next = nullptr;
     h->d_wprefix = nullptr;
+    h->d_marker = nullptr;
+    h->d_inj_cnt = nullptr;
+    h->d_inj_bucket = nullptr;
+    h->inj_cap = 0;
     h->d_part = nullptr;
     h->d_part_u64 = nullptr;
-    h->d_heavy = nullptr;
-    h->heavy_cap = 0;
     h->d_stage = nullptr;
     h->n = 0;
 }
@@ -193,10 +193,10 @@ int device_error(PfHandle* h) {
     return 0;
 }
 
-// Queue estimate pass 1 + Markley + speculative covariance pass + the copy
-// of the control block.
-int queue_estimate(PfHandle* h) {
-    if (launch_est_sums(h)) return -1;
+// Queue estimate pass 1 + Markley (unless a fused resample already did) +
+// speculative covariance pass + the copy of the control block.
+int queue_estimate(PfHandle* h, bool sums_done = false) {
+    if (!sums_done && launch_est_sums(h)) return -1;
     if (launch_covs(h, false, nullptr, nullptr, false)) return -1;
     PFB_CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(CycleCtl),
                            cudaMemcpyDeviceToHost, h->stream));
@@ -292,9 +292,10 @@ int run_cycle_graph(PfHandle* h, const PfcOdom* odom, const CObservation* obs_de
     a.nobs = nobs;
     a.gen = h->gen;
     const int kinj = (prm->random_inject_ratio > 0.f)
-                         ? (int)(prm->random_inject_ratio * (float)h->n)
+                         ? std::min(h->n, (int)(prm->random_inject_ratio * (float)h->n))
                          : 0;
-    a.inj_epoch = kinj > 0 ? next_inj_epoch(h) : h->inj_epoch;
+    // buffers the captured kernels use are allocated before the capture
+    if (ensure_inject_buckets(h, kinj)) return -1;
     PFB_CK(cudaMemcpyAsync(h->d_cargs, &a, sizeof(CycleArgs), cudaMemcpyHostToDevice,
                            h->stream));
     PFB_CK(cudaEventRecord(h->cargs_ev[slot], h->stream));
@@ -368,9 +369,10 @@ int enqueue_cycle(PfHandle* h, const PredictArgs& pa, const CObservation* obs_de
                       dargs))
         return -1;
     if (launch_cycle_decide(h, prm->resample_ess_ratio)) return -1;
-    if (launch_resample(h, prm->random_inject_ratio, true, false, 0.0, dargs))
+    // resample (when decided) fused with the estimate sums of the cycle's
+    // final cloud, then its covariance pass and the output record
+    if (launch_resample_est(h, prm->random_inject_ratio, true, false, 0.0, dargs))
         return -1;
-    if (launch_est_sums(h)) return -1;
     if (launch_covs(h, false, nullptr, nullptr, true)) return -1;
     PFB_CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(CycleCtl),
                            cudaMemcpyDeviceToHost, h->stream));
@@ -508,25 +510,26 @@ int pfc_init(void* hv, int n, unsigned int seed) {
     h->prefix_valid = false;
     const size_t np = (size_t)h->n_pad;
     const int nprefix = ceil_div(n, kPrefixBlock);
-    const int part = std::max(2 * ceil_div(n, kThreads), 1184 * 16);
+    const int part = std::max(std::max(2 * ceil_div(n, kThreads), resample_part_doubles(n)),
+                              1184 * 16);
     PFB_CK(cudaMalloc((void**)&h->d_state[0], 7 * np * sizeof(float)));
     PFB_CK(cudaMalloc((void**)&h->d_state[1], 7 * np * sizeof(float)));
     PFB_CK(cudaMalloc((void**)&h->d_ll, np * sizeof(float)));
     PFB_CK(cudaMalloc((void**)&h->d_w, np * sizeof(float)));
-    h->heavy_cap = n / 32 + n / 4096 + 2;  // runs > 32 outputs, in pieces of <= 4096
-    PFB_CK(cudaMalloc((void**)&h->d_heavy, (size_t)h->heavy_cap * sizeof(HeavyRun)));
     PFB_CK(cudaMalloc((void**)&h->d_part_u64,
                       2 * (size_t)std::max(nprefix, 1184) * sizeof(unsigned long long)));
     PFB_CK(cudaMalloc((void**)&h->d_anc, (size_t)n * sizeof(int)));
-    PFB_CK(cudaMalloc((void**)&h->d_inj_head, (size_t)n * sizeof(uint64_t)));
-    PFB_CK(cudaMalloc((void**)&h->d_inj_next, (size_t)n * sizeof(int)));
     PFB_CK(cudaMalloc((void**)&h->d_wprefix, (size_t)nprefix * sizeof(uint64_t)));
+    PFB_CK(cudaMalloc((void**)&h->d_marker, np * sizeof(int)));
+    PFB_CK(cudaMemsetAsync(h->d_marker, 0xFF, np * sizeof(int), h->stream));
+    const int rtiles = resample_tiles(n);
+    PFB_CK(cudaMalloc((void**)&h->d_inj_cnt, (size_t)rtiles * sizeof(int)));
+    PFB_CK(cudaMemsetAsync(h->d_inj_cnt, 0, (size_t)rtiles * sizeof(int), h->stream));
     PFB_CK(cudaMalloc((void**)&h->d_part, (size_t)part * sizeof(double)));
     h->part_cap = part;
     PFB_CK(cudaMemsetAsync(h->d_state[0], 0, 7 * np * sizeof(float), h->stream));
     PFB_CK(cudaMemsetAsync(h->d_state[1], 0, 7 * np * sizeof(float), h->stream));
     PFB_CK(cudaMemsetAsync(h->d_ll, 0, np * sizeof(float), h->stream));
-    PFB_CK(cudaMemsetAsync(h->d_inj_head, 0, (size_t)n * sizeof(uint64_t), h->stream));
     PFB_CK(cudaMemsetAsync(h->d_done, 0, 8 * sizeof(unsigned), h->stream));
     h->inj_epoch = 0;
     k_ctl_reset<<<1, 1, 0, h->stream>>>(h->d_ctl, 0);
@@ -636,16 +639,16 @@ int pfc_resample(void* hv, float random_inject_ratio) {
     PfHandle* h = as_pf(hv);
     if (!valid_handle(h)) return -1;
     if (flush_predict(h)) return -1;
-    if (launch_resample(h, random_inject_ratio, false, false, 0.0)) return -1;
-    return queue_estimate(h);
+    if (launch_resample_est(h, random_inject_ratio, false, false, 0.0)) return -1;
+    return queue_estimate(h, true);
 }
 
 int pfc_resample_u01(void* hv, double u01, float random_inject_ratio) {
     PfHandle* h = as_pf(hv);
     if (!valid_handle(h) || !(u01 >= 0.0) || !(u01 < 1.0)) return -1;
     if (flush_predict(h)) return -1;
-    if (launch_resample(h, random_inject_ratio, false, true, u01)) return -1;
-    return queue_estimate(h);
+    if (launch_resample_est(h, random_inject_ratio, false, true, u01)) return -1;
+    return queue_estimate(h, true);
 }
 
 int pfc_est_sums(void* hv, double* out) {

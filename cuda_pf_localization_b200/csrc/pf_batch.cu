@@ -68,7 +68,7 @@ struct BTile {
 };
 
 struct BCtl {
-    double M, S;
+    float M, S;
     int wmode, wvalid;
     double est[kEstN], qmean[4], covs[kCovN];
     double ess, ess_pre;
@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(kThreads)
     k_b_weight(Arena A, const BFilter* __restrict__ F, const BTile* __restrict__ T,
                BCtl* C, const PfcBatchCycle* __restrict__ cyc,
                const CObservation* __restrict__ obs, const float* __restrict__ lm,
-               double2* __restrict__ wpart, int use_packed) {
+               float2* __restrict__ wpart, int use_packed) {
     const BTile t = T[blockIdx.x];
     const BFilter& fl = F[t.f];
     BCtl* c = C + t.f;
@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(kThreads)
     float* ll = A.ll + fl.off;
     if (v0) ll[i0] = acc0;
     if (v1) ll[i1] = acc1;
-    const double2 pb = block_softmax_partial(acc0, v0, acc1, v1);
+    const float2 pb = block_softmax_partial(acc0, v0, acc1, v1);
     __shared__ bool s_last;
     if (threadIdx.x == 0) {
         wpart[fl.wtile0 + t.local] = pb;
@@ -227,11 +227,11 @@ __global__ void __launch_bounds__(kThreads)
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    const double2 ms = softmax_combine(wpart + fl.wtile0, fl.nwtiles);
+    const float2 ms = softmax_combine(wpart + fl.wtile0, fl.nwtiles);
     if (threadIdx.x == 0) {
         c->M = ms.x;
         c->S = ms.y;
-        const int ok = (ms.y > 0.0 && isfinite(ms.y)) ? 1 : 0;
+        const int ok = (ms.y > 0.0f && isfinite(ms.y)) ? 1 : 0;
         c->wvalid = ok;
         c->wmode = ok ? WMODE_LL : WMODE_UNIFORM;
         c->done_w = 0u;
@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(kThreads)
     const BFilter& fl = F[t.f];
     BCtl* c = C + t.f;
     const int wmode = c->wmode;
-    const double M = c->M, S = c->S;
+    const float M = c->M, S = c->S;
     const float wuni = 1.0f / (float)fl.n;
     float* w = A.w + fl.off;
     const float* ll = A.ll + fl.off;
@@ -310,10 +310,8 @@ __global__ void __launch_bounds__(kThreads)
             W = make_float4(wuni, wuni, wuni, wuni);
         } else {
             const float4 L = reinterpret_cast<const float4*>(ll)[i4];
-            W = make_float4((float)(exp((double)L.x - M) / S),
-                            (float)(exp((double)L.y - M) / S),
-                            (float)(exp((double)L.z - M) / S),
-                            (float)(exp((double)L.w - M) / S));
+            W = make_float4(weight_from_ll(L.x, M, S), weight_from_ll(L.y, M, S),
+                            weight_from_ll(L.z, M, S), weight_from_ll(L.w, M, S));
             reinterpret_cast<float4*>(w)[i4] = W;
         }
 #pragma unroll
@@ -380,7 +378,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     BCtl* c = C + t.f;
     const Planes s = filter_planes(A, c->live, fl.off);
     const int wmode = c->wmode;
-    const double M = c->M, S = c->S;
+    const float M = c->M, S = c->S;
     const float wuni = 1.0f / (float)fl.n;
     float* w = A.w + fl.off;
     const float* ll = A.ll + fl.off;
@@ -405,10 +403,8 @@ __global__ void __launch_bounds__(kThreads, 2)
             W = make_float4(wuni, wuni, wuni, wuni);
         } else {
             const float4 L = reinterpret_cast<const float4*>(ll)[i4];
-            W = make_float4((float)(exp((double)L.x - M) / S),
-                            (float)(exp((double)L.y - M) / S),
-                            (float)(exp((double)L.z - M) / S),
-                            (float)(exp((double)L.w - M) / S));
+            W = make_float4(weight_from_ll(L.x, M, S), weight_from_ll(L.y, M, S),
+                            weight_from_ll(L.z, M, S), weight_from_ll(L.w, M, S));
             reinterpret_cast<float4*>(w)[i4] = W;
         }
 #pragma unroll
@@ -446,7 +442,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     BCtl* c = C + t.f;
     const Planes s = filter_planes(A, c->live, fl.off);
     const int wmode = c->wmode;
-    const double M = c->M, S = c->S;
+    const float M = c->M, S = c->S;
     const float wuni = 1.0f / (float)fl.n;
     const float* w = A.w + fl.off;
     const float* ll = A.ll + fl.off;
@@ -474,10 +470,8 @@ __global__ void __launch_bounds__(kThreads, 2)
             W = make_float4(wuni, wuni, wuni, wuni);
         } else {
             const float4 L = reinterpret_cast<const float4*>(ll)[i4];
-            W = make_float4((float)(exp((double)L.x - M) / S),
-                            (float)(exp((double)L.y - M) / S),
-                            (float)(exp((double)L.z - M) / S),
-                            (float)(exp((double)L.w - M) / S));
+            W = make_float4(weight_from_ll(L.x, M, S), weight_from_ll(L.y, M, S),
+                            weight_from_ll(L.z, M, S), weight_from_ll(L.w, M, S));
         }
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -542,7 +536,7 @@ __global__ void __launch_bounds__(kThreads)
         c->resample_valid = 1;
     }
     const int wmode = c->wmode;
-    const double M = c->M, S = c->S;
+    const float M = c->M, S = c->S;
     const int live = c->live;
     const Planes src = filter_planes(A, live, fl.off);
     const Planes dst = filter_planes(A, 1 - live, fl.off);
@@ -779,7 +773,7 @@ struct BatchHandle {
     BCtl* d_C = nullptr;
     BGlobal* d_G = nullptr;
     BGlobal* h_G = nullptr;
-    double2* d_wpart = nullptr;
+    float2* d_wpart = nullptr;
     double* d_epart = nullptr;
     unsigned long long* d_eupart = nullptr;
     double* d_cpart = nullptr;
@@ -1076,7 +1070,7 @@ void* pfc_batch_create(int n_filters, const int* n, const unsigned* seeds,
             cudaMalloc((void**)&h->d_C, sizeof(BCtl) * n_filters) != cudaSuccess ||
             cudaMalloc((void**)&h->d_G, sizeof(BGlobal)) != cudaSuccess ||
             cudaMallocHost((void**)&h->h_G, sizeof(BGlobal)) != cudaSuccess ||
-            cudaMalloc((void**)&h->d_wpart, sizeof(double2) * wt.size()) != cudaSuccess ||
+            cudaMalloc((void**)&h->d_wpart, sizeof(float2) * wt.size()) != cudaSuccess ||
             cudaMalloc((void**)&h->d_flags, sizeof(unsigned) * rt.size()) != cudaSuccess ||
             cudaMalloc((void**)&h->d_vals, sizeof(uint64_t) * 2 * rt.size()) != cudaSuccess)
             break;

@@ -133,6 +133,11 @@ __device__ __forceinline__ float warp_max_f(float v) {
     for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(~0u, v, o));
     return v;
 }
+__device__ __forceinline__ float warp_sum_f(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = __fadd_rn(v, __shfl_xor_sync(~0u, v, o));
+    return v;
+}
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(~0u, v, o);
@@ -280,13 +285,13 @@ __device__ __forceinline__ float2 packed_r2(const PackedPose& k, float4 A,
 }
 
 // Softmax partial of one block of up to 2 * kBlk log-likelihoods (two per
-// thread): (block max, sum exp(ll - block max)) in FP64, in a fixed order
+// thread): (block max, sum expf(ll - block max)) in f32, in a fixed order
 // (xor butterfly inside warps, warps in index order).  Valid in every thread.
-__device__ __forceinline__ double2 block_softmax_partial(float acc0, bool v0,
-                                                         float acc1, bool v1) {
+__device__ __forceinline__ float2 block_softmax_partial(float acc0, bool v0,
+                                                        float acc1, bool v1) {
     __shared__ float s_m[kBlk / 32];
-    __shared__ double s_s[kBlk / 32];
-    __shared__ double s_bm, s_sb;
+    __shared__ float s_s[kBlk / 32];
+    __shared__ float s_bm, s_sb;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     float m = warp_max_f(fmaxf(v0 ? acc0 : -INFINITY, v1 ? acc1 : -INFINITY));
     if (lane == 0) s_m[warp] = m;
@@ -294,61 +299,62 @@ __device__ __forceinline__ double2 block_softmax_partial(float acc0, bool v0,
     if (tid == 0) {
         float bm = s_m[0];
         for (int k = 1; k < kBlk / 32; ++k) bm = fmaxf(bm, s_m[k]);
-        s_bm = (double)bm;
+        s_bm = bm;
     }
     __syncthreads();
-    const double bm = s_bm;
-    double e = (v0 ? exp((double)acc0 - bm) : 0.0) + (v1 ? exp((double)acc1 - bm) : 0.0);
-    e = warp_sum_d(e);
+    const float bm = s_bm;
+    float e = __fadd_rn(v0 ? expf(__fsub_rn(acc0, bm)) : 0.0f,
+                        v1 ? expf(__fsub_rn(acc1, bm)) : 0.0f);
+    e = warp_sum_f(e);
     if (lane == 0) s_s[warp] = e;
     __syncthreads();
     if (tid == 0) {
-        double sb = 0.0;
-        for (int k = 0; k < kBlk / 32; ++k) sb += s_s[k];
+        float sb = 0.0f;
+        for (int k = 0; k < kBlk / 32; ++k) sb = __fadd_rn(sb, s_s[k]);
         s_sb = sb;
     }
     __syncthreads();
-    return make_double2(bm, s_sb);
+    return make_float2(bm, s_sb);
 }
 
 // Combine G block partials (executed by a whole block of kBlk threads):
-// M = max of the block maxima, S = sum_b exp(m_b - M) * s_b, each reduced
-// thread-strided, then by xor butterfly, then over warps in order.  The
-// result is valid in every thread.
-__device__ __forceinline__ double2 softmax_combine(const double2* part, int G) {
-    __shared__ double s_d[kBlk / 32];
-    __shared__ double s_r;
+// M = max of the block maxima, S = sum_b expf(m_b - M) * s_b in f32, each
+// reduced thread-strided, then by xor butterfly, then over warps in order.
+// The result is valid in every thread.
+__device__ __forceinline__ float2 softmax_combine(const float2* part, int G) {
+    __shared__ float s_d[kBlk / 32];
+    __shared__ float s_r;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    double mx = -INFINITY;
+    float mx = -INFINITY;
 #pragma unroll 4
-    for (int b = tid; b < G; b += kBlk) mx = fmax(mx, __ldcg(&part[b].x));
-    mx = warp_max_d(mx);
+    for (int b = tid; b < G; b += kBlk) mx = fmaxf(mx, __ldcg(&part[b].x));
+    mx = warp_max_f(mx);
     if (lane == 0) s_d[warp] = mx;
     __syncthreads();
     if (tid == 0) {
-        double v = s_d[0];
-        for (int k = 1; k < kBlk / 32; ++k) v = fmax(v, s_d[k]);
+        float v = s_d[0];
+        for (int k = 1; k < kBlk / 32; ++k) v = fmaxf(v, s_d[k]);
         s_r = v;
     }
     __syncthreads();
-    const double M = s_r;
-    double sum = 0.0;
+    const float M = s_r;
+    float sum = 0.0f;
 #pragma unroll 4
     for (int b = tid; b < G; b += kBlk) {
-        const double2 pb = __ldcg(&part[b]);
-        sum += exp(pb.x - M) * pb.y;
+        const float2 pb = __ldcg(&part[b]);
+        sum = __fadd_rn(sum, __fmul_rn(expf(__fsub_rn(pb.x, M)), pb.y));
     }
-    sum = warp_sum_d(sum);
+    sum = warp_sum_f(sum);
     __syncthreads();
     if (lane == 0) s_d[warp] = sum;
     __syncthreads();
     if (tid == 0) {
-        double S = 0.0;
-        for (int k = 0; k < kBlk / 32; ++k) S += s_d[k];
+        float S = 0.0f;
+        for (int k = 0; k < kBlk / 32; ++k) S = __fadd_rn(S, s_d[k]);
         s_r = S;
     }
     __syncthreads();
-    return make_double2(M, s_r);
+    return make_float2(M, s_r);
 }
 
 // Gated log-likelihoods of two particles (p0,q0) and (p1,q1) against nobs
@@ -547,9 +553,12 @@ __device__ __forceinline__ uint64_t threshold_fx(long long i, double u0,
 // thresholds are non-decreasing in i, so this is one more than the last such
 // index; it is estimated from the arithmetic sequence and then corrected
 // against the exact thresholds.
+// inv_step (optional, 1 / step): the estimate by a multiplication instead of
+// a division; the corrections below make the count exact either way.
 __device__ __forceinline__ long long count_le(uint64_t X, int n, double u0,
-                                              double step) {
-    const double e = floor(((double)X * 0x1p-62 - u0) / step);
+                                              double step, double inv_step = 0.0) {
+    const double e = inv_step > 0.0 ? floor(((double)X * 0x1p-62 - u0) * inv_step)
+                                     : floor(((double)X * 0x1p-62 - u0) / step);
     long long i;
     if (!(e >= -1.0))
         i = -1;

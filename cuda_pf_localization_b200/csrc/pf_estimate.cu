@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     pdl_wait();
     const Planes s = pick_planes(ps, ctl->live);
     const int wmode = ctl->wmode;
-    const double M = ctl->ll_max, S = ctl->ll_sumexp;
+    const float M = ctl->ll_max, S = ctl->ll_sumexp;
     const float wuni = 1.0f / (float)n;
     double acc[kEstN];
 #pragma unroll
@@ -125,10 +125,8 @@ __global__ void __launch_bounds__(kThreads, 2)
             W = make_float4(wuni, wuni, wuni, wuni);
         } else {
             const float4 L = reinterpret_cast<const float4*>(ll)[i4];
-            W = make_float4((float)(exp((double)L.x - M) / S),
-                            (float)(exp((double)L.y - M) / S),
-                            (float)(exp((double)L.z - M) / S),
-                            (float)(exp((double)L.w - M) / S));
+            W = make_float4(weight_from_ll(L.x, M, S), weight_from_ll(L.y, M, S),
+                            weight_from_ll(L.z, M, S), weight_from_ll(L.w, M, S));
             reinterpret_cast<float4*>(w)[i4] = W;
         }
 #pragma unroll
@@ -162,7 +160,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     pdl_wait();
     const Planes s = pick_planes(ps, ctl->live);
     const int wmode = ctl->wmode;
-    const double M = ctl->ll_max, S = ctl->ll_sumexp;
+    const float M = ctl->ll_max, S = ctl->ll_sumexp;
     const float wuni = 1.0f / (float)n;
     float3 mpf;
     float4 mqf;
@@ -200,10 +198,8 @@ __global__ void __launch_bounds__(kThreads, 2)
             W = make_float4(wuni, wuni, wuni, wuni);
         } else {
             const float4 L = reinterpret_cast<const float4*>(ll)[i4];
-            W = make_float4((float)(exp((double)L.x - M) / S),
-                            (float)(exp((double)L.y - M) / S),
-                            (float)(exp((double)L.z - M) / S),
-                            (float)(exp((double)L.w - M) / S));
+            W = make_float4(weight_from_ll(L.x, M, S), weight_from_ll(L.y, M, S),
+                            weight_from_ll(L.z, M, S), weight_from_ll(L.w, M, S));
         }
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
@@ -252,16 +248,18 @@ __global__ void __launch_bounds__(kThreads)
           double* part, unsigned long long* partu, uint64_t* prefix,
           unsigned* done, CycleCtl* ctl, int decide, double ess_ratio) {
     pdl_wait();
-    static_assert(kPrefixBlock == 4 * kThreads, "one float4 per thread");
+    static_assert(kPrefixBlock == 8 * kThreads, "two float4 per thread");
     const int wmode = ctl->wmode;
-    const double M = ctl->ll_max, S = ctl->ll_sumexp;
+    const float M = ctl->ll_max, S = ctl->ll_sumexp;
     const float wuni = 1.0f / (float)n;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int i4 = blockIdx.x * kThreads + tid;
     double sq = 0.0;
     unsigned long long tfx = 0;
     int bad = 0;
-    if (4 * i4 < n) {
+#pragma unroll
+    for (int hh = 0; hh < 2; ++hh) {
+        const int i4 = blockIdx.x * 2 * kThreads + hh * kThreads + tid;
+        if (4 * i4 >= n) break;
         float4 W;
         if (wmode == WMODE_STORED) {
             W = reinterpret_cast<const float4*>(w)[i4];
@@ -269,10 +267,8 @@ __global__ void __launch_bounds__(kThreads)
             W = make_float4(wuni, wuni, wuni, wuni);
         } else {
             const float4 L = reinterpret_cast<const float4*>(ll)[i4];
-            W = make_float4((float)(exp((double)L.x - M) / S),
-                            (float)(exp((double)L.y - M) / S),
-                            (float)(exp((double)L.z - M) / S),
-                            (float)(exp((double)L.w - M) / S));
+            W = make_float4(weight_from_ll(L.x, M, S), weight_from_ll(L.y, M, S),
+                            weight_from_ll(L.z, M, S), weight_from_ll(L.w, M, S));
             reinterpret_cast<float4*>(w)[i4] = W;
         }
 #pragma unroll
@@ -379,7 +375,7 @@ __global__ void __launch_bounds__(kThreads)
 __global__ void k_materialize_w(int n, const float* __restrict__ ll,
                                 float* __restrict__ w, CycleCtl* ctl) {
     const int wmode = ctl->wmode;
-    const double M = ctl->ll_max, S = ctl->ll_sumexp;
+    const float M = ctl->ll_max, S = ctl->ll_sumexp;
     for (int i = blockIdx.x * kThreads + threadIdx.x; i < n;
          i += gridDim.x * kThreads) {
         const float wf = weight_of(wmode, i, n, w, ll, M, S);

@@ -22,7 +22,7 @@
 namespace pfb {
 
 constexpr int kEstN = 14;  // pfc_est_sums layout
-constexpr int kPrefixBlock = 1024;  // particles per fixed-point prefix entry
+constexpr int kPrefixBlock = 2048;  // particles per fixed-point prefix entry
 constexpr int kCovN = 12;  // pfc_covs layout
 
 // Weight plane semantics.
@@ -46,8 +46,8 @@ struct Planes {
 // lives in device memory, one mirror in pinned host memory.
 struct CycleCtl {
     // softmax
-    double ll_max;        // M = max ll
-    double ll_sumexp;     // S = sum exp(ll - M)
+    float ll_max;         // M = max ll
+    float ll_sumexp;      // S = sum expf(ll - M), f32 in a fixed order
     int weights_valid;    // 1 when S is finite and > 0
     int wmode;            // WeightMode of the current cloud
     // estimate pass 1
@@ -76,7 +76,6 @@ struct CycleCtl {
     // the estimate pass) and whether any weight is outside [0,1] / NaN
     uint64_t w_total_fx;
     int w_bad;
-    int heavy_count;                 // deferred long copy runs of a resample
     unsigned long long lcg_next;     // LCG word after the running resample
 };
 
@@ -89,14 +88,21 @@ __device__ __forceinline__ bool weight_bad(float w) {
     return !(w >= 0.0f) || !(w <= 1.0f);
 }
 
+// Normalised weight of a log-likelihood, in f32 as the reference computes
+// it (expf(ll - max) / total, src/cuda/pf_kernels.cu:292-297), with the
+// roundings spelled out so every kernel produces the same bits.
+__device__ __forceinline__ float weight_from_ll(float l, float M, float S) {
+    return __fdiv_rn(expf(__fsub_rn(l, M)), S);
+}
+
 // Normalised f32 weight of particle i under the cloud's weight mode.
 __device__ __forceinline__ float weight_of(int wmode, long long i, int n,
                                            const float* __restrict__ w,
                                            const float* __restrict__ ll,
-                                           double M, double S) {
+                                           float M, float S) {
     if (wmode == 0) return 1.0f / (float)n;
     if (wmode == 2) return w[i];
-    return (float)(exp((double)ll[i] - M) / S);
+    return weight_from_ll(ll[i], M, S);
 }
 
 // A copy run of the resampler too long for one thread: particle j fills
@@ -173,6 +179,10 @@ struct PfHandle {
     uint64_t* d_inj_head = nullptr;
     int* d_inj_next = nullptr;
     uint64_t* d_wprefix = nullptr;      // fixed-point weight prefix per block
+    int* d_marker = nullptr;            // run starts of a resample (-1: none)
+    int* d_inj_cnt = nullptr;           // injection draws per resampling tile
+    int* d_inj_bucket = nullptr;        // their draw indices (inj_cap per tile)
+    int inj_cap = 0;
     double* d_part = nullptr;           // per-block partials (max over uses)
     int part_cap = 0;                   // doubles in d_part
     unsigned long long* d_part_u64 = nullptr;  // per-block integer partials
@@ -296,14 +306,20 @@ int launch_weight(PfHandle* h, const PredictArgs& pa, const CObservation* d_obs,
 int launch_est_sums(PfHandle* h);
 int launch_covs(PfHandle* h, bool use_args, const float mp[3],
                 const float mq[4], bool cycle_output);
-// Systematic resampling: tile scan from the weight pass's fixed-point block
-// prefixes (the pass runs first when the weights changed since), ancestors,
-// long runs, output-parallel gather, deterministic injection.  cond_on_ctl:
-// skip unless ctl->resample_now.
-int launch_resample(PfHandle* h, float inject_ratio, bool cond_on_ctl,
-                    bool use_u01, double u01, const CycleArgs* dargs = nullptr);
-// Injection list epoch (32-bit counter, never 0).
-unsigned next_inj_epoch(PfHandle* h);
+// Systematic resampling fused with the gather, the injection and the
+// estimate pass of the resulting cloud (14 FP64 sums, device Markley mean,
+// then the commit of the new live set): the weight pass runs first when the
+// weights changed since the last, and the injection draws are filed by output
+// tile.  cond_on_ctl: resample only when ctl->resample_now, else run the
+// estimate pass over the current cloud.
+int launch_resample_est(PfHandle* h, float inject_ratio, bool cond_on_ctl,
+                        bool use_u01, double u01, const CycleArgs* dargs = nullptr);
+// Output tiles of the resampler (injection counts are kept per tile), and the
+// injection buckets for k draws (allocated outside any graph capture).
+int resample_tiles(int n);
+// FP64 partials (doubles of d_part) the resampler uses.
+int resample_part_doubles(int n);
+int ensure_inject_buckets(PfHandle* h, int k);
 // Weight pass before a resample: materialises the weights, their ESS, the
 // fixed-point total and the per-block prefixes (kPrefixBlock particles per
 // block); with decide set it also takes the fused cycle's resample decision

@@ -78,11 +78,11 @@ __global__ void __launch_bounds__(kThreads)
 // last-block combine into M and S.
 __device__ __forceinline__ void softmax_partials(float acc0, bool v0,
                                                  float acc1, bool v1,
-                                                 double2* part,
+                                                 float2* part,
                                                  unsigned* done,
                                                  CycleCtl* ctl) {
     __shared__ bool s_last;
-    const double2 pb = block_softmax_partial(acc0, v0, acc1, v1);
+    const float2 pb = block_softmax_partial(acc0, v0, acc1, v1);
     if (threadIdx.x == 0) {
         part[blockIdx.x] = pb;
         __threadfence();
@@ -91,12 +91,12 @@ __device__ __forceinline__ void softmax_partials(float acc0, bool v0,
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    const double2 ms = softmax_combine(part, gridDim.x);
+    const float2 ms = softmax_combine(part, gridDim.x);
     if (threadIdx.x == 0) {
-        const double M = ms.x, S = ms.y;
+        const float M = ms.x, S = ms.y;
         ctl->ll_max = M;
         ctl->ll_sumexp = S;
-        const int ok = (S > 0.0 && isfinite(S)) ? 1 : 0;
+        const int ok = (S > 0.0f && isfinite(S)) ? 1 : 0;
         ctl->weights_valid = ok;
         ctl->wmode = ok ? WMODE_LL : WMODE_UNIFORM;
         *done = 0u;
@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(kThreads, 3)
              const CObservation* __restrict__ obs, int nobs,
              const float* __restrict__ lm, int lm_count, float sigma_r,
              float sigma_b, float gate, float* __restrict__ ll,
-             double2* part, unsigned* done, CycleCtl* ctl, int use_packed,
+             float2* part, unsigned* done, CycleCtl* ctl, int use_packed,
              const CycleArgs* ca) {
     pdl_wait();
     if (ca) {  // graph replay: this cycle's values
@@ -188,7 +188,7 @@ int launch_weight(PfHandle* h, const PredictArgs& pa, const CObservation* d_obs,
                   int nobs, float sigma_r, float sigma_b, float gate,
                   const CycleArgs* dargs) {
     const int grid = ceil_div(h->n, 2 * kThreads);
-    double2* part = reinterpret_cast<double2*>(h->d_part);
+    float2* part = reinterpret_cast<float2*>(h->d_part);
     KernelScope ks(h, KK_WEIGHT);
     if (pa.enabled) {
         PFB_CK(launch_pdl(k_weight<true>, grid, kThreads, 0, h->stream, plane_set(h),

@@ -239,6 +239,24 @@ def helix_scenario(cycles: int, n_landmarks: int, box: tuple, n_obs: int | None 
     return sc
 
 
+def as_range_bearing(sc: Scenario) -> Scenario:
+    """The same scenario with every observation in range-bearing form (mode
+    1): range |v| and the unit direction -v/|v| of the body-frame vector v
+    (the measurement model compares the direction with -pred / |pred|,
+    src/cuda/pf_kernels.cu:253-268), the Cartesian noise carried over."""
+    out = Scenario(sc.landmarks, sc.prior_p, sc.prior_q, trans_noise=sc.trans_noise,
+                   rot_noise=sc.rot_noise)
+    for st in sc.steps:
+        rows = st.obs.copy()
+        v = rows[:, 2:5]
+        r = np.linalg.norm(v, axis=1)
+        rows[:, 1] = 1
+        rows[:, 5] = r
+        rows[:, 2:5] = -v / np.maximum(r, 1e-9)[:, None]
+        out.steps.append(Step(st.odom_t, st.odom_q, rows, st.truth_p, st.truth_q))
+    return out
+
+
 def tracking_config(cycles=100, seed=7) -> Scenario:
     """Plain PF tracking workload: 12 landmarks in a 20 x 20 x 5 m box, every
     landmark observed each cycle, 3-sigma gate, 0.02 m / 0.01 rad odometry."""

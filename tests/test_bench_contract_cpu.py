@@ -30,3 +30,36 @@ def test_reference_arm_prints_one_contract_line():
     e = d["e2e"]
     assert e["value"] == d["value"] and e["unit"] == d["unit"]
     assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
+
+
+def _ref_run(extra_env, *args):
+    env = dict(os.environ, **extra_env)
+    return subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "2",
+                           "--warmup", "1", "--particles", "20000", *args],
+                          cwd=ROOT, capture_output=True, text=True, timeout=600, env=env)
+
+
+def test_reference_arm_config_is_the_gpu_arms():
+    sys.path.insert(0, ROOT)
+    import argparse
+    import bench
+    r = _ref_run({})
+    assert r.returncode == 0, r.stderr[-2000:]
+    d = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][0])
+    ns = argparse.Namespace(particles=20000)
+    assert d["config"] == bench.workload_config(ns, 1)
+    assert d["steps"] == 2 and d["warmup"] == 1
+
+
+def test_reference_arm_ranks_of_a_two_rank_world():
+    base = {"WORLD_SIZE": "2", "LOCAL_RANK": "0", "MASTER_ADDR": "127.0.0.1",
+            "MASTER_PORT": "29500"}
+    r0 = _ref_run(dict(base, RANK="0"), "--gpus", "2")
+    assert r0.returncode == 0, r0.stderr[-2000:]
+    lines = [l for l in r0.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1 and json.loads(lines[0])["n_gpus"] == 2
+    r1 = _ref_run(dict(base, RANK="1", LOCAL_RANK="1"), "--gpus", "2")
+    assert r1.returncode == 0 and not r1.stdout.strip()
+    # a torchrun world of another size is refused
+    bad = _ref_run(dict(base, RANK="0"), "--gpus", "4")
+    assert bad.returncode != 0

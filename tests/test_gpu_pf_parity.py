@@ -338,8 +338,8 @@ def test_range_bearing_loglik_matches_reference(kernels, ref):
             assert ours.weight(rows, 0.05, 0.02, gate) == 0
             assert theirs.weight(rows, 0.05, 0.02, gate) == 0
             a, b = ours_ll(ours), ref_ll(ref, theirs)
-            print(f"range-bearing gate={gate}: bit-identical {np.mean(a == b):.6f}")
-            assert np.all(rel_close(a, b, 2e-6, 1e-5))
+            # the same rounded operations as the reference kernel: identical bits
+            assert np.array_equal(a, b), np.mean(a == b)
     finally:
         ours.close()
         theirs.close()
