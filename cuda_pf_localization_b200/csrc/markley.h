@@ -150,4 +150,92 @@ PFB_HD inline void markley_mean(const double m10[10], double q_out[4]) {
     for (int i = 0; i < 4; ++i) q_out[i] = sgn * q[i] / nrm;
 }
 
+#ifdef __CUDACC__
+// The serial solve as a call of its own (the rare fallback below), so its
+// registers do not count against its caller.
+static __device__ __noinline__ void markley_mean_serial(const double* m10, double* q_out) {
+    markley_mean(m10, q_out);
+}
+
+// markley_mean by one warp: lanes 4r + c (r, c < 4) of the first 16 hold
+// element (r, c) of the 4x4 matrix, so a squaring is four shuffled products
+// per lane instead of 64 serial ones; the same method and acceptance test as
+// dominant_eigvec_psd4, and the same serial Jacobi fallback (one lane) for a
+// near-degenerate top eigenvalue.  Every lane of the warp must call it; the
+// result is valid in every lane.
+__device__ inline void markley_mean_warp(const double m10[10], double q_out[4]) {
+    const unsigned full = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    const int r = (lane >> 2) & 3, c = lane & 3;
+    const int lo = r < c ? r : c, hi = r < c ? c : r;
+    const double a = m10[lo * 4 - lo * (lo - 1) / 2 + (hi - lo)];  // a[r][c]
+    auto at = [&](double v, int rr, int cc) { return __shfl_sync(full, v, rr * 4 + cc); };
+    auto trace = [&](double v) {
+        return at(v, 0, 0) + at(v, 1, 1) + at(v, 2, 2) + at(v, 3, 3);
+    };
+    const double tr = trace(a);
+    bool ok = tr > 0.0;
+    double x[4] = {0.0, 0.0, 0.0, 0.0};
+    if (ok) {
+        const double itr = 1.0 / tr;
+        double pm = a * itr;
+        for (int s = 0; s < 12 && ok; ++s) {
+            const double t = at(pm, r, 0) * at(pm, 0, c) + at(pm, r, 1) * at(pm, 1, c) +
+                             at(pm, r, 2) * at(pm, 2, c) + at(pm, r, 3) * at(pm, 3, c);
+            const double tt = trace(t);
+            ok = tt > 0.0;
+            pm = t * (1.0 / tt);
+        }
+        if (ok) {
+            // the column of the largest diagonal entry, then two power steps
+            // with the original matrix
+            int cb = 0;
+            double db = at(pm, 0, 0);
+            for (int i = 1; i < 4; ++i) {
+                const double d = at(pm, i, i);
+                if (d > db) {
+                    db = d;
+                    cb = i;
+                }
+            }
+            for (int i = 0; i < 4; ++i) x[i] = at(pm, i, cb);
+            for (int it = 0; it < 2 && ok; ++it) {
+                double y[4];
+                for (int i = 0; i < 4; ++i)
+                    y[i] = at(a, i, 0) * x[0] + at(a, i, 1) * x[1] + at(a, i, 2) * x[2] +
+                           at(a, i, 3) * x[3];
+                const double ny = sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2] + y[3] * y[3]);
+                ok = ny > 0.0;
+                for (int i = 0; i < 4; ++i) x[i] = y[i] / ny;
+            }
+            if (ok) {
+                double y[4];
+                for (int i = 0; i < 4; ++i)
+                    y[i] = at(a, i, 0) * x[0] + at(a, i, 1) * x[1] + at(a, i, 2) * x[2] +
+                           at(a, i, 3) * x[3];
+                const double lam = x[0] * y[0] + x[1] * y[1] + x[2] * y[2] + x[3] * y[3];
+                double res = 0.0;
+                for (int i = 0; i < 4; ++i) res += (y[i] - lam * x[i]) * (y[i] - lam * x[i]);
+                ok = sqrt(res) <= 1e-13 * tr;
+            }
+        }
+    }
+    if (!ok) {
+        // near-degenerate spectrum: the serial solve, by lane 0
+        double q[4];
+        if (lane == 0) markley_mean_serial(m10, q);
+        for (int i = 0; i < 4; ++i) q_out[i] = __shfl_sync(full, q[i], 0);
+        return;
+    }
+    const double nrm = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2] + x[3] * x[3]);
+    if (!(nrm > 0.0)) {
+        q_out[0] = 1.0;
+        q_out[1] = q_out[2] = q_out[3] = 0.0;
+        return;
+    }
+    const double sgn = (x[0] < 0.0) ? -1.0 : 1.0;
+    for (int i = 0; i < 4; ++i) q_out[i] = sgn * x[i] / nrm;
+}
+#endif
+
 }  // namespace pfb

@@ -25,15 +25,17 @@
 //     output-tile boundary inside it (so every output tile starts with a
 //     marker, and a source writes one marker plus one per tile its run
 //     crosses), and adds its particle, weighted by its run length / n, to the
-//     14 FP64 estimate sums of the new cloud; the last block combines them in
-//     block order and runs the Markley mean;
-//   * k_gather (output-parallel, persistent): a block loads the markers of an
-//     output tile; a block-wide running maximum (ancestors increase with the
-//     output index) gives every output its ancestor, kept in shared memory.
-//     It resets the markers it read, copies the particles plane by plane from
-//     the live set (16-byte stores) and adds the injection jitters of the
-//     draws that landed in the tile; its last block adds the jitters' change
-//     to the position sums and commits the resample (live set, LCG).
+//     14 FP64 estimate sums of the new cloud (one partial per block);
+//   * k_gather (output-parallel, persistent): block 0 combines k_mark's
+//     partials in block order and runs the Markley mean (warp-parallel).
+//     Blocks 1.. each load the markers of an output tile; a block-wide
+//     running maximum (ancestors increase with the output index) gives every
+//     output its ancestor, kept in shared memory.  A block resets the
+//     markers it read, copies the seven planes of four outputs at a time
+//     from the live set (16-byte stores) and adds the injection jitters of
+//     the draws that landed in the tile; the last block to finish adds the
+//     jitters' change to the position sums and commits the resample (live
+//     set, LCG).
 // No output needs a search and no block does more than its outputs or its
 // sources, whatever the weights.  When the cycle does not resample (or the
 // total is invalid), k_mark is the estimate pass over the cloud instead and
@@ -144,7 +146,7 @@ __device__ __forceinline__ void combine_staged(const double* part, int G, double
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int tot = G * NV;
     constexpr int kPer = (NV * kMaxG + kThreads - 1) / kThreads;
-    constexpr int kBatch = 4;  // loads in flight per thread
+    constexpr int kBatch = 8;  // loads in flight per thread
 #pragma unroll 1
     for (int r0 = 0; r0 < kPer; r0 += kBatch) {
         double v[kBatch];
@@ -388,11 +390,10 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
 }
 
-// The Markley mean as a call of its own: it runs once per cycle (block 0,
-// thread 0), and not inlined its registers do not count against the copy
-// loop of k_gather.
+// The Markley mean by warp 0 of block 0, once per cycle, as a call of its
+// own: not inlined, its registers do not count against the copy loop.
 __device__ __noinline__ void markley_mean_once(const double* m10, double* q_out) {
-    markley_mean(m10, q_out);
+    markley_mean_warp(m10, q_out);
 }
 
 // Shared memory of k_gather: a tile's ancestors and injection list, or the
@@ -433,11 +434,11 @@ __global__ void __launch_bounds__(kThreads, 4)
     const bool valid = resample && ctl->w_total_fx != 0 && !ctl->w_bad;
     if (blockIdx.x == 0) {
         combine_staged<kEstN, kMarkGrid>(part_m, mark_grid, sm.pm, s_out);
+        double qm[4];
+        if (warp == 0) markley_mean_once(&s_out[3], qm);
         if (tid == 0) {
             for (int q = 0; q < kEstN; ++q) ctl->est[q] = s_out[q];
             ctl->ess = s_out[13] > 0.0 ? 1.0 / s_out[13] : 0.0;
-            double qm[4];
-            markley_mean_once(&s_out[3], qm);
             for (int q = 0; q < 4; ++q) ctl->qmean[q] = qm[q];
             for (int q = 0; q < 3; ++q) ctl->cov_mean_p[q] = (float)s_out[q];
             for (int q = 0; q < 4; ++q) ctl->cov_mean_q[q] = (float)qm[q];
