@@ -134,6 +134,13 @@ _KERNEL_SIGS = {
                                  POINTER(PfcCycleParams), _dp]),
     "pfc_cycle_result": (c_int, [c_void_p, _dp]),
     "pfc_set_graph": (c_int, [c_void_p, c_int]),
+    "pfc_shard_init": (c_int, [c_void_p, c_int, c_int, c_int, c_uint]),
+    "pfc_shard_layout": (c_int, [c_void_p, _ip, _ip]),
+    "pfc_shard_weight": (c_int, [c_void_p, POINTER(PfcOdom), c_void_p, c_int,
+                                 POINTER(PfcCycleParams)]),
+    "pfc_shard_views": (c_int, [c_void_p, POINTER(c_void_p), POINTER(c_void_p),
+                                POINTER(c_void_p)]),
+    "pfc_shard_finish": (c_int, [c_void_p, POINTER(PfcCycleParams), _dp]),
     "pfc_stream": (c_void_p, [c_void_p]),
     "pfc_size": (c_int, [c_void_p]),
     "pfc_get_weights": (c_int, [c_void_p, _fp]),

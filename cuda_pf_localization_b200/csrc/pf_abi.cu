@@ -18,6 +18,7 @@
 //                 caller's means.
 //   pfc_resample  fixed-point scan + merge-path gather + injection, then the
 //                 speculative estimate again.
+#include <limits.h>
 #include <math.h>
 #include <stdarg.h>
 #include <stdlib.h>
@@ -139,7 +140,6 @@ void free_particles(PfHandle* h) {
     cudaFree(h->d_state[1]);
     cudaFree(h->d_ll);
     cudaFree(h->d_w);
-    cudaFree(h->d_cum);
     cudaFree(h->d_anc);
     cudaFree(h->d_wprefix);
     cudaFree(h->d_marker);
@@ -150,7 +150,6 @@ void free_particles(PfHandle* h) {
     cudaFree(h->d_stage);
     h->d_state[0] = h->d_state[1] = nullptr;
     h->d_ll = h->d_w = nullptr;
-    h->d_cum = nullptr;
     h->d_anc = nullptr;
     h->d_wprefix = nullptr;
     h->d_marker = nullptr;
@@ -383,6 +382,8 @@ int enqueue_cycle(PfHandle* h, const PredictArgs& pa, const CObservation* obs_de
     return 0;
 }
 
+int init_particles(PfHandle* h, int n, unsigned int seed, int n_pad);
+
 int finish_cycle(PfHandle* h, double* est_out) {
     if (wait_estimate(h)) return -1;
     if (est_out) memcpy(est_out, h->h_ctl->out, sizeof(double) * PFC_EST_LEN);
@@ -498,10 +499,22 @@ int pfc_destroy(void* hv) {
 int pfc_init(void* hv, int n, unsigned int seed) {
     PfHandle* h = as_pf(hv);
     if (!h || n <= 0) return -1;
+    h->shard_world = h->shard_rank = h->shard_chunk = 0;
+    return init_particles(h, n, seed, (int)(ceil_div_ll(n, 1024) * 1024));
+}
+
+}  // extern "C"
+
+namespace pfb {
+namespace {
+
+// Allocate and reset a cloud of n particles in planes of n_pad (a multiple
+// of 1024, at least n).
+int init_particles(PfHandle* h, int n, unsigned int seed, int n_pad) {
     PFB_CK(cudaStreamSynchronize(h->stream));
     free_particles(h);
     h->n = n;
-    h->n_pad = (int)(ceil_div_ll(n, 1024) * 1024);
+    h->n_pad = n_pad;
     h->seed = seed ? (uint64_t)seed : 42ull;
     h->gen = 0;
     h->pending_predict = false;
@@ -510,8 +523,10 @@ int pfc_init(void* hv, int n, unsigned int seed) {
     h->prefix_valid = false;
     const size_t np = (size_t)h->n_pad;
     const int nprefix = ceil_div(n, kPrefixBlock);
+    // doubles: the largest of the kernels' partial arrays (float2 softmax
+    // partials of every 512-particle block of the planes included)
     const int part = std::max(std::max(2 * ceil_div(n, kThreads), resample_part_doubles(n)),
-                              1184 * 16);
+                              std::max(1184 * 16, n_pad / (2 * kThreads)));
     PFB_CK(cudaMalloc((void**)&h->d_state[0], 7 * np * sizeof(float)));
     PFB_CK(cudaMalloc((void**)&h->d_state[1], 7 * np * sizeof(float)));
     PFB_CK(cudaMalloc((void**)&h->d_ll, np * sizeof(float)));
@@ -537,6 +552,11 @@ int pfc_init(void* hv, int n, unsigned int seed) {
     PFB_CK(cudaStreamSynchronize(h->stream));
     return 0;
 }
+
+}  // namespace
+}  // namespace pfb
+
+extern "C" {
 
 int pfc_upload_landmarks(void* hv, const float* xyz, int count) {
     PfHandle* h = as_pf(hv);
@@ -747,6 +767,100 @@ int pfc_set_graph(void* hv, int on) {
 int pfc_cycle_result(void* hv, double* est_out) {
     PfHandle* h = as_pf(hv);
     if (!valid_handle(h) || !est_out) return -1;
+    return finish_cycle(h, est_out);
+}
+
+// ---------------------------------------------------------- sharded filter
+
+int pfc_shard_init(void* hv, int n, int world, int rank, unsigned int seed) {
+    PfHandle* h = as_pf(hv);
+    if (!h || n <= 0 || world < 1 || rank < 0 || rank >= world) {
+        set_error("pf_b200: pfc_shard_init: bad arguments (n %d, world %d, rank %d)", n,
+                  world, rank);
+        return -1;
+    }
+    const long long chunk = ceil_div_ll(ceil_div_ll(n, world), kPrefixBlock) * kPrefixBlock;
+    const long long n_pad = std::max<long long>(ceil_div_ll(n, 1024) * 1024, chunk * world);
+    if (n_pad > (long long)INT_MAX / 7) {
+        set_error("pf_b200: pfc_shard_init: %d particles over %d ranks too large", n, world);
+        return -1;
+    }
+    h->shard_world = world;
+    h->shard_rank = rank;
+    h->shard_chunk = (int)chunk;
+    h->shard_nobs = 0;
+    if (init_particles(h, n, seed, (int)n_pad)) {
+        h->shard_world = h->shard_rank = h->shard_chunk = 0;
+        return -1;
+    }
+    return 0;
+}
+
+int pfc_shard_layout(void* hv, int* chunk, int* n_pad) {
+    PfHandle* h = as_pf(hv);
+    if (!valid_handle(h) || h->shard_world < 1) return -1;
+    if (chunk) *chunk = h->shard_chunk;
+    if (n_pad) *n_pad = h->n_pad;
+    return 0;
+}
+
+int pfc_shard_weight(void* hv, const PfcOdom* odom, const CObservation* obs, int nobs,
+                     const PfcCycleParams* prm) {
+    PfHandle* h = as_pf(hv);
+    if (!valid_handle(h) || !odom || !prm) return -1;
+    if (h->shard_world < 1) {
+        set_error("pf_b200: pfc_shard_weight: not a shard handle (pfc_shard_init)");
+        return -1;
+    }
+    if (nobs > h->cap_obs) nobs = h->cap_obs;
+    if (!obs || nobs < 0) nobs = 0;
+    if (flush_predict(h)) return -1;
+    if (nobs > 0 && stage_observations(h, obs, nobs)) return -1;
+    h->gen++;
+    PredictArgs pa{};
+    pa.enabled = 1;
+    pa.gen = h->gen;
+    for (int k = 0; k < 3; ++k) {
+        pa.t[k] = odom->t[k];
+        pa.tstd[k] = odom->tstd[k];
+        pa.rstd[k] = odom->rstd[k];
+    }
+    for (int k = 0; k < 4; ++k) pa.q[k] = odom->q[k];
+    if (launch_weight_shard(h, pa, h->d_obs, nobs, prm->sigma_r, prm->sigma_b, prm->gate))
+        return -1;
+    h->shard_nobs = nobs;
+    h->est_valid = false;
+    return 0;
+}
+
+int pfc_shard_views(void* hv, float** planes7, float** ll, float** part) {
+    PfHandle* h = as_pf(hv);
+    if (!valid_handle(h) || !planes7 || h->shard_world < 1) return -1;
+    PFB_CK(cudaStreamSynchronize(h->stream));
+    int live = 0;
+    PFB_CK(cudaMemcpy(&live, &h->d_ctl->live, sizeof(int), cudaMemcpyDeviceToHost));
+    const Planes s = h->planes(live ? 1 : 0);
+    float* const p[7] = {s.px, s.py, s.pz, s.qw, s.qx, s.qy, s.qz};
+    for (int k = 0; k < 7; ++k) planes7[k] = p[k];
+    if (ll) *ll = h->d_ll;
+    if (part) *part = reinterpret_cast<float*>(h->d_part);
+    return 0;
+}
+
+int pfc_shard_finish(void* hv, const PfcCycleParams* prm, double* est_out) {
+    PfHandle* h = as_pf(hv);
+    if (!valid_handle(h) || !prm) return -1;
+    if (h->shard_world < 1) {
+        set_error("pf_b200: pfc_shard_finish: not a shard handle (pfc_shard_init)");
+        return -1;
+    }
+    // the cycle without observations keeps uniform weights, as pfc_cycle's
+    if (h->shard_nobs > 0 ? launch_softmax_combine(h) : set_wmode(h, WMODE_UNIFORM))
+        return -1;
+    const PredictArgs none{};
+    if (enqueue_cycle(h, none, nullptr, 0, prm, nullptr)) return -1;
+    h->est_inflight = true;
+    h->est_valid = false;
     return finish_cycle(h, est_out);
 }
 

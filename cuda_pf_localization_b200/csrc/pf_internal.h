@@ -7,9 +7,10 @@
 //   ll        f32 log-likelihood of the last weighting          (1 plane)
 //   w         f32 normalised weight (materialised on demand)    (1 plane)
 //   anc       i32 ancestor of each particle in the last resample
-//   inj_head  u64 epoch-tagged injection list heads (one per particle)
-//   inj_next  i32 injection list links
-// plus small per-block partial buffers and one CycleCtl control block.
+//   marker    i32 run starts of a resample (-1 elsewhere)
+//   prefix    u64 exclusive fixed-point weight prefix per 2048 particles
+// plus the injection buckets per 2048-output tile, small per-block partial
+// buffers and one CycleCtl control block.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -169,15 +170,17 @@ struct PfHandle {
     int cap_obs = 64;
     uint64_t seed = 42;
     uint64_t gen = 0;
-    int cur = 0;  // which ping-pong state is live
+    // sharded filter (pfc_shard_init): this handle holds the whole cloud and
+    // predicts and weights particles [shard_rank * shard_chunk, ...) of it
+    int shard_world = 0;
+    int shard_rank = 0;
+    int shard_chunk = 0;
+    int shard_nobs = 0;  // observations of the slice weighting in flight
 
     float* d_state[2] = {nullptr, nullptr};  // 7 planes each
     float* d_ll = nullptr;
     float* d_w = nullptr;
-    uint64_t* d_cum = nullptr;
     int* d_anc = nullptr;
-    uint64_t* d_inj_head = nullptr;
-    int* d_inj_next = nullptr;
     uint64_t* d_wprefix = nullptr;      // fixed-point weight prefix per block
     int* d_marker = nullptr;            // run starts of a resample (-1: none)
     int* d_inj_cnt = nullptr;           // injection draws per resampling tile
@@ -186,8 +189,6 @@ struct PfHandle {
     double* d_part = nullptr;           // per-block partials (max over uses)
     int part_cap = 0;                   // doubles in d_part
     unsigned long long* d_part_u64 = nullptr;  // per-block integer partials
-    HeavyRun* d_heavy = nullptr;        // deferred copy runs (n/32 + 1)
-    int heavy_cap = 0;
     bool prefix_valid = false;  // ctl w_total_fx and d_wprefix describe the
                                 // current weights
     unsigned* d_done = nullptr;         // last-block counters
@@ -245,7 +246,6 @@ struct PfHandle {
         return {b, b + p, b + 2 * p, b + 3 * p, b + 4 * p, b + 5 * p,
                 b + 6 * p};
     }
-    Planes live() const { return planes(cur); }
 };
 
 // ------------------------------------------------------- accounting helpers
@@ -299,6 +299,11 @@ int launch_predict(PfHandle* h, const PredictArgs& pa);
 int launch_weight(PfHandle* h, const PredictArgs& pa, const CObservation* d_obs,
                   int nobs, float sigma_r, float sigma_b, float gate,
                   const CycleArgs* dargs = nullptr);
+// A sharded filter's slice (predict + weighting, block partials kept for the
+// exchange), and the softmax combine over every rank's partials after it.
+int launch_weight_shard(PfHandle* h, const PredictArgs& pa, const CObservation* d_obs,
+                        int nobs, float sigma_r, float sigma_b, float gate);
+int launch_softmax_combine(PfHandle* h);
 // Estimate pass 1 (+ device Markley mean) and the speculative covariance pass
 // around (float)mean, (float)qmean.  When use_args is set the covariance pass
 // uses the given f32 means instead; cycle_output also assembles the fused

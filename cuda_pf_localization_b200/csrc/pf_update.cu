@@ -74,6 +74,17 @@ __global__ void __launch_bounds__(kThreads)
     store_pose(s, i, p, q);
 }
 
+// M and S of the softmax into the control block (weights valid when S is a
+// positive finite sum).
+__device__ __forceinline__ void softmax_commit(float2 ms, CycleCtl* ctl) {
+    const float M = ms.x, S = ms.y;
+    ctl->ll_max = M;
+    ctl->ll_sumexp = S;
+    const int ok = (S > 0.0f && isfinite(S)) ? 1 : 0;
+    ctl->weights_valid = ok;
+    ctl->wmode = ok ? WMODE_LL : WMODE_UNIFORM;
+}
+
 // Softmax partial of one block (two log-likelihoods per thread) + the
 // last-block combine into M and S.
 __device__ __forceinline__ void softmax_partials(float acc0, bool v0,
@@ -93,27 +104,34 @@ __device__ __forceinline__ void softmax_partials(float acc0, bool v0,
     __threadfence();
     const float2 ms = softmax_combine(part, gridDim.x);
     if (threadIdx.x == 0) {
-        const float M = ms.x, S = ms.y;
-        ctl->ll_max = M;
-        ctl->ll_sumexp = S;
-        const int ok = (S > 0.0f && isfinite(S)) ? 1 : 0;
-        ctl->weights_valid = ok;
-        ctl->wmode = ok ? WMODE_LL : WMODE_UNIFORM;
+        softmax_commit(ms, ctl);
         *done = 0u;
     }
+}
+
+// The combine of a sharded filter, once every rank's block partials are in
+// part[0, G): one block, the same combine as the last block above, so M and
+// S equal the unsharded filter's bit for bit.
+__global__ void __launch_bounds__(kThreads) k_softmax_combine(const float2* part, int G,
+                                                              CycleCtl* ctl) {
+    const float2 ms = softmax_combine(part, G);
+    if (threadIdx.x == 0) softmax_commit(ms, ctl);
 }
 
 // Two particles per thread (i and i + 256): every staged observation read
 // from shared memory serves both.  Three blocks per SM (up to 85 registers,
 // no spills): measured 4 % faster than four blocks at 64 registers.
-template <bool kPredict>
+// kShard: one rank's slice of a sharded filter; block b of the launch is
+// block block0 + b of the whole cloud, and the block partials are left for
+// the combine that follows the exchange (k_softmax_combine).
+template <bool kPredict, bool kShard>
 __global__ void __launch_bounds__(kThreads, 3)
     k_weight(PlaneSet ps, int n, uint64_t seed, PredictArgs pa,
              const CObservation* __restrict__ obs, int nobs,
              const float* __restrict__ lm, int lm_count, float sigma_r,
              float sigma_b, float gate, float* __restrict__ ll,
              float2* part, unsigned* done, CycleCtl* ctl, int use_packed,
-             const CycleArgs* ca) {
+             const CycleArgs* ca, int block0) {
     pdl_wait();
     if (ca) {  // graph replay: this cycle's values
         pa = ca->pa;
@@ -121,7 +139,8 @@ __global__ void __launch_bounds__(kThreads, 3)
         nobs = ca->nobs;
     }
     const Planes s = pick_planes(ps, ctl->live);
-    const int i0 = blockIdx.x * (2 * kThreads) + threadIdx.x;
+    const int blk = kShard ? (int)blockIdx.x + block0 : (int)blockIdx.x;
+    const int i0 = blk * (2 * kThreads) + threadIdx.x;
     const int i1 = i0 + kThreads;
     const bool v0 = i0 < n, v1 = i1 < n;
     float3 p0 = make_float3(0.f, 0.f, 0.f), p1 = p0;
@@ -145,7 +164,12 @@ __global__ void __launch_bounds__(kThreads, 3)
                use_packed, acc0, acc1);
     if (v0) ll[i0] = acc0;
     if (v1) ll[i1] = acc1;
-    softmax_partials(acc0, v0, acc1, v1, part, done, ctl);
+    if (kShard) {
+        const float2 pb = block_softmax_partial(acc0, v0, acc1, v1);
+        if (threadIdx.x == 0) part[blk] = pb;
+    } else {
+        softmax_partials(acc0, v0, acc1, v1, part, done, ctl);
+    }
 }
 
 }  // namespace
@@ -191,16 +215,48 @@ int launch_weight(PfHandle* h, const PredictArgs& pa, const CObservation* d_obs,
     float2* part = reinterpret_cast<float2*>(h->d_part);
     KernelScope ks(h, KK_WEIGHT);
     if (pa.enabled) {
-        PFB_CK(launch_pdl(k_weight<true>, grid, kThreads, 0, h->stream, plane_set(h),
+        PFB_CK(launch_pdl(k_weight<true, false>, grid, kThreads, 0, h->stream, plane_set(h),
                           h->n, h->seed, pa, d_obs, nobs, h->d_lm, h->lm_count,
                           sigma_r, sigma_b, gate, h->d_ll, part, h->d_done + 0,
-                          h->d_ctl, h->weight_variant == 0 ? 1 : 0, dargs));
+                          h->d_ctl, h->weight_variant == 0 ? 1 : 0, dargs, 0));
     } else {
-        PFB_CK(launch_pdl(k_weight<false>, grid, kThreads, 0, h->stream, plane_set(h),
+        PFB_CK(launch_pdl(k_weight<false, false>, grid, kThreads, 0, h->stream, plane_set(h),
                           h->n, h->seed, pa, d_obs, nobs, h->d_lm, h->lm_count,
                           sigma_r, sigma_b, gate, h->d_ll, part, h->d_done + 0,
-                          h->d_ctl, h->weight_variant == 0 ? 1 : 0, dargs));
+                          h->d_ctl, h->weight_variant == 0 ? 1 : 0, dargs, 0));
     }
+    PFB_KL();
+    h->prefix_valid = false;
+    return 0;
+}
+
+// One rank's slice of a sharded filter: particles [rank * chunk,
+// min((rank + 1) * chunk, n)), predicted and weighted; their block partials
+// land at their global block index of d_part (as float2) for the exchange.
+int launch_weight_shard(PfHandle* h, const PredictArgs& pa, const CObservation* d_obs,
+                        int nobs, float sigma_r, float sigma_b, float gate) {
+    const long long first = (long long)h->shard_rank * h->shard_chunk;
+    const long long last = std::min<long long>(first + h->shard_chunk, h->n);
+    if (last <= first) return 0;  // a rank past the end of the cloud
+    const int block0 = (int)(first / (2 * kThreads));
+    const int grid = (int)ceil_div_ll(last - first, 2 * kThreads);
+    float2* part = reinterpret_cast<float2*>(h->d_part);
+    KernelScope ks(h, KK_WEIGHT);
+    PFB_CK(launch_pdl(k_weight<true, true>, grid, kThreads, 0, h->stream, plane_set(h), h->n,
+                      h->seed, pa, d_obs, nobs, h->d_lm, h->lm_count, sigma_r, sigma_b, gate,
+                      h->d_ll, part, h->d_done + 0, h->d_ctl,
+                      h->weight_variant == 0 ? 1 : 0, (const CycleArgs*)nullptr, block0));
+    PFB_KL();
+    h->prefix_valid = false;
+    return 0;
+}
+
+// The softmax of a sharded filter over all ceil(n / 512) block partials.
+int launch_softmax_combine(PfHandle* h) {
+    const int G = (int)ceil_div_ll(h->n, 2 * kThreads);
+    KernelScope ks(h, KK_WEIGHT);
+    k_softmax_combine<<<1, kThreads, 0, h->stream>>>(
+        reinterpret_cast<const float2*>(h->d_part), G, h->d_ctl);
     PFB_KL();
     h->prefix_valid = false;
     return 0;

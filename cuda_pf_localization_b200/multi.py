@@ -1,13 +1,20 @@
 """Host-side plumbing for one process per GPU (torch.distributed).
 
-The single particle filter does not shard in this library: N GPUs run N
-independent replica filters (weak scaling), and the cross-rank steps are the
-barrier around a timed region and the max over ranks of the measured times.
-A global-localization query shards by hypotheses: every rank scores a
-contiguous slice of one global hypothesis set, keeps its k best (CAER,
-global index) keys, and one all-gather of k keys and poses per rank gives the
-global bottom-k (sharded_localize).  This module keeps those steps in one
-place so that the CPU tests can exercise them with the gloo backend.
+Three multi-GPU modes live here:
+  * replicas: N GPUs run N independent filters (weak scaling); the
+    cross-rank steps are the barrier around a timed region and the max over
+    ranks of the measured times;
+  * a sharded filter: one filter over N ranks (ShardedFilter).  Every rank
+    predicts and weights its slice of the particles, an all-gather of the
+    slices (poses, log-likelihoods, softmax block partials) gives every rank
+    the whole weighted cloud, and every rank finishes the cycle on it, so
+    the result equals the one-GPU filter's bit for bit;
+  * a sharded global-localization query: every rank scores a contiguous
+    slice of one global hypothesis set, keeps its k best (CAER, global
+    index) keys, and one all-gather of k keys and poses per rank gives the
+    global bottom-k (sharded_localize).
+This module keeps those steps in one place so that the CPU tests can
+exercise them with the gloo backend.
 """
 from __future__ import annotations
 
@@ -222,3 +229,146 @@ def sharded_localize(gl_handle, scan: np.ndarray, n_pos: int, n_yaw: int, seed: 
                                  rmax, span)
     kk, pp = merge_bottom_k(keys, poses, k, dist, device)
     return kk, pp, key_caer(kk), (kk & np.uint64(0xFFFFFFFF)).astype(np.int64)
+
+
+# ------------------------------------------------------------ sharded filter
+
+class DeviceArray:
+    """A 1-D view of library-owned device memory that torch can wrap without
+    a copy (``torch.as_tensor(DeviceArray(...), device=...)``, through the
+    CUDA array interface).  The memory belongs to the library handle, which
+    must outlive the tensor."""
+
+    def __init__(self, ptr: int, length: int, typestr: str = "<f4"):
+        self.__cuda_array_interface__ = {
+            "shape": (int(length),), "typestr": typestr, "data": (int(ptr), False),
+            "strides": None, "version": 3}
+
+
+def exchange_views(views, rank: int, dist) -> None:
+    """All-gather of one rank's chunks: views is a list of (tensor of
+    world * c elements, c); every rank contributes elements
+    [rank * c, (rank + 1) * c) of each tensor and receives the others' in
+    place.  NCCL gathers straight into the tensor; other backends (gloo on
+    CPU tensors) gather into its chunk views."""
+    for full, c in views:
+        mine = full[rank * c:(rank + 1) * c].clone()
+        if dist.get_backend() == "nccl":
+            dist.all_gather_into_tensor(full, mine)
+        else:
+            dist.all_gather(list(full.split(c)), mine)
+
+
+def exchange_in_process(shard_views) -> None:
+    """The same exchange between the shards of one process (one GPU, or CPU
+    tensors): shard_views[r] is rank r's view list; chunk r of every tensor
+    is copied from rank r to every other rank."""
+    world = len(shard_views)
+    for a in range(len(shard_views[0])):
+        for r in range(world):
+            full, c = shard_views[r][a]
+            src = full[r * c:(r + 1) * c]
+            for q in range(world):
+                if q != r:
+                    shard_views[q][a][0][r * c:(r + 1) * c].copy_(src)
+
+
+class ShardedFilter:
+    """One rank's handle of a particle filter sharded over ``world`` ranks
+    (pfc_shard_*): it holds the whole cloud, predicts and weights particles
+    [rank * chunk, min((rank + 1) * chunk, n)), and finishes every cycle on
+    the whole cloud after the exchange.  Give every rank the same n, seed,
+    landmarks, prior and cycle inputs."""
+
+    def __init__(self, n: int, world: int, rank: int, seed: int = 42, cap_obs: int = 256,
+                 device=None):
+        import ctypes as C
+
+        import torch
+
+        from . import kernels, last_error
+        self.lib = kernels()
+        self.h = self.lib.pfc_create(cap_obs)
+        if not self.h:
+            raise RuntimeError("pfc_create failed: " + last_error())
+        if self.lib.pfc_shard_init(self.h, n, world, rank, seed) != 0:
+            err = last_error()
+            self.lib.pfc_destroy(self.h)
+            self.h = None
+            raise RuntimeError("pfc_shard_init failed: " + err)
+        chunk, n_pad = C.c_int(), C.c_int()
+        self.lib.pfc_shard_layout(self.h, C.byref(chunk), C.byref(n_pad))
+        self.n, self.world, self.rank = n, world, rank
+        self.chunk = chunk.value
+        self.device = device if device is not None else torch.device(
+            "cuda", torch.cuda.current_device())
+
+    def weigh(self, odom, obs_rows, prm) -> None:
+        """Predict and weight this rank's slice (asynchronous)."""
+        import ctypes as C
+
+        from . import last_error, make_cobs
+        arr = make_cobs(obs_rows) if len(obs_rows) else None
+        ptr = C.cast(arr, C.c_void_p) if arr is not None else None
+        if self.lib.pfc_shard_weight(self.h, C.byref(odom), ptr, len(obs_rows),
+                                     C.byref(prm)) != 0:
+            raise RuntimeError("pfc_shard_weight failed: " + last_error())
+
+    def views(self):
+        """(tensor, chunk) for the seven live planes, the log-likelihoods and
+        the f32 softmax block partials (two floats per 512 particles), each
+        covering world chunks; after the slice's kernels completed."""
+        import ctypes as C
+
+        import torch
+
+        from . import last_error
+        p7 = (C.c_void_p * 7)()
+        ll, part = C.c_void_p(), C.c_void_p()
+        if self.lib.pfc_shard_views(self.h, p7, C.byref(ll), C.byref(part)) != 0:
+            raise RuntimeError("pfc_shard_views failed: " + last_error())
+        full, c = self.world * self.chunk, self.chunk
+        out = [(torch.as_tensor(DeviceArray(p7[k], full), device=self.device), c)
+               for k in range(7)]
+        out.append((torch.as_tensor(DeviceArray(ll.value, full), device=self.device), c))
+        out.append((torch.as_tensor(DeviceArray(part.value, full // 256), device=self.device),
+                    c // 256))
+        return out
+
+    def finish(self, prm) -> np.ndarray:
+        """The rest of the cycle on the whole cloud; the 24-value record of
+        pfc_cycle."""
+        import ctypes as C
+
+        from . import PFC_EST_LEN, dptr, last_error
+        est = np.zeros(PFC_EST_LEN)
+        if self.lib.pfc_shard_finish(self.h, C.byref(prm), dptr(est)) != 0:
+            raise RuntimeError("pfc_shard_finish failed: " + last_error())
+        return est
+
+    def update(self, odom, obs_rows, prm, dist) -> np.ndarray:
+        """One cycle with the exchange over ``dist`` (every rank calls it)."""
+        import torch
+        self.weigh(odom, obs_rows, prm)
+        views = self.views()
+        if dist is not None and self.world > 1:
+            exchange_views(views, self.rank, dist)
+            torch.cuda.synchronize(self.device)
+        return self.finish(prm)
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.pfc_destroy(self.h)
+            self.h = None
+
+
+def update_in_process(shards, odom, obs_rows, prm):
+    """One cycle of the shards of one filter held by one process (tests on
+    one GPU): every slice weighted, the in-process exchange, every shard
+    finished.  Returns each shard's record."""
+    import torch
+    for s in shards:
+        s.weigh(odom, obs_rows, prm)
+    exchange_in_process([s.views() for s in shards])
+    torch.cuda.synchronize(shards[0].device)
+    return [s.finish(prm) for s in shards]

@@ -205,6 +205,33 @@ int pfc_cycle_result(void* h, double* est_out);
  * (pfc_profile) always use direct launches. */
 int pfc_set_graph(void* h, int on);
 
+/* Sharded filter (no counterpart in the reference): one filter of n
+ * particles over `world` ranks (one handle per rank, normally one GPU each).
+ * Every rank's handle holds the whole cloud; a cycle predicts and weights
+ * only the rank's slice [rank*chunk, min((rank+1)*chunk, n)), then the
+ * caller exchanges the slices (an all-gather over the ranks of the seven
+ * live planes, the log-likelihoods and the f32 softmax block partials, at
+ * chunk particles or chunk/512 partials per rank), and every rank finishes
+ * the cycle (softmax, ESS decision, resample, injection, estimate) on the
+ * whole cloud.  With the same seed, landmarks and inputs on every rank the
+ * cycle's result and particles equal pfc_cycle's on one handle, bit for
+ * bit.
+ *   pfc_shard_init:   instead of pfc_init (chunk = ceil(n/world) rounded
+ *                     up to 2048; planes padded to world*chunk);
+ *   pfc_shard_layout: chunk and plane length (n_pad);
+ *   pfc_shard_weight: predict + weighting of the slice (asynchronous);
+ *   pfc_shard_views:  device pointers of the live planes (7), ll and the
+ *                     softmax partials (float2 per 512 particles), after
+ *                     the slice's kernels completed (synchronises);
+ *   pfc_shard_finish: the rest of the cycle once every slice is in place;
+ *                     est_out as pfc_cycle's. */
+int pfc_shard_init(void* h, int n, int world, int rank, unsigned int seed);
+int pfc_shard_layout(void* h, int* chunk, int* n_pad);
+int pfc_shard_weight(void* h, const PfcOdom* odom, const CObservation* obs, int nobs,
+                     const PfcCycleParams* prm);
+int pfc_shard_views(void* h, float** planes7, float** ll, float** part);
+int pfc_shard_finish(void* h, const PfcCycleParams* prm, double* est_out);
+
 /* The CUDA stream (cudaStream_t) the handle runs on. */
 void* pfc_stream(void* h);
 

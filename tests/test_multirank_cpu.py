@@ -2,9 +2,9 @@
 gloo ranks rendezvous at 127.0.0.1, meet at the barrier, and agree on the max
 over ranks of their timings (the whole-job rate is world x the units of one
 rank over that max); a benchmark asked for N GPUs outside torchrun spawns N
-ranks; and the bottom-k of a global-localization query sharded by
-hypotheses, merged with one all-gather, equals the bottom-k of the whole
-set."""
+ranks; the bottom-k of a global-localization query sharded by hypotheses,
+merged with one all-gather, equals the bottom-k of the whole set; and the
+sharded filter's exchange gives every rank every rank's slice."""
 import os
 import socket
 import subprocess
@@ -165,3 +165,68 @@ def test_emulated_shards_merge_in_one_process():
     kk, _ = multi.merge_bottom_k(np.concatenate(keys), np.concatenate(poses), k, None)
     np.testing.assert_array_equal((kk & np.uint64(0xFFFFFFFF)).astype(np.int64),
                                   np.argsort(c, kind="stable")[:k])
+
+
+def _chunks(world, c, rank, seed):
+    """Rank `rank`'s view list for the shard exchange: two arrays of world
+    chunks, its own chunk filled with values that name the rank, the others
+    with a fill the exchange must overwrite."""
+    import torch
+    g = torch.Generator().manual_seed(seed + rank)
+    a = torch.full((world * c,), -1.0)
+    b = torch.full((world * (c // 4),), -2.0)
+    a[rank * c:(rank + 1) * c] = rank + torch.rand(c, generator=g)
+    b[rank * (c // 4):(rank + 1) * (c // 4)] = 100 * rank + torch.rand(c // 4, generator=g)
+    return [(a, c), (b, c // 4)]
+
+
+def _exchange_worker(rank, world, port, c, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE=str(world),
+                      RANK=str(rank), LOCAL_RANK=str(rank))
+    from cuda_pf_localization_b200 import multi
+    dist = multi.init("gloo", timeout_s=30)
+    try:
+        views = _chunks(world, c, rank, 5)
+        multi.exchange_views(views, rank, dist)
+        out[rank] = [v.tolist() for v, _ in views]
+    finally:
+        multi.finish(dist)
+
+
+def test_shard_exchange_over_gloo_ranks():
+    """The sharded filter's all-gather (exchange_views): every rank ends with
+    every rank's chunk of every array, in rank order."""
+    world, c = 2, 64
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as man:
+        out = man.dict()
+        procs = [ctx.Process(target=_exchange_worker, args=(r, world, port, c, out))
+                 for r in range(world)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(120)
+            assert p.exitcode == 0
+        res = dict(out)
+    want = [_chunks(world, c, r, 5) for r in range(world)]
+    for rank in range(world):
+        for a in range(2):
+            got = np.array(res[rank][a], np.float32)
+            cc = want[0][a][1]
+            for r in range(world):
+                np.testing.assert_array_equal(got[r * cc:(r + 1) * cc],
+                                              want[r][a][0][r * cc:(r + 1) * cc].numpy())
+
+
+def test_shard_exchange_in_process():
+    """The one-process form used by the single-GPU tests (three shards)."""
+    from cuda_pf_localization_b200 import multi
+    world, c = 3, 32
+    views = [_chunks(world, c, r, 11) for r in range(world)]
+    own = [[v[r * cc:(r + 1) * cc].clone() for v, cc in views[r]] for r in range(world)]
+    multi.exchange_in_process(views)
+    for q in range(world):
+        for a, (v, cc) in enumerate(views[q]):
+            for r in range(world):
+                assert (v[r * cc:(r + 1) * cc] == own[r][a]).all()
