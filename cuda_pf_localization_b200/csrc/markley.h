@@ -73,7 +73,11 @@ PFB_HD inline int jacobi_eig4(double a[16], double v[16]) {
 
 // Dominant eigenvector of a symmetric positive semi-definite 4x4 matrix by
 // repeated squaring (the power method on M^(2^k)): after 12 squarings the
-// other eigen-directions are damped by (lambda2/lambda1)^4096.  Accepted only
+// other eigen-directions are damped by (lambda2/lambda1)^4096.  The squaring
+// stops earlier once the trace-normalised matrix P is rank one to rounding,
+// 1 - tr(P^2) < 1e-14 (tr(P^2) is the sum of the squared normalised
+// eigenvalues; it is 1 - 2e for a remainder e off the top direction), which
+// for a particle cloud takes three or four squarings.  Accepted only
 // when the Rayleigh residual |M v - (v'Mv) v| is below 1e-13 |M|; returns
 // false otherwise (near-degenerate top eigenvalue), and the caller falls back
 // to the Jacobi solve.
@@ -92,6 +96,7 @@ PFB_HD inline bool dominant_eigvec_psd4(const double a[16], double v[4]) {
         if (!(tt > 0.0)) return false;
         const double itt = 1.0 / tt;
         for (int i = 0; i < 16; ++i) p[i] = t[i] * itt;
+        if (tt > 1.0 - 1e-14) break;
     }
     // p ~ v v^T: take the column with the largest diagonal entry.
     int c = 0;
@@ -185,6 +190,7 @@ __device__ inline void markley_mean_warp(const double m10[10], double q_out[4]) 
             const double tt = trace(t);
             ok = tt > 0.0;
             pm = t * (1.0 / tt);
+            if (tt > 1.0 - 1e-14) break;  // warp-uniform: every lane has tt
         }
         if (ok) {
             // the column of the largest diagonal entry, then two power steps

@@ -93,7 +93,7 @@ def test_cycle_without_observations_matches(kernels):
         for st, rows in zip(sc.steps, ([], sc.steps[1].obs)):
             odom = _odom(st, sc)
             e1 = np.zeros(pkg.PFC_EST_LEN)
-            cobs = pkg.make_cobs(rows) if rows else None
+            cobs = pkg.make_cobs(rows) if len(rows) else None
             assert kernels.pfc_cycle(single.h, C.byref(odom), cobs, len(rows), C.byref(prm),
                                      pkg.dptr(e1)) == 0
             for e in multi.update_in_process(shards, odom, rows, prm):
