@@ -524,9 +524,9 @@ int init_particles(PfHandle* h, int n, unsigned int seed, int n_pad) {
     const size_t np = (size_t)h->n_pad;
     const int nprefix = ceil_div(n, kPrefixBlock);
     // doubles: the largest of the kernels' partial arrays (float2 softmax
-    // partials of every 512-particle block of the planes included)
+    // partials of every 256-particle block of the planes included)
     const int part = std::max(std::max(2 * ceil_div(n, kThreads), resample_part_doubles(n)),
-                              std::max(1184 * 16, n_pad / (2 * kThreads)));
+                              std::max(1184 * 16, n_pad / (2 * kWThreads)));
     PFB_CK(cudaMalloc((void**)&h->d_state[0], 7 * np * sizeof(float)));
     PFB_CK(cudaMalloc((void**)&h->d_state[1], 7 * np * sizeof(float)));
     PFB_CK(cudaMalloc((void**)&h->d_ll, np * sizeof(float)));

@@ -15,7 +15,7 @@
 // fed by one copy of the per-filter inputs.
 //
 // Equality with the single-filter path.  The weighting tiles are the
-// single-filter kernel's blocks (512 particles, two per thread) and the
+// single-filter kernel's blocks (256 particles, two per thread) and the
 // softmax partials and their combine are the same device routines, so the
 // log-likelihoods, the normaliser, the f32 weights, the fixed-point scan, the
 // ancestors, the injection and hence the particle states of filter f equal
@@ -38,7 +38,7 @@ namespace batch {
 using namespace pfb::dev;
 
 constexpr int kThreads = kBlk;
-constexpr int kWTile = 2 * kBlk;  // particles per weighting tile
+constexpr int kWTile = 2 * kWThreads;  // particles per weighting tile (= the single filter's block)
 constexpr int kScanItems = 16;
 constexpr int kRTile = kBlk * kScanItems;  // particles per resampling tile
 constexpr int kHeavy = 32;
@@ -169,9 +169,10 @@ __global__ void __launch_bounds__(kThreads)
     if (threadIdx.x == 0 && t.local == 0) C[t.f].wmode = WMODE_UNIFORM;
 }
 
-// Predict (generation gen + 1) and gated weighting of one 512-particle tile;
-// the last tile of a filter combines the softmax partials.
-__global__ void __launch_bounds__(kThreads)
+// Predict (generation gen + 1) and gated weighting of one 256-particle tile
+// (kWThreads threads, two particles each, as the single filter's weighting
+// blocks); the last tile of a filter combines the softmax partials.
+__global__ void __launch_bounds__(kWThreads, 6)
     k_b_weight(Arena A, const BFilter* __restrict__ F, const BTile* __restrict__ T,
                BCtl* C, const PfcBatchCycle* __restrict__ cyc,
                const CObservation* __restrict__ obs, const float* __restrict__ lm,
@@ -190,8 +191,8 @@ __global__ void __launch_bounds__(kThreads)
         pa.rstd[k] = in.odom.rstd[k];
     }
     for (int k = 0; k < 4; ++k) pa.q[k] = in.odom.q[k];
-    const int i0 = t.start + threadIdx.x, i1 = i0 + kThreads;
-    const bool v0 = threadIdx.x < t.count, v1 = threadIdx.x + kThreads < t.count;
+    const int i0 = t.start + threadIdx.x, i1 = i0 + kWThreads;
+    const bool v0 = threadIdx.x < t.count, v1 = threadIdx.x + kWThreads < t.count;
     float3 p0 = make_float3(0.f, 0.f, 0.f), p1 = p0;
     Quat q0 = {1.f, 0.f, 0.f, 0.f}, q1 = q0;
     if (v0) {
@@ -882,7 +883,7 @@ int launch_est_covs(BatchHandle* h) {
 int enqueue_cycle(BatchHandle* h) {
     cudaStream_t s = h->stream;
     k_b_gen_inc<<<ceil_div(h->nf, kThreads), kThreads, 0, s>>>(h->d_C, h->nf);
-    k_b_weight<<<h->n_wt, kThreads, 0, s>>>(h->A, h->d_F, h->d_wt, h->d_C, h->d_cyc,
+    k_b_weight<<<h->n_wt, kWThreads, 0, s>>>(h->A, h->d_F, h->d_wt, h->d_C, h->d_cyc,
                                             h->d_obs, h->d_lm, h->d_wpart,
                                             h->use_packed);
     k_b_ess<<<h->n_et, kThreads, 0, s>>>(h->A, h->d_F, h->d_et, h->d_C, h->d_epart,

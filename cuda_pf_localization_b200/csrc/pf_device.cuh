@@ -15,7 +15,9 @@ namespace pfb {
 namespace dev {
 
 constexpr int kBlk = 256;       // threads per block of every particle kernel
-constexpr int kObsChunk = 256;  // observations staged in shared memory at once
+// The staging, softmax-partial and combine helpers below run on weighting
+// blocks of exactly kWThreads threads (pf_internal.h).
+constexpr int kObsChunk = kWThreads;  // observations staged in shared memory at once
 
 __device__ __forceinline__ void load_pose(const Planes& s, int i, float3& p,
                                           Quat& q) {
@@ -169,7 +171,7 @@ __device__ __forceinline__ int stage_chunk(const CObservation* __restrict__ obs,
                                            int lm_count, int c0, int cn,
                                            float4* s_a, float4* s_b,
                                            float4* s_p, bool* all_cart) {
-    __shared__ int s_wcount[kBlk / 32];
+    __shared__ int s_wcount[kWThreads / 32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     CObservation o;
     bool keep = false;
@@ -181,7 +183,7 @@ __device__ __forceinline__ int stage_chunk(const CObservation* __restrict__ obs,
     if (lane == 0) s_wcount[warp] = __popc(ballot);
     const int cart = __syncthreads_and(!keep || o.mode == 0);
     int off = 0, total = 0;
-    for (int k = 0; k < kBlk / 32; ++k) {
+    for (int k = 0; k < kWThreads / 32; ++k) {
         const int c = s_wcount[k];
         off += (k < warp) ? c : 0;
         total += c;
@@ -284,13 +286,13 @@ __device__ __forceinline__ float2 packed_r2(const PackedPose& k, float4 A,
     return __ffma2_rn(ez, ez, __ffma2_rn(ex, ex, __fmul2_rn(ey, ey)));
 }
 
-// Softmax partial of one block of up to 2 * kBlk log-likelihoods (two per
+// Softmax partial of one block of up to 2 * kWThreads log-likelihoods (two per
 // thread): (block max, sum expf(ll - block max)) in f32, in a fixed order
 // (xor butterfly inside warps, warps in index order).  Valid in every thread.
 __device__ __forceinline__ float2 block_softmax_partial(float acc0, bool v0,
                                                         float acc1, bool v1) {
-    __shared__ float s_m[kBlk / 32];
-    __shared__ float s_s[kBlk / 32];
+    __shared__ float s_m[kWThreads / 32];
+    __shared__ float s_s[kWThreads / 32];
     __shared__ float s_bm, s_sb;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     float m = warp_max_f(fmaxf(v0 ? acc0 : -INFINITY, v1 ? acc1 : -INFINITY));
@@ -298,7 +300,7 @@ __device__ __forceinline__ float2 block_softmax_partial(float acc0, bool v0,
     __syncthreads();
     if (tid == 0) {
         float bm = s_m[0];
-        for (int k = 1; k < kBlk / 32; ++k) bm = fmaxf(bm, s_m[k]);
+        for (int k = 1; k < kWThreads / 32; ++k) bm = fmaxf(bm, s_m[k]);
         s_bm = bm;
     }
     __syncthreads();
@@ -310,37 +312,37 @@ __device__ __forceinline__ float2 block_softmax_partial(float acc0, bool v0,
     __syncthreads();
     if (tid == 0) {
         float sb = 0.0f;
-        for (int k = 0; k < kBlk / 32; ++k) sb = __fadd_rn(sb, s_s[k]);
+        for (int k = 0; k < kWThreads / 32; ++k) sb = __fadd_rn(sb, s_s[k]);
         s_sb = sb;
     }
     __syncthreads();
     return make_float2(bm, s_sb);
 }
 
-// Combine G block partials (executed by a whole block of kBlk threads):
+// Combine G block partials (executed by a whole block of kWThreads threads):
 // M = max of the block maxima, S = sum_b expf(m_b - M) * s_b in f32, each
 // reduced thread-strided, then by xor butterfly, then over warps in order.
 // The result is valid in every thread.
 __device__ __forceinline__ float2 softmax_combine(const float2* part, int G) {
-    __shared__ float s_d[kBlk / 32];
+    __shared__ float s_d[kWThreads / 32];
     __shared__ float s_r;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     float mx = -INFINITY;
 #pragma unroll 4
-    for (int b = tid; b < G; b += kBlk) mx = fmaxf(mx, __ldcg(&part[b].x));
+    for (int b = tid; b < G; b += kWThreads) mx = fmaxf(mx, __ldcg(&part[b].x));
     mx = warp_max_f(mx);
     if (lane == 0) s_d[warp] = mx;
     __syncthreads();
     if (tid == 0) {
         float v = s_d[0];
-        for (int k = 1; k < kBlk / 32; ++k) v = fmaxf(v, s_d[k]);
+        for (int k = 1; k < kWThreads / 32; ++k) v = fmaxf(v, s_d[k]);
         s_r = v;
     }
     __syncthreads();
     const float M = s_r;
     float sum = 0.0f;
 #pragma unroll 4
-    for (int b = tid; b < G; b += kBlk) {
+    for (int b = tid; b < G; b += kWThreads) {
         const float2 pb = __ldcg(&part[b]);
         sum = __fadd_rn(sum, __fmul_rn(expf(__fsub_rn(pb.x, M)), pb.y));
     }
@@ -350,7 +352,7 @@ __device__ __forceinline__ float2 softmax_combine(const float2* part, int G) {
     __syncthreads();
     if (tid == 0) {
         float S = 0.0f;
-        for (int k = 0; k < kBlk / 32; ++k) S = __fadd_rn(S, s_d[k]);
+        for (int k = 0; k < kWThreads / 32; ++k) S = __fadd_rn(S, s_d[k]);
         s_r = S;
     }
     __syncthreads();

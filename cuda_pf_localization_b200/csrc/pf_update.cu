@@ -112,20 +112,21 @@ __device__ __forceinline__ void softmax_partials(float acc0, bool v0,
 // The combine of a sharded filter, once every rank's block partials are in
 // part[0, G): one block, the same combine as the last block above, so M and
 // S equal the unsharded filter's bit for bit.
-__global__ void __launch_bounds__(kThreads) k_softmax_combine(const float2* part, int G,
+__global__ void __launch_bounds__(kWThreads) k_softmax_combine(const float2* part, int G,
                                                               CycleCtl* ctl) {
     const float2 ms = softmax_combine(part, G);
     if (threadIdx.x == 0) softmax_commit(ms, ctl);
 }
 
-// Two particles per thread (i and i + 256): every staged observation read
-// from shared memory serves both.  Three blocks per SM (up to 85 registers,
-// no spills): measured 4 % faster than four blocks at 64 registers.
+// Two particles per thread (i and i + kWThreads): every staged observation
+// read from shared memory serves both.  Six 128-thread blocks per SM (up to
+// 85 registers, no spills; 24 warps, as three 256-thread blocks, which
+// measured 4 % faster than four at 64 registers).
 // kShard: one rank's slice of a sharded filter; block b of the launch is
 // block block0 + b of the whole cloud, and the block partials are left for
 // the combine that follows the exchange (k_softmax_combine).
 template <bool kPredict, bool kShard>
-__global__ void __launch_bounds__(kThreads, 3)
+__global__ void __launch_bounds__(kWThreads, 6)
     k_weight(PlaneSet ps, int n, uint64_t seed, PredictArgs pa,
              const CObservation* __restrict__ obs, int nobs,
              const float* __restrict__ lm, int lm_count, float sigma_r,
@@ -140,8 +141,8 @@ __global__ void __launch_bounds__(kThreads, 3)
     }
     const Planes s = pick_planes(ps, ctl->live);
     const int blk = kShard ? (int)blockIdx.x + block0 : (int)blockIdx.x;
-    const int i0 = blk * (2 * kThreads) + threadIdx.x;
-    const int i1 = i0 + kThreads;
+    const int i0 = blk * (2 * kWThreads) + threadIdx.x;
+    const int i1 = i0 + kWThreads;
     const bool v0 = i0 < n, v1 = i1 < n;
     float3 p0 = make_float3(0.f, 0.f, 0.f), p1 = p0;
     Quat q0 = {1.f, 0.f, 0.f, 0.f}, q1 = q0;
@@ -211,16 +212,16 @@ int launch_predict(PfHandle* h, const PredictArgs& pa) {
 int launch_weight(PfHandle* h, const PredictArgs& pa, const CObservation* d_obs,
                   int nobs, float sigma_r, float sigma_b, float gate,
                   const CycleArgs* dargs) {
-    const int grid = ceil_div(h->n, 2 * kThreads);
+    const int grid = ceil_div(h->n, 2 * kWThreads);
     float2* part = reinterpret_cast<float2*>(h->d_part);
     KernelScope ks(h, KK_WEIGHT);
     if (pa.enabled) {
-        PFB_CK(launch_pdl(k_weight<true, false>, grid, kThreads, 0, h->stream, plane_set(h),
+        PFB_CK(launch_pdl(k_weight<true, false>, grid, kWThreads, 0, h->stream, plane_set(h),
                           h->n, h->seed, pa, d_obs, nobs, h->d_lm, h->lm_count,
                           sigma_r, sigma_b, gate, h->d_ll, part, h->d_done + 0,
                           h->d_ctl, h->weight_variant == 0 ? 1 : 0, dargs, 0));
     } else {
-        PFB_CK(launch_pdl(k_weight<false, false>, grid, kThreads, 0, h->stream, plane_set(h),
+        PFB_CK(launch_pdl(k_weight<false, false>, grid, kWThreads, 0, h->stream, plane_set(h),
                           h->n, h->seed, pa, d_obs, nobs, h->d_lm, h->lm_count,
                           sigma_r, sigma_b, gate, h->d_ll, part, h->d_done + 0,
                           h->d_ctl, h->weight_variant == 0 ? 1 : 0, dargs, 0));
@@ -232,17 +233,18 @@ int launch_weight(PfHandle* h, const PredictArgs& pa, const CObservation* d_obs,
 
 // One rank's slice of a sharded filter: particles [rank * chunk,
 // min((rank + 1) * chunk, n)), predicted and weighted; their block partials
-// land at their global block index of d_part (as float2) for the exchange.
+// land at their global block index of d_part (float2 per 256 particles) for
+// the exchange.
 int launch_weight_shard(PfHandle* h, const PredictArgs& pa, const CObservation* d_obs,
                         int nobs, float sigma_r, float sigma_b, float gate) {
     const long long first = (long long)h->shard_rank * h->shard_chunk;
     const long long last = std::min<long long>(first + h->shard_chunk, h->n);
     if (last <= first) return 0;  // a rank past the end of the cloud
-    const int block0 = (int)(first / (2 * kThreads));
-    const int grid = (int)ceil_div_ll(last - first, 2 * kThreads);
+    const int block0 = (int)(first / (2 * kWThreads));
+    const int grid = (int)ceil_div_ll(last - first, 2 * kWThreads);
     float2* part = reinterpret_cast<float2*>(h->d_part);
     KernelScope ks(h, KK_WEIGHT);
-    PFB_CK(launch_pdl(k_weight<true, true>, grid, kThreads, 0, h->stream, plane_set(h), h->n,
+    PFB_CK(launch_pdl(k_weight<true, true>, grid, kWThreads, 0, h->stream, plane_set(h), h->n,
                       h->seed, pa, d_obs, nobs, h->d_lm, h->lm_count, sigma_r, sigma_b, gate,
                       h->d_ll, part, h->d_done + 0, h->d_ctl,
                       h->weight_variant == 0 ? 1 : 0, (const CycleArgs*)nullptr, block0));
@@ -251,11 +253,11 @@ int launch_weight_shard(PfHandle* h, const PredictArgs& pa, const CObservation* 
     return 0;
 }
 
-// The softmax of a sharded filter over all ceil(n / 512) block partials.
+// The softmax of a sharded filter over all ceil(n / 256) block partials.
 int launch_softmax_combine(PfHandle* h) {
-    const int G = (int)ceil_div_ll(h->n, 2 * kThreads);
+    const int G = (int)ceil_div_ll(h->n, 2 * kWThreads);
     KernelScope ks(h, KK_WEIGHT);
-    k_softmax_combine<<<1, kThreads, 0, h->stream>>>(
+    k_softmax_combine<<<1, kWThreads, 0, h->stream>>>(
         reinterpret_cast<const float2*>(h->d_part), G, h->d_ctl);
     PFB_KL();
     h->prefix_valid = false;

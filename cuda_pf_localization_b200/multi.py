@@ -316,7 +316,7 @@ class ShardedFilter:
 
     def views(self):
         """(tensor, chunk) for the seven live planes, the log-likelihoods and
-        the f32 softmax block partials (two floats per 512 particles), each
+        the f32 softmax block partials (two floats per 256 particles), each
         covering world chunks; after the slice's kernels completed."""
         import ctypes as C
 
@@ -331,8 +331,8 @@ class ShardedFilter:
         out = [(torch.as_tensor(DeviceArray(p7[k], full), device=self.device), c)
                for k in range(7)]
         out.append((torch.as_tensor(DeviceArray(ll.value, full), device=self.device), c))
-        out.append((torch.as_tensor(DeviceArray(part.value, full // 256), device=self.device),
-                    c // 256))
+        out.append((torch.as_tensor(DeviceArray(part.value, full // 128), device=self.device),
+                    c // 128))
         return out
 
     def finish(self, prm) -> np.ndarray:

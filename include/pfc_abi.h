@@ -211,7 +211,7 @@ int pfc_set_graph(void* h, int on);
  * only the rank's slice [rank*chunk, min((rank+1)*chunk, n)), then the
  * caller exchanges the slices (an all-gather over the ranks of the seven
  * live planes, the log-likelihoods and the f32 softmax block partials, at
- * chunk particles or chunk/512 partials per rank), and every rank finishes
+ * chunk particles or chunk/256 partials per rank), and every rank finishes
  * the cycle (softmax, ESS decision, resample, injection, estimate) on the
  * whole cloud.  With the same seed, landmarks and inputs on every rank the
  * cycle's result and particles equal pfc_cycle's on one handle, bit for
@@ -221,7 +221,7 @@ int pfc_set_graph(void* h, int on);
  *   pfc_shard_layout: chunk and plane length (n_pad);
  *   pfc_shard_weight: predict + weighting of the slice (asynchronous);
  *   pfc_shard_views:  device pointers of the live planes (7), ll and the
- *                     softmax partials (float2 per 512 particles), after
+ *                     softmax partials (float2 per 256 particles), after
  *                     the slice's kernels completed (synchronises);
  *   pfc_shard_finish: the rest of the cycle once every slice is in place;
  *                     est_out as pfc_cycle's. */
