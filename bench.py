@@ -255,7 +255,7 @@ FP32_OPS_PER_PAIR = 29  # gated Cartesian term with the reference's roundings
 # from ncu (dram__bytes_read.sum + dram__bytes_write.sum; the capture command
 # is in profiles/pf_cycle_1M_scale.md): the poses are read from HBM, the
 # predicted poses and log-likelihoods it writes stay in L2.
-KWEIGHT_DRAM_BYTES_1M = 28.7e6 + 0.06e6
+KWEIGHT_DRAM_BYTES_1M = 28.06e6
 # Algorithmic bytes per particle of each kernel of a resampling cycle, by the
 # library's kernel kinds: weight (fused predict + weighting: pose R 28 + W 28,
 # ll W 4), est (weight pass: ll R 4, w W 4), scan (run starts: w R 4), gather
