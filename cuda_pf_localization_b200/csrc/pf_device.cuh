@@ -14,7 +14,8 @@
 namespace pfb {
 namespace dev {
 
-constexpr int kBlk = 256;       // threads per block of every particle kernel
+constexpr int kBlk = 256;       // threads per block of the particle kernels (the
+                                // weighting kernels use kWThreads)
 // The staging, softmax-partial and combine helpers below run on weighting
 // blocks of exactly kWThreads threads (pf_internal.h).
 constexpr int kObsChunk = kWThreads;  // observations staged in shared memory at once
