@@ -26,10 +26,9 @@ constexpr int kEstN = 14;  // pfc_est_sums layout
 constexpr int kPrefixBlock = 2048;  // particles per fixed-point prefix entry
 constexpr int kCovN = 12;  // pfc_covs layout
 // Threads per weighting block (two particles each, 256 particles per block):
-// six resident blocks per SM keep the 24 warps of three 256-thread blocks
-// while halving the work of the blocks that finish the kernel's last wave.
-// The block partition fixes the softmax partials, so the single-filter,
-// batched and sharded weighting kernels all use it.
+// the blocks that finish the kernel's last wave carry half the work of
+// 512-particle blocks.  The block partition fixes the softmax partials, so
+// the single-filter, batched and sharded weighting kernels all use it.
 constexpr int kWThreads = 128;
 
 // Weight plane semantics.

@@ -119,14 +119,14 @@ __global__ void __launch_bounds__(kWThreads) k_softmax_combine(const float2* par
 }
 
 // Two particles per thread (i and i + kWThreads): every staged observation
-// read from shared memory serves both.  Six 128-thread blocks per SM (up to
-// 85 registers, no spills; 24 warps, as three 256-thread blocks, which
-// measured 4 % faster than four at 64 registers).
+// read from shared memory serves both.  Five 128-thread blocks per SM (84
+// registers, no spills; 20 warps): measured 1.4 % faster than six (77
+// registers) and faster than four, seven or eight.
 // kShard: one rank's slice of a sharded filter; block b of the launch is
 // block block0 + b of the whole cloud, and the block partials are left for
 // the combine that follows the exchange (k_softmax_combine).
 template <bool kPredict, bool kShard>
-__global__ void __launch_bounds__(kWThreads, 6)
+__global__ void __launch_bounds__(kWThreads, 5)
     k_weight(PlaneSet ps, int n, uint64_t seed, PredictArgs pa,
              const CObservation* __restrict__ obs, int nobs,
              const float* __restrict__ lm, int lm_count, float sigma_r,
