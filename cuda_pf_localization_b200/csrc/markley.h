@@ -242,6 +242,13 @@ __device__ inline void markley_mean_warp(const double m10[10], double q_out[4]) 
     const double sgn = (x[0] < 0.0) ? -1.0 : 1.0;
     for (int i = 0; i < 4; ++i) q_out[i] = sgn * x[i] / nrm;
 }
+
+// markley_mean_warp as a call of its own: not inlined, so its registers do
+// not count against the streaming loop of the kernel that calls it at its
+// end.  Every lane of the calling warp must call it.
+static __device__ __noinline__ void markley_mean_warp_call(const double* m10, double* q_out) {
+    markley_mean_warp(m10, q_out);
+}
 #endif
 
 }  // namespace pfb

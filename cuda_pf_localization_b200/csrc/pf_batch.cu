@@ -424,11 +424,11 @@ __global__ void __launch_bounds__(kThreads, 2)
         return;
     __shared__ double s_out[kEstN];
     tiles_combine<kEstN>(epart + (size_t)fl.etile0 * kEstN, fl.netiles, s_out);
+    double qm[4];
+    if (threadIdx.x < 32) markley_mean_warp_call(&s_out[3], qm);  // warp 0
     if (threadIdx.x == 0) {
         for (int k = 0; k < kEstN; ++k) c->est[k] = s_out[k];
         c->ess = s_out[13] > 0.0 ? 1.0 / s_out[13] : 0.0;
-        double qm[4];
-        markley_mean(&s_out[3], qm);
         for (int k = 0; k < 4; ++k) c->qmean[k] = qm[k];
         for (int k = 0; k < 3; ++k) c->cmp[k] = (float)s_out[k];
         for (int k = 0; k < 4; ++k) c->cmq[k] = (float)qm[k];

@@ -139,11 +139,11 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
     __shared__ double s_out[kEstN];
     if (!block_reduce_last<kEstN>(acc, part, done, s_out)) return;
+    double qm[4];
+    if (threadIdx.x < 32) markley_mean_warp_call(&s_out[3], qm);  // warp 0
     if (threadIdx.x == 0) {
         for (int k = 0; k < kEstN; ++k) ctl->est[k] = s_out[k];
         ctl->ess = s_out[13] > 0.0 ? 1.0 / s_out[13] : 0.0;
-        double qm[4];
-        markley_mean(&s_out[3], qm);
         for (int k = 0; k < 4; ++k) ctl->qmean[k] = qm[k];
         for (int k = 0; k < 3; ++k) ctl->cov_mean_p[k] = (float)s_out[k];
         for (int k = 0; k < 4; ++k) ctl->cov_mean_q[k] = (float)qm[k];

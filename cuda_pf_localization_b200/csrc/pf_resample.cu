@@ -390,12 +390,6 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
 }
 
-// The Markley mean by warp 0 of block 0, once per cycle, as a call of its
-// own: not inlined, its registers do not count against the copy loop.
-__device__ __noinline__ void markley_mean_once(const double* m10, double* q_out) {
-    markley_mean_warp(m10, q_out);
-}
-
 // Shared memory of k_gather: a tile's ancestors and injection list, or the
 // partials a combine stages (used before or after the tiles).
 union GatherSmem {
@@ -435,7 +429,7 @@ __global__ void __launch_bounds__(kThreads, 4)
     if (blockIdx.x == 0) {
         combine_staged<kEstN, kMarkGrid>(part_m, mark_grid, sm.pm, s_out);
         double qm[4];
-        if (warp == 0) markley_mean_once(&s_out[3], qm);
+        if (warp == 0) markley_mean_warp_call(&s_out[3], qm);
         if (tid == 0) {
             for (int q = 0; q < kEstN; ++q) ctl->est[q] = s_out[q];
             ctl->ess = s_out[13] > 0.0 ? 1.0 / s_out[13] : 0.0;
