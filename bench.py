@@ -469,7 +469,7 @@ def _success(top, poses):
 # learned configurations (samples per query, calibration quantile), the one
 # quoted in the headline ratio
 UNIFORM_SWEEP = (50_000, 56_000, 64_000, 100_000, 200_000)
-LEARNED_SWEEP = ((100, 0.995), (250, 0.995), (1000, 0.995), (20_000, 0.98))
+LEARNED_SWEEP = ((100, 0.995), (250, 0.995), (250, 0.999), (1000, 0.995), (20_000, 0.98))
 UNIFORM_1M_POSES = 20   # poses per map of the 1M-hypothesis uniform leg
 
 
