@@ -473,6 +473,34 @@ LEARNED_SWEEP = ((100, 0.995), (250, 0.995), (250, 0.999), (1000, 0.995), (20_00
 UNIFORM_1M_POSES = 20   # poses per map of the 1M-hypothesis uniform leg
 
 
+def iso_headline(iso: dict, min_queries: int, bar: float = 0.95) -> None:
+    """The C5 comparison at iso-success, one rule for both sides: the cheapest
+    uniform hypothesis count whose success within 0.5 m / 0.1 rad reaches
+    `bar` (in its faster mode, one query at a time or batched) and the
+    fastest learned configuration that reaches it, both over at least
+    min_queries queries.  Adds iso["comparator"], iso["learned_headline"] and
+    iso["learned_vs_uniform_solves_ratio"] when both sides have one."""
+    cands = sorted((u, d) for u, d in ((int(k2), d2) for k2, d2 in iso["uniform"].items())
+                   if d["success_pos_yaw"] >= bar and d["queries"] >= min_queries)
+    learned_ok = [d for d in iso["learned"].values()
+                  if d["success_pos_yaw"] >= bar and d["queries"] >= min_queries]
+    if not cands or not learned_ok:
+        return
+    head = max(learned_ok, key=lambda d: d["solves_per_s"])
+    u, d = cands[0]
+    best_uni = max(d["solves_per_s"],
+                   iso.get("uniform_batched", {}).get(str(u), {}).get("solves_per_s", 0.0))
+    iso["comparator"] = dict(hyps=u, success_pos_yaw=d["success_pos_yaw"],
+                             solves_per_s=best_uni,
+                             rule="cheapest uniform count of the sweep with success "
+                                  "within 0.5 m / 0.1 rad >= 0.95 on the same poses; "
+                                  "its faster mode")
+    iso["learned_headline"] = dict(head, rule="fastest learned configuration of the "
+                                              "sweep with success within 0.5 m / 0.1 rad "
+                                              ">= 0.95 on the same poses")
+    iso["learned_vs_uniform_solves_ratio"] = head["solves_per_s"] / best_uni
+
+
 def run_gl(args):
     """CBGL on 10 x 10 m rooms with 30 boxes (200 x 200 at 0.05 m), 360-ray
     scans (rmax 10 m, N(0, 0.01 m) noise) rendered by the library's raycaster.
@@ -630,26 +658,7 @@ def run_gl(args):
                            tflops=LP_FLOPS_PER_SAMPLE * args.gl_batch * args.gl_train_steps
                            * args.gl_maps / t_steps / 1e12,
                            final_loss_mean=float(np.mean(losses)))
-    # the comparator: the cheapest uniform count reaching 95 % (pos + yaw)
-    cands = sorted((u, d) for u, d in ((int(k2), d2) for k2, d2 in iso["uniform"].items())
-                   if d["success_pos_yaw"] >= 0.95 and d["queries"] >= args.gl_queries)
-    # the learned side by the same rule: its fastest configuration at >= 95 %
-    learned_ok = [d for d in iso["learned"].values()
-                  if d["success_pos_yaw"] >= 0.95 and d["queries"] >= args.gl_queries]
-    head = max(learned_ok, key=lambda d: d["solves_per_s"]) if learned_ok else None
-    if cands and head is not None:
-        u, d = cands[0]
-        best_uni = max(d["solves_per_s"],
-                       iso["uniform_batched"].get(str(u), {}).get("solves_per_s", 0.0))
-        iso["comparator"] = dict(hyps=u, success_pos_yaw=d["success_pos_yaw"],
-                                 solves_per_s=best_uni,
-                                 rule="cheapest uniform count of the sweep with success "
-                                      "within 0.5 m / 0.1 rad >= 0.95 on the same poses; "
-                                      "its faster mode")
-        iso["learned_headline"] = dict(head, rule="fastest learned configuration of the "
-                                                  "sweep with success within 0.5 m / 0.1 rad "
-                                                  ">= 0.95 on the same poses")
-        iso["learned_vs_uniform_solves_ratio"] = head["solves_per_s"] / best_uni
+    iso_headline(iso, args.gl_queries)
     return res
 
 

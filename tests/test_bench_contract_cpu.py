@@ -63,3 +63,27 @@ def test_reference_arm_ranks_of_a_two_rank_world():
     # a torchrun world of another size is refused
     bad = _ref_run(dict(base, RANK="0"), "--gpus", "4")
     assert bad.returncode != 0
+
+
+def test_iso_success_rule_is_the_same_for_both_sides():
+    """C5's headline: the cheapest uniform count and the fastest learned
+    configuration that reach 95 % on at least the required queries; slower
+    or failing configurations and short sweeps are not chosen."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    def u(succ, rate, q=1000):
+        return {"success_pos_yaw": succ, "solves_per_s": rate, "queries": q}
+    iso = {"uniform": {"50000": u(0.94, 1300.0), "56000": u(0.956, 1200.0),
+                       "64000": u(0.97, 1100.0), "1000000": u(1.0, 120.0, q=20)},
+           "uniform_batched": {"56000": u(0.956, 1250.0)},
+           "learned": {"100_q0.995": u(0.93, 90000.0), "250_q0.995": u(0.99, 40000.0),
+                       "250_q0.999": u(0.97, 60000.0), "20000_q0.98": u(1.0, 3000.0)}}
+    bench.iso_headline(iso, 1000)
+    assert iso["comparator"]["hyps"] == 56000
+    assert iso["comparator"]["solves_per_s"] == 1250.0      # its faster mode
+    assert iso["learned_headline"]["solves_per_s"] == 60000.0  # 100 samples fail the bar
+    assert iso["learned_vs_uniform_solves_ratio"] == 60000.0 / 1250.0
+    none = {"uniform": {"50000": u(0.9, 1.0)}, "learned": {"x": u(0.99, 2.0)}}
+    bench.iso_headline(none, 1000)
+    assert "learned_vs_uniform_solves_ratio" not in none
