@@ -2,7 +2,8 @@
 the reference CPU path) and prints the one JSON line the benchmark contract
 asks for: the metric, unit and direction of the GPU arm, `impl: reference`,
 a `cpu_baseline` describing the run and an `e2e` with no host<->device bytes.
-Run here at 20k particles so it takes about a second."""
+Run here at 20k particles so it takes about a second.  Also the rule that
+picks the C5 iso-success comparison from the global-localization sweeps."""
 import json
 import os
 import subprocess
