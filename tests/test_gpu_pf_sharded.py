@@ -48,7 +48,7 @@ def _snapshot(lib, h, n):
     return pos, quat
 
 
-@pytest.mark.parametrize("n,world", [(100_003, 2), (100_003, 3), (4097, 4)])
+@pytest.mark.parametrize("n,world", [(100_003, 2), (100_003, 3), (4097, 4), (1_000_000, 2)])
 def test_sharded_filter_equals_single_filter(kernels, n, world):
     sc = sim.scale_config(cycles=6, seed=5)
     prm = pkg.PfcCycleParams(0.05, 0.02, 3.0, 0.5, 0.01, 0)
