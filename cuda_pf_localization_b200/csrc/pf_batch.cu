@@ -2,15 +2,17 @@
 // one CUDA-graph launch per cycle.
 //
 // Layout.  All filters' particles live in one arena of SoA planes (two
-// ping-pong sets of px py pz qw qx qy qz, plus ll and w); filter f owns the
+// ping-pong sets of px py pz qw qx qy qz, plus ll, w and the resampler's
+// run-start markers); filter f owns the
 // slice [off_f, off_f + n_f), off_f a multiple of 1024.  Every kernel of the
 // cycle covers all filters through a tile table: a tile is a particle range
 // of one filter.  Per-filter reductions are finished by the last tile of that
 // filter to complete (an atomic counter per filter), so a cycle is a fixed
 // chain of kernels whatever the filter sizes:
 //   begin -> weight (+ predict) -> weights + ESS decision -> resample
-//   (look-back scan + run copy) -> long runs -> injection (link, apply) ->
-//   commit -> estimate -> covariances (output record).
+//   (look-back scan, run-start markers) -> gather (ancestors from the
+//   markers, the copy) -> injection (link, apply) -> commit -> estimate ->
+//   covariances (output record).
 // The chain is captured once into a CUDA graph; a cycle is one graph launch
 // fed by one copy of the per-filter inputs.
 //
@@ -41,7 +43,7 @@ constexpr int kThreads = kBlk;
 constexpr int kWTile = 2 * kWThreads;  // particles per weighting tile (= the single filter's block)
 constexpr int kScanItems = 16;
 constexpr int kRTile = kBlk * kScanItems;  // particles per resampling tile
-constexpr int kHeavy = 32;
+constexpr int kGTile = 2048;  // outputs per gather tile
 constexpr int kBuckets = 4;
 // Size buckets for the autotuned estimate tile: n < 8k, < 32k, < 128k, more.
 constexpr int kBucketLimit[kBuckets - 1] = {8192, 32768, 131072};
@@ -86,7 +88,6 @@ struct BGlobal {
     unsigned scan_epoch;
     unsigned inj_epoch;
     unsigned tile_counter;
-    int heavy_count;
     unsigned err;
     // look-back polls before a wait gives up (kSpinLimit unless the host
     // lowers it), and the filter whose first resampling tile publishes its
@@ -100,6 +101,7 @@ struct Arena {
     float* p[2][7];
     float* ll;
     float* w;
+    int* marker;  // run starts of a resample (-1 elsewhere; reset by the gather)
 };
 
 // Planes of one filter in set `which`, selected with register selects (an
@@ -125,7 +127,6 @@ __global__ void k_b_init(BCtl* C, BGlobal* G, int nf) {
         G->scan_epoch = 1u;
         G->inj_epoch = 1u;
         G->tile_counter = 0u;
-        G->heavy_count = 0;
         G->err = 0u;
         G->spin_limit = kSpinLimit;
         G->stall_f = -1;
@@ -505,13 +506,14 @@ __global__ void __launch_bounds__(kThreads, 2)
 }
 
 // Resampling of one 4096-particle tile of a filter that resamples: the
-// single-filter specification and kernel structure, with tiles taken in a
-// global dynamic order (a filter's tiles are consecutive in that order, so
-// each tile's predecessors are already running when it looks back).
+// single-filter specification, with tiles taken in a global dynamic order (a
+// filter's tiles are consecutive in that order, so each tile's predecessors
+// are already running when it looks back).  Source j writes j at the first
+// output of its run and at every gather-tile boundary inside it (runs are
+// disjoint, so no two sources write the same marker); k_b_gather copies.
 __global__ void __launch_bounds__(kThreads)
     k_b_resample(Arena A, const BFilter* __restrict__ F, const BTile* __restrict__ T,
-                 BCtl* C, BGlobal* G, unsigned* flags, uint64_t* vals,
-                 HeavyRun* heavy, int heavy_cap) {
+                 BCtl* C, BGlobal* G, unsigned* flags, uint64_t* vals) {
     __shared__ unsigned s_tile;
     __shared__ uint64_t s_warp[kThreads / 32];
     __shared__ uint64_t s_prefix, s_agg;
@@ -541,9 +543,7 @@ __global__ void __launch_bounds__(kThreads)
     }
     const int wmode = c->wmode;
     const float M = c->M, S = c->S;
-    const int live = c->live;
-    const Planes src = filter_planes(A, live, fl.off);
-    const Planes dst = filter_planes(A, 1 - live, fl.off);
+    int* mk = A.marker + fl.off;
     const float* w = A.w + fl.off;
     const float* ll = A.ll + fl.off;
     unsigned* fflags = flags + fl.rtile0;
@@ -624,30 +624,98 @@ __global__ void __launch_bounds__(kThreads)
         if (j >= n) break;
         const long long e =
             (j == n - 1) ? (long long)n : count_le(c_prev + v[k], n, u0, step);
-        const long long cnt = e - st;
-        if (cnt > kHeavy) {
-            push_run(heavy, heavy_cap, &G->heavy_count, &G->err, (int)j, st, e, t.f);
-        } else if (cnt > 0) {
-            copy_particle(src, dst, (int)j, st, e, nullptr, 0);
+        if (e > st) {
+            mk[st] = (int)j;
+            for (long long b = (st / kGTile + 1) * kGTile; b < e; b += kGTile) mk[b] = (int)j;
         }
         st = e;
     }
 }
 
-// Long copy runs of all filters (HeavyRun.pad = filter), one block per
-// recorded piece.
+// Output-parallel copy of one 2048-output tile of a filter that resampled:
+// the tile's markers (every tile starts with one) give each output its
+// ancestor by a running maximum (ancestors increase with the output index),
+// the markers read are reset for the next resample, and the seven planes are
+// copied with 16-byte stores (filter offsets are multiples of 1024).
 __global__ void __launch_bounds__(kThreads)
-    k_b_expand(Arena A, const BFilter* __restrict__ F, const BCtl* C,
-               const BGlobal* G, const HeavyRun* heavy, int heavy_cap) {
-    const int count = min(G->heavy_count, heavy_cap);
-    for (int r = blockIdx.x; r < count; r += gridDim.x) {
-        const HeavyRun h = heavy[r];
-        const int f = h.pad;
-        const int live = C[f].live;
-        const Planes src = filter_planes(A, live, F[f].off);
-        const Planes dst = filter_planes(A, 1 - live, F[f].off);
-        fill_range(src, dst, h.j, h.start + (int)threadIdx.x, h.end, kThreads, nullptr,
-                   0);
+    k_b_gather(Arena A, const BFilter* __restrict__ F, const BTile* __restrict__ T,
+               const BCtl* C) {
+    __shared__ int s_anc[kGTile];
+    __shared__ int s_wmax[kThreads / 32];
+    const BTile t = T[blockIdx.x];
+    const BFilter& fl = F[t.f];
+    const BCtl* c = C + t.f;
+    if (!c->resample_now || !c->resample_valid) return;
+    const int n = fl.n;
+    int* mk = A.marker + fl.off;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int i0 = t.start + 8 * tid;
+    int m[8];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int ib = i0 + 4 * h;
+        int4 v = make_int4(-1, -1, -1, -1);
+        if (ib + 4 <= n) {
+            v = __ldcg(reinterpret_cast<const int4*>(mk + ib));
+        } else {
+            if (ib < n) v.x = __ldcg(mk + ib);
+            if (ib + 1 < n) v.y = __ldcg(mk + ib + 1);
+            if (ib + 2 < n) v.z = __ldcg(mk + ib + 2);
+        }
+        m[4 * h] = v.x;
+        m[4 * h + 1] = v.y;
+        m[4 * h + 2] = v.z;
+        m[4 * h + 3] = v.w;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+        if (m[q] >= 0) mk[i0 + q] = -1;
+#pragma unroll
+    for (int q = 1; q < 8; ++q) m[q] = max(m[q], m[q - 1]);
+    int x = m[7];
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int y = __shfl_up_sync(~0u, x, d);
+        if (lane >= d) x = max(x, y);
+    }
+    const int excl = __shfl_up_sync(~0u, x, 1);
+    if (lane == 31) s_wmax[warp] = x;
+    __syncthreads();
+    int before = lane > 0 ? excl : -1;
+    for (int k = 0; k < warp; ++k) before = max(before, s_wmax[k]);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) s_anc[8 * tid + q] = min(max(max(m[q], before), 0), n - 1);
+    __syncthreads();
+    const Planes src = filter_planes(A, c->live, fl.off);
+    const Planes dst = filter_planes(A, 1 - c->live, fl.off);
+    float* const sp[7] = {src.px, src.py, src.pz, src.qw, src.qx, src.qy, src.qz};
+    float* const dp[7] = {dst.px, dst.py, dst.pz, dst.qw, dst.qx, dst.qy, dst.qz};
+    // thread t copies outputs [4t, 4t + 4) and [1024 + 4t, 1024 + 4t + 4)
+#pragma unroll 1
+    for (int h = 0; h < 2; ++h) {
+        const int l0 = h * (kGTile / 2) + 4 * tid;
+        const int ib = t.start + l0;
+        if (ib >= n) break;
+        int a[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) a[q] = s_anc[l0 + q];
+        float v[7][4];
+#pragma unroll
+        for (int k = 0; k < 7; ++k)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) v[k][q] = sp[k][a[q]];
+        if (ib + 4 <= n) {
+#pragma unroll
+            for (int k = 0; k < 7; ++k)
+                reinterpret_cast<float4*>(dp[k] + ib)[0] =
+                    make_float4(v[k][0], v[k][1], v[k][2], v[k][3]);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 7; ++k)
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (ib + q < n) dp[k][ib + q] = v[k][q];
+        }
     }
 }
 
@@ -721,7 +789,6 @@ __global__ void k_b_commit(BCtl* C, BGlobal* G, int nf) {
     }
     if (f == 0) {
         G->tile_counter = 0u;
-        G->heavy_count = 0;
         unsigned e = (G->scan_epoch + 1u) & 0x3FFFFFFFu;
         G->scan_epoch = e ? e : 1u;
         e = G->inj_epoch + 1u;
@@ -783,8 +850,9 @@ struct BatchHandle {
     double* d_cpart = nullptr;
     unsigned* d_flags = nullptr;
     uint64_t* d_vals = nullptr;
-    HeavyRun* d_heavy = nullptr;
-    int heavy_cap = 0;
+    BTile* d_gt = nullptr;
+    int n_gt = 0;
+    int* d_marker = nullptr;
     int* d_draw_f = nullptr;
     int total_draws = 0;
     uint64_t* d_inj_head = nullptr;
@@ -820,9 +888,10 @@ std::vector<BTile> make_tiles(const std::vector<BFilter>& F, int which,
                               const std::vector<int>& est_tile) {
     std::vector<BTile> t;
     for (int f = 0; f < (int)F.size(); ++f) {
-        const int sz = which == 0 ? kWTile
+        const int sz = which == 0   ? kWTile
                        : which == 1 ? est_tile[bucket_of(F[f].n)]
-                                    : kRTile;
+                       : which == 2 ? kRTile
+                                    : kGTile;
         const int nt = ceil_div(F[f].n, sz);
         for (int k = 0; k < nt; ++k)
             t.push_back(BTile{f, k * sz, std::min(sz, F[f].n - k * sz), k});
@@ -894,10 +963,8 @@ int enqueue_cycle(BatchHandle* h) {
     h->launches += 3;
     PFB_KL();
     k_b_resample<<<h->n_rt, kThreads, 0, s>>>(h->A, h->d_F, h->d_rt, h->d_C, h->d_G,
-                                              h->d_flags, h->d_vals, h->d_heavy,
-                                              h->heavy_cap);
-    k_b_expand<<<2 * 148, kThreads, 0, s>>>(h->A, h->d_F, h->d_C, h->d_G, h->d_heavy,
-                                            h->heavy_cap);
+                                              h->d_flags, h->d_vals);
+    k_b_gather<<<h->n_gt, kThreads, 0, s>>>(h->A, h->d_F, h->d_gt, h->d_C);
     h->launches += 2;
     if (h->total_draws > 0) {
         const int g = ceil_div(h->total_draws, kThreads);
@@ -950,10 +1017,6 @@ int finish(BatchHandle* h, double* est_out) {
         set_error("pf_b200: batch look-back wait timed out");
         return -1;
     }
-    if (h->h_G->err & ERR_SCAN_OVERFLOW) {
-        set_error("pf_b200: batch long-run list overflow");
-        return -1;
-    }
     if (est_out)
         memcpy(est_out, h->h_out, sizeof(double) * PFC_EST_LEN * (size_t)h->nf);
     return 0;
@@ -977,7 +1040,8 @@ void free_batch(BatchHandle* h) {
     cudaFree(h->d_cpart);
     cudaFree(h->d_flags);
     cudaFree(h->d_vals);
-    cudaFree(h->d_heavy);
+    cudaFree(h->d_gt);
+    cudaFree(h->d_marker);
     cudaFree(h->d_draw_f);
     cudaFree(h->d_inj_head);
     cudaFree(h->d_inj_next);
@@ -1079,9 +1143,15 @@ void* pfc_batch_create(int n_filters, const int* n, const unsigned* seeds,
             cudaMalloc((void**)&h->d_vals, sizeof(uint64_t) * 2 * rt.size()) != cudaSuccess)
             break;
         if (cudaMemset(h->d_flags, 0, sizeof(unsigned) * rt.size()) != cudaSuccess) break;
-        h->heavy_cap = (int)std::min<long long>(
-            h->arena / kHeavy + h->arena / kSplit + 2 * n_filters, 1 << 26);
-        if (cudaMalloc((void**)&h->d_heavy, sizeof(HeavyRun) * h->heavy_cap) != cudaSuccess)
+        if (cudaMalloc((void**)&h->d_marker, sizeof(int) * ap) != cudaSuccess ||
+            cudaMemset(h->d_marker, 0xFF, sizeof(int) * ap) != cudaSuccess)
+            break;
+        h->A.marker = h->d_marker;
+        std::vector<BTile> gt = make_tiles(h->filters, 3, h->est_tile);
+        h->n_gt = (int)gt.size();
+        if (cudaMalloc((void**)&h->d_gt, sizeof(BTile) * gt.size()) != cudaSuccess ||
+            cudaMemcpy(h->d_gt, gt.data(), sizeof(BTile) * gt.size(),
+                       cudaMemcpyHostToDevice) != cudaSuccess)
             break;
         if (cudaMalloc((void**)&h->d_inj_head, sizeof(uint64_t) * ap) != cudaSuccess ||
             cudaMemset(h->d_inj_head, 0, sizeof(uint64_t) * ap) != cudaSuccess)

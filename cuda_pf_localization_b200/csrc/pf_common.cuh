@@ -54,7 +54,6 @@ void clear_error();
 // sync).  A bounded spin that runs out sets SPIN_TIMEOUT instead of hanging.
 enum : unsigned {
     ERR_SPIN_TIMEOUT = 1u,
-    ERR_SCAN_OVERFLOW = 2u,
 };
 
 constexpr int kSpinLimit = 1 << 22;  // polls before a look-back gives up

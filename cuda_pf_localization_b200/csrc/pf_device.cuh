@@ -574,23 +574,6 @@ __device__ __forceinline__ long long count_le(uint64_t X, int n, double u0,
     return i + 1;
 }
 
-__device__ __forceinline__ void copy_particle(const Planes& src, const Planes& dst,
-                                              int j, long long s, long long e,
-                                              int* anc, int record) {
-    const float x = src.px[j], y = src.py[j], z = src.pz[j];
-    const float a = src.qw[j], b = src.qx[j], c = src.qy[j], d = src.qz[j];
-    for (long long i = s; i < e; ++i) {
-        dst.px[i] = x;
-        dst.py[i] = y;
-        dst.pz[i] = z;
-        dst.qw[i] = a;
-        dst.qx[i] = b;
-        dst.qy[i] = c;
-        dst.qz[i] = d;
-        if (record) anc[i] = j;
-    }
-}
-
 // Warp-parallel look-back (run by warp 0 of a tile > 0): returns the sum of
 // all predecessors' weights.  Lane l inspects tile base - l; the nearest
 // predecessor that already knows its inclusive prefix ends the walk.  After
@@ -628,42 +611,6 @@ __device__ inline uint64_t look_back(const unsigned* flags, const uint64_t* vals
         prefix += warp_sum_u64(v);
         if (incl) return prefix;
         base -= 32;
-    }
-}
-
-constexpr int kSplit = 4096;  // longest piece of a long copy run
-
-// Record the copy run [s, e) of source particle j as pieces of at most
-// kSplit outputs; the expansion kernel gives each piece to one block.
-__device__ __forceinline__ void push_run(HeavyRun* heavy, int cap, int* count,
-                                         unsigned* err, int j, long long s,
-                                         long long e, int tag) {
-    const int pieces = (int)((e - s + kSplit - 1) / kSplit);
-    const int slot = atomicAdd(count, pieces);
-    for (int k = 0; k < pieces; ++k) {
-        const long long a = s + (long long)k * kSplit;
-        const long long b = a + kSplit < e ? a + kSplit : e;
-        if (slot + k < cap)
-            heavy[slot + k] = HeavyRun{j, (int)a, (int)b, tag};
-        else
-            atomicOr(err, ERR_SCAN_OVERFLOW);
-    }
-}
-
-__device__ __forceinline__ void fill_range(const Planes& src, const Planes& dst,
-                                           int j, int lo, int hi, int stride,
-                                           int* anc, int record) {
-    const float x = src.px[j], y = src.py[j], z = src.pz[j];
-    const float a = src.qw[j], b = src.qx[j], c = src.qy[j], d = src.qz[j];
-    for (int i = lo; i < hi; i += stride) {
-        dst.px[i] = x;
-        dst.py[i] = y;
-        dst.pz[i] = z;
-        dst.qw[i] = a;
-        dst.qx[i] = b;
-        dst.qy[i] = c;
-        dst.qz[i] = d;
-        if (record) anc[i] = j;
     }
 }
 

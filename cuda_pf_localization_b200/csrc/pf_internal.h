@@ -111,15 +111,6 @@ __device__ __forceinline__ float weight_of(int wmode, long long i, int n,
     return weight_from_ll(ll[i], M, S);
 }
 
-// A copy run of the resampler too long for one thread: particle j fills
-// outputs [start, end).
-struct HeavyRun {
-    int j;
-    int start;
-    int end;
-    int pad;
-};
-
 // Both ping-pong particle sets, passed to kernels by value.
 struct PlaneSet {
     Planes s[2];
