@@ -285,6 +285,53 @@ __device__ __forceinline__ void tiles_combine(const double* part, int ntiles,
     __syncthreads();
 }
 
+// Sum w^2 (FP64), the fixed-point weight total and the bad-weight flag over
+// the float4 groups [q0, q1) of one tile, the weights materialised when they
+// are still log-likelihoods.  A thread takes groups q0 + tid, q0 + tid + 256,
+// ... in that order; four groups are loaded before any is used so a thread
+// keeps four loads in flight (the weight store cannot alias the next load).
+template <int kMode>
+__device__ __forceinline__ void ess_span(const float* __restrict__ ll, float* __restrict__ w,
+                                         int q0, int q1, int n, float M, float S,
+                                         float wuni, double& sq,
+                                         unsigned long long& tfx, int& bad) {
+    constexpr int kU = 4;
+    const float4* __restrict__ src =
+        reinterpret_cast<const float4*>(kMode == WMODE_STORED ? w : ll);
+    float4* __restrict__ dst = reinterpret_cast<float4*>(w);
+    for (int b = q0 + threadIdx.x; b < q1; b += kU * kThreads) {
+        float4 V[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int i4 = b + u * kThreads;
+            if (kMode == WMODE_UNIFORM)
+                V[u] = make_float4(wuni, wuni, wuni, wuni);
+            else
+                V[u] = i4 < q1 ? src[i4] : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int i4 = b + u * kThreads;
+            if (i4 >= q1) break;
+            float4 W = V[u];
+            if (kMode == WMODE_LL) {
+                W = make_float4(weight_from_ll(W.x, M, S), weight_from_ll(W.y, M, S),
+                                weight_from_ll(W.z, M, S), weight_from_ll(W.w, M, S));
+                dst[i4] = W;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (4 * i4 + k >= n) break;
+                const float wf = comp(W, k);
+                bad |= weight_bad(wf) ? 1 : 0;
+                tfx += weight_bad(wf) ? 0ull : weight_fx(wf);
+                const double wd = (double)wf;
+                sq = __fma_rn(wd, wd, sq);
+            }
+        }
+    }
+}
+
 // Weight pass over one estimate tile before the resample decision: the
 // weights materialised from the log-likelihoods, sum w^2 in FP64, the exact
 // fixed-point weight total and the bad-weight flag; the filter's last tile
@@ -307,28 +354,12 @@ __global__ void __launch_bounds__(kThreads)
     unsigned long long tfx = 0;
     int bad = 0;
     const int q0 = t.start >> 2, q1 = (t.start + t.count + 3) >> 2;
-    for (int i4 = q0 + threadIdx.x; i4 < q1; i4 += kThreads) {
-        float4 W;
-        if (wmode == WMODE_STORED) {
-            W = reinterpret_cast<const float4*>(w)[i4];
-        } else if (wmode == WMODE_UNIFORM) {
-            W = make_float4(wuni, wuni, wuni, wuni);
-        } else {
-            const float4 L = reinterpret_cast<const float4*>(ll)[i4];
-            W = make_float4(weight_from_ll(L.x, M, S), weight_from_ll(L.y, M, S),
-                            weight_from_ll(L.z, M, S), weight_from_ll(L.w, M, S));
-            reinterpret_cast<float4*>(w)[i4] = W;
-        }
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            if (4 * i4 + k >= fl.n) break;
-            const float wf = comp(W, k);
-            bad |= weight_bad(wf) ? 1 : 0;
-            tfx += weight_bad(wf) ? 0ull : weight_fx(wf);
-            const double wd = (double)wf;
-            acc[0] = __fma_rn(wd, wd, acc[0]);
-        }
-    }
+    if (wmode == WMODE_STORED)
+        ess_span<WMODE_STORED>(ll, w, q0, q1, fl.n, M, S, wuni, acc[0], tfx, bad);
+    else if (wmode == WMODE_UNIFORM)
+        ess_span<WMODE_UNIFORM>(ll, w, q0, q1, fl.n, M, S, wuni, acc[0], tfx, bad);
+    else
+        ess_span<WMODE_LL>(ll, w, q0, q1, fl.n, M, S, wuni, acc[0], tfx, bad);
     // integer total and bad flag of the tile
     __shared__ unsigned long long s_u[kThreads / 32];
     const unsigned long long u = warp_sum_u64(tfx);
@@ -343,19 +374,21 @@ __global__ void __launch_bounds__(kThreads)
     if (!tile_partial<1>(acc, epart + (size_t)(fl.etile0 + t.local) * kEstN,
                          &c->done_e, fl.netiles))
         return;
+    // warp 0 combines the tiles: sum w^2 in the lane-strided order, the
+    // integer total and the flag (exact, any order)
+    if (threadIdx.x >= 32) return;
+    const int lane = threadIdx.x;
     double sq = 0.0;
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-        for (int b = lane; b < fl.netiles; b += 32)
-            sq += __ldcg(&epart[(size_t)(fl.etile0 + b) * kEstN]);
-        sq = warp_sum_d(sq);
+    unsigned long long tot = 0, fb = 0;
+    for (int b = lane; b < fl.netiles; b += 32) {
+        sq += __ldcg(&epart[(size_t)(fl.etile0 + b) * kEstN]);
+        tot += __ldcg(&eupart[2 * (size_t)(fl.etile0 + b)]);
+        fb |= __ldcg(&eupart[2 * (size_t)(fl.etile0 + b) + 1]);
     }
-    if (threadIdx.x == 0) {
-        unsigned long long tot = 0, fb = 0;
-        for (int b = 0; b < fl.netiles; ++b) {
-            tot += __ldcg(&eupart[2 * (size_t)(fl.etile0 + b)]);
-            fb |= __ldcg(&eupart[2 * (size_t)(fl.etile0 + b) + 1]);
-        }
+    sq = warp_sum_d(sq);
+    tot = warp_sum_u64(tot);
+    const bool any_fb = __any_sync(0xffffffffu, fb != 0ull);
+    if (lane == 0) {
         const double ess = sq > 0.0 ? 1.0 / sq : 0.0;
         c->ess = ess;
         c->ess_pre = ess;
@@ -365,7 +398,7 @@ __global__ void __launch_bounds__(kThreads)
         c->resampled = 0;
         o[PFC_EST_RESAMPLED] = 0.0;
         c->w_total_fx = tot;
-        c->w_bad = fb ? 1 : 0;
+        c->w_bad = any_fb ? 1 : 0;
         if (wmode == WMODE_LL) c->wmode = WMODE_STORED;
         c->done_e = 0u;
     }
