@@ -982,6 +982,28 @@ int pfc_pick_from_cum(void* hv, const double* cum, int n, double u0,
     return rc;
 }
 
+int pfc_weight_div_check(void* hv, const float* e, const float* s, int n,
+                         float* fast, float* ieee) {
+    PfHandle* h = as_pf(hv);
+    if (!h || !e || !s || !fast || !ieee || n <= 0) return -1;
+    float* d = nullptr;
+    const size_t bytes = sizeof(float) * (size_t)n;
+    int rc = -1;
+    if (cudaMalloc((void**)&d, 4 * bytes) == cudaSuccess &&
+        cudaMemcpyAsync(d, e, bytes, cudaMemcpyHostToDevice, h->stream) == cudaSuccess &&
+        cudaMemcpyAsync(d + n, s, bytes, cudaMemcpyHostToDevice, h->stream) == cudaSuccess &&
+        launch_weight_div_check(h, d, d + n, n, d + 2 * (size_t)n, d + 3 * (size_t)n) == 0 &&
+        cudaMemcpyAsync(fast, d + 2 * (size_t)n, bytes, cudaMemcpyDeviceToHost,
+                        h->stream) == cudaSuccess &&
+        cudaMemcpyAsync(ieee, d + 3 * (size_t)n, bytes, cudaMemcpyDeviceToHost,
+                        h->stream) == cudaSuccess &&
+        cudaStreamSynchronize(h->stream) == cudaSuccess)
+        rc = 0;
+    if (rc) set_error("pf_b200: pfc_weight_div_check failed");
+    cudaFree(d);
+    return rc;
+}
+
 int pfc_get_lcg(void* hv, unsigned long long* lcg) {
     PfHandle* h = as_pf(hv);
     if (!h || !lcg) return -1;

@@ -293,7 +293,7 @@ __device__ __forceinline__ void tiles_combine(const double* part, int ntiles,
 template <int kMode>
 __device__ __forceinline__ void ess_span(const float* __restrict__ ll, float* __restrict__ w,
                                          int q0, int q1, int n, float M, float S,
-                                         float wuni, double& sq,
+                                         double rS, float wuni, double& sq,
                                          unsigned long long& tfx, int& bad) {
     constexpr int kU = 4;
     const float4* __restrict__ src =
@@ -315,8 +315,8 @@ __device__ __forceinline__ void ess_span(const float* __restrict__ ll, float* __
             if (i4 >= q1) break;
             float4 W = V[u];
             if (kMode == WMODE_LL) {
-                W = make_float4(weight_from_ll(W.x, M, S), weight_from_ll(W.y, M, S),
-                                weight_from_ll(W.z, M, S), weight_from_ll(W.w, M, S));
+                W = make_float4(weight_from_ll(W.x, M, S, rS), weight_from_ll(W.y, M, S, rS),
+                                weight_from_ll(W.z, M, S, rS), weight_from_ll(W.w, M, S, rS));
                 dst[i4] = W;
             }
 #pragma unroll
@@ -347,6 +347,7 @@ __global__ void __launch_bounds__(kThreads)
     BCtl* c = C + t.f;
     const int wmode = c->wmode;
     const float M = c->M, S = c->S;
+    const double rS = __drcp_rn((double)S);
     const float wuni = 1.0f / (float)fl.n;
     float* w = A.w + fl.off;
     const float* ll = A.ll + fl.off;
@@ -355,11 +356,11 @@ __global__ void __launch_bounds__(kThreads)
     int bad = 0;
     const int q0 = t.start >> 2, q1 = (t.start + t.count + 3) >> 2;
     if (wmode == WMODE_STORED)
-        ess_span<WMODE_STORED>(ll, w, q0, q1, fl.n, M, S, wuni, acc[0], tfx, bad);
+        ess_span<WMODE_STORED>(ll, w, q0, q1, fl.n, M, S, rS, wuni, acc[0], tfx, bad);
     else if (wmode == WMODE_UNIFORM)
-        ess_span<WMODE_UNIFORM>(ll, w, q0, q1, fl.n, M, S, wuni, acc[0], tfx, bad);
+        ess_span<WMODE_UNIFORM>(ll, w, q0, q1, fl.n, M, S, rS, wuni, acc[0], tfx, bad);
     else
-        ess_span<WMODE_LL>(ll, w, q0, q1, fl.n, M, S, wuni, acc[0], tfx, bad);
+        ess_span<WMODE_LL>(ll, w, q0, q1, fl.n, M, S, rS, wuni, acc[0], tfx, bad);
     // integer total and bad flag of the tile
     __shared__ unsigned long long s_u[kThreads / 32];
     const unsigned long long u = warp_sum_u64(tfx);
@@ -407,8 +408,10 @@ __global__ void __launch_bounds__(kThreads)
 // Estimate pass over one estimate tile: 14 FP64 sums (and the weight
 // materialisation when the weights are still log-likelihoods); the filter's
 // last tile combines, runs the Markley mean and stores the f32 covariance
-// means.
-__global__ void __launch_bounds__(kThreads, 2)
+// means.  Three blocks per SM (80 registers): the pass waits on its loads,
+// and the third block's warps hide more of that than the spill of a few
+// values costs (1.797 against 1.812 ms per 512-filter cycle at two).
+__global__ void __launch_bounds__(kThreads, 3)
     k_b_est(Arena A, const BFilter* __restrict__ F, const BTile* __restrict__ T,
             BCtl* C, double* __restrict__ epart) {
     const BTile t = T[blockIdx.x];
@@ -417,6 +420,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     const Planes s = filter_planes(A, c->live, fl.off);
     const int wmode = c->wmode;
     const float M = c->M, S = c->S;
+    const double rS = __drcp_rn((double)S);
     const float wuni = 1.0f / (float)fl.n;
     float* w = A.w + fl.off;
     const float* ll = A.ll + fl.off;
@@ -441,8 +445,8 @@ __global__ void __launch_bounds__(kThreads, 2)
             W = make_float4(wuni, wuni, wuni, wuni);
         } else {
             const float4 L = reinterpret_cast<const float4*>(ll)[i4];
-            W = make_float4(weight_from_ll(L.x, M, S), weight_from_ll(L.y, M, S),
-                            weight_from_ll(L.z, M, S), weight_from_ll(L.w, M, S));
+            W = make_float4(weight_from_ll(L.x, M, S, rS), weight_from_ll(L.y, M, S, rS),
+                            weight_from_ll(L.z, M, S, rS), weight_from_ll(L.w, M, S, rS));
             reinterpret_cast<float4*>(w)[i4] = W;
         }
 #pragma unroll
@@ -481,6 +485,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     const Planes s = filter_planes(A, c->live, fl.off);
     const int wmode = c->wmode;
     const float M = c->M, S = c->S;
+    const double rS = __drcp_rn((double)S);
     const float wuni = 1.0f / (float)fl.n;
     const float* w = A.w + fl.off;
     const float* ll = A.ll + fl.off;
@@ -508,8 +513,8 @@ __global__ void __launch_bounds__(kThreads, 2)
             W = make_float4(wuni, wuni, wuni, wuni);
         } else {
             const float4 L = reinterpret_cast<const float4*>(ll)[i4];
-            W = make_float4(weight_from_ll(L.x, M, S), weight_from_ll(L.y, M, S),
-                            weight_from_ll(L.z, M, S), weight_from_ll(L.w, M, S));
+            W = make_float4(weight_from_ll(L.x, M, S, rS), weight_from_ll(L.y, M, S, rS),
+                            weight_from_ll(L.z, M, S, rS), weight_from_ll(L.w, M, S, rS));
         }
 #pragma unroll
         for (int k = 0; k < 4; ++k) {

@@ -102,6 +102,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     const Planes s = pick_planes(ps, ctl->live);
     const int wmode = ctl->wmode;
     const float M = ctl->ll_max, S = ctl->ll_sumexp;
+    const double rS = __drcp_rn((double)S);
     const float wuni = 1.0f / (float)n;
     double acc[kEstN];
 #pragma unroll
@@ -125,8 +126,8 @@ __global__ void __launch_bounds__(kThreads, 2)
             W = make_float4(wuni, wuni, wuni, wuni);
         } else {
             const float4 L = reinterpret_cast<const float4*>(ll)[i4];
-            W = make_float4(weight_from_ll(L.x, M, S), weight_from_ll(L.y, M, S),
-                            weight_from_ll(L.z, M, S), weight_from_ll(L.w, M, S));
+            W = make_float4(weight_from_ll(L.x, M, S, rS), weight_from_ll(L.y, M, S, rS),
+                            weight_from_ll(L.z, M, S, rS), weight_from_ll(L.w, M, S, rS));
             reinterpret_cast<float4*>(w)[i4] = W;
         }
 #pragma unroll
@@ -161,6 +162,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     const Planes s = pick_planes(ps, ctl->live);
     const int wmode = ctl->wmode;
     const float M = ctl->ll_max, S = ctl->ll_sumexp;
+    const double rS = __drcp_rn((double)S);
     const float wuni = 1.0f / (float)n;
     float3 mpf;
     float4 mqf;
@@ -198,8 +200,8 @@ __global__ void __launch_bounds__(kThreads, 2)
             W = make_float4(wuni, wuni, wuni, wuni);
         } else {
             const float4 L = reinterpret_cast<const float4*>(ll)[i4];
-            W = make_float4(weight_from_ll(L.x, M, S), weight_from_ll(L.y, M, S),
-                            weight_from_ll(L.z, M, S), weight_from_ll(L.w, M, S));
+            W = make_float4(weight_from_ll(L.x, M, S, rS), weight_from_ll(L.y, M, S, rS),
+                            weight_from_ll(L.z, M, S, rS), weight_from_ll(L.w, M, S, rS));
         }
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
@@ -251,6 +253,7 @@ __global__ void __launch_bounds__(kThreads)
     static_assert(kPrefixBlock == 8 * kThreads, "two float4 per thread");
     const int wmode = ctl->wmode;
     const float M = ctl->ll_max, S = ctl->ll_sumexp;
+    const double rS = __drcp_rn((double)S);
     const float wuni = 1.0f / (float)n;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     double sq = 0.0;
@@ -267,8 +270,8 @@ __global__ void __launch_bounds__(kThreads)
             W = make_float4(wuni, wuni, wuni, wuni);
         } else {
             const float4 L = reinterpret_cast<const float4*>(ll)[i4];
-            W = make_float4(weight_from_ll(L.x, M, S), weight_from_ll(L.y, M, S),
-                            weight_from_ll(L.z, M, S), weight_from_ll(L.w, M, S));
+            W = make_float4(weight_from_ll(L.x, M, S, rS), weight_from_ll(L.y, M, S, rS),
+                            weight_from_ll(L.z, M, S, rS), weight_from_ll(L.w, M, S, rS));
             reinterpret_cast<float4*>(w)[i4] = W;
         }
 #pragma unroll
@@ -385,6 +388,17 @@ __global__ void k_materialize_w(int n, const float* __restrict__ ll,
 
 __global__ void k_set_stored(CycleCtl* ctl) { ctl->wmode = WMODE_STORED; }
 
+// Both quotient forms of the weight normalisation on caller pairs (e, S).
+__global__ void k_weight_div_check(const float* __restrict__ e, const float* __restrict__ s,
+                                   int n, float* __restrict__ fast,
+                                   float* __restrict__ ieee) {
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= n) return;
+    const float S = s[i];
+    fast[i] = weight_div(e[i], S, __drcp_rn((double)S));
+    ieee[i] = __fdiv_rn(e[i], S);
+}
+
 int est_grid(int n) {
     int g = ceil_div(ceil_div(n, 4), kThreads);
     return g < kMaxBlocks ? g : kMaxBlocks;
@@ -426,6 +440,14 @@ int launch_weight_prefix(PfHandle* h, bool decide, double ess_ratio) {
 
 int launch_cycle_decide(PfHandle* h, double ess_ratio) {
     return launch_weight_prefix(h, true, ess_ratio);
+}
+
+int launch_weight_div_check(PfHandle* h, const float* d_e, const float* d_s, int n,
+                            float* d_fast, float* d_ieee) {
+    k_weight_div_check<<<ceil_div(n, kThreads), kThreads, 0, h->stream>>>(d_e, d_s, n,
+                                                                          d_fast, d_ieee);
+    PFB_KL();
+    return 0;
 }
 
 int launch_materialize_weights(PfHandle* h) {

@@ -101,6 +101,54 @@ __device__ __forceinline__ float weight_from_ll(float l, float M, float S) {
     return __fdiv_rn(expf(__fsub_rn(l, M)), S);
 }
 
+// The correctly rounded f32 quotient e / S without the f32 division on the
+// common path, given rS = RN(1 / S) in FP64.  The FP64 product p = e * rS
+// differs from q = e / S by a relative error below 2^-52 (two FP64
+// roundings).  For 24-bit e and S, a quotient in the normal f32 range is
+// never a midpoint of the f32 grid (a midpoint's odd part needs 25 bits, the
+// odd part of e has at most 24) and lies at least 2^-49 (relative) from every
+// midpoint (|e - m S| is a nonzero multiple of ulp(m) * 2^se, S < 2^(se+24)),
+// so RN_f32(p) == RN_f32(q): the double-rounding argument of S. A. Figueroa,
+// "When is double rounding innocuous?" (SIGNUM Newsletter 30(3), 1995), with
+// the product's two roundings counted.
+// Below 2^-126 the f32 step is fixed at 2^-149 and exact midpoints occur, so
+// the quotient is rounded as an integer count of 2^-149: x = e * 2^149 is an
+// integer (exact in FP64) and the result is RNE(x / S) * 2^-149.  With
+// q < 2^-125, x / S < 2^24 and y = x * rS is within 2^-29 of it; y decides
+// unless it lies within 2^-28 of a half-integer, where the exact residual
+// x - (floor(y) + 1/2) S (one FMA: both terms are multiples of 2^min(0, se-1)
+// and the residual is tiny) gives the direction and ties go to even.  This
+// holds for 1 <= S <= 2^100 (the normaliser is at least 1, the maximum's own
+// term).  Zero numerators (underflowed exponentials, most of a sharply
+// weighted cloud) return +0 first, so only warps holding a nonzero weight
+// below 2^-126 run the integer rounding.  Other operands (NaN, infinities,
+// S < 1) take the IEEE division.
+__device__ __forceinline__ float weight_div(float e, float S, double rS) {
+    const double p = (double)e * rS;
+    if (p >= 0x1.0000000000004p-126) return __double2float_rn(p);
+    if (e == 0.0f && S > 0.0f) return 0.0f;
+    if (e >= 0.0f && S >= 1.0f && S <= 0x1p100f) {
+        const double x = (double)e * 0x1p149;
+        const double y = __dmul_rn(x, rS);
+        const double fl = floor(y);
+        const double dm = __dsub_rn(y, fl + 0.5);
+        double k = dm > 0.0 ? fl + 1.0 : fl;
+        if (fabs(dm) <= 0x1p-28) {
+            const double r = fma(-(fl + 0.5), (double)S, x);
+            const bool odd = ((long long)fl & 1) != 0;
+            k = (r > 0.0 || (r == 0.0 && odd)) ? fl + 1.0 : fl;
+        }
+        return __double2float_rn(k * 0x1p-149);
+    }
+    return __fdiv_rn(e, S);
+}
+
+// weight_from_ll with rS = RN(1 / S) in FP64 computed once by the caller;
+// the same bits as the three-argument form.
+__device__ __forceinline__ float weight_from_ll(float l, float M, float S, double rS) {
+    return weight_div(expf(__fsub_rn(l, M)), S, rS);
+}
+
 // Normalised f32 weight of particle i under the cloud's weight mode.
 __device__ __forceinline__ float weight_of(int wmode, long long i, int n,
                                            const float* __restrict__ w,
@@ -330,5 +378,8 @@ int launch_cycle_decide(PfHandle* h, double ess_ratio);
 int launch_materialize_weights(PfHandle* h);
 int launch_pick_from_cum(PfHandle* h, const double* d_cum, int n, double u0,
                          double total, int* d_anc);
+// weight_div and the IEEE division side by side on n device pairs (e, S).
+int launch_weight_div_check(PfHandle* h, const float* d_e, const float* d_s, int n,
+                            float* d_fast, float* d_ieee);
 
 }  // namespace pfb

@@ -276,6 +276,12 @@ int pfc_get_ancestors(void* h, int* anc);
 int pfc_pick_from_cum(void* h, const double* cum, int n, double u0,
                       double total, int* anc);
 
+/* The weight normalisation's quotient e / S both ways on the device: fast[i]
+ * from the FP64 product e * RN(1/S) (the form the weighting kernels use),
+ * ieee[i] from the IEEE f32 division.  Host arrays of n entries. */
+int pfc_weight_div_check(void* h, const float* e, const float* s, int n,
+                         float* fast, float* ieee);
+
 /* Device-side LCG word that drives the resampling offset (see
  * pf_kernels.cu:653-657); set it to replay a resample. */
 int pfc_get_lcg(void* h, unsigned long long* lcg);
