@@ -145,7 +145,10 @@ struct CudaBackend {
     bool init(int count, const PfcoreConfig& c) {
         n = count;
         cfg = c;
-        return pfc_init(handle, count, (unsigned)c.seed) == 0;
+        if (pfc_init(handle, count, (unsigned)c.seed) != 0) return false;
+        // update() resamples when the first estimate's ESS is below
+        // ratio * N and then discards that estimate's covariances
+        return pfc_set_ess_hint(handle, c.resample_ess_ratio) == 0;
     }
 
     void reinit(const double pose[7], const double ps[3], const double rs[3]) {
@@ -219,8 +222,12 @@ struct CudaBackend {
 
     void resample(double inject) { pfc_resample(handle, (float)inject); }
 
-    // cuda.rs:264-329.
-    bool estimate(PfcoreEstimate& e) {
+    // cuda.rs:264-329, in two steps: the moments (pfc_est_sums, the Markley
+    // mean on the host, the ESS), then the covariances around that mean
+    // (pfc_covs).  pfc_covs reads the particle state and changes nothing, so
+    // a caller that only needs the ESS of an estimate it will discard may
+    // stop after the first step.
+    bool estimate_moments(PfcoreEstimate& e) {
         memset(&e, 0, sizeof(e));
         if (n == 0) {
             e.attitude[0] = 1.0;
@@ -234,15 +241,21 @@ struct CudaBackend {
         }
         double q[4];
         pfb::markley_mean(&sums[3], q);
+        for (int k = 0; k < 3; ++k) e.position[k] = sums[k];
+        for (int k = 0; k < 4; ++k) e.attitude[k] = q[k];
+        e.ess = sums[13] > 0.0 ? 1.0 / sums[13] : 0.0;
+        return true;
+    }
+
+    bool estimate_covs(PfcoreEstimate& e) {
+        if (n == 0) return true;
         double cv[12];
-        if (pfc_covs(handle, (float)sums[0], (float)sums[1], (float)sums[2],
-                     (float)q[0], (float)q[1], (float)q[2], (float)q[3],
-                     cv) != 0) {
+        if (pfc_covs(handle, (float)e.position[0], (float)e.position[1],
+                     (float)e.position[2], (float)e.attitude[0], (float)e.attitude[1],
+                     (float)e.attitude[2], (float)e.attitude[3], cv) != 0) {
             set_err("pfc_covs failed");
             return false;
         }
-        for (int k = 0; k < 3; ++k) e.position[k] = sums[k];
-        for (int k = 0; k < 4; ++k) e.attitude[k] = q[k];
         auto sym3 = [&](int o, double* m) {
             for (int r = 0; r < 3; ++r)
                 for (int c = r; c < 3; ++c) {
@@ -253,10 +266,11 @@ struct CudaBackend {
         };
         sym3(0, e.pos_cov);
         sym3(6, e.att_cov);
-        e.ess = sums[13] > 0.0 ? 1.0 / sums[13] : 0.0;
         e.valid = 1;
         return true;
     }
+
+    bool estimate(PfcoreEstimate& e) { return estimate_moments(e) && estimate_covs(e); }
 };
 
 // ParticleFilter, crates/pf_core/src/particle_filter.rs:73-133.
@@ -425,8 +439,13 @@ int pfcore_filter_update(void* p, const PfcoreOdom* odom,
     if (!pf || !odom || !out) return -1;
     pf->backend.predict(*odom);
     pf->backend.weight(obs, obs ? nobs : 0, pf->map);
+    // update() estimates, then resamples and estimates again when the ESS is
+    // low.  The first estimate's covariances are only taken when it is the
+    // one returned; the library, told the rule (pfc_set_ess_hint), skips the
+    // covariance pass it would otherwise queue for a discarded estimate.  The
+    // returned estimate is the same.
     PfcoreEstimate est;
-    if (!pf->backend.estimate(est)) return -1;
+    if (!pf->backend.estimate_moments(est)) return -1;
     const double threshold =
         pf->cfg.resample_ess_ratio * (double)pf->cfg.particle_count;
     int resampled = 0;
@@ -434,6 +453,8 @@ int pfcore_filter_update(void* p, const PfcoreOdom* odom,
         pf->backend.resample(pf->cfg.random_inject_ratio);
         if (!pf->backend.estimate(est)) return -1;
         resampled = 1;
+    } else if (!pf->backend.estimate_covs(est)) {
+        return -1;
     }
     est.resampled = resampled;
     *out = est;

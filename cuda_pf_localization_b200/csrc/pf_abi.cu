@@ -194,9 +194,9 @@ int device_error(PfHandle* h) {
 
 // Queue estimate pass 1 + Markley (unless a fused resample already did) +
 // speculative covariance pass + the copy of the control block.
-int queue_estimate(PfHandle* h, bool sums_done = false) {
+int queue_estimate(PfHandle* h, bool sums_done = false, double skip_ratio = 0.0) {
     if (!sums_done && launch_est_sums(h)) return -1;
-    if (launch_covs(h, false, nullptr, nullptr, false)) return -1;
+    if (launch_covs(h, false, nullptr, nullptr, false, skip_ratio)) return -1;
     PFB_CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(CycleCtl),
                            cudaMemcpyDeviceToHost, h->stream));
     h->stats.d2h_bytes += sizeof(CycleCtl);
@@ -643,7 +643,7 @@ int pfc_weight(void* hv, const CObservation* obs, int nobs, float sigma_r,
     if (nobs <= 0 || !obs) {
         if (flush_predict(h)) return -1;
         if (set_wmode(h, WMODE_UNIFORM)) return -1;
-        return queue_estimate(h);
+        return queue_estimate(h, false, h->ess_hint);
     }
     if (stage_observations(h, obs, nobs)) return -1;
     PredictArgs pa = pending_args(h);
@@ -652,7 +652,14 @@ int pfc_weight(void* hv, const CObservation* obs, int nobs, float sigma_r,
     // materialise the weights with the resampler's prefixes now: the estimate
     // pass then reads them instead of re-deriving them from ll
     if (launch_weight_prefix(h, false, 0.0)) return -1;
-    return queue_estimate(h);
+    return queue_estimate(h, false, h->ess_hint);
+}
+
+int pfc_set_ess_hint(void* hv, double resample_ess_ratio) {
+    PfHandle* h = as_pf(hv);
+    if (!h || !(resample_ess_ratio == resample_ess_ratio)) return -1;
+    h->ess_hint = resample_ess_ratio > 0.0 ? resample_ess_ratio : 0.0;
+    return 0;
 }
 
 int pfc_resample(void* hv, float random_inject_ratio) {

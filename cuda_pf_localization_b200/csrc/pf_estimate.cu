@@ -153,12 +153,20 @@ __global__ void __launch_bounds__(kThreads, 2)
 }
 
 // mode: 0 plain, 1 last pass of a fused cycle (also emits the output record).
+// skip_ratio > 0: the caller resamples whenever the ESS of the estimate just
+// computed is below skip_ratio * n (ParticleFilter::update's rule), and then
+// discards this estimate's covariances; the pass is skipped in that case and
+// the cached mean is made unusable, so pfc_covs computes them on demand.
 __global__ void __launch_bounds__(kThreads, 2)
     k_covs(PlaneSet ps, int n, const float* __restrict__ ll,
            const float* __restrict__ w, double* part, unsigned* done,
            CycleCtl* ctl, int use_args, float3 mp_arg, float4 mq_arg,
-           int mode) {
+           int mode, double skip_ratio) {
     pdl_wait();
+    if (skip_ratio > 0.0 && ctl->ess < skip_ratio * (double)n) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) ctl->cov_mean_p[0] = __int_as_float(0x7fc00000);
+        return;
+    }
     const Planes s = pick_planes(ps, ctl->live);
     const int wmode = ctl->wmode;
     const float M = ctl->ll_max, S = ctl->ll_sumexp;
@@ -415,7 +423,7 @@ int launch_est_sums(PfHandle* h) {
 }
 
 int launch_covs(PfHandle* h, bool use_args, const float mp[3],
-                const float mq[4], bool cycle_output) {
+                const float mq[4], bool cycle_output, double skip_ratio) {
     float3 a = use_args ? make_float3(mp[0], mp[1], mp[2])
                         : make_float3(0.f, 0.f, 0.f);
     float4 b = use_args ? make_float4(mq[0], mq[1], mq[2], mq[3])
@@ -423,7 +431,7 @@ int launch_covs(PfHandle* h, bool use_args, const float mp[3],
     KernelScope ks(h, KK_COVS);
     PFB_CK(launch_pdl(k_covs, est_grid(h->n), kThreads, 0, h->stream, plane_set(h), h->n,
                       h->d_ll, h->d_w, h->d_part, h->d_done + 2, h->d_ctl,
-                      use_args ? 1 : 0, a, b, cycle_output ? 1 : 0));
+                      use_args ? 1 : 0, a, b, cycle_output ? 1 : 0, skip_ratio));
     PFB_KL();
     return 0;
 }

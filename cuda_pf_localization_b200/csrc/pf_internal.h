@@ -258,6 +258,9 @@ struct PfHandle {
     PfcOdom pending_odom{};
 
     // speculative estimate bookkeeping
+    // > 0: the caller resamples when the ESS of the estimate that follows a
+    // weighting is below ess_hint * n (pfc_set_ess_hint)
+    double ess_hint = 0.0;
     bool est_valid = false;    // h_ctl est/covs describe the current cloud
     bool est_inflight = false; // est + covs launched, not yet synced
     cudaEvent_t est_ev = nullptr;
@@ -351,10 +354,12 @@ int launch_softmax_combine(PfHandle* h);
 // Estimate pass 1 (+ device Markley mean) and the speculative covariance pass
 // around (float)mean, (float)qmean.  When use_args is set the covariance pass
 // uses the given f32 means instead; cycle_output also assembles the fused
-// cycle's output record.
+// cycle's output record.  skip_ratio > 0 skips the covariance pass on the
+// device when the estimate's ESS is below skip_ratio * n (a resample follows
+// and discards it; pfc_covs then computes it on demand).
 int launch_est_sums(PfHandle* h);
 int launch_covs(PfHandle* h, bool use_args, const float mp[3],
-                const float mq[4], bool cycle_output);
+                const float mq[4], bool cycle_output, double skip_ratio = 0.0);
 // Systematic resampling fused with the gather, the injection and the
 // estimate pass of the resulting cloud (14 FP64 sums, device Markley mean,
 // then the commit of the new live set): the weight pass runs first when the

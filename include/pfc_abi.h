@@ -276,6 +276,15 @@ int pfc_get_ancestors(void* h, int* anc);
 int pfc_pick_from_cum(void* h, const double* cum, int n, double u0,
                       double total, int* anc);
 
+/* Tell the library the caller's resampling rule (ParticleFilter::update,
+ * crates/pf_core/src/particle_filter.rs:111-124): after every pfc_weight the
+ * caller reads the estimate and resamples when its ESS is below
+ * resample_ess_ratio * n, discarding that estimate.  The covariance pass
+ * queued with that estimate is then skipped on the device; pfc_covs still
+ * returns the covariances (computed on demand), so results are unchanged.
+ * 0 (the default) turns it off.  Returns -1 for a NaN ratio. */
+int pfc_set_ess_hint(void* h, double resample_ess_ratio);
+
 /* The weight normalisation's quotient e / S both ways on the device: fast[i]
  * from the FP64 product e * RN(1/S) (the form the weighting kernels use),
  * ieee[i] from the IEEE f32 division.  Host arrays of n entries. */
