@@ -11,8 +11,11 @@
 // chain of kernels whatever the filter sizes:
 //   begin -> weight (+ predict) -> weights + ESS decision -> resample
 //   (look-back scan, run-start markers) -> gather (ancestors from the
-//   markers, the copy) -> injection (link, apply) -> commit -> estimate ->
-//   covariances (output record).
+//   markers, the copy, the estimate sums of the new cloud per tile) ->
+//   injection (link, apply, each draw's position change) -> commit ->
+//   estimate sums of the resampled filters (tile partials + injection
+//   changes, Markley mean) -> estimate pass of the others -> covariances
+//   (output record).
 // The chain is captured once into a CUDA graph; a cycle is one graph launch
 // fed by one copy of the per-filter inputs.
 //
@@ -22,8 +25,9 @@
 // log-likelihoods, the normaliser, the f32 weights, the fixed-point scan, the
 // ancestors, the injection and hence the particle states of filter f equal
 // those of the same filter run alone through pfc_cycle.  Only the FP64
-// estimate/covariance sums are partitioned differently (the estimate tile
-// size is autotuned per size bucket), which changes them in the last bits.
+// estimate/covariance sums are partitioned differently (gather tiles for a
+// filter that resampled, estimate tiles autotuned per size bucket for one
+// that did not), which changes them in the last bits.
 #include <math.h>
 #include <string.h>
 
@@ -56,6 +60,7 @@ struct BFilter {
     int wtile0, nwtiles;
     int etile0, netiles;
     int rtile0, nrtiles;
+    int gtile0, ngtiles;
     int inj_k, inj_off;
     uint64_t seed;
     float sigma_r, sigma_b, gate, inject_ratio;
@@ -245,11 +250,11 @@ __global__ void __launch_bounds__(kWThreads, 6)
 
 // Block partial of NV FP64 sums (fixed order) into part[NV]; returns true in
 // every thread of the filter's last tile after its partials are visible.
+// Block partial of NV per-thread FP64 accumulators (xor butterfly per warp,
+// warps in order) into part[0..NV).
 template <int NV>
-__device__ __forceinline__ bool tile_partial(double (&acc)[NV], double* part,
-                                             unsigned* done, int ntiles) {
+__device__ __forceinline__ void block_partial(double (&acc)[NV], double* part) {
     __shared__ double s_w[NV][kThreads / 32];
-    __shared__ bool s_last;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
@@ -262,9 +267,18 @@ __device__ __forceinline__ bool tile_partial(double (&acc)[NV], double* part,
         for (int k = 0; k < kThreads / 32; ++k) v += s_w[tid][k];
         part[tid] = v;
     }
+}
+
+// block_partial, then true in every thread of the filter's last tile to
+// finish (an atomic counter per filter).
+template <int NV>
+__device__ __forceinline__ bool tile_partial(double (&acc)[NV], double* part,
+                                             unsigned* done, int ntiles) {
+    __shared__ bool s_last;
+    block_partial<NV>(acc, part);
     __threadfence();
     __syncthreads();
-    if (tid == 0) s_last = (atomicAdd(done, 1u) == (unsigned)ntiles - 1u);
+    if (threadIdx.x == 0) s_last = (atomicAdd(done, 1u) == (unsigned)ntiles - 1u);
     __syncthreads();
     if (!s_last) return false;
     __threadfence();
@@ -413,10 +427,12 @@ __global__ void __launch_bounds__(kThreads)
 // values costs (1.797 against 1.812 ms per 512-filter cycle at two).
 __global__ void __launch_bounds__(kThreads, 3)
     k_b_est(Arena A, const BFilter* __restrict__ F, const BTile* __restrict__ T,
-            BCtl* C, double* __restrict__ epart) {
+            BCtl* C, double* __restrict__ epart, int skip_resampled) {
     const BTile t = T[blockIdx.x];
     const BFilter& fl = F[t.f];
     BCtl* c = C + t.f;
+    // in a cycle, a filter that resampled has its sums from k_b_est_src
+    if (skip_resampled && c->resampled) return;
     const Planes s = filter_planes(A, c->live, fl.off);
     const int wmode = c->wmode;
     const float M = c->M, S = c->S;
@@ -675,10 +691,16 @@ __global__ void __launch_bounds__(kThreads)
 // the tile's markers (every tile starts with one) give each output its
 // ancestor by a running maximum (ancestors increase with the output index),
 // the markers read are reset for the next resample, and the seven planes are
-// copied with 16-byte stores (filter offsets are multiples of 1024).
+// copied with 16-byte stores (filter offsets are multiples of 1024).  The
+// copied values, already in registers, go into the 14 estimate sums of the
+// new cloud: every output has the weight wd = 1/n, so a thread sums x, y, z
+// and the exact FP64 products of the quaternion components, counts its
+// outputs and scales by wd (wd^2 for the sum of squared weights) once; one
+// partial per tile in gpart, so the cycle needs no estimate pass over the
+// resampled filters.
 __global__ void __launch_bounds__(kThreads)
     k_b_gather(Arena A, const BFilter* __restrict__ F, const BTile* __restrict__ T,
-               const BCtl* C) {
+               const BCtl* C, double* __restrict__ gpart) {
     __shared__ int s_anc[kGTile];
     __shared__ int s_wmax[kThreads / 32];
     const BTile t = T[blockIdx.x];
@@ -729,6 +751,10 @@ __global__ void __launch_bounds__(kThreads)
     const Planes dst = filter_planes(A, 1 - c->live, fl.off);
     float* const sp[7] = {src.px, src.py, src.pz, src.qw, src.qx, src.qy, src.qz};
     float* const dp[7] = {dst.px, dst.py, dst.pz, dst.qw, dst.qx, dst.qy, dst.qz};
+    const float wuni = 1.0f / (float)n;
+    double acc[kEstN];
+#pragma unroll
+    for (int q = 0; q < kEstN; ++q) acc[q] = 0.0;
     // thread t copies outputs [4t, 4t + 4) and [1024 + 4t, 1024 + 4t + 4)
 #pragma unroll 1
     for (int h = 0; h < 2; ++h) {
@@ -755,7 +781,29 @@ __global__ void __launch_bounds__(kThreads)
                 for (int q = 0; q < 4; ++q)
                     if (ib + q < n) dp[k][ib + q] = v[k][q];
         }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (ib + q < n) {
+                acc[0] += (double)v[0][q];
+                acc[1] += (double)v[1][q];
+                acc[2] += (double)v[2][q];
+                const double qd[4] = {v[3][q], v[4][q], v[5][q], v[6][q]};
+                int e = 3;
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+#pragma unroll
+                    for (int cc = r; cc < 4; ++cc) {
+                        acc[e] = fma(qd[r], qd[cc], acc[e]);
+                        ++e;
+                    }
+                acc[13] += 1.0;
+            }
     }
+    const double wd = (double)wuni;
+#pragma unroll
+    for (int q = 0; q < 13; ++q) acc[q] *= wd;
+    acc[13] *= wd * wd;
+    block_partial<kEstN>(acc, gpart + (size_t)(fl.gtile0 + t.local) * kEstN);
 }
 
 // Injection: global draw d belongs to filter draw_f[d] (local draw
@@ -777,10 +825,14 @@ __global__ void k_b_inject_link(const BFilter* __restrict__ F, const BCtl* C,
     next[d] = ((uint32_t)(prev >> 32) == epoch) ? (int)(uint32_t)prev : -1;
 }
 
+// The thread of a particle's first draw applies its draws in ascending draw
+// order and records each draw's exact position change (a difference of two
+// f32 values) in icorr[3d..3d+2] for the filter's estimate sums.
 __global__ void k_b_inject_apply(Arena A, const BFilter* __restrict__ F,
                                  const BCtl* C, const BGlobal* G,
                                  const int* __restrict__ draw_f, int total,
-                                 const uint64_t* head, const int* next) {
+                                 const uint64_t* head, const int* next,
+                                 double* __restrict__ icorr) {
     const int d = blockIdx.x * kThreads + threadIdx.x;
     if (d >= total) return;
     const int f = draw_f[d];
@@ -802,9 +854,13 @@ __global__ void k_b_inject_apply(Arena A, const BFilter* __restrict__ F,
         if (best < 0) break;
         const InjDraw e =
             (best == d) ? dr : inj_draw(lcg, c.gen, best - fl.inj_off, fl.n);
-        px += e.jx;
-        py += e.jy;
-        pz += e.jz;
+        const float nx = px + e.jx, ny = py + e.jy, nz = pz + e.jz;
+        icorr[3 * (size_t)best] = (double)nx - (double)px;
+        icorr[3 * (size_t)best + 1] = (double)ny - (double)py;
+        icorr[3 * (size_t)best + 2] = (double)nz - (double)pz;
+        px = nx;
+        py = ny;
+        pz = nz;
         last = best;
     }
     dst.px[dr.idx] = px;
@@ -832,6 +888,43 @@ __global__ void k_b_commit(BCtl* C, BGlobal* G, int nf) {
         G->scan_epoch = e ? e : 1u;
         e = G->inj_epoch + 1u;
         G->inj_epoch = e ? e : 1u;
+    }
+}
+
+// Estimate sums of a filter that resampled this cycle, without a pass over
+// the new cloud: its gather tiles' sums in tile order, plus wd times the
+// injection's position changes in draw order; then the Markley mean and the
+// f32 means of the covariance pass, as the estimate pass's last tile leaves
+// them.  One block per filter; the others take the estimate pass.
+__global__ void __launch_bounds__(kThreads)
+    k_b_est_src(const BFilter* __restrict__ F, BCtl* C, const double* __restrict__ gpart,
+                const double* __restrict__ icorr) {
+    const BFilter& fl = F[blockIdx.x];
+    BCtl* c = C + blockIdx.x;
+    if (!c->resampled) return;
+    __shared__ double s_out[kEstN];
+    tiles_combine<kEstN>(gpart + (size_t)fl.gtile0 * kEstN, fl.ngtiles, s_out);
+    double qm[4];
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        double d[3] = {0.0, 0.0, 0.0};
+        for (int j = lane; j < fl.inj_k; j += 32)
+#pragma unroll
+            for (int q = 0; q < 3; ++q) d[q] += icorr[3 * (size_t)(fl.inj_off + j) + q];
+        const double wd = (double)(1.0f / (float)fl.n);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) d[q] = warp_sum_d(d[q]);
+        if (lane == 0)
+            for (int q = 0; q < 3; ++q) s_out[q] += wd * d[q];
+        __syncwarp();
+        markley_mean_warp_call(&s_out[3], qm);
+    }
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < kEstN; ++k) c->est[k] = s_out[k];
+        c->ess = s_out[13] > 0.0 ? 1.0 / s_out[13] : 0.0;
+        for (int k = 0; k < 4; ++k) c->qmean[k] = qm[k];
+        for (int k = 0; k < 3; ++k) c->cmp[k] = (float)s_out[k];
+        for (int k = 0; k < 4; ++k) c->cmq[k] = (float)qm[k];
     }
 }
 
@@ -889,6 +982,7 @@ struct BatchHandle {
     double* d_cpart = nullptr;
     unsigned* d_flags = nullptr;
     uint64_t* d_vals = nullptr;
+    double* d_gpart = nullptr;   // estimate sums of the new cloud per gather tile
     BTile* d_gt = nullptr;
     int n_gt = 0;
     int* d_marker = nullptr;
@@ -896,6 +990,7 @@ struct BatchHandle {
     int total_draws = 0;
     uint64_t* d_inj_head = nullptr;
     int* d_inj_next = nullptr;
+    double* d_icorr = nullptr;   // position change of every injection draw
     float* d_lm = nullptr;
     int lm_total = 0;
     PfcBatchCycle* d_cyc = nullptr;
@@ -980,9 +1075,9 @@ int rebuild_est_tiles(BatchHandle* h) {
     return 0;
 }
 
-int launch_est_covs(BatchHandle* h) {
+int launch_est_covs(BatchHandle* h, bool in_cycle = false) {
     k_b_est<<<h->n_et, kThreads, 0, h->stream>>>(h->A, h->d_F, h->d_et, h->d_C,
-                                                 h->d_epart);
+                                                 h->d_epart, in_cycle ? 1 : 0);
     k_b_covs<<<h->n_et, kThreads, 0, h->stream>>>(h->A, h->d_F, h->d_et, h->d_C,
                                                   h->d_cpart, h->d_out);
     h->launches += 2;
@@ -1003,7 +1098,7 @@ int enqueue_cycle(BatchHandle* h) {
     PFB_KL();
     k_b_resample<<<h->n_rt, kThreads, 0, s>>>(h->A, h->d_F, h->d_rt, h->d_C, h->d_G,
                                               h->d_flags, h->d_vals);
-    k_b_gather<<<h->n_gt, kThreads, 0, s>>>(h->A, h->d_F, h->d_gt, h->d_C);
+    k_b_gather<<<h->n_gt, kThreads, 0, s>>>(h->A, h->d_F, h->d_gt, h->d_C, h->d_gpart);
     h->launches += 2;
     if (h->total_draws > 0) {
         const int g = ceil_div(h->total_draws, kThreads);
@@ -1012,13 +1107,14 @@ int enqueue_cycle(BatchHandle* h) {
                                                h->d_inj_next);
         k_b_inject_apply<<<g, kThreads, 0, s>>>(h->A, h->d_F, h->d_C, h->d_G,
                                                 h->d_draw_f, h->total_draws,
-                                                h->d_inj_head, h->d_inj_next);
+                                                h->d_inj_head, h->d_inj_next, h->d_icorr);
         h->launches += 2;
     }
     k_b_commit<<<ceil_div(h->nf, kThreads), kThreads, 0, s>>>(h->d_C, h->d_G, h->nf);
-    h->launches += 1;
+    k_b_est_src<<<h->nf, kThreads, 0, s>>>(h->d_F, h->d_C, h->d_gpart, h->d_icorr);
+    h->launches += 2;
     PFB_KL();
-    if (launch_est_covs(h)) return -1;
+    if (launch_est_covs(h, true)) return -1;
     PFB_CK(cudaMemcpyAsync(h->h_G, h->d_G, sizeof(BGlobal), cudaMemcpyDeviceToHost, s));
     return 0;
 }
@@ -1079,11 +1175,13 @@ void free_batch(BatchHandle* h) {
     cudaFree(h->d_cpart);
     cudaFree(h->d_flags);
     cudaFree(h->d_vals);
+    cudaFree(h->d_gpart);
     cudaFree(h->d_gt);
     cudaFree(h->d_marker);
     cudaFree(h->d_draw_f);
     cudaFree(h->d_inj_head);
     cudaFree(h->d_inj_next);
+    cudaFree(h->d_icorr);
     cudaFree(h->d_lm);
     cudaFree(h->d_cyc);
     cudaFreeHost(h->h_cyc);
@@ -1132,7 +1230,7 @@ void* pfc_batch_create(int n_filters, const int* n, const unsigned* seeds,
     h->est_tile.assign(kBuckets, 8192);
     h->filters.resize(n_filters);
     long long off = 0;
-    int w0 = 0, r0 = 0;
+    int w0 = 0, r0 = 0, g0 = 0;
     for (int f = 0; f < n_filters; ++f) {
         BFilter& b = h->filters[f];
         memset(&b, 0, sizeof(b));
@@ -1145,6 +1243,9 @@ void* pfc_batch_create(int n_filters, const int* n, const unsigned* seeds,
         b.rtile0 = r0;
         b.nrtiles = ceil_div(n[f], kRTile);
         r0 += b.nrtiles;
+        b.gtile0 = g0;
+        b.ngtiles = ceil_div(n[f], kGTile);
+        g0 += b.ngtiles;
         const unsigned sd = seeds ? seeds[f] : 42u;
         b.seed = sd == 0 ? 42ull : (uint64_t)sd;
         b.sigma_r = 0.05f;
@@ -1189,6 +1290,7 @@ void* pfc_batch_create(int n_filters, const int* n, const unsigned* seeds,
         std::vector<BTile> gt = make_tiles(h->filters, 3, h->est_tile);
         h->n_gt = (int)gt.size();
         if (cudaMalloc((void**)&h->d_gt, sizeof(BTile) * gt.size()) != cudaSuccess ||
+            cudaMalloc((void**)&h->d_gpart, sizeof(double) * kEstN * gt.size()) != cudaSuccess ||
             cudaMemcpy(h->d_gt, gt.data(), sizeof(BTile) * gt.size(),
                        cudaMemcpyHostToDevice) != cudaSuccess)
             break;
@@ -1267,10 +1369,13 @@ int pfc_batch_set_params(void* p, const PfcCycleParams* prm) {
     if ((int)draw_f.size() > h->total_draws) {
         cudaFree(h->d_draw_f);
         cudaFree(h->d_inj_next);
+        cudaFree(h->d_icorr);
         h->d_draw_f = nullptr;
         h->d_inj_next = nullptr;
+        h->d_icorr = nullptr;
         PFB_CK(cudaMalloc((void**)&h->d_draw_f, sizeof(int) * draw_f.size()));
         PFB_CK(cudaMalloc((void**)&h->d_inj_next, sizeof(int) * draw_f.size()));
+        PFB_CK(cudaMalloc((void**)&h->d_icorr, sizeof(double) * 3 * draw_f.size()));
     }
     h->total_draws = (int)draw_f.size();
     if (!draw_f.empty())
