@@ -172,7 +172,10 @@ __global__ void __launch_bounds__(kThreads)
         const Quat q0{pr[3], pr[4], pr[5], pr[6]};
         store_pose(s, i, p, q_product(q0, q_from_axis_angle(axis, ang)));
     }
-    if (threadIdx.x == 0 && t.local == 0) C[t.f].wmode = WMODE_UNIFORM;
+    if (threadIdx.x == 0 && t.local == 0) {
+        C[t.f].wmode = WMODE_UNIFORM;
+        C[t.f].resampled = 0;  // a new cloud: the estimate pass covers it
+    }
 }
 
 // Predict (generation gen + 1) and gated weighting of one 256-particle tile
@@ -427,12 +430,12 @@ __global__ void __launch_bounds__(kThreads)
 // values costs (1.797 against 1.812 ms per 512-filter cycle at two).
 __global__ void __launch_bounds__(kThreads, 3)
     k_b_est(Arena A, const BFilter* __restrict__ F, const BTile* __restrict__ T,
-            BCtl* C, double* __restrict__ epart, int skip_resampled) {
+            BCtl* C, double* __restrict__ epart) {
     const BTile t = T[blockIdx.x];
     const BFilter& fl = F[t.f];
     BCtl* c = C + t.f;
-    // in a cycle, a filter that resampled has its sums from k_b_est_src
-    if (skip_resampled && c->resampled) return;
+    // a filter that resampled in the last cycle has its sums from k_b_est_src
+    if (c->resampled) return;
     const Planes s = filter_planes(A, c->live, fl.off);
     const int wmode = c->wmode;
     const float M = c->M, S = c->S;
@@ -1075,9 +1078,9 @@ int rebuild_est_tiles(BatchHandle* h) {
     return 0;
 }
 
-int launch_est_covs(BatchHandle* h, bool in_cycle = false) {
+int launch_est_covs(BatchHandle* h) {
     k_b_est<<<h->n_et, kThreads, 0, h->stream>>>(h->A, h->d_F, h->d_et, h->d_C,
-                                                 h->d_epart, in_cycle ? 1 : 0);
+                                                 h->d_epart);
     k_b_covs<<<h->n_et, kThreads, 0, h->stream>>>(h->A, h->d_F, h->d_et, h->d_C,
                                                   h->d_cpart, h->d_out);
     h->launches += 2;
@@ -1114,7 +1117,7 @@ int enqueue_cycle(BatchHandle* h) {
     k_b_est_src<<<h->nf, kThreads, 0, s>>>(h->d_F, h->d_C, h->d_gpart, h->d_icorr);
     h->launches += 2;
     PFB_KL();
-    if (launch_est_covs(h, true)) return -1;
+    if (launch_est_covs(h)) return -1;
     PFB_CK(cudaMemcpyAsync(h->h_G, h->d_G, sizeof(BGlobal), cudaMemcpyDeviceToHost, s));
     return 0;
 }
@@ -1530,6 +1533,7 @@ int pfc_batch_autotune(void* p, int reps, int* est_tile_out, int* packed_out) {
         *best = 1e30f;
         for (int r = 0; r < reps; ++r) {
             if (cudaEventRecord(e0, h->stream) != cudaSuccess) return -1;
+            // as in a cycle: filters that resampled take only the covariances
             if (launch_est_covs(h)) return -1;
             if (cudaEventRecord(e1, h->stream) != cudaSuccess) return -1;
             if (cudaEventSynchronize(e1) != cudaSuccess) return -1;
