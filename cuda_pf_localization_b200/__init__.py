@@ -152,6 +152,7 @@ _KERNEL_SIGS = {
     "pfc_pick_from_cum": (c_int, [c_void_p, _dp, c_int, c_double, c_double, _ip]),
     "pfc_weight_div_check": (c_int, [c_void_p, _fp, _fp, c_int, _fp, _fp]),
     "pfc_set_ess_hint": (c_int, [c_void_p, c_double]),
+    "pfc_est_ess": (c_int, [c_void_p, _dp]),
     "pfc_get_lcg": (c_int, [c_void_p, POINTER(c_ulonglong)]),
     "pfc_set_lcg": (c_int, [c_void_p, c_ulonglong]),
     "pfc_set_weight_kernel": (c_int, [c_void_p, c_int]),

@@ -271,6 +271,18 @@ struct CudaBackend {
     }
 
     bool estimate(PfcoreEstimate& e) { return estimate_moments(e) && estimate_covs(e); }
+
+    // The ESS of the current estimate alone (1 / sums[13], as estimate()
+    // reports it), which is all update() reads of an estimate it discards.
+    bool estimate_ess(double& ess) {
+        ess = 0.0;
+        if (n == 0) return true;
+        if (pfc_est_ess(handle, &ess) != 0) {
+            set_err("pfc_est_ess failed");
+            return false;
+        }
+        return true;
+    }
 };
 
 // ParticleFilter, crates/pf_core/src/particle_filter.rs:73-133.
@@ -440,20 +452,21 @@ int pfcore_filter_update(void* p, const PfcoreOdom* odom,
     pf->backend.predict(*odom);
     pf->backend.weight(obs, obs ? nobs : 0, pf->map);
     // update() estimates, then resamples and estimates again when the ESS is
-    // low.  The first estimate's covariances are only taken when it is the
-    // one returned; the library, told the rule (pfc_set_ess_hint), skips the
-    // covariance pass it would otherwise queue for a discarded estimate.  The
-    // returned estimate is the same.
+    // low.  Of the first estimate only its ESS decides when it is discarded;
+    // the library, told the rule (pfc_set_ess_hint), then reports only the
+    // ESS, and the full estimate is taken of the one returned.  The returned
+    // estimate is the same.
     PfcoreEstimate est;
-    if (!pf->backend.estimate_moments(est)) return -1;
+    double ess0 = 0.0;
+    if (!pf->backend.estimate_ess(ess0)) return -1;
     const double threshold =
         pf->cfg.resample_ess_ratio * (double)pf->cfg.particle_count;
     int resampled = 0;
-    if (pf->cfg.resample_ess_ratio > 0.0 && est.ess < threshold) {
+    if (pf->cfg.resample_ess_ratio > 0.0 && ess0 < threshold) {
         pf->backend.resample(pf->cfg.random_inject_ratio);
         if (!pf->backend.estimate(est)) return -1;
         resampled = 1;
-    } else if (!pf->backend.estimate_covs(est)) {
+    } else if (!pf->backend.estimate(est)) {
         return -1;
     }
     est.resampled = resampled;

@@ -194,8 +194,11 @@ int device_error(PfHandle* h) {
 
 // Queue estimate pass 1 + Markley (unless a fused resample already did) +
 // speculative covariance pass + the copy of the control block.
-int queue_estimate(PfHandle* h, bool sums_done = false, double skip_ratio = 0.0) {
-    if (!sums_done && launch_est_sums(h)) return -1;
+// sq_from_ess: queued right after the weight pass (k_ess), whose sum w^2 the
+// estimate reports; skip_ratio: the caller's resampling rule (ess hint).
+int queue_estimate(PfHandle* h, bool sums_done = false, double skip_ratio = 0.0,
+                   bool sq_from_ess = false) {
+    if (!sums_done && launch_est_sums(h, sq_from_ess, skip_ratio)) return -1;
     if (launch_covs(h, false, nullptr, nullptr, false, skip_ratio)) return -1;
     PFB_CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(CycleCtl),
                            cudaMemcpyDeviceToHost, h->stream));
@@ -652,7 +655,7 @@ int pfc_weight(void* hv, const CObservation* obs, int nobs, float sigma_r,
     // materialise the weights with the resampler's prefixes now: the estimate
     // pass then reads them instead of re-deriving them from ll
     if (launch_weight_prefix(h, false, 0.0)) return -1;
-    return queue_estimate(h, false, h->ess_hint);
+    return queue_estimate(h, false, h->ess_hint, true);
 }
 
 int pfc_set_ess_hint(void* hv, double resample_ess_ratio) {
@@ -686,7 +689,34 @@ int pfc_est_sums(void* hv, double* out) {
         if (queue_estimate(h)) return -1;
     }
     if (wait_estimate(h)) return -1;
+    if (h->h_ctl->est_partial) {
+        // the estimate after the last weighting reported only sum w^2 (ess
+        // hint); the cloud and its weights are unchanged since, so the full
+        // pass reports the same sum w^2 (the weight pass's).  The covariance
+        // pass follows, as with every queued estimate, so the cached
+        // covariances match the cached mean.
+        if (launch_est_sums(h, true, 0.0)) return -1;
+        if (launch_covs(h, false, nullptr, nullptr, false)) return -1;
+        PFB_CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(CycleCtl),
+                               cudaMemcpyDeviceToHost, h->stream));
+        PFB_CK(cudaStreamSynchronize(h->stream));
+        h->stats.d2h_bytes += sizeof(CycleCtl);
+        h->stats.host_syncs += 1;
+        if (device_error(h)) return -1;
+    }
     memcpy(out, h->h_ctl->est, sizeof(double) * kEstN);
+    return 0;
+}
+
+int pfc_est_ess(void* hv, double* ess) {
+    PfHandle* h = as_pf(hv);
+    if (!valid_handle(h) || !ess) return -1;
+    if (h->pending_predict || (!h->est_inflight && !h->est_valid)) {
+        if (flush_predict(h)) return -1;
+        if (queue_estimate(h)) return -1;
+    }
+    if (wait_estimate(h)) return -1;
+    *ess = h->h_ctl->ess;
     return 0;
 }
 

@@ -97,8 +97,23 @@ __device__ bool block_reduce_last(double (&acc)[NV], double* part,
 __global__ void __launch_bounds__(kThreads, 2)
     k_est_sums(PlaneSet ps, int n, const float* __restrict__ ll,
                float* __restrict__ w, double* part, unsigned* done,
-               CycleCtl* ctl) {
+               CycleCtl* ctl, int sq_from_ess, double skip_ratio) {
     pdl_wait();
+    if (sq_from_ess && skip_ratio > 0.0) {
+        // the caller resamples when this estimate's ESS is below
+        // skip_ratio * n and then discards it: only sum w^2 is reported
+        const double sq = ctl->sq_w;
+        const double ess = sq > 0.0 ? 1.0 / sq : 0.0;
+        if (ess < skip_ratio * (double)n) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                ctl->est[13] = sq;
+                ctl->ess = ess;
+                ctl->est_partial = 1;
+                ctl->cov_mean_p[0] = __int_as_float(0x7fc00000);
+            }
+            return;
+        }
+    }
     const Planes s = pick_planes(ps, ctl->live);
     const int wmode = ctl->wmode;
     const float M = ctl->ll_max, S = ctl->ll_sumexp;
@@ -143,8 +158,10 @@ __global__ void __launch_bounds__(kThreads, 2)
     double qm[4];
     if (threadIdx.x < 32) markley_mean_warp_call(&s_out[3], qm);  // warp 0
     if (threadIdx.x == 0) {
+        if (sq_from_ess) s_out[13] = ctl->sq_w;
         for (int k = 0; k < kEstN; ++k) ctl->est[k] = s_out[k];
         ctl->ess = s_out[13] > 0.0 ? 1.0 / s_out[13] : 0.0;
+        ctl->est_partial = 0;
         for (int k = 0; k < 4; ++k) ctl->qmean[k] = qm[k];
         for (int k = 0; k < 3; ++k) ctl->cov_mean_p[k] = (float)s_out[k];
         for (int k = 0; k < 4; ++k) ctl->cov_mean_q[k] = (float)qm[k];
@@ -378,6 +395,7 @@ __global__ void __launch_bounds__(kThreads)
         }
         ctl->w_total_fx = T;
         ctl->w_bad = any_fb;
+        ctl->sq_w = sum;
         if (wmode == WMODE_LL) ctl->wmode = WMODE_STORED;
         *done = 0u;
     }
@@ -414,10 +432,11 @@ int est_grid(int n) {
 
 }  // namespace
 
-int launch_est_sums(PfHandle* h) {
+int launch_est_sums(PfHandle* h, bool sq_from_ess, double skip_ratio) {
     KernelScope ks(h, KK_EST);
     PFB_CK(launch_pdl(k_est_sums, est_grid(h->n), kThreads, 0, h->stream, plane_set(h),
-                      h->n, h->d_ll, h->d_w, h->d_part, h->d_done + 1, h->d_ctl));
+                      h->n, h->d_ll, h->d_w, h->d_part, h->d_done + 1, h->d_ctl,
+                      sq_from_ess ? 1 : 0, skip_ratio));
     PFB_KL();
     return 0;
 }

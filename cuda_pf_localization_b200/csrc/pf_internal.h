@@ -83,6 +83,12 @@ struct CycleCtl {
     uint64_t w_total_fx;
     int w_bad;
     unsigned long long lcg_next;     // LCG word after the running resample
+    // sum w^2 of the weights the weight pass (k_ess) materialised, in its
+    // fixed order; the estimate queued after it reports this value
+    double sq_w;
+    // the estimate pass skipped sums 0..12 (a resample follows, the caller
+    // said so with pfc_set_ess_hint); pfc_est_sums computes them on demand
+    int est_partial;
 };
 
 // Fixed-point image of a normalised f32 weight: round-to-nearest-even of
@@ -357,7 +363,10 @@ int launch_softmax_combine(PfHandle* h);
 // cycle's output record.  skip_ratio > 0 skips the covariance pass on the
 // device when the estimate's ESS is below skip_ratio * n (a resample follows
 // and discards it; pfc_covs then computes it on demand).
-int launch_est_sums(PfHandle* h);
+// sq_from_ess: the weights were just materialised by k_ess, whose sum w^2
+// the estimate reports; with skip_ratio > 0 it then skips its other sums when
+// the ESS is below skip_ratio * n.
+int launch_est_sums(PfHandle* h, bool sq_from_ess = false, double skip_ratio = 0.0);
 int launch_covs(PfHandle* h, bool use_args, const float mp[3],
                 const float mq[4], bool cycle_output, double skip_ratio = 0.0);
 // Systematic resampling fused with the gather, the injection and the

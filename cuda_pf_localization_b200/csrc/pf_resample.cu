@@ -433,6 +433,7 @@ __global__ void __launch_bounds__(kThreads, 4)
         if (tid == 0) {
             for (int q = 0; q < kEstN; ++q) ctl->est[q] = s_out[q];
             ctl->ess = s_out[13] > 0.0 ? 1.0 / s_out[13] : 0.0;
+            ctl->est_partial = 0;
             for (int q = 0; q < 4; ++q) ctl->qmean[q] = qm[q];
             for (int q = 0; q < 3; ++q) ctl->cov_mean_p[q] = (float)s_out[q];
             for (int q = 0; q < 4; ++q) ctl->cov_mean_q[q] = (float)qm[q];

@@ -278,12 +278,18 @@ int pfc_pick_from_cum(void* h, const double* cum, int n, double u0,
 
 /* Tell the library the caller's resampling rule (ParticleFilter::update,
  * crates/pf_core/src/particle_filter.rs:111-124): after every pfc_weight the
- * caller reads the estimate and resamples when its ESS is below
- * resample_ess_ratio * n, discarding that estimate.  The covariance pass
- * queued with that estimate is then skipped on the device; pfc_covs still
- * returns the covariances (computed on demand), so results are unchanged.
- * 0 (the default) turns it off.  Returns -1 for a NaN ratio. */
+ * caller reads the estimate's ESS and resamples when it is below
+ * resample_ess_ratio * n, discarding that estimate.  The estimate and
+ * covariance passes queued with it then report only sum w^2 on the device;
+ * pfc_est_sums and pfc_covs still return the full values (computed on
+ * demand), so results are unchanged.  0 (the default) turns it off.
+ * Returns -1 for a NaN ratio. */
 int pfc_set_ess_hint(void* h, double resample_ess_ratio);
+
+/* ESS of the current cloud's estimate: 1 / out14[13] of pfc_est_sums (0 when
+ * that sum is not positive), without the other sums when the ess hint lets
+ * the library skip them. */
+int pfc_est_ess(void* h, double* ess);
 
 /* The weight normalisation's quotient e / S both ways on the device: fast[i]
  * from the FP64 product e * RN(1/S) (the form the weighting kernels use),

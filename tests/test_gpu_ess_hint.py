@@ -1,10 +1,11 @@
 """pfc_set_ess_hint: told ParticleFilter::update's rule (resample when the ESS
-of the estimate after a weighting is below ratio * N), the library skips the
-covariance pass it queues with an estimate that a resample will discard.
-Bar: a handle with the hint and one without, stepped through the same calls,
-return the same estimate sums and covariances bit for bit, on cycles that
-resample and cycles that do not, including when the caller asks for the
-skipped covariances (computed on demand)."""
+of the estimate after a weighting is below ratio * N), the library reports
+only the ESS of an estimate that a resample will discard (pfc_est_ess) and
+skips its other sums and its covariance pass.  Bar: a handle with the hint
+and one without, stepped through the same calls, return the same ESS,
+estimate sums and covariances bit for bit, on cycles that resample and
+cycles that do not, including when the caller asks for the skipped sums and
+covariances (computed on demand)."""
 import numpy as np
 import pytest
 
@@ -29,6 +30,12 @@ def _mean(sums):
     return sums[:3].astype(np.float32), q.astype(np.float32)
 
 
+def _ess(kernels, f):
+    out = np.zeros(1)
+    assert kernels.pfc_est_ess(f.h, pkg.dptr(out)) == 0
+    return float(out[0])
+
+
 def test_hint_keeps_every_result(kernels):
     n = 100_003
     sc = sim.scale_config(cycles=8, seed=5)
@@ -45,14 +52,17 @@ def test_hint_keeps_every_result(kernels):
             for f in (a, b):
                 f.predict(st.odom_t, st.odom_q, sc.trans_noise, sc.rot_noise)
                 assert f.weight(rows) == 0
-            sa, sb = a.est_sums(), b.est_sums()
-            np.testing.assert_array_equal(sa, sb)
-            ess = 1.0 / sa[13] if sa[13] > 0 else 0.0
+            ess = _ess(kernels, a)
+            assert ess == _ess(kernels, b)
             resample = ess < RATIO * n
             seen[resample] += 1
-            mp, mq = _mean(sa)
             if not resample or k % 4 == 0:
-                # kept estimate, or the caller asks for the discarded one
+                # the kept estimate, or the caller asks for the discarded one
+                # (the hinted handle computes it on demand)
+                sa, sb = a.est_sums(), b.est_sums()
+                np.testing.assert_array_equal(sa, sb)
+                assert ess == (1.0 / sa[13] if sa[13] > 0 else 0.0)
+                mp, mq = _mean(sa)
                 np.testing.assert_array_equal(a.covs(mp, mq), b.covs(mp, mq))
             if resample:
                 for f in (a, b):
